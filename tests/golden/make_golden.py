@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Generate the golden vectors of the ETD2 path by running the PriNCe reference.
+
+Run in a checkout where the reference source tree is available (default
+``/root/reference``, override with ``PRINCE_REFERENCE``)::
+
+    python tests/golden/make_golden.py
+
+The reference package is copied to a scratch directory (it tries to
+download its HDF5 database at import unless a file is present, and it
+imports ``h5py``, which this environment lacks), so the script
+
+* places an empty ``prince_db_05.h5`` next to the copied package,
+* puts a minimal ``h5py`` stand-in first on ``sys.path``,
+* selects the FP64 settings (dense fold kernel, float64 cross-section
+  dtype, scipy backend, ``tau_dec_threshold = 0``),
+* defines a small synthetic cross-section model (Lorentzian resonances plus
+  a photo-pion bump) because the FLUKA
+  database is not available offline.
+
+It then builds the light-nuclei run (p, n, 2H, 3H, 3He, 4He; 64 bins over
+1e6-1e14 GeV at 8 bins/decade; CMB; z = 1 -> 0, dz = 1e-3) and records the
+inputs the ETD2 path consumes together with the reference's own outputs
+(final states of single- and multi-RHS solves, per-window intermediates).
+The result is ``tests/golden/light_network.npz``.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("PRINCE_REFERENCE", "/root/reference")
+
+
+def _prepare_reference():
+    tmp = tempfile.mkdtemp(prefix="prince_golden_")
+    shutil.copytree(os.path.join(REF, "src", "prince_cr"), os.path.join(tmp, "prince_cr"))
+    os.chmod(os.path.join(tmp, "prince_cr", "data"), 0o755)
+    open(os.path.join(tmp, "prince_cr", "data", "prince_db_05.h5"), "wb").close()
+
+    h5 = types.ModuleType("h5py")
+
+    class _File:
+        def __init__(self, *a, **k):
+            self.attrs = {"version": "stub"}
+
+        def __enter__(self):
+            return self
+
+        def __exit__(self, *a):
+            return False
+
+        def __contains__(self, k):
+            return False
+
+    h5.File = _File
+    sys.modules["h5py"] = h5
+    sys.path.insert(0, tmp)
+    return tmp
+
+
+def _lorentz(eg, e0, w, peak, thr):
+    return peak * (eg * w) ** 2 / ((eg ** 2 - e0 ** 2) ** 2 + (eg * w) ** 2) * (eg > thr)
+
+
+def build(config, base):
+    """Return (run, make_sources) for the light-nuclei workload."""
+    from prince_cr import core, photonfields
+
+    class SynthXS(base):
+        def __init__(self):
+            self.supports_redistributions = True
+            base.__init__(self)
+            # The table reaches y = E eps / m_p beyond the largest value the grids
+            # probe (1e14 GeV x 1e-6 GeV / m_p), so no kernel row crosses the end of
+            # the tabulated response.
+            eg = np.logspace(-3, 9, 481)
+            self._egrid_tab = eg
+            self.xbins = np.logspace(-5, 0, 101)
+            mb = 1e-27
+            pion = lambda A: (_lorentz(eg, 0.34, 0.12, 0.5 * A * mb, 0.145)
+                              + 0.12 * A * mb * (eg > 0.5))
+            gdr = {1000010020: (0.0042, 0.004, 2.4), 1000010030: (0.012, 0.006, 1.3),
+                   1000020030: (0.012, 0.006, 1.4), 1000020040: (0.026, 0.008, 2.2)}
+            A_of = {2212: 1, 2112: 1, 1000010020: 2, 1000010030: 3, 1000020030: 3,
+                    1000020040: 4}
+            for mo, A in A_of.items():
+                tab = pion(A)
+                if mo in gdr:
+                    e0, w, s = gdr[mo]
+                    tab = tab + _lorentz(eg, e0, w, s * mb, 0.0022)
+                self._nonel_tab[mo] = tab
+            # Channel yields conserve the nucleon number: 4He -> 3He+n | 3H+p | d+d,
+            # 3He -> d+p | p+p+n, 3H -> d+n | p+n+n, d -> p+n.
+            bc = {1000020040: [(1000020030, 0.45), (1000010030, 0.45), (1000010020, 0.2)],
+                  1000020030: [(1000010020, 0.9)], 1000010030: [(1000010020, 0.9)]}
+            nuc = {1000020040: (0.45, 0.45), 1000020030: (1.1, 0.1), 1000010030: (0.1, 1.1),
+                   1000010020: (1.0, 1.0)}
+            for mo, das in bc.items():
+                for da, w in das:
+                    self._incl_tab[(mo, da)] = w * self._nonel_tab[mo]
+            for mo, (mp, mn) in nuc.items():
+                self._incl_tab[(mo, 2212)] = mp * self._nonel_tab[mo]
+                self._incl_tab[(mo, 2112)] = mn * self._nonel_tab[mo]
+            # Nucleon yields are given as total cross sections; the reference
+            # places them in the x = 1 bin of its redistribution grid.
+            for mo in (2212, 2112):
+                self._incl_tab[(mo, mo)] = 0.7 * self._nonel_tab[mo]
+                self._incl_tab[(mo, 4324 - mo)] = 0.3 * self._nonel_tab[mo]
+            self.set_range()
+            self._optimize_and_generate_index()
+
+    run = core.PriNCeRun(max_mass=4, photon_field=photonfields.CMBPhotonSpectrum(),
+                         cross_sections=SynthXS())
+    return run
+
+
+def main():
+    _prepare_reference()
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (6, 14, 8)
+    config.photon_grid = (-15, -6, 8)
+    config.tau_dec_threshold = 0.0
+    config.max_mass = 4
+    config.batch_matrix_format = "dense"
+    config.xs_dtype = "float64"
+    config.linear_algebra_backend = "scipy"
+
+    from prince_cr import cr_sources
+    from prince_cr.cross_sections.base import CrossSectionBase
+    from prince_cr.solvers import MultiRHSPropagationSolverETD2, UHECRPropagationSolverETD2
+    from prince_cr.solvers import etd2 as ref_etd2
+
+    run = build(config, CrossSectionBase)
+    run.backend.xs_dtype = "float64"
+    ir = run.int_rates
+    sm = run.spec_man
+    species = np.array(sm.known_species, dtype=np.int64)
+
+    class ZmaxRigidity(cr_sources.RigdityCutoffSource):
+        def __init__(self, *a, z_max=np.inf, **k):
+            self.z_max = z_max
+            super().__init__(*a, **k)
+
+        def evolution(self, z):
+            if z > self.z_max:
+                return 0.0
+            return super().evolution(z)
+
+    # Source set: (kind, params, norm, m, z_max).  Columns of the multi-RHS run
+    # are lists of these.
+    eq = {int(p): (2.0, 1e10, 1.0) for p in species}
+    SRC = {
+        "eq": ("RigdityCutoffSource", eq, 1.0, "flat", np.inf),
+        "auger": ("AugerFitSource", {2212: (1.0, 10 ** 9.5, 2.0), 1000020040: (1.0, 10 ** 9.5, 1.0)},
+                  3.0, ("simple", 3.0), np.inf),
+        "soft": ("SimpleSource", {2212: (2.6, 1e11, 1.0), 1000010020: (2.2, 1e11, 0.5)},
+                 0.5, ("simple", -1.0), np.inf),
+        "late": ("RigdityCutoffSource", {1000020040: (-0.5, 10 ** 9.2, 1.0), 2212: (1.5, 10 ** 10.5, 0.3)},
+                 2.0, ("simple", 1.5), 0.55),
+    }
+
+    def make(key):
+        kind, params, norm, m, zmax = SRC[key]
+        if kind == "RigdityCutoffSource" and np.isfinite(zmax):
+            return ZmaxRigidity(run, norm=norm, params=params, m=m, z_max=zmax)
+        return getattr(cr_sources, kind)(run, norm=norm, params=params, m=m)
+
+    out = {}
+    out["species"] = species
+    out["cr_grid"] = np.array(config.cosmic_ray_grid, dtype=np.float64)
+    out["ph_grid"] = np.array(config.photon_grid, dtype=np.float64)
+    out["batch_matrix"] = np.asarray(ir._batch_matrix, dtype=np.float64)
+    out["batch_rows"] = np.asarray(ir._batch_rows, dtype=np.int64)
+    out["batch_cols"] = np.asarray(ir._batch_cols, dtype=np.int64)
+    out["cpl_indptr"] = np.asarray(ir.coupling_mat.indptr, dtype=np.int64)
+    out["cpl_indices"] = np.asarray(ir.coupling_mat.indices, dtype=np.int64)
+    out["photon_vector_z1"] = ir.photon_vector(1.0)
+    out["xi"] = run.pair_loss_rates_grid.xi
+    out["phi_xi2"] = run.pair_loss_rates_grid.phi_xi2
+    out["pair_scale_vec"] = run.pair_loss_rates_grid.scale_vec
+    out["adia_energy"] = run.adia_loss_rates_grid.energy_vector
+    out["kappa_pair_z1"] = run.pair_loss_rates_grid.loss_vector(1.0)
+    out["kappa_pair_z05"] = run.pair_loss_rates_grid.loss_vector(0.5)
+    for key in SRC:
+        kind, params, norm, m, zmax = SRC[key]
+        out[f"src_{key}_grid"] = make(key).injection_grid
+
+    def fresh_fold_cache():
+        # The reference caches its row-subset fold kernels on the run after the
+        # first solve and reuses them in later solves, although the M_off
+        # pattern depends on the first window's photon field: a later solve
+        # from another initial z would read a stale cache.  Dropping the cache
+        # before each solve keeps every solve on its own first-window pattern.
+        ir._sf_off_kernel = None
+
+    def single(keys, zi=1.0, zf=0.0, dz=1e-3, thr=None, **flags):
+        fresh_fold_cache()
+        s = UHECRPropagationSolverETD2(initial_z=zi, final_z=zf, prince_run=run, **flags)
+        if thr is not None:
+            s.recomp_z_threshold = thr
+        windows = []
+        orig = s._refresh_z_caches
+
+        def rec(z):
+            windows.append(z)
+            return orig(z)
+
+        s._refresh_z_caches = rec
+        for k in keys:
+            s.add_source_class(make(k))
+        s.solve(dz=dz)
+        return s, np.asarray(s.state), np.asarray(windows)
+
+    s, st, win = single(["eq"])
+    out["state_plain"] = st
+    out["windows_plain"] = win
+    # Intermediates from a fresh solver stopped after its first window.
+    fresh_fold_cache()
+    probe = UHECRPropagationSolverETD2(initial_z=1.0, final_z=0.0, prince_run=run)
+    probe._reset_for_solve()
+    probe._ensure_D_split()
+    probe._refresh_z_caches(1.0)
+    out["M_off_indptr"] = np.asarray(probe._etd2_M_raw_off.indptr, dtype=np.int64)
+    out["M_off_indices"] = np.asarray(probe._etd2_M_raw_off.indices, dtype=np.int64)
+    out["M_off_data_z1"] = np.asarray(probe._etd2_M_raw_off.data)
+    out["M_diag_z1"] = np.asarray(probe._etd2_M_raw_diag)
+    out["D_diag"] = np.asarray(probe._etd2_D_diag)
+    out["D_off_indptr"] = np.asarray(probe._etd2_D_off.indptr, dtype=np.int64)
+    out["D_off_indices"] = np.asarray(probe._etd2_D_off.indices, dtype=np.int64)
+    out["D_off_data"] = np.asarray(probe._etd2_D_off.data)
+
+    out["state_no_pair"] = single(["eq"], enable_pairprod_losses=False)[1]
+    out["state_no_adia"] = single(["eq"], enable_adiabatic_losses=False)[1]
+    out["state_no_pdiff"] = single(["eq"], enable_partial_diff_jacobian=False)[1]
+    out["state_no_photohad"] = single(["eq"], enable_photohad_losses=False)[1]
+    out["state_two_src"] = single(["auger", "soft"])[1]
+    s_thr, st_thr, win_thr = single(["eq"], zi=0.5, zf=0.0, dz=2e-3, thr=1e-3)
+    out["state_thr"] = st_thr
+    out["windows_thr"] = win_thr
+    s_dec, st_dec, _ = single(["eq"], enable_decay=True)
+    out["state_decay"] = st_dec
+    lam_d = s_dec._etd2_Lambda_diag
+    lam_o = s_dec._etd2_Lambda_off
+    out["lambda_diag"] = np.zeros(run.dim_states) if lam_d is None else np.asarray(lam_d)
+    if lam_o is not None:
+        lam_o = lam_o.tocsr()
+        lam_o.sort_indices()
+        out["lambda_indptr"] = np.asarray(lam_o.indptr, dtype=np.int64)
+        out["lambda_indices"] = np.asarray(lam_o.indices, dtype=np.int64)
+        out["lambda_data"] = np.asarray(lam_o.data)
+
+    cols = [["eq"], ["auger"], ["soft", "auger"], ["late"]]
+    fresh_fold_cache()
+    m = MultiRHSPropagationSolverETD2(initial_z=1.0, final_z=0.0, prince_run=run, K=len(cols))
+    for k, keys in enumerate(cols):
+        for key in keys:
+            m[k].add_source_class(make(key))
+    m.solve(dz=1e-3)
+    out["state_multi"] = np.asarray(m.state)
+    out["multi_columns"] = np.array([",".join(c) for c in cols])
+
+    # Kernel-level known answers of the integrator with a constant operator.
+    zg = np.linspace(0.0, 6.0, 2001)
+    x = np.array([1.0, 0.0, 0.0])
+    dconst = np.array([-1.0, -0.4, 0.0])
+    import scipy.sparse as sps
+
+    L = sps.csr_matrix(np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.4, 0.0]]))
+
+    def op(z):
+        def apply_F(v, o):
+            np.copyto(o, L @ v)
+        return dconst, apply_F
+
+    ref_etd2.integrate(x, zg, op)
+    out["chain3_state"] = x
+
+    for key, (kind, params, norm, mm, zmax) in SRC.items():
+        out[f"src_{key}_kind"] = np.array(kind)
+        out[f"src_{key}_norm"] = np.array(norm)
+        out[f"src_{key}_zmax"] = np.array(zmax)
+        out[f"src_{key}_m"] = np.array(repr(mm))
+        out[f"src_{key}_params"] = np.array(repr(params))
+
+    path = os.path.join(HERE, "light_network.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,61 @@
+"""Load the golden fixtures produced by ``tests/golden/make_golden.py``.
+
+``light_network()`` returns the fixture arrays and a ``prince_b200`` run
+built from the fixture's own fold kernel, grids and species, plus a source
+factory that rebuilds each recorded source with ``prince_b200.cr_sources``.
+"""
+
+from __future__ import annotations
+
+import ast
+import os
+
+import numpy as np
+
+from prince_b200 import cr_sources, photonfields
+from prince_b200.run import FixedKernelModel, PriNCeRun
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def light_network():
+    z = dict(np.load(os.path.join(GOLDEN, "light_network.npz")))
+    model = FixedKernelModel(z["species"], z["batch_matrix"], z["batch_rows"], z["batch_cols"])
+    run = PriNCeRun(model, photonfields.CMBPhotonSpectrum(),
+                    cosmic_ray_grid=tuple(z["cr_grid"]), photon_grid=tuple(z["ph_grid"]),
+                    max_mass=4)
+
+    def source(key):
+        kind = str(z[f"src_{key}_kind"])
+        params = ast.literal_eval(str(z[f"src_{key}_params"]))
+        m = ast.literal_eval(str(z[f"src_{key}_m"]))
+        zmax = float(z[f"src_{key}_zmax"])
+        cls = getattr(cr_sources, kind)
+        return cls(run, norm=float(z[f"src_{key}_norm"]), params=params, m=m,
+                   z_max=None if not np.isfinite(zmax) else zmax)
+
+    return z, run, source
+
+
+def rel_err_on_support(x, ref, species_blocks, floor=1e-20):
+    """Max relative error over bins whose |ref| exceeds ``floor`` x the species max."""
+    worst = 0.0
+    for sl in species_blocks:
+        r = ref[sl]
+        if r.ndim == 1:
+            r = r[:, None]
+            v = x[sl][:, None]
+        else:
+            v = x[sl]
+        for k in range(r.shape[1]):
+            rk = r[:, k]
+            m = np.abs(rk).max()
+            if m == 0:
+                if np.abs(v[:, k]).max() != 0:
+                    return np.inf
+                continue
+            mask = np.abs(rk) > floor * m
+            e = np.abs(v[mask, k] - rk[mask]) / np.abs(rk[mask])
+            if e.size:
+                worst = max(worst, float(e.max()))
+    return worst
