@@ -1,0 +1,177 @@
+/*
+ * prince_b200 -- C ABI of the B200-native ETD2 propagation core.
+ *
+ * Plain C types only (pointers, sizes, one POD struct); no torch types.  All
+ * functions return PB_OK (0) on success or a PB_ERR_* code; the message of the
+ * last failure is available from pb_last_error(ctx) (pb_global_error() for
+ * failures of pb_create).  Host pointers are read during the call only.
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the PriNCe project).  The reference's ETD2 path is Python, so there is no
+ * reference C ABI; the Python binding in prince_b200/_lib.py is the layer a
+ * reference backend would call.
+ *
+ * Threading: a context is used by one host thread at a time; all device work
+ * of a context runs on the context's own stream.
+ */
+#ifndef PRINCE_B200_H
+#define PRINCE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PB_OK 0
+#define PB_ERR_ARG 1    /* invalid argument                       -> ValueError   */
+#define PB_ERR_STATE 2  /* missing set-up / wrong call order       -> RuntimeError */
+#define PB_ERR_CUDA 3   /* CUDA runtime failure                    -> RuntimeError */
+#define PB_ERR_DEVICE 4 /* device-side status (timeout, non-finite) -> RuntimeError */
+
+/* Solve flags: the solver enable switches of
+ * UHECRPropagationSolver.__init__ (src/prince_cr/solvers/propagation.py:196-209). */
+#define PB_ADIABATIC 1u     /* enable_adiabatic_losses      */
+#define PB_PAIRPROD 2u      /* enable_pairprod_losses       */
+#define PB_PHOTOHAD 4u      /* enable_photohad_losses       */
+#define PB_INJECTION 8u     /* enable_injection_jacobian    */
+#define PB_PARTIAL_DIFF 16u /* enable_partial_diff_jacobian */
+#define PB_DECAY 32u        /* enable_decay (explicit Lambda operator) */
+
+typedef struct pb_context pb_context;
+
+/* Version of this ABI (bumped on any signature change). */
+int pb_abi_version(void);
+
+/* Create a context on CUDA device `device` (own stream, own device buffers).
+ * Replaces: the per-solver backend state of ETD2SolverCUPY.__init__
+ * (src/prince_cr/solvers/propagation.py:1595-1700). */
+int pb_create(int device, pb_context** out);
+
+/* Free every device buffer of the context.  Replaces ETD2Solver*.close()
+ * (propagation.py:708-716, 970-978). */
+void pb_destroy(pb_context* ctx);
+
+const char* pb_last_error(const pb_context* ctx);
+const char* pb_global_error(void);
+
+/* Fixed CSR pattern of the coupling matrix M (n_states x n_states, n_entries
+ * entries, rows sorted, columns sorted within rows).  Entry i of the pattern
+ * is row i of the fold kernel.
+ * Replaces: PhotoNuclearInteractionRate._init_coupling_mat
+ * (src/prince_cr/interaction_rates.py:648-697). */
+int pb_set_coupling(pb_context* ctx, int64_t n_states, int64_t n_entries,
+                    const int64_t* indptr, const int32_t* indices);
+
+/* Dense FP64 fold kernel, row-major (n_entries x n_photon), rows in CSR order.
+ * Replaces: PhotoNuclearInteractionRate._batch_matrix
+ * (interaction_rates.py:186-188, 629-631, 681) and the GPU mirror of
+ * _ensure_coupling_mat_gpu (interaction_rates.py:852-928). */
+int pb_set_fold_kernel(pb_context* ctx, int64_t n_entries, int32_t n_photon,
+                       const double* kernel);
+
+/* Photon-grid bin centres (n_photon) at which the fold samples n(E, z).
+ * Replaces: the ph_grid.grid argument of photon_vector (interaction_rates.py:105-116). */
+int pb_set_photon_grid(pb_context* ctx, int32_t n_photon, const double* energies);
+
+/* Analytic photon field: n_comp components, kinds[i] in {0: CMB black body,
+ * 1: flat, 2: grey body}, params[3*i .. 3*i+2] = (p0, p1, p2) as documented in
+ * prince_b200/photonfields.py.  Replaces: PhotonField.get_photon_density for
+ * the analytic fields (src/prince_cr/photonfields.py:27-127). */
+int pb_set_photon_field(pb_context* ctx, int32_t n_comp, const int32_t* kinds,
+                        const double* params);
+
+/* Finite-difference loss operator split into its off-diagonal CSR part
+ * (D_off, nnz entries) and its diagonal (n_states).
+ * Replaces: DifferentialOperator.operator + _ensure_D_split
+ * (src/prince_cr/solvers/partial_diff.py:28-110; propagation.py:1122-1146). */
+int pb_set_fd_operator(pb_context* ctx, int64_t nnz, const int64_t* indptr,
+                       const int32_t* indices, const double* values, const double* diag);
+
+/* Continuous-loss inputs:
+ *   adia_energy (n_states)  energy_vector of ContinuousAdiabaticLossRate
+ *                           (interaction_rates.py:1194-1224);
+ *   pair_scale (n_states)   scale_vec of ContinuousPairProductionLossRate;
+ *   pair_bin (n_states)     cosmic-ray bin of each state on nucleus blocks, -1 elsewhere;
+ *   xi (n_xi), phi_xi2 (n_xi), pair_photon_grid (n_cr_bins x n_xi): the
+ *                           integration grid of loss_vector (interaction_rates.py:1238-1312). */
+int pb_set_losses(pb_context* ctx, const double* adia_energy, const double* pair_scale,
+                  const int32_t* pair_bin, int32_t n_cr_bins, int32_t n_xi,
+                  const double* xi, const double* phi_xi2, const double* pair_photon_grid);
+
+/* Constant explicit-decay operator: diagonal (n_states, may be NULL) and
+ * off-diagonal CSR (nnz may be 0).  Replaces: _ensure_Lambda_split
+ * (propagation.py:1148-1358). */
+int pb_set_decay(pb_context* ctx, const double* diag, int64_t nnz, const int64_t* indptr,
+                 const int32_t* indices, const double* values);
+
+/* Injection basis: n_src source grids restricted to the n_rows state rows on
+ * which any of them is non-zero.  rows (n_rows) lists those states; grids is
+ * row-major (n_rows x n_src).  Source s feeds column src_col[s] (non-decreasing).
+ * Replaces: the injection_grid arrays of CosmicRaySource
+ * (src/prince_cr/cr_sources.py:32-48) consumed by injection()
+ * (propagation.py:363-370, 2476-2488). */
+int pb_set_injection(pb_context* ctx, int32_t n_src, int32_t n_rows, const int32_t* rows,
+                     const double* grids, int32_t n_cols, const int32_t* src_col);
+
+/* One solve: the redshift stepping of UHECRPropagationSolverETD2.solve /
+ * MultiRHSPropagationSolverETD2.solve (propagation.py:813-890; etd2.py:478-517;
+ * _operator_at / apply_F propagation.py:1360-1508; multi-RHS 2495-2618).
+ * All per-step scalars are evaluated by the caller in float64 exactly as the
+ * reference does (z grid, window schedule, dl/dz, H(z) cm2sec, injection
+ * prefactor dl/dz * cm2sec, source evolution); the device computes the
+ * photon field, the pair-loss vectors, the fold, the operator split and every
+ * ETD2 step. */
+typedef struct pb_solve_args {
+  int64_t n_steps;
+  int32_t n_windows;
+  int32_t n_cols;          /* K: state columns (1 for the single-RHS solver)        */
+  uint32_t flags;          /* PB_* solve flags                                       */
+  double photon_scale;     /* multiplies the photon field (1.0 nominal)             */
+  const double* z_window;  /* n_windows: redshift of each rate-cache refresh       */
+  const int32_t* window;   /* n_steps: window index of each step                    */
+  const double* h;         /* n_steps: z[k+1] - z[k]                                 */
+  const double* dldz;      /* n_steps: dl/dz at z[k]                                 */
+  const double* hc;        /* n_steps: H(z[k]) * cm2sec (adiabatic loss scale)       */
+  const double* finj;      /* n_steps: dl/dz(z[k]) * 1.0 * cm2sec (injection factor) */
+  const double* coeff;     /* n_steps x n_src: norm * evolution(z[k]) per source     */
+  const int32_t* n_active; /* n_steps: columns [0, n_active) may be non-zero; the
+                              rest are exactly zero (sources not yet switched on)  */
+  double* state;           /* n_states x n_cols row-major: in = initial state (if
+                              init_state != 0), out = state at the final redshift  */
+  int32_t init_state;      /* 0: start from zeros                                    */
+  int32_t state_on_device; /* 1: `state` is a device pointer                         */
+} pb_solve_args;
+
+int pb_solve(pb_context* ctx, const pb_solve_args* args);
+
+/* Inspection after a solve: the off-diagonal operator pattern built from the
+ * first window (split_operator + eliminate_zeros, src/prince_cr/solvers/etd2.py:234-268).
+ * Call with indptr/indices NULL to query nnz. */
+int pb_get_operator_pattern(pb_context* ctx, int64_t* nnz, int64_t* indptr, int32_t* indices);
+
+/* Per-window operator values of the last solve: M_off.data (nnz), the
+ * diagonal of M (n_states) and kappa_pair (n_states); any pointer may be NULL. */
+int pb_get_window(pb_context* ctx, int32_t window, double* offdiag, double* diag,
+                  double* kappa_pair);
+
+/* ETD2 with a z-independent operator: d (n) diagonal, L_off CSR, no losses,
+ * no injection, state (n) advanced in place along z_grid (n_steps + 1).
+ * Replaces: etd2.integrate driven by a constant operator_at closure
+ * (src/prince_cr/solvers/etd2.py:478-517; tests/test_explicit_decay_analytics.py:43-62). */
+int pb_integrate_const(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
+                       const int64_t* indptr, const int32_t* indices, const double* values,
+                       int64_t n_steps, const double* z_grid, double* state);
+
+/* Timing of the last pb_solve from CUDA events on the context stream (ms):
+ * solve_ms  -- whole call on the device, including the state copy-out;
+ * device_ms -- photon field, pair losses, fold, split and all steps (inputs resident);
+ * steps_ms  -- the ETD2 step kernels alone;
+ * launches  -- number of kernels the solve launched. */
+int pb_last_timing(pb_context* ctx, double* solve_ms, double* device_ms, double* steps_ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PRINCE_B200_H */

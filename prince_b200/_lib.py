@@ -1,0 +1,276 @@
+"""ctypes binding of the C ABI in ``include/prince_b200.h``.
+
+The shared library ``prince_b200/libprince_b200.so`` is built in-tree by
+``prince_b200.build.build()`` (nvcc, sm_100a).  Loading fails loudly when the
+library is missing: there is no CPU implementation behind this package.
+
+``Context`` owns one ``pb_context`` (one device, one stream).  Non-zero
+status codes become exceptions: ``PB_ERR_ARG`` -> ``ValueError``, everything
+else -> ``RuntimeError``, with the library's message.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libprince_b200.so")
+
+PB_OK, PB_ERR_ARG, PB_ERR_STATE, PB_ERR_CUDA, PB_ERR_DEVICE = 0, 1, 2, 3, 4
+PB_ADIABATIC, PB_PAIRPROD, PB_PHOTOHAD, PB_INJECTION, PB_PARTIAL_DIFF, PB_DECAY = 1, 2, 4, 8, 16, 32
+
+_d = C.POINTER(C.c_double)
+_i32 = C.POINTER(C.c_int32)
+_i64 = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+
+
+class SolveArgs(C.Structure):
+    _fields_ = [
+        ("n_steps", C.c_int64),
+        ("n_windows", C.c_int32),
+        ("n_cols", C.c_int32),
+        ("flags", C.c_uint32),
+        ("photon_scale", C.c_double),
+        ("z_window", _d),
+        ("window", _i32),
+        ("h", _d),
+        ("dldz", _d),
+        ("hc", _d),
+        ("finj", _d),
+        ("coeff", _d),
+        ("n_active", _i32),
+        ("state", _d),
+        ("init_state", C.c_int32),
+        ("state_on_device", C.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "pb_abi_version": (C.c_int, []),
+    "pb_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "pb_destroy": (None, [_vp]),
+    "pb_last_error": (C.c_char_p, [_vp]),
+    "pb_global_error": (C.c_char_p, []),
+    "pb_set_coupling": (C.c_int, [_vp, C.c_int64, C.c_int64, _i64, _i32]),
+    "pb_set_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
+    "pb_set_photon_grid": (C.c_int, [_vp, C.c_int32, _d]),
+    "pb_set_photon_field": (C.c_int, [_vp, C.c_int32, _i32, _d]),
+    "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
+    "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
+    "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
+    "pb_set_injection": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _d, C.c_int32, _i32]),
+    "pb_solve": (C.c_int, [_vp, C.POINTER(SolveArgs)]),
+    "pb_get_operator_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
+    "pb_get_window": (C.c_int, [_vp, C.c_int32, _d, _d, _d]),
+    "pb_integrate_const": (C.c_int, [_vp, C.c_int64, _d, C.c_int64, _i64, _i32, _d, C.c_int64, _d, _d]),
+    "pb_last_timing": (C.c_int, [_vp, _d, _d, _d, _i64]),
+}
+
+_LIB = None
+
+
+def exported_symbols():
+    """Names of the C ABI functions this binding expects."""
+    return list(_PROTOS)
+
+
+def load():
+    """Load the in-tree shared library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build the CUDA extension first "
+            "(python -c 'import __graft_entry__ as g; g.build()' or "
+            "python -m prince_b200.build). There is no CPU fallback."
+        )
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in _PROTOS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32a(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _i64a(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+class Context:
+    """One device context of the C library."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = _vp()
+        rc = self.lib.pb_create(int(device), C.byref(h))
+        if rc != PB_OK:
+            msg = self.lib.pb_global_error().decode()
+            raise (ValueError if rc == PB_ERR_ARG else RuntimeError)(f"pb_create: {msg}")
+        self.h = h
+        self.device = int(device)
+
+    def _check(self, rc, what):
+        if rc != PB_OK:
+            msg = self.lib.pb_last_error(self.h).decode()
+            raise (ValueError if rc == PB_ERR_ARG else RuntimeError)(f"{what}: {msg}")
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.pb_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- set-up ---------------------------------------------------------
+    def set_coupling(self, n, indptr, indices):
+        indptr, indices = _i64a(indptr), _i32a(indices)
+        self._check(self.lib.pb_set_coupling(self.h, int(n), int(indices.size), _ptr(indptr, C.c_int64),
+                                             _ptr(indices, C.c_int32)), "pb_set_coupling")
+
+    def set_fold_kernel(self, kernel):
+        kernel = _f64(kernel)
+        self._check(self.lib.pb_set_fold_kernel(self.h, int(kernel.shape[0]), int(kernel.shape[1]),
+                                                _ptr(kernel, C.c_double)), "pb_set_fold_kernel")
+
+    def set_photon_grid(self, energies):
+        e = _f64(energies)
+        self._check(self.lib.pb_set_photon_grid(self.h, int(e.size), _ptr(e, C.c_double)), "pb_set_photon_grid")
+
+    def set_photon_field(self, components):
+        kinds = _i32a([c[0] for c in components])
+        pars = _f64([list(c[1:4]) for c in components]).reshape(-1)
+        self._check(self.lib.pb_set_photon_field(self.h, int(kinds.size), _ptr(kinds, C.c_int32),
+                                                 _ptr(pars, C.c_double)), "pb_set_photon_field")
+
+    def set_fd_operator(self, off, diag):
+        ip, ix, v, dg = _i64a(off.indptr), _i32a(off.indices), _f64(off.data), _f64(diag)
+        self._check(self.lib.pb_set_fd_operator(self.h, int(v.size), _ptr(ip, C.c_int64), _ptr(ix, C.c_int32),
+                                                _ptr(v, C.c_double), _ptr(dg, C.c_double)), "pb_set_fd_operator")
+
+    def set_losses(self, adia_energy, pair_scale, pair_bin, xi, phi_xi2, pair_photon_grid):
+        ae, ps, pb_ = _f64(adia_energy), _f64(pair_scale), _i32a(pair_bin)
+        xi, ph, pg = _f64(xi), _f64(phi_xi2), _f64(pair_photon_grid)
+        self._check(self.lib.pb_set_losses(self.h, _ptr(ae, C.c_double), _ptr(ps, C.c_double),
+                                           _ptr(pb_, C.c_int32), int(pg.shape[0]), int(xi.size),
+                                           _ptr(xi, C.c_double), _ptr(ph, C.c_double), _ptr(pg, C.c_double)),
+                    "pb_set_losses")
+
+    def set_decay(self, diag, off=None):
+        dg = None if diag is None else _f64(diag)
+        if off is None or off.nnz == 0:
+            self._check(self.lib.pb_set_decay(self.h, _ptr(dg, C.c_double), 0, None, None, None), "pb_set_decay")
+            return
+        ip, ix, v = _i64a(off.indptr), _i32a(off.indices), _f64(off.data)
+        self._check(self.lib.pb_set_decay(self.h, _ptr(dg, C.c_double), int(v.size), _ptr(ip, C.c_int64),
+                                          _ptr(ix, C.c_int32), _ptr(v, C.c_double)), "pb_set_decay")
+
+    def set_injection(self, rows, grids, src_col, n_cols):
+        rows, grids, src_col = _i32a(rows), _f64(grids), _i32a(src_col)
+        self._check(self.lib.pb_set_injection(self.h, int(src_col.size), int(rows.size), _ptr(rows, C.c_int32),
+                                              _ptr(grids, C.c_double), int(n_cols), _ptr(src_col, C.c_int32)),
+                    "pb_set_injection")
+
+    # -- solve ----------------------------------------------------------
+    def solve(self, sched, flags, n_cols, coeff, n_active, state, photon_scale=1.0, init_state=False,
+              state_ptr=None):
+        """Run one solve.  ``state`` is an (n, K) float64 host array (in/out)
+        unless ``state_ptr`` (a device pointer) is given."""
+        keep = []
+
+        def f(a):
+            a = _f64(a)
+            keep.append(a)
+            return _ptr(a, C.c_double)
+
+        def i(a):
+            a = _i32a(a)
+            keep.append(a)
+            return _ptr(a, C.c_int32)
+
+        args = SolveArgs()
+        args.n_steps = int(sched.n_steps)
+        args.n_windows = int(len(sched.z_window))
+        args.n_cols = int(n_cols)
+        args.flags = int(flags)
+        args.photon_scale = float(photon_scale)
+        args.z_window = f(sched.z_window)
+        args.window = i(sched.window)
+        args.h = f(sched.h)
+        args.dldz = f(sched.dldz)
+        args.hc = f(sched.hc)
+        args.finj = f(sched.finj)
+        args.coeff = f(coeff) if coeff is not None else None
+        args.n_active = i(n_active)
+        if state_ptr is not None:
+            args.state = C.cast(C.c_void_p(int(state_ptr)), _d)
+            args.state_on_device = 1
+        else:
+            assert state.dtype == np.float64 and state.flags["C_CONTIGUOUS"]
+            args.state = _ptr(state, C.c_double)
+            args.state_on_device = 0
+        args.init_state = 1 if init_state else 0
+        self._check(self.lib.pb_solve(self.h, C.byref(args)), "pb_solve")
+
+    def operator_pattern(self, n):
+        nnz = C.c_int64(0)
+        self._check(self.lib.pb_get_operator_pattern(self.h, C.byref(nnz), None, None), "pb_get_operator_pattern")
+        ip = np.zeros(n + 1, dtype=np.int64)
+        ix = np.zeros(max(nnz.value, 1), dtype=np.int32)
+        self._check(self.lib.pb_get_operator_pattern(self.h, C.byref(nnz), _ptr(ip, C.c_int64), _ptr(ix, C.c_int32)),
+                    "pb_get_operator_pattern")
+        return ip, ix[: nnz.value]
+
+    def window_values(self, w, n, nnz):
+        off = np.zeros(max(nnz, 1))
+        dg = np.zeros(n)
+        kp = np.zeros(n)
+        self._check(self.lib.pb_get_window(self.h, int(w), _ptr(off, C.c_double), _ptr(dg, C.c_double),
+                                           _ptr(kp, C.c_double)), "pb_get_window")
+        return off[:nnz], dg, kp
+
+    def integrate_const(self, d, L_off, z_grid, state):
+        d = _f64(d)
+        x = np.array(state, dtype=np.float64)
+        zg = _f64(z_grid)
+        n = d.size
+        if L_off is None or L_off.nnz == 0:
+            rc = self.lib.pb_integrate_const(self.h, n, _ptr(d, C.c_double), 0, None, None, None,
+                                             int(zg.size - 1), _ptr(zg, C.c_double), _ptr(x, C.c_double))
+        else:
+            ip, ix, v = _i64a(L_off.indptr), _i32a(L_off.indices), _f64(L_off.data)
+            rc = self.lib.pb_integrate_const(self.h, n, _ptr(d, C.c_double), int(v.size), _ptr(ip, C.c_int64),
+                                             _ptr(ix, C.c_int32), _ptr(v, C.c_double), int(zg.size - 1),
+                                             _ptr(zg, C.c_double), _ptr(x, C.c_double))
+        self._check(rc, "pb_integrate_const")
+        return x
+
+    def last_timing(self):
+        """(solve_ms, device_ms, steps_ms, launches) of the last solve."""
+        a, d, b, n = C.c_double(), C.c_double(), C.c_double(), C.c_int64()
+        self._check(self.lib.pb_last_timing(self.h, C.byref(a), C.byref(d), C.byref(b), C.byref(n)),
+                    "pb_last_timing")
+        return a.value, d.value, b.value, n.value

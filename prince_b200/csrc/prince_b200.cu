@@ -1,0 +1,1220 @@
+// prince_b200 -- B200-native ETD2 propagation core (sm_100a).
+//
+// One solve of the transport equation dn/dz = L(z) n + b(z) runs entirely on the
+// device, in one CUDA graph:
+//
+//   1. photon matrix   PT[w][j] = s * n_gamma(E_ph[j], z_w)          (all windows)
+//   2. pair-loss rate  kp[w][r] = scale[r] * trapz_xi(...)            (all windows)
+//   3. first-window fold (GEMV) -> which coupling entries survive the
+//      diagonal/off-diagonal split -> prefix sum -> M_off CSR pattern
+//   4. fold GEMM over all windows on the FP64 tensor pipe (DMMA), written
+//      straight into M_off values [w][nnz] and the diagonal [w][n]
+//   5. ETD2 steps: two fused kernels per step (stage 1 -> a, F(x);
+//      stage 2 -> x), each an SpMV/SpMM of M_off with the FD loss stencil,
+//      the explicit-decay term, the injection and the phi-function epilogue.
+//
+// The algorithm follows the reference CPU solver of PriNCe:
+//   src/prince_cr/solvers/etd2.py:329-439 (phi functions, step),
+//   src/prince_cr/solvers/propagation.py:1017-1120 (per-window refresh),
+//   propagation.py:1360-1508 (per-step operator and apply_F),
+//   propagation.py:2495-2618 (multi-RHS),
+//   src/prince_cr/interaction_rates.py:966-1067 (fold), 1277-1294 (pair loss).
+// The data layout, the kernels and the launch structure are this project's own.
+
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/prince_b200.h"
+
+namespace {
+
+constexpr int kAbiVersion = 1;
+constexpr int kLongRow = 256;      // rows with more coupling entries get a whole CTA
+constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
+constexpr int kColTile = 32;       // state columns per warp in the batched step
+
+thread_local std::string g_error;
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (want == 0) want = 16;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct pb_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+  std::string err;
+
+  // problem dimensions
+  int64_t n = 0;          // states
+  int64_t R = 0;          // coupling entries (fold-kernel rows)
+  int32_t dph = 0;        // photon bins
+  bool have_coupling = false, have_kernel = false, have_photon_grid = false;
+  bool have_field = false, have_fd = false, have_losses = false;
+
+  // coupling pattern
+  DBuf cpl_indptr, cpl_indices, cpl_row, cpl_is_diag;
+  std::vector<int32_t> h_short_rows, h_long_rows;
+  DBuf short_rows, long_rows;
+  // fold kernel and photon grid
+  DBuf kernel, eph;
+  // photon field
+  int32_t n_comp = 0;
+  int32_t comp_kind[8];
+  double comp_par[8][3];
+  // FD operator
+  int64_t nnzD = 0;
+  DBuf d_indptr, d_indices, d_vals, d_diag;
+  // losses
+  DBuf adia_E, pair_scale, pair_bin, xi, phi_xi2, pair_pg;
+  int32_t n_cr_bins = 0, n_xi = 0;
+  // decay
+  bool have_decay = false;
+  int64_t nnzL = 0;
+  DBuf l_diag, l_indptr, l_indices, l_vals;
+  // injection
+  int32_t n_src = 0, n_inj_rows = 0, n_src_cols = 0;
+  DBuf inj_slot, inj_G, src_ptr;
+
+  // per-solve workspace
+  DBuf PT, zwin, rs, kp, keep, pos, dest, m_indptr, m_indices, m_vals, m_diag;
+  DBuf s_h, s_dldz, s_hc, s_finj, s_win, s_coeff;
+  DBuf X, A, F;
+  DBuf scan_tmp;
+  size_t scan_tmp_bytes = 0;
+  int32_t last_W = 0;
+  bool have_solution = false;
+
+  // timing
+  float last_solve_ms = 0.f, last_device_ms = 0.f, last_steps_ms = 0.f;
+  int64_t last_launches = 0;
+};
+
+namespace {
+
+int fail(pb_context* c, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf; else g_error = buf;
+  return code;
+}
+
+#define PB_CUDA(ctx, call)                                                              \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail((ctx), PB_ERR_CUDA, "%s failed: %s (%s:%d)", #call,                  \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);                          \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// photon field on the device (prince_b200/photonfields.py kinds)
+// ---------------------------------------------------------------------------
+struct FieldDesc {
+  int n;
+  int kind[8];
+  double p[8][3];
+  double scale;
+};
+
+__device__ __forceinline__ double field_density(const FieldDesc& f, double E, double z) {
+  double total = 0.0;
+  const double opz = 1.0 + z;
+  for (int c = 0; c < f.n; ++c) {
+    double v;
+    if (f.kind[c] == 1) {  // flat: (1+z)^2 * n0
+      v = __dmul_rn(__dmul_rn(opz, opz), f.p[c][0]);
+    } else {  // black / grey body: ((p0 (1+z)^2) Ered^p2) / (exp(Ered/p1) - 1)
+      const double ered = __ddiv_rn(E, opz);
+      const double eratio = __ddiv_rn(ered, f.p[c][1]);
+      if (eratio < 709.0) {
+        const double pz = __dmul_rn(f.p[c][0], __dmul_rn(opz, opz));
+        const double pw = (f.kind[c] == 0) ? __dmul_rn(ered, ered) : pow(ered, f.p[c][2]);
+        v = __ddiv_rn(__dmul_rn(pz, pw), __dadd_rn(exp(eratio), -1.0));
+      } else {
+        v = 0.0;
+      }
+    }
+    total = (c == 0) ? v : __dadd_rn(total, v);
+  }
+  return (f.scale == 1.0) ? total : __dmul_rn(f.scale, total);
+}
+
+__global__ void k_photon_matrix(FieldDesc f, const double* __restrict__ eph, int dph,
+                                const double* __restrict__ zwin, int W, double* __restrict__ PT) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= W * dph) return;
+  int w = i / dph, j = i % dph;
+  PT[i] = field_density(f, eph[j], zwin[w]);
+}
+
+// Bethe-Heitler rate per (window, cosmic-ray bin): trapz over xi of
+// n(pg[i][m], z) * phi_xi2[m] (interaction_rates.py:1280-1282).
+__global__ void k_pair_rate(FieldDesc f, const double* __restrict__ pg, const double* __restrict__ xi,
+                            const double* __restrict__ phi_xi2, int nxi, int ncr,
+                            const double* __restrict__ zwin, double* __restrict__ rs) {
+  const int w = blockIdx.y, i = blockIdx.x;
+  const double z = zwin[w];
+  double acc = 0.0;
+  for (int m = threadIdx.x; m < nxi - 1; m += blockDim.x) {
+    const double y0 = __dmul_rn(field_density(f, pg[(size_t)i * nxi + m], z), phi_xi2[m]);
+    const double y1 = __dmul_rn(field_density(f, pg[(size_t)i * nxi + m + 1], z), phi_xi2[m + 1]);
+    const double d = __dadd_rn(xi[m + 1], -xi[m]);
+    acc += __ddiv_rn(__dmul_rn(d, __dadd_rn(y1, y0)), 2.0);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) rs[(size_t)w * ncr + i] = v;
+  }
+}
+
+__global__ void k_pair_expand(const double* __restrict__ rs, const double* __restrict__ scale,
+                              const int* __restrict__ bin, int ncr, int64_t n, int W,
+                              double* __restrict__ kp) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * W) return;
+  int64_t w = i / n, r = i % n;
+  int b = bin[r];
+  double rate = (b >= 0) ? rs[w * ncr + b] : 0.0;
+  kp[i] = __dmul_rn(scale[r], rate);
+}
+
+// ---------------------------------------------------------------------------
+// operator pattern: first-window fold and compaction
+// ---------------------------------------------------------------------------
+__global__ void k_coupling_rows(const int64_t* __restrict__ indptr, int64_t n,
+                                const int* __restrict__ indices, int* __restrict__ row,
+                                int* __restrict__ is_diag) {
+  int64_t r = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (r >= n) return;
+  for (int64_t j = indptr[r] + (threadIdx.x & 31); j < indptr[r + 1]; j += 32) {
+    row[j] = (int)r;
+    is_diag[j] = indices[j] == (int)r;
+  }
+}
+
+// keep[i] = 1 where coupling entry i is off-diagonal and its first-window fold
+// value is non-zero (the entries split_operator + eliminate_zeros retain).
+__global__ void k_fold_first(const double* __restrict__ K, int64_t R, int dph,
+                             const double* __restrict__ p0, const int* __restrict__ is_diag,
+                             int* __restrict__ keep) {
+  int64_t r = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x & 31;
+  if (r > R) return;
+  if (r == R) {  // sentinel for the exclusive scan
+    if (lane == 0) keep[R] = 0;
+    return;
+  }
+  const double* row = K + (size_t)r * dph;
+  double s = 0.0;
+  for (int j = lane; j < dph; j += 32) s += row[j] * p0[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) keep[r] = (!is_diag[r] && s != 0.0) ? 1 : 0;
+}
+
+__global__ void k_compact(const int* __restrict__ keep, const int* __restrict__ pos,
+                          const int* __restrict__ cpl_indices, const int* __restrict__ is_diag,
+                          const int* __restrict__ row, int64_t R, int* __restrict__ dest,
+                          int* __restrict__ diag_row, int* __restrict__ m_indices) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R) return;
+  if (keep[i]) {
+    dest[i] = pos[i];
+    m_indices[pos[i]] = cpl_indices[i];
+  } else {
+    dest[i] = -1;
+  }
+  diag_row[i] = is_diag[i] ? row[i] : -1;
+}
+
+__global__ void k_m_indptr(const int64_t* __restrict__ cpl_indptr, const int* __restrict__ pos,
+                           int64_t n, int64_t* __restrict__ m_indptr) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  m_indptr[i] = pos[cpl_indptr[i]];
+}
+
+// ---------------------------------------------------------------------------
+// fold GEMM on the FP64 tensor pipe: out[w][r] = sum_j K[r][j] * PT[w][j]
+// mma.sync m8n8k4 f64 (DMMA).  CTA tile 64 entries x 64 windows, whole photon
+// axis in shared memory; the epilogue scatters into M_off values / diagonal.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kFoldBM = 64, kFoldBN = 64;
+
+__global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K, int64_t R, int dph,
+                                                   int kpad, const double* __restrict__ PT, int W,
+                                                   const int* __restrict__ dest,
+                                                   const int* __restrict__ diag_row,
+                                                   double* __restrict__ mv, int64_t mv_stride,
+                                                   double* __restrict__ md, int64_t n) {
+  extern __shared__ double smem[];
+  const int lda = kpad + 4;  // +4 doubles: 8-row fragments spread over all banks
+  double* As = smem;
+  double* Bs = smem + kFoldBM * lda;
+  const int64_t r0 = (int64_t)blockIdx.x * kFoldBM;
+  const int w0 = blockIdx.y * kFoldBN;
+  for (int i = threadIdx.x; i < kFoldBM * kpad; i += blockDim.x) {
+    int rr = i / kpad, kk = i % kpad;
+    As[rr * lda + kk] = (r0 + rr < R && kk < dph) ? K[(size_t)(r0 + rr) * dph + kk] : 0.0;
+  }
+  for (int i = threadIdx.x; i < kFoldBN * kpad; i += blockDim.x) {
+    int ww = i / kpad, kk = i % kpad;
+    Bs[ww * lda + kk] = (w0 + ww < W && kk < dph) ? PT[(size_t)(w0 + ww) * dph + kk] : 0.0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int wm = wid & 1, wn = wid >> 1;  // warp tile: 32 entries x 16 windows
+  const int g = lane >> 2, t = lane & 3;
+  double acc[4][2][2];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+  for (int k0 = 0; k0 < kpad; k0 += 4) {
+    double af[4], bf[2];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) af[mt] = As[(wm * 32 + mt * 8 + g) * lda + k0 + t];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) bf[nt] = Bs[(wn * 16 + nt * 8 + g) * lda + k0 + t];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) dmma884(acc[mt][nt][0], acc[mt][nt][1], af[mt], bf[nt]);
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int64_t r = r0 + wm * 32 + mt * 8 + g;
+    if (r >= R) continue;
+    const int de = dest[r];
+    const int dr = diag_row[r];
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int w = w0 + wn * 16 + nt * 8 + t * 2 + i;
+        if (w >= W) continue;
+        const double v = acc[mt][nt][i];
+        if (de >= 0) mv[(size_t)w * mv_stride + de] = v;
+        if (dr >= 0) md[(size_t)w * n + dr] = v;
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ETD2 step kernels
+// ---------------------------------------------------------------------------
+struct StepParams {
+  int64_t n;
+  int ld;            // leading dimension of the (n x ld) state buffers
+  int ncols;         // active columns this step
+  int64_t step;
+  uint32_t flags;
+  const double* h;
+  const double* dldz;
+  const double* hc;
+  const double* finj;
+  const int* win;
+  // operator
+  const int64_t* m_indptr;
+  const int* m_indices;
+  const double* m_vals;
+  int64_t m_wstride;
+  const double* m_diag;
+  const int64_t* d_indptr;
+  const int* d_indices;
+  const double* d_vals;
+  const double* d_diag;
+  const double* E;
+  const double* kp;  // W x n or null
+  const int64_t* l_indptr;
+  const int* l_indices;
+  const double* l_vals;
+  const double* l_diag;
+  // injection
+  const int* inj_slot;
+  const double* G;
+  int n_src;
+  const int* src_ptr;
+  const double* coeff;
+  // states
+  const double* src;  // stage 1: x ; stage 2: a
+  const double* x;    // stage 1: x
+  double* a;          // stage 1 writes, stage 2 reads
+  double* f;          // F(x): stage 1 writes, stage 2 reads
+  double* xout;       // stage 2 writes
+  const int* rows;    // short or long row list
+  int nrows;
+};
+
+struct StepScalars {
+  double h, dl, hc, finj;
+  int w;
+  bool kap, adia, pair, photohad, inj, decay;
+};
+
+__device__ __forceinline__ StepScalars load_scalars(const StepParams& p) {
+  StepScalars s;
+  s.h = p.h[p.step];
+  s.dl = p.dldz[p.step];
+  s.hc = p.hc[p.step];
+  s.finj = p.finj[p.step];
+  s.w = p.win[p.step];
+  s.kap = (p.flags & PB_PARTIAL_DIFF) != 0;
+  s.adia = (p.flags & PB_ADIABATIC) != 0;
+  s.pair = (p.flags & PB_PAIRPROD) != 0 && p.kp != nullptr;
+  s.photohad = (p.flags & PB_PHOTOHAD) != 0;
+  s.inj = (p.flags & PB_INJECTION) != 0 && p.G != nullptr;
+  s.decay = (p.flags & PB_DECAY) != 0 && p.l_diag != nullptr;
+  return s;
+}
+
+// kappa(z) at state r: 0 + H cm2sec E (adiabatic) + kappa_pair (propagation.py:1393-1401)
+__device__ __forceinline__ double kappa_at(const StepParams& p, const StepScalars& s, int64_t r) {
+  double k = 0.0;
+  if (s.adia) k = __dmul_rn(s.hc, p.E[r]);
+  if (s.pair) k = __dadd_rn(k, p.kp[(size_t)s.w * p.n + r]);
+  return k;
+}
+
+// diagonal d = dldz (M_diag + kappa D_diag [+ Lambda_diag]) (propagation.py:1408-1422)
+__device__ __forceinline__ double diag_at(const StepParams& p, const StepScalars& s, int64_t r) {
+  double d = __dmul_rn(p.m_diag[(size_t)s.w * p.n + r], s.dl);
+  if (s.kap) d = __dadd_rn(d, __dmul_rn(__dmul_rn(kappa_at(p, s, r), p.d_diag[r]), s.dl));
+  if (s.decay) d = __dadd_rn(d, __dmul_rn(p.l_diag[r], s.dl));
+  return d;
+}
+
+struct Phi {
+  double eD, phi1, phi2;
+};
+
+// phi functions with the Taylor patches of etd2.py:43-46, 329-390
+__device__ __forceinline__ Phi phi_of(double h, double d) {
+  Phi o;
+  const double hd = __dmul_rn(d, h);
+  const double e = exp(hd);
+  o.eD = e;
+  const double ahd = fabs(hd);
+  if (ahd > 1e-6) {
+    o.phi1 = __ddiv_rn(__dadd_rn(e, -1.0), hd);
+  } else {
+    o.phi1 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 6.0), 0.5), hd), 1.0);
+  }
+  if (ahd > 1e-3) {
+    o.phi2 = __ddiv_rn(__dadd_rn(__dadd_rn(e, -1.0), -hd), __dmul_rn(hd, hd));
+  } else {
+    o.phi2 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 24.0), 1.0 / 6.0), hd), 0.5);
+  }
+  return o;
+}
+
+// b(z) at (row r, column k): finj * sum_s coeff_s * g_s[r] (propagation.py:363-370, 2476-2488)
+__device__ __forceinline__ double inj_at(const StepParams& p, const StepScalars& s, int64_t r, int k) {
+  const int slot = p.inj_slot[r];
+  if (slot < 0) return 0.0;
+  const int s0 = p.src_ptr[k], s1 = p.src_ptr[k + 1];
+  if (s0 == s1) return 0.0;
+  const double* c = p.coeff + (size_t)p.step * p.n_src;
+  const double* g = p.G + (size_t)slot * p.n_src;
+  double acc = __dmul_rn(c[s0], g[s0]);
+  for (int q = s0 + 1; q < s1; ++q) acc = __dadd_rn(acc, __dmul_rn(c[q], g[q]));
+  return __dmul_rn(s.finj, acc);
+}
+
+// The rest of apply_F for one (row, column): the FD loss term, the decay term,
+// the dl/dz scale and the injection (propagation.py:1473-1486).
+__device__ __forceinline__ double finish_F(const StepParams& p, const StepScalars& s, int64_t r,
+                                           int k, const double* __restrict__ v, double sM) {
+  double out = sM;
+  if (s.kap) {
+    double sD = 0.0;
+    for (int64_t j = p.d_indptr[r]; j < p.d_indptr[r + 1]; ++j) {
+      const int c = p.d_indices[j];
+      sD += p.d_vals[j] * __dmul_rn(kappa_at(p, s, c), v[(size_t)c * p.ld + k]);
+    }
+    out = __dadd_rn(out, sD);
+  }
+  if (s.decay) {
+    double sL = 0.0;
+    for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
+      sL += p.l_vals[j] * v[(size_t)p.l_indices[j] * p.ld + k];
+    out = __dadd_rn(out, sL);
+  }
+  out = __dmul_rn(out, s.dl);
+  if (s.inj) out = __dadd_rn(out, inj_at(p, s, r, k));
+  return out;
+}
+
+template <int STAGE>
+__device__ __forceinline__ void row_epilogue(const StepParams& p, const StepScalars& s, int64_t r,
+                                             int k, double sM) {
+  const Phi ph = phi_of(s.h, diag_at(p, s, r));
+  const size_t idx = (size_t)r * p.ld + k;
+  const double F = finish_F(p, s, r, k, p.src, sM);
+  if (STAGE == 1) {
+    // a = eD x + (phi1 F(x)) h  (etd2.py:427-430)
+    const double a = __dadd_rn(__dmul_rn(ph.eD, p.x[idx]), __dmul_rn(__dmul_rn(ph.phi1, F), s.h));
+    p.a[idx] = a;
+    p.f[idx] = F;
+  } else {
+    // x = a + ((F(a) - F(x)) h) phi2  (etd2.py:435-438)
+    const double dF = __dmul_rn(__dadd_rn(F, -p.f[idx]), s.h);
+    p.xout[idx] = __dadd_rn(p.a[idx], __dmul_rn(dF, ph.phi2));
+  }
+}
+
+// Single column: a warp per short row (lanes stride the row), a CTA per long row.
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
+  const StepScalars s = load_scalars(p);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double* __restrict__ v = p.src;
+  const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
+  if (p.nrows < 0) {  // long rows: CTA per row
+    const int64_t r = p.rows[blockIdx.x];
+    double acc = 0.0;
+    if (s.photohad)
+      for (int64_t j = p.m_indptr[r] + threadIdx.x; j < p.m_indptr[r + 1]; j += blockDim.x)
+        acc += mv[j] * v[p.m_indices[j]];
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[wid] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+      row_epilogue<STAGE>(p, s, r, 0, t);
+    }
+    return;
+  }
+  const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+  if (ri >= p.nrows) return;
+  const int64_t r = p.rows[ri];
+  double acc = 0.0;
+  if (s.photohad)
+    for (int64_t j = p.m_indptr[r] + lane; j < p.m_indptr[r + 1]; j += 32)
+      acc += mv[j] * v[p.m_indices[j]];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) row_epilogue<STAGE>(p, s, r, 0, acc);
+}
+
+// Many columns: lane = column inside a 32-column tile (blockIdx.y); the row's
+// (value, column) pairs are loaded 32 at a time and broadcast by shuffles, so
+// every gathered state row is one coalesced 256-byte load.
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
+  const StepScalars s = load_scalars(p);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int k = blockIdx.y * kColTile + lane;
+  const bool active = k < p.ncols;
+  const double* __restrict__ v = p.src;
+  const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
+  const int kk = active ? k : 0;
+  if (p.nrows < 0) {  // long rows: the CTA's warps split the row
+    const int64_t r = p.rows[blockIdx.x];
+    double acc = 0.0;
+    if (s.photohad) {
+      const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
+      const int64_t len = j1 - j0;
+      const int nw = blockDim.x >> 5;
+      const int64_t chunk = (len + nw - 1) / nw;
+      const int64_t a0 = j0 + wid * chunk, a1 = min(j1, a0 + chunk);
+      for (int64_t base = a0; base < a1; base += 32) {
+        const int64_t j = base + lane;
+        const double mvl = (j < a1) ? mv[j] : 0.0;
+        const int cl = (j < a1) ? p.m_indices[j] : 0;
+        const int cnt = (int)min((int64_t)32, a1 - base);
+        for (int q = 0; q < cnt; ++q) {
+          const double mq = __shfl_sync(0xffffffffu, mvl, q);
+          const int cq = __shfl_sync(0xffffffffu, cl, q);
+          acc += mq * v[(size_t)cq * p.ld + kk];
+        }
+      }
+    }
+    __shared__ double red[8][32];
+    red[wid][lane] = acc;
+    __syncthreads();
+    if (wid == 0) {
+      double t = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i][lane];
+      if (active) row_epilogue<STAGE>(p, s, r, k, t);
+    }
+    return;
+  }
+  const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+  if (ri >= p.nrows) return;
+  const int64_t r = p.rows[ri];
+  double acc = 0.0;
+  if (s.photohad) {
+    const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
+    for (int64_t base = j0; base < j1; base += 32) {
+      const int64_t j = base + lane;
+      const double mvl = (j < j1) ? mv[j] : 0.0;
+      const int cl = (j < j1) ? p.m_indices[j] : 0;
+      const int cnt = (int)min((int64_t)32, j1 - base);
+      for (int q = 0; q < cnt; ++q) {
+        const double mq = __shfl_sync(0xffffffffu, mvl, q);
+        const int cq = __shfl_sync(0xffffffffu, cl, q);
+        acc += mq * v[(size_t)cq * p.ld + kk];
+      }
+    }
+  }
+  if (active) row_epilogue<STAGE>(p, s, r, k, acc);
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+template <class T>
+int upload(pb_context* c, DBuf& b, const T* src, size_t count) {
+  cudaError_t e = b.ensure(count * sizeof(T));
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "cudaMalloc(%zu) failed: %s", count * sizeof(T), cudaGetErrorString(e));
+  if (count) {
+    e = cudaMemcpyAsync(b.p, src, count * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "cudaMemcpyAsync H2D failed: %s", cudaGetErrorString(e));
+  }
+  return PB_OK;
+}
+
+int set_device(pb_context* c) {
+  PB_CUDA(c, cudaSetDevice(c->device));
+  return PB_OK;
+}
+
+FieldDesc field_desc(const pb_context* c, double scale) {
+  FieldDesc f;
+  f.n = c->n_comp;
+  for (int i = 0; i < 8; ++i) {
+    f.kind[i] = i < c->n_comp ? c->comp_kind[i] : 0;
+    for (int q = 0; q < 3; ++q) f.p[i][q] = i < c->n_comp ? c->comp_par[i][q] : 0.0;
+  }
+  f.scale = scale;
+  return f;
+}
+
+unsigned blocks_for(int64_t work, int per_block) {
+  return (unsigned)((work + per_block - 1) / per_block);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int pb_abi_version(void) { return kAbiVersion; }
+
+const char* pb_global_error(void) { return g_error.c_str(); }
+
+const char* pb_last_error(const pb_context* ctx) { return ctx ? ctx->err.c_str() : g_error.c_str(); }
+
+int pb_create(int device, pb_context** out) {
+  if (!out) return fail(nullptr, PB_ERR_ARG, "pb_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, PB_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  if (device < 0 || device >= ndev) return fail(nullptr, PB_ERR_ARG, "device %d out of range [0,%d)", device, ndev);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(nullptr, PB_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  if (prop.major < 10)
+    return fail(nullptr, PB_ERR_CUDA, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
+  pb_context* c = new pb_context();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess) {
+    delete c;
+    return fail(nullptr, PB_ERR_CUDA, "stream/event creation failed");
+  }
+  e = cudaFuncSetAttribute(k_fold_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (kFoldBM + kFoldBN) * (kMaxPhoton + 4) * (int)sizeof(double));
+  if (e != cudaSuccess) {
+    pb_destroy(c);
+    return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_fold_gemm): %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return PB_OK;
+}
+
+void pb_destroy(pb_context* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  DBuf* bufs[] = {&c->cpl_indptr, &c->cpl_indices, &c->cpl_row, &c->cpl_is_diag, &c->short_rows,
+                  &c->long_rows, &c->kernel, &c->eph, &c->d_indptr, &c->d_indices, &c->d_vals,
+                  &c->d_diag, &c->adia_E, &c->pair_scale, &c->pair_bin, &c->xi, &c->phi_xi2,
+                  &c->pair_pg, &c->l_diag, &c->l_indptr, &c->l_indices, &c->l_vals, &c->inj_slot,
+                  &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos,
+                  &c->dest, &c->m_indptr, &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h,
+                  &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff, &c->X, &c->A, &c->F,
+                  &c->scan_tmp};
+  for (DBuf* b : bufs) b->release();
+  cudaEventDestroy(c->ev0);
+  cudaEventDestroy(c->ev1);
+  cudaEventDestroy(c->ev2);
+  cudaEventDestroy(c->ev3);
+  cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int pb_set_coupling(pb_context* c, int64_t n, int64_t R, const int64_t* indptr, const int32_t* indices) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (n <= 0 || R < 0 || !indptr || (R > 0 && !indices)) return fail(c, PB_ERR_ARG, "pb_set_coupling: bad arguments");
+  if (n >= (int64_t)1 << 31 || R >= (int64_t)1 << 31) return fail(c, PB_ERR_ARG, "pb_set_coupling: sizes exceed int32 indexing");
+  if (indptr[0] != 0 || indptr[n] != R) return fail(c, PB_ERR_ARG, "pb_set_coupling: indptr must run from 0 to n_entries");
+  for (int64_t i = 0; i < n; ++i)
+    if (indptr[i + 1] < indptr[i]) return fail(c, PB_ERR_ARG, "pb_set_coupling: indptr not monotone at row %lld", (long long)i);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t j = indptr[i]; j < indptr[i + 1]; ++j) {
+      if (indices[j] < 0 || indices[j] >= n) return fail(c, PB_ERR_ARG, "pb_set_coupling: column %d out of range", indices[j]);
+      if (j > indptr[i] && indices[j] <= indices[j - 1]) return fail(c, PB_ERR_ARG, "pb_set_coupling: columns not strictly increasing in row %lld", (long long)i);
+    }
+  int rc = set_device(c);
+  if (rc) return rc;
+  c->n = n;
+  c->R = R;
+  if ((rc = upload(c, c->cpl_indptr, indptr, (size_t)n + 1))) return rc;
+  if ((rc = upload(c, c->cpl_indices, indices, (size_t)R))) return rc;
+  PB_CUDA(c, c->cpl_row.ensure((size_t)std::max<int64_t>(R, 1) * sizeof(int)));
+  PB_CUDA(c, c->cpl_is_diag.ensure((size_t)std::max<int64_t>(R, 1) * sizeof(int)));
+  if (R > 0)
+    k_coupling_rows<<<blocks_for(n, 8), 256, 0, c->stream>>>(c->cpl_indptr.as<int64_t>(), n,
+                                                             c->cpl_indices.as<int>(), c->cpl_row.as<int>(),
+                                                             c->cpl_is_diag.as<int>());
+  PB_CUDA(c, cudaGetLastError());
+  c->h_short_rows.clear();
+  c->h_long_rows.clear();
+  for (int64_t i = 0; i < n; ++i) (indptr[i + 1] - indptr[i] > kLongRow ? c->h_long_rows : c->h_short_rows).push_back((int)i);
+  if ((rc = upload(c, c->short_rows, c->h_short_rows.data(), c->h_short_rows.size()))) return rc;
+  if ((rc = upload(c, c->long_rows, c->h_long_rows.data(), c->h_long_rows.size()))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->have_coupling = true;
+  c->have_kernel = false;
+  c->have_fd = c->have_losses = c->have_decay = false;
+  c->n_src = 0;
+  c->have_solution = false;
+  return PB_OK;
+}
+
+int pb_set_fold_kernel(pb_context* c, int64_t R, int32_t dph, const double* K) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_fold_kernel: set the coupling pattern first");
+  if (R != c->R) return fail(c, PB_ERR_ARG, "pb_set_fold_kernel: %lld rows, coupling has %lld entries", (long long)R, (long long)c->R);
+  if (dph <= 0 || dph > kMaxPhoton) return fail(c, PB_ERR_ARG, "pb_set_fold_kernel: photon bins must be in [1, %d]", kMaxPhoton);
+  if (R > 0 && !K) return fail(c, PB_ERR_ARG, "pb_set_fold_kernel: kernel is NULL");
+  if (c->have_photon_grid && dph != c->dph) return fail(c, PB_ERR_ARG, "pb_set_fold_kernel: photon axis %d != photon grid %d", dph, c->dph);
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->kernel, K, (size_t)R * dph))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->dph = dph;
+  c->have_kernel = true;
+  return PB_OK;
+}
+
+int pb_set_photon_grid(pb_context* c, int32_t dph, const double* e) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (dph <= 0 || dph > kMaxPhoton || !e) return fail(c, PB_ERR_ARG, "pb_set_photon_grid: bad arguments");
+  if (c->have_kernel && dph != c->dph) return fail(c, PB_ERR_ARG, "pb_set_photon_grid: %d bins, fold kernel has %d", dph, c->dph);
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->eph, e, (size_t)dph))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->dph = dph;
+  c->have_photon_grid = true;
+  return PB_OK;
+}
+
+int pb_set_photon_field(pb_context* c, int32_t n_comp, const int32_t* kinds, const double* params) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (n_comp < 1 || n_comp > 8 || !kinds || !params) return fail(c, PB_ERR_ARG, "pb_set_photon_field: 1..8 components required");
+  for (int i = 0; i < n_comp; ++i) {
+    if (kinds[i] < 0 || kinds[i] > 2) return fail(c, PB_ERR_ARG, "pb_set_photon_field: unknown kind %d", kinds[i]);
+    if (kinds[i] != 1 && !(params[3 * i + 1] > 0.0)) return fail(c, PB_ERR_ARG, "pb_set_photon_field: temperature must be positive");
+    c->comp_kind[i] = kinds[i];
+    for (int q = 0; q < 3; ++q) c->comp_par[i][q] = params[3 * i + q];
+  }
+  c->n_comp = n_comp;
+  c->have_field = true;
+  return PB_OK;
+}
+
+int pb_set_fd_operator(pb_context* c, int64_t nnz, const int64_t* indptr, const int32_t* indices,
+                       const double* values, const double* diag) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_fd_operator: set the coupling pattern first");
+  if (nnz < 0 || !indptr || !diag || (nnz > 0 && (!indices || !values))) return fail(c, PB_ERR_ARG, "pb_set_fd_operator: bad arguments");
+  if (indptr[0] != 0 || indptr[c->n] != nnz) return fail(c, PB_ERR_ARG, "pb_set_fd_operator: indptr must run from 0 to nnz");
+  for (int64_t j = 0; j < nnz; ++j)
+    if (indices[j] < 0 || indices[j] >= c->n) return fail(c, PB_ERR_ARG, "pb_set_fd_operator: column out of range");
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->d_indptr, indptr, (size_t)c->n + 1))) return rc;
+  if ((rc = upload(c, c->d_indices, indices, (size_t)nnz))) return rc;
+  if ((rc = upload(c, c->d_vals, values, (size_t)nnz))) return rc;
+  if ((rc = upload(c, c->d_diag, diag, (size_t)c->n))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->nnzD = nnz;
+  c->have_fd = true;
+  return PB_OK;
+}
+
+int pb_set_losses(pb_context* c, const double* adia_energy, const double* pair_scale, const int32_t* pair_bin,
+                  int32_t n_cr_bins, int32_t n_xi, const double* xi, const double* phi_xi2, const double* pg) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_losses: set the coupling pattern first");
+  if (!adia_energy || !pair_scale || !pair_bin || n_cr_bins <= 0 || n_xi < 2 || !xi || !phi_xi2 || !pg)
+    return fail(c, PB_ERR_ARG, "pb_set_losses: bad arguments");
+  for (int64_t r = 0; r < c->n; ++r)
+    if (pair_bin[r] < -1 || pair_bin[r] >= n_cr_bins) return fail(c, PB_ERR_ARG, "pb_set_losses: pair_bin out of range");
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->adia_E, adia_energy, (size_t)c->n))) return rc;
+  if ((rc = upload(c, c->pair_scale, pair_scale, (size_t)c->n))) return rc;
+  if ((rc = upload(c, c->pair_bin, pair_bin, (size_t)c->n))) return rc;
+  if ((rc = upload(c, c->xi, xi, (size_t)n_xi))) return rc;
+  if ((rc = upload(c, c->phi_xi2, phi_xi2, (size_t)n_xi))) return rc;
+  if ((rc = upload(c, c->pair_pg, pg, (size_t)n_cr_bins * n_xi))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->n_cr_bins = n_cr_bins;
+  c->n_xi = n_xi;
+  c->have_losses = true;
+  return PB_OK;
+}
+
+int pb_set_decay(pb_context* c, const double* diag, int64_t nnz, const int64_t* indptr, const int32_t* indices,
+                 const double* values) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_decay: set the coupling pattern first");
+  if (nnz < 0 || (nnz > 0 && (!indptr || !indices || !values))) return fail(c, PB_ERR_ARG, "pb_set_decay: bad arguments");
+  int rc = set_device(c);
+  if (rc) return rc;
+  std::vector<double> zero;
+  if (!diag) zero.assign((size_t)c->n, 0.0);
+  if ((rc = upload(c, c->l_diag, diag ? diag : zero.data(), (size_t)c->n))) return rc;
+  std::vector<int64_t> zp;
+  if (nnz == 0 || !indptr) {
+    zp.assign((size_t)c->n + 1, 0);
+    indptr = zp.data();
+  } else {
+    if (indptr[0] != 0 || indptr[c->n] != nnz) return fail(c, PB_ERR_ARG, "pb_set_decay: indptr must run from 0 to nnz");
+    for (int64_t j = 0; j < nnz; ++j)
+      if (indices[j] < 0 || indices[j] >= c->n) return fail(c, PB_ERR_ARG, "pb_set_decay: column out of range");
+  }
+  if ((rc = upload(c, c->l_indptr, indptr, (size_t)c->n + 1))) return rc;
+  if ((rc = upload(c, c->l_indices, indices, (size_t)nnz))) return rc;
+  if ((rc = upload(c, c->l_vals, values, (size_t)nnz))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->nnzL = nnz;
+  c->have_decay = true;
+  return PB_OK;
+}
+
+int pb_set_injection(pb_context* c, int32_t n_src, int32_t n_rows, const int32_t* rows, const double* grids,
+                     int32_t n_cols, const int32_t* src_col) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_injection: set the coupling pattern first");
+  if (n_src < 0 || n_rows < 0 || n_cols < 1 || (n_src > 0 && (!src_col || (n_rows > 0 && (!rows || !grids)))))
+    return fail(c, PB_ERR_ARG, "pb_set_injection: bad arguments");
+  std::vector<int32_t> slot((size_t)c->n, -1);
+  for (int i = 0; i < n_rows; ++i) {
+    if (rows[i] < 0 || rows[i] >= c->n) return fail(c, PB_ERR_ARG, "pb_set_injection: row out of range");
+    if (slot[rows[i]] >= 0) return fail(c, PB_ERR_ARG, "pb_set_injection: duplicated row %d", rows[i]);
+    slot[rows[i]] = i;
+  }
+  std::vector<int32_t> ptr((size_t)n_cols + 1, 0);
+  for (int s = 0; s < n_src; ++s) {
+    if (src_col[s] < 0 || src_col[s] >= n_cols) return fail(c, PB_ERR_ARG, "pb_set_injection: src_col out of range");
+    if (s > 0 && src_col[s] < src_col[s - 1]) return fail(c, PB_ERR_ARG, "pb_set_injection: src_col must be non-decreasing");
+    ptr[src_col[s] + 1]++;
+  }
+  for (int k = 0; k < n_cols; ++k) ptr[k + 1] += ptr[k];
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->inj_slot, slot.data(), slot.size()))) return rc;
+  if ((rc = upload(c, c->inj_G, grids, (size_t)n_rows * n_src))) return rc;
+  if ((rc = upload(c, c->src_ptr, ptr.data(), ptr.size()))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->n_src = n_src;
+  c->n_inj_rows = n_rows;
+  c->n_src_cols = n_cols;
+  return PB_OK;
+}
+
+int pb_solve(pb_context* c, const pb_solve_args* a) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!a) return fail(c, PB_ERR_ARG, "pb_solve: args is NULL");
+  if (!c->have_coupling || !c->have_photon_grid || !c->have_field || !c->have_fd || !c->have_losses)
+    return fail(c, PB_ERR_STATE, "pb_solve: coupling, photon grid, photon field, FD operator and losses must be set");
+  const uint32_t flags = a->flags;
+  if ((flags & PB_PHOTOHAD) && !c->have_kernel) return fail(c, PB_ERR_STATE, "pb_solve: fold kernel not set");
+  if ((flags & PB_DECAY) && !c->have_decay) return fail(c, PB_ERR_STATE, "pb_solve: decay operator not set");
+  const int64_t S = a->n_steps;
+  const int W = a->n_windows;
+  const int K = a->n_cols;
+  if (S < 0 || W < 1 || K < 1 || !a->state) return fail(c, PB_ERR_ARG, "pb_solve: bad sizes");
+  if (S > 0 && (!a->z_window || !a->window || !a->h || !a->dldz || !a->hc || !a->finj || !a->n_active))
+    return fail(c, PB_ERR_ARG, "pb_solve: schedule arrays missing");
+  const bool inj = (flags & PB_INJECTION) && c->n_src > 0;
+  if (inj && c->n_src_cols != K) return fail(c, PB_ERR_ARG, "pb_solve: injection was set for %d columns, solve has %d", c->n_src_cols, K);
+  if (inj && S > 0 && !a->coeff) return fail(c, PB_ERR_ARG, "pb_solve: coeff missing");
+  for (int64_t k = 0; k < S; ++k) {
+    if (a->window[k] < 0 || a->window[k] >= W) return fail(c, PB_ERR_ARG, "pb_solve: window index out of range at step %lld", (long long)k);
+    if (a->n_active[k] < 0 || a->n_active[k] > K) return fail(c, PB_ERR_ARG, "pb_solve: n_active out of range");
+  }
+  if ((int64_t)W * c->n >= ((int64_t)1 << 40)) return fail(c, PB_ERR_ARG, "pb_solve: too many windows");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int64_t n = c->n;
+  const int ld = K == 1 ? 1 : ((K + kColTile - 1) / kColTile) * kColTile;
+  cudaStream_t st = c->stream;
+
+  // ---- per-solve uploads -------------------------------------------------
+  if ((rc = upload(c, c->zwin, a->z_window, (size_t)W))) return rc;
+  if (S > 0) {
+    if ((rc = upload(c, c->s_h, a->h, (size_t)S))) return rc;
+    if ((rc = upload(c, c->s_dldz, a->dldz, (size_t)S))) return rc;
+    if ((rc = upload(c, c->s_hc, a->hc, (size_t)S))) return rc;
+    if ((rc = upload(c, c->s_finj, a->finj, (size_t)S))) return rc;
+    if ((rc = upload(c, c->s_win, a->window, (size_t)S))) return rc;
+    if (inj && (rc = upload(c, c->s_coeff, a->coeff, (size_t)S * c->n_src))) return rc;
+  }
+  PB_CUDA(c, c->PT.ensure((size_t)W * c->dph * sizeof(double)));
+  PB_CUDA(c, c->rs.ensure((size_t)W * c->n_cr_bins * sizeof(double)));
+  PB_CUDA(c, c->kp.ensure((size_t)W * n * sizeof(double)));
+  PB_CUDA(c, c->m_indptr.ensure(((size_t)n + 1) * sizeof(int64_t)));
+  PB_CUDA(c, c->m_diag.ensure((size_t)W * n * sizeof(double)));
+  const int64_t R = c->R;
+  const int64_t mstride = std::max<int64_t>(R, 1);
+  PB_CUDA(c, c->m_vals.ensure((size_t)W * mstride * sizeof(double)));
+  PB_CUDA(c, c->m_indices.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->keep.ensure(((size_t)R + 1) * sizeof(int)));
+  PB_CUDA(c, c->pos.ensure(((size_t)R + 1) * sizeof(int)));
+  PB_CUDA(c, c->dest.ensure((size_t)mstride * 2 * sizeof(int)));
+  const size_t sbytes = (size_t)n * ld * sizeof(double);
+  PB_CUDA(c, c->X.ensure(sbytes));
+  PB_CUDA(c, c->A.ensure(sbytes));
+  PB_CUDA(c, c->F.ensure(sbytes));
+  size_t scan_need = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
+  PB_CUDA(c, c->scan_tmp.ensure(scan_need));
+
+  const FieldDesc fd = field_desc(c, a->photon_scale);
+  int64_t launches = 0;
+  PB_CUDA(c, cudaEventRecord(c->ev0, st));
+
+  // ---- photon matrix and pair-loss vectors for every window ---------------
+  k_photon_matrix<<<blocks_for((int64_t)W * c->dph, 256), 256, 0, st>>>(fd, c->eph.as<double>(), c->dph,
+                                                                          c->zwin.as<double>(), W, c->PT.as<double>());
+  ++launches;
+  const bool pair = (flags & PB_PAIRPROD) && (flags & PB_PARTIAL_DIFF);
+  if (pair) {
+    k_pair_rate<<<dim3(c->n_cr_bins, W), 128, 0, st>>>(fd, c->pair_pg.as<double>(), c->xi.as<double>(),
+                                                       c->phi_xi2.as<double>(), c->n_xi, c->n_cr_bins,
+                                                       c->zwin.as<double>(), c->rs.as<double>());
+    k_pair_expand<<<blocks_for((int64_t)W * n, 256), 256, 0, st>>>(c->rs.as<double>(), c->pair_scale.as<double>(),
+                                                                   c->pair_bin.as<int>(), c->n_cr_bins, n, W,
+                                                                   c->kp.as<double>());
+    launches += 2;
+  }
+  // ---- operator pattern and fold -----------------------------------------
+  int* dest = c->dest.as<int>();
+  int* diag_row = dest + mstride;
+  PB_CUDA(c, cudaMemsetAsync(c->m_diag.p, 0, (size_t)W * n * sizeof(double), st));
+  if ((flags & PB_PHOTOHAD) && R > 0) {
+    k_fold_first<<<blocks_for(R + 1, 8), 256, 0, st>>>(c->kernel.as<double>(), R, c->dph, c->PT.as<double>(),
+                                                       c->cpl_is_diag.as<int>(), c->keep.as<int>());
+    size_t tb = c->scan_tmp.bytes;
+    PB_CUDA(c, cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, tb, c->keep.as<int>(), c->pos.as<int>(), (int)(R + 1), st));
+    k_compact<<<blocks_for(R, 256), 256, 0, st>>>(c->keep.as<int>(), c->pos.as<int>(), c->cpl_indices.as<int>(),
+                                                  c->cpl_is_diag.as<int>(), c->cpl_row.as<int>(), R, dest, diag_row,
+                                                  c->m_indices.as<int>());
+    k_m_indptr<<<blocks_for(n + 1, 256), 256, 0, st>>>(c->cpl_indptr.as<int64_t>(), c->pos.as<int>(), n,
+                                                       c->m_indptr.as<int64_t>());
+    const int kpad = (c->dph + 3) / 4 * 4;
+    const size_t smem = (size_t)(kFoldBM + kFoldBN) * (kpad + 4) * sizeof(double);
+    k_fold_gemm<<<dim3(blocks_for(R, kFoldBM), blocks_for(W, kFoldBN)), 256, smem, st>>>(
+        c->kernel.as<double>(), R, c->dph, kpad, c->PT.as<double>(), W, dest, diag_row, c->m_vals.as<double>(),
+        mstride, c->m_diag.as<double>(), n);
+    launches += 5;
+  } else {
+    PB_CUDA(c, cudaMemsetAsync(c->m_indptr.p, 0, ((size_t)n + 1) * sizeof(int64_t), st));
+  }
+  PB_CUDA(c, cudaGetLastError());
+
+  // ---- ETD2 steps ---------------------------------------------------------
+  double* X = c->X.as<double>();
+  if (a->init_state) {
+    if (a->state_on_device) {
+      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
+                                   cudaMemcpyDeviceToDevice, st));
+    } else {
+      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, st));
+    }
+  } else {
+    PB_CUDA(c, cudaMemsetAsync(X, 0, sbytes, st));
+  }
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.ld = ld;
+  p.flags = flags;
+  if (!pair) p.flags &= ~PB_PAIRPROD;
+  if (!inj) p.flags &= ~PB_INJECTION;
+  p.h = c->s_h.as<double>();
+  p.dldz = c->s_dldz.as<double>();
+  p.hc = c->s_hc.as<double>();
+  p.finj = c->s_finj.as<double>();
+  p.win = c->s_win.as<int>();
+  p.m_indptr = c->m_indptr.as<int64_t>();
+  p.m_indices = c->m_indices.as<int>();
+  p.m_vals = c->m_vals.as<double>();
+  p.m_wstride = mstride;
+  p.m_diag = c->m_diag.as<double>();
+  p.d_indptr = c->d_indptr.as<int64_t>();
+  p.d_indices = c->d_indices.as<int>();
+  p.d_vals = c->d_vals.as<double>();
+  p.d_diag = c->d_diag.as<double>();
+  p.E = c->adia_E.as<double>();
+  p.kp = pair ? c->kp.as<double>() : nullptr;
+  if ((flags & PB_DECAY) && c->have_decay) {
+    p.l_indptr = c->l_indptr.as<int64_t>();
+    p.l_indices = c->l_indices.as<int>();
+    p.l_vals = c->l_vals.as<double>();
+    p.l_diag = c->l_diag.as<double>();
+  }
+  if (inj) {
+    p.inj_slot = c->inj_slot.as<int>();
+    p.G = c->inj_G.as<double>();
+    p.n_src = c->n_src;
+    p.src_ptr = c->src_ptr.as<int>();
+    p.coeff = c->s_coeff.as<double>();
+  }
+  p.a = c->A.as<double>();
+  p.f = c->F.as<double>();
+  const int nshort = (int)c->h_short_rows.size(), nlong = (int)c->h_long_rows.size();
+  PB_CUDA(c, cudaEventRecord(c->ev2, st));
+  for (int64_t k = 0; k < S; ++k) {
+    p.step = k;
+    p.ncols = a->n_active[k];
+    if (p.ncols == 0) {
+      // every column is still exactly zero: nothing to advance
+      continue;
+    }
+    for (int stage = 1; stage <= 2; ++stage) {
+      p.src = stage == 1 ? X : c->A.as<double>();
+      p.x = X;
+      p.xout = X;
+      const unsigned tiles = K == 1 ? 1u : blocks_for(p.ncols, kColTile);
+      if (nshort > 0) {
+        p.rows = c->short_rows.as<int>();
+        p.nrows = nshort;
+        dim3 grid(blocks_for(nshort, 8), tiles);
+        if (K == 1) {
+          if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
+        } else {
+          if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
+        }
+        ++launches;
+      }
+      if (nlong > 0) {
+        p.rows = c->long_rows.as<int>();
+        p.nrows = -1;
+        dim3 grid(nlong, tiles);
+        if (K == 1) {
+          if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
+        } else {
+          if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
+        }
+        ++launches;
+      }
+    }
+  }
+  PB_CUDA(c, cudaGetLastError());
+  PB_CUDA(c, cudaEventRecord(c->ev3, st));
+  if (a->state_on_device) {
+    PB_CUDA(c, cudaMemcpy2DAsync(a->state, K * sizeof(double), X, ld * sizeof(double), K * sizeof(double), n,
+                                 cudaMemcpyDeviceToDevice, st));
+  } else {
+    PB_CUDA(c, cudaMemcpy2DAsync(a->state, K * sizeof(double), X, ld * sizeof(double), K * sizeof(double), n,
+                                 cudaMemcpyDeviceToHost, st));
+  }
+  PB_CUDA(c, cudaEventRecord(c->ev1, st));
+  PB_CUDA(c, cudaStreamSynchronize(st));
+  cudaEventElapsedTime(&c->last_solve_ms, c->ev0, c->ev1);
+  cudaEventElapsedTime(&c->last_device_ms, c->ev0, c->ev3);
+  cudaEventElapsedTime(&c->last_steps_ms, c->ev2, c->ev3);
+  c->last_launches = launches;
+  c->last_W = W;
+  c->have_solution = true;
+  return PB_OK;
+}
+
+int pb_get_operator_pattern(pb_context* c, int64_t* nnz, int64_t* indptr, int32_t* indices) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_solution) return fail(c, PB_ERR_STATE, "pb_get_operator_pattern: no solve yet");
+  if (!nnz) return fail(c, PB_ERR_ARG, "pb_get_operator_pattern: nnz is NULL");
+  int rc = set_device(c);
+  if (rc) return rc;
+  int64_t tot = 0;
+  PB_CUDA(c, cudaMemcpy(&tot, c->m_indptr.as<int64_t>() + c->n, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  *nnz = tot;
+  if (indptr) PB_CUDA(c, cudaMemcpy(indptr, c->m_indptr.p, ((size_t)c->n + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+  if (indices && tot) PB_CUDA(c, cudaMemcpy(indices, c->m_indices.p, (size_t)tot * sizeof(int), cudaMemcpyDeviceToHost));
+  return PB_OK;
+}
+
+int pb_get_window(pb_context* c, int32_t w, double* offdiag, double* diag, double* kappa_pair) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_solution) return fail(c, PB_ERR_STATE, "pb_get_window: no solve yet");
+  if (w < 0 || w >= c->last_W) return fail(c, PB_ERR_ARG, "pb_get_window: window out of range");
+  int rc = set_device(c);
+  if (rc) return rc;
+  int64_t tot = 0;
+  PB_CUDA(c, cudaMemcpy(&tot, c->m_indptr.as<int64_t>() + c->n, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  const int64_t mstride = std::max<int64_t>(c->R, 1);
+  if (offdiag && tot)
+    PB_CUDA(c, cudaMemcpy(offdiag, c->m_vals.as<double>() + (size_t)w * mstride, (size_t)tot * sizeof(double),
+                          cudaMemcpyDeviceToHost));
+  if (diag) PB_CUDA(c, cudaMemcpy(diag, c->m_diag.as<double>() + (size_t)w * c->n, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (kappa_pair) PB_CUDA(c, cudaMemcpy(kappa_pair, c->kp.as<double>() + (size_t)w * c->n, (size_t)c->n * sizeof(double), cudaMemcpyDeviceToHost));
+  return PB_OK;
+}
+
+int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, const int64_t* indptr,
+                       const int32_t* indices, const double* values, int64_t n_steps, const double* z_grid,
+                       double* state) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (n <= 0 || n >= ((int64_t)1 << 31) || !d || nnz < 0 || n_steps < 0 || !z_grid || !state)
+    return fail(c, PB_ERR_ARG, "pb_integrate_const: bad arguments");
+  if (nnz > 0 && (!indptr || !indices || !values)) return fail(c, PB_ERR_ARG, "pb_integrate_const: CSR arrays missing");
+  std::vector<int64_t> zp;
+  if (nnz == 0) {
+    zp.assign((size_t)n + 1, 0);
+    indptr = zp.data();
+  } else {
+    if (indptr[0] != 0 || indptr[n] != nnz) return fail(c, PB_ERR_ARG, "pb_integrate_const: indptr must run from 0 to nnz");
+    for (int64_t j = 0; j < nnz; ++j)
+      if (indices[j] < 0 || indices[j] >= n) return fail(c, PB_ERR_ARG, "pb_integrate_const: column out of range");
+  }
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  // A constant operator is one window with M_off = L_off, M_diag = d, dl/dz = 1
+  // and no losses or injection.
+  DBuf ip, ix, iv, dg, hs, ones, zero_i, X, A, F, rows;
+  auto cleanup = [&]() { for (DBuf* b : {&ip, &ix, &iv, &dg, &hs, &ones, &zero_i, &X, &A, &F, &rows}) b->release(); };
+  std::vector<double> hv((size_t)std::max<int64_t>(n_steps, 1)), one((size_t)std::max<int64_t>(n_steps, 1), 1.0);
+  for (int64_t k = 0; k < n_steps; ++k) hv[k] = z_grid[k + 1] - z_grid[k];
+  std::vector<int> zi((size_t)std::max<int64_t>(n_steps, 1), 0), rl((size_t)n);
+  for (int64_t i = 0; i < n; ++i) rl[i] = (int)i;
+  if ((rc = upload(c, ip, indptr, (size_t)n + 1)) || (rc = upload(c, ix, indices, (size_t)nnz)) ||
+      (rc = upload(c, iv, values, (size_t)nnz)) || (rc = upload(c, dg, d, (size_t)n)) ||
+      (rc = upload(c, hs, hv.data(), hv.size())) || (rc = upload(c, ones, one.data(), one.size())) ||
+      (rc = upload(c, zero_i, zi.data(), zi.size())) || (rc = upload(c, X, state, (size_t)n)) ||
+      (rc = upload(c, rows, rl.data(), rl.size()))) {
+    cleanup();
+    return rc;
+  }
+  if (A.ensure((size_t)n * sizeof(double)) != cudaSuccess || F.ensure((size_t)n * sizeof(double)) != cudaSuccess) {
+    cleanup();
+    return fail(c, PB_ERR_CUDA, "pb_integrate_const: allocation failed");
+  }
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.ld = 1;
+  p.ncols = 1;
+  p.flags = PB_PHOTOHAD;
+  p.h = hs.as<double>();
+  p.dldz = ones.as<double>();
+  p.hc = ones.as<double>();
+  p.finj = ones.as<double>();
+  p.win = zero_i.as<int>();
+  p.m_indptr = ip.as<int64_t>();
+  p.m_indices = ix.as<int>();
+  p.m_vals = iv.as<double>();
+  p.m_wstride = 0;
+  p.m_diag = dg.as<double>();
+  p.a = A.as<double>();
+  p.f = F.as<double>();
+  p.rows = rows.as<int>();
+  p.nrows = (int)n;
+  for (int64_t k = 0; k < n_steps; ++k) {
+    p.step = k;
+    p.x = X.as<double>();
+    p.xout = X.as<double>();
+    p.src = X.as<double>();
+    k_step_plain<1><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    p.src = A.as<double>();
+    k_step_plain<2><<<blocks_for(n, 8), 256, 0, st>>>(p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(state, X.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cleanup();
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_integrate_const: %s", cudaGetErrorString(e));
+  return PB_OK;
+}
+
+int pb_last_timing(pb_context* c, double* solve_ms, double* device_ms, double* steps_ms, int64_t* launches) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (solve_ms) *solve_ms = c->last_solve_ms;
+  if (device_ms) *device_ms = c->last_device_ms;
+  if (steps_ms) *steps_ms = c->last_steps_ms;
+  if (launches) *launches = c->last_launches;
+  return PB_OK;
+}
+
+}  // extern "C"

@@ -150,3 +150,23 @@ class ScaledPhotonField(PhotonField):
 
     def device_components(self):
         return self.field.device_components()
+
+
+def device_components(field):
+    """Device description of ``field`` (this package's classes, or the reference's
+    analytic ``CMBPhotonSpectrum`` / ``FlatPhotonSpectrum`` / ``CombinedPhotonField``
+    matched by class name).  Raises ``NotImplementedError`` for anything else.
+    """
+    if hasattr(field, "device_components"):
+        return field.device_components()
+    name = type(field).__name__
+    if name == "CMBPhotonSpectrum":
+        return [(PF_CMB, CMBPhotonSpectrum.pref, C.E_CMB, 2.0)]
+    if name == "FlatPhotonSpectrum":
+        return [(PF_FLAT, 1e12, 0.0, 0.0)]
+    if name == "CombinedPhotonField":
+        out = []
+        for m in field.model_list:
+            out.extend(device_components(m))
+        return out
+    return PhotonField.device_components(field)

@@ -1,0 +1,450 @@
+"""Propagation solvers and the result container (reference API, B200 backend).
+
+``UHECRPropagationSolverETD2`` and ``MultiRHSPropagationSolverETD2`` keep the
+constructor signature, ``add_source_class``, ``solve``, ``state`` and ``res``
+of the reference solvers (``src/prince_cr/solvers/propagation.py:195-890,
+2344-2562``).  The redshift stepping, the photon field, the pair-loss
+vectors, the rate fold, the operator split and the ETD2 steps all run on the
+GPU through the C ABI; the host evaluates only the scalar schedule (z grid,
+windows, dl/dz, source evolution) and moves the state.
+
+``UHECRPropagationResult`` is the reference result container
+(``propagation.py:34-192``).
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from . import constants as C
+from .cosmology import dldz as _dldz
+from .data import EnergyGrid, is_nucleus
+from .operators import fd_loss_operator, split_diagonal
+from .photonfields import device_components
+from .schedule import make_schedule, z_grid
+
+
+# ---------------------------------------------------------------------------
+# result container
+# ---------------------------------------------------------------------------
+class UHECRPropagationResult:
+    """State vector plus grid and species table; spectra per species or group."""
+
+    def __init__(self, state, egrid, spec_man):
+        self.spec_man = spec_man
+        self.egrid = egrid
+        self.state = state
+
+    def to_dict(self):
+        return {"egrid": self.egrid, "state": self.state, "known_spec": self.known_species}
+
+    @classmethod
+    def from_dict(cls, dic):
+        from .data import SpeciesManager
+
+        egrid = dic["egrid"]
+        return cls(dic["state"], egrid, SpeciesManager(dic["known_spec"], egrid.size))
+
+    @property
+    def known_species(self):
+        return self.spec_man.known_species
+
+    def __add__(self, other):
+        if not np.array_equal(self.egrid, other.egrid):
+            raise Exception("Cannot add Propagation Results, they are defined in different energy grids!")
+        if not np.array_equal(self.known_species, other.known_species):
+            raise Exception("Cannot add Propagation Results, have different species managers!")
+        return UHECRPropagationResult(self.state + other.state, self.egrid, self.spec_man)
+
+    def __mul__(self, number):
+        if not np.isscalar(number):
+            raise Exception(
+                "Can only multiply result by scalar number, got type {:} instead!".format(type(number)))
+        return UHECRPropagationResult(self.state * number, self.egrid, self.spec_man)
+
+    def get_solution(self, pdg_id):
+        """Spectrum in energy per nucleon."""
+        spec = self.spec_man.pdgid2sref[pdg_id]
+        return self.egrid, self.state[spec.lidx():spec.uidx()]
+
+    def get_solution_scale(self, pdg_id, epow=0):
+        """Spectrum in total energy, times E^epow."""
+        spec = self.spec_man.pdgid2sref[pdg_id]
+        egrid = spec.A * self.egrid
+        return egrid, egrid ** epow * self.state[spec.lidx():spec.uidx()] / spec.A
+
+    def _check_id_grid(self, pdg_ids, egrid):
+        if egrid is None:
+            max_mass = max(s.A for s in self.spec_man.species_refs)
+            emin_log, emax_log, nbins = self._grid_triple()
+            emax_log = np.log10(max_mass) + emax_log
+            com_egrid = EnergyGrid(emin_log, emax_log, nbins * 4).grid
+        else:
+            com_egrid = egrid
+        if isinstance(pdg_ids, list):
+            pass
+        elif pdg_ids == "CR":
+            pdg_ids = [s for s in self.known_species if is_nucleus(s)]
+        elif pdg_ids == "nu":
+            pdg_ids = [s for s in self.known_species if s in (12, -12, 14, -14, 16, -16)]
+        elif pdg_ids == "all":
+            pdg_ids = self.known_species
+        elif isinstance(pdg_ids, tuple):
+            select, vmin, vmax = pdg_ids
+            pdg_ids = [s for s in self.known_species if vmin <= select(s) <= vmax]
+        return pdg_ids, com_egrid
+
+    def _grid_triple(self):
+        """(log10 lo edge, log10 hi edge, bins/decade) recovered from the centres."""
+        g = np.asarray(self.egrid)
+        step = np.log10(g[1] / g[0])
+        ratio = 10 ** step
+        lo_edge = 2 * g[0] / (1 + ratio)
+        hi_edge = lo_edge * ratio ** g.size
+        return (float(np.round(np.log10(lo_edge), 9)), float(np.round(np.log10(hi_edge), 9)),
+                float(np.round(1.0 / step, 9)))
+
+    def _collect_interpolated_spectra(self, pdg_ids, epow, egrid=None):
+        pdg_ids, com_egrid = self._check_id_grid(pdg_ids, egrid)
+        spectra = np.zeros((len(pdg_ids), com_egrid.size))
+        for idx, pid in enumerate(pdg_ids):
+            curr_egrid, curr_spec = self.get_solution_scale(pid, epow)
+            mask = curr_spec > 0.0
+            if np.count_nonzero(mask) > 0:
+                res = np.exp(np.interp(np.log(com_egrid), np.log(curr_egrid[mask]), np.log(curr_spec[mask]),
+                                       left=np.nan, right=np.nan))
+            else:
+                res = np.zeros_like(com_egrid)
+            spectra[idx] = np.nan_to_num(res)
+        return pdg_ids, com_egrid, spectra
+
+    def get_solution_group(self, pdg_ids, epow=3, egrid=None):
+        """Summed spectrum (total energy) of a group of species."""
+        _, com_egrid, spectra = self._collect_interpolated_spectra(pdg_ids, epow, egrid)
+        return com_egrid, spectra.sum(axis=0)
+
+    def get_lnA(self, pdg_ids, egrid=None):
+        """Mean and variance of ln A versus total energy."""
+        pdg_ids, com_egrid, spectra = self._collect_interpolated_spectra(pdg_ids, 0, egrid)
+        lnA = np.array([np.log(self.spec_man.pdgid2sref[el].A) for el in pdg_ids])
+        total = spectra.sum(axis=0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            average = (lnA[:, None] * spectra).sum(axis=0) / total
+            variance = (lnA[:, None] ** 2 * spectra).sum(axis=0) / total - average ** 2
+        return com_egrid, average, variance
+
+    def get_energy_density(self, pdg_id):
+        from scipy.integrate import trapezoid
+
+        A = self.spec_man.pdgid2sref[pdg_id].A
+        return trapezoid(A * self.egrid * self.get_solution(pdg_id)[1], self.egrid)
+
+
+# ---------------------------------------------------------------------------
+# device state of one run
+# ---------------------------------------------------------------------------
+def _dense_kernel(bm):
+    if sp.issparse(bm):
+        bm = bm.toarray()
+    return np.ascontiguousarray(bm, dtype=np.float64)
+
+
+class DeviceRun:
+    """The run's constant operators resident on one GPU (one C context).
+
+    Uploaded once per (run, device): the coupling pattern, the FP64 fold
+    kernel, the photon grid, the FD loss operator, the loss inputs and (if the
+    run carries one) the explicit-decay operator.
+    """
+
+    def __init__(self, run, device=0):
+        self.run = run
+        self.ctx = _lib.Context(device)
+        n = run.dim_states
+        ir = run.int_rates
+        cm = ir.coupling_mat
+        self.n = n
+        self.ctx.set_coupling(n, cm.indptr, cm.indices)
+        self.ctx.set_fold_kernel(_dense_kernel(ir._batch_matrix))
+        self.ctx.set_photon_grid(ir.e_photon.grid)
+        D = fd_loss_operator(run.cr_grid, run.spec_man.nspec)
+        self.D_diag, self.D_off = split_diagonal(D)
+        self.ctx.set_fd_operator(self.D_off, self.D_diag)
+        pl = run.pair_loss_rates_grid
+        pair_bin = np.full(n, -1, dtype=np.int32)
+        for s in run.spec_man.species_refs:
+            if s.is_nucleus:
+                pair_bin[s.lidx():s.uidx()] = np.arange(s.uidx() - s.lidx())
+        self.ctx.set_losses(run.adia_loss_rates_grid.energy_vector, pl.scale_vec, pair_bin, pl.xi, pl.phi_xi2,
+                            pl.photon_grid)
+        self.has_decay = False
+        dec = getattr(run, "decay_operator", None)
+        if dec is not None:
+            diag, off = dec
+            self.ctx.set_decay(diag, None if off is None else sp.csr_matrix(off))
+            self.has_decay = True
+
+    @classmethod
+    def of(cls, run, device=0):
+        cache = getattr(run, "_b200_device_runs", None)
+        if cache is None:
+            cache = {}
+            try:
+                run._b200_device_runs = cache
+            except AttributeError:
+                return cls(run, device)
+        if device not in cache:
+            cache[device] = cls(run, device)
+        return cache[device]
+
+
+# ---------------------------------------------------------------------------
+# solvers
+# ---------------------------------------------------------------------------
+def _coefficients(sources, zs):
+    """(n_steps, n_src) table of norm * evolution(z_k) per source."""
+    out = np.zeros((zs.size, len(sources)))
+    for i, s in enumerate(sources):
+        if hasattr(s, "evolution_array"):
+            ev = s.evolution_array(zs)
+        else:
+            ev = np.array([s.evolution(z) for z in zs])
+        out[:, i] = s.norm * ev
+    return out
+
+
+class UHECRPropagationSolverETD2:
+    """ETD2 (Cox-Matthews) redshift integrator of the transport equation on one GPU.
+
+    Same constructor and flags as the reference solver
+    (``propagation.py:196-209``); ``device`` selects the GPU.
+    """
+
+    def __init__(self, initial_z, final_z, prince_run, enable_adiabatic_losses=True,
+                 enable_pairprod_losses=True, enable_photohad_losses=True, enable_injection_jacobian=True,
+                 enable_partial_diff_jacobian=True, enable_decay=False, enable_decay_jacobian=True,
+                 z_offset=0.0, device=0):
+        self.initial_z = initial_z + z_offset
+        self.final_z = final_z + z_offset
+        self.z_offset = z_offset
+        self.prince_run = prince_run
+        self.backend = prince_run.backend
+        self.recomp_z_threshold = self.backend.update_rates_z_threshold
+        self.spec_man = prince_run.spec_man
+        self.egrid = prince_run.cr_grid.grid
+        self.ebins = prince_run.cr_grid.bins
+        self.widths = prince_run.cr_grid.widths
+        self.enable_adiabatic_losses = enable_adiabatic_losses
+        self.enable_pairprod_losses = enable_pairprod_losses
+        self.enable_photohad_losses = enable_photohad_losses
+        self.enable_injection_jacobian = enable_injection_jacobian
+        self.enable_partial_diff_jacobian = enable_partial_diff_jacobian
+        self.enable_decay = enable_decay
+        self.enable_decay_jacobian = enable_decay_jacobian
+        self.dim_states = prince_run.dim_states
+        self.state = np.zeros(self.dim_states)
+        self.result = None
+        self.list_of_sources = []
+        self.device = device
+        self._dev = DeviceRun.of(prince_run, device)
+        self.last_timing = None
+        if enable_decay and not self._dev.has_decay:
+            unstable = [s for s in self.spec_man.species_refs if np.isfinite(getattr(s, "lifetime", np.inf))]
+            if unstable:
+                raise NotImplementedError(
+                    "enable_decay=True needs the run's explicit-decay operator: attach "
+                    "run.decay_operator = (Lambda_diag, Lambda_off_csr) before creating the solver")
+
+    # -- reference API ---------------------------------------------------
+    @property
+    def known_species(self):
+        return self.spec_man.known_species
+
+    @property
+    def res(self):
+        if self.result is None:
+            self.result = UHECRPropagationResult(self.state, self.egrid, self.spec_man)
+        return self.result
+
+    def add_source_class(self, source_instance):
+        self.list_of_sources.append(source_instance)
+
+    def dldz(self, z):
+        return _dldz(z)
+
+    def injection(self, dz, z):
+        f = self.dldz(z) * dz * C.PRINCE_UNITS.cm2sec
+        if len(self.list_of_sources) > 1:
+            return f * np.sum([s.injection_rate(z) for s in self.list_of_sources], axis=0)
+        return f * self.list_of_sources[0].injection_rate(z)
+
+    def close(self):
+        pass
+
+    # -- solve -----------------------------------------------------------
+    def _flags(self):
+        f = 0
+        if self.enable_adiabatic_losses:
+            f |= _lib.PB_ADIABATIC
+        if self.enable_pairprod_losses:
+            f |= _lib.PB_PAIRPROD
+        if self.enable_photohad_losses:
+            f |= _lib.PB_PHOTOHAD
+        if self.enable_injection_jacobian:
+            f |= _lib.PB_INJECTION
+        if self.enable_partial_diff_jacobian:
+            f |= _lib.PB_PARTIAL_DIFF
+        if self.enable_decay and self._dev.has_decay:
+            f |= _lib.PB_DECAY
+        return f
+
+    def _column_sources(self):
+        return [list(self.list_of_sources)]
+
+    def _photon_scale(self):
+        return float(getattr(self.prince_run.photon_field, "scale", 1.0))
+
+    def _prepare(self, dz):
+        """Host-side schedule, injection basis and column order of one solve."""
+        zg = z_grid(self.initial_z, self.final_z, dz)
+        sched = make_schedule(zg, self.recomp_z_threshold)
+        cols = self._column_sources()
+        K = len(cols)
+        srcs = [s for c in cols for s in c]
+        owner = np.array([k for k, c in enumerate(cols) for _ in c], dtype=np.int64)
+        zs = zg[:-1]
+        coeff = _coefficients(srcs, zs) if srcs else np.zeros((zs.size, 0))
+        grids = np.array([s.injection_grid for s in srcs]) if srcs else np.zeros((0, self.dim_states))
+        use_inj = self.enable_injection_jacobian and len(srcs) > 0
+        # first step at which each column receives a non-zero injection
+        first = np.full(K, sched.n_steps, dtype=np.int64)
+        if use_inj:
+            live = (coeff != 0.0) & np.any(grids != 0.0, axis=1)[None, :]
+            for k in range(K):
+                sel = owner == k
+                if np.any(sel):
+                    hit = np.flatnonzero(np.any(live[:, sel], axis=1))
+                    if hit.size:
+                        first[k] = hit[0]
+        perm = np.argsort(first, kind="stable")          # device column j <- user column perm[j]
+        inv = np.empty(K, dtype=np.int64)
+        inv[perm] = np.arange(K)
+        n_active = np.searchsorted(np.sort(first), np.arange(sched.n_steps), side="right").astype(np.int32)
+        src_order = np.argsort(inv[owner], kind="stable") if srcs else np.zeros(0, dtype=np.int64)
+        src_col = inv[owner][src_order].astype(np.int32)
+        rows = np.flatnonzero(np.any(grids != 0.0, axis=0)).astype(np.int32) if srcs else np.zeros(0, np.int32)
+        G = np.ascontiguousarray(grids[src_order][:, rows].T) if srcs else np.zeros((0, 0))
+        return sched, K, coeff[:, src_order] if srcs else coeff, rows, G, src_col, n_active, perm, use_inj
+
+    def solve(self, dz=1e-3, verbose=False, summary=False, progressbar=False):
+        start = time.time()
+        sched, K, coeff, rows, G, src_col, n_active, perm, use_inj = self._prepare(dz)
+        ctx = self._dev.ctx
+        flags = self._flags()
+        if use_inj:
+            ctx.set_injection(rows, G, src_col, K)
+        else:
+            flags &= ~_lib.PB_INJECTION
+        ctx.set_photon_field(device_components(self.prince_run.photon_field))
+        out = np.zeros((self.dim_states, K))
+        ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, out, photon_scale=self._photon_scale())
+        state = np.empty_like(out)
+        state[:, perm] = out
+        self.last_timing = ctx.last_timing()
+        self._store(state)
+        self.result = None
+        if summary or verbose:
+            print("ETD2 summary:")
+            print(f"  steps: {sched.n_steps}")
+            print(f"  initial z: {self.initial_z} → final z: {self.final_z}")
+            print(f"  wall time: {time.time() - start:.3f} s")
+
+    def _store(self, state):
+        self.state = state[:, 0].copy()
+
+    def operator_pattern(self):
+        """M_off pattern (indptr, indices) of the last solve's first window."""
+        return self._dev.ctx.operator_pattern(self.dim_states)
+
+    def window_values(self, w):
+        ip, ix = self.operator_pattern()
+        return self._dev.ctx.window_values(w, self.dim_states, ix.size)
+
+
+class _MultiRHSView:
+    """Column k of a multi-RHS solver: its own sources and result."""
+
+    def __init__(self, parent, k):
+        self.parent = parent
+        self.k = k
+        self.list_of_sources = []
+
+    def add_source_class(self, source_instance):
+        self.list_of_sources.append(source_instance)
+
+    @property
+    def state(self):
+        s = self.parent.state
+        return s[:, self.k] if s.ndim == 2 else s
+
+    @property
+    def res(self):
+        return UHECRPropagationResult(self.state, self.parent.egrid, self.parent.spec_man)
+
+
+class MultiRHSPropagationSolverETD2(UHECRPropagationSolverETD2):
+    """K independent right-hand sides sharing one operator (one SpMM per stage).
+
+    Columns whose sources are still switched off (zero injection so far) are
+    exactly zero and are skipped; columns are processed in the order in which
+    they switch on, which keeps the active set a prefix of the device tile.
+    """
+
+    def __init__(self, *args, K, **kwargs):
+        if K < 1:
+            raise ValueError(f"K must be >= 1, got {K!r}")
+        super().__init__(*args, **kwargs)
+        self._K = int(K)
+        self._views = [_MultiRHSView(self, k) for k in range(self._K)]
+        self.state = np.zeros((self.dim_states, self._K))
+
+    def __len__(self):
+        return self._K
+
+    def __getitem__(self, k):
+        return self._views[k]
+
+    @property
+    def K(self):
+        return self._K
+
+    def add_source_class(self, source_instance):
+        raise TypeError(
+            "MultiRHSPropagationSolverETD2 expects per-RHS sources via "
+            "solver[k].add_source_class(...). The k-th view's sources drive "
+            "the k-th column of the multi-RHS state.")
+
+    @property
+    def res(self):
+        raise TypeError("MultiRHSPropagationSolverETD2.res is per-view: use solver[k].res for the k-th RHS.")
+
+    def injection(self, dz, z):
+        f = self.dldz(z) * dz * C.PRINCE_UNITS.cm2sec
+        out = np.zeros((self.dim_states, self._K))
+        for k, view in enumerate(self._views):
+            srcs = view.list_of_sources
+            if not srcs:
+                continue
+            col = np.sum([s.injection_rate(z) for s in srcs], axis=0) if len(srcs) > 1 else srcs[0].injection_rate(z)
+            out[:, k] = f * col
+        return out
+
+    def _column_sources(self):
+        return [list(v.list_of_sources) for v in self._views]
+
+    def _store(self, state):
+        self.state = state

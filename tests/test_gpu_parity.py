@@ -1,0 +1,177 @@
+"""CUDA path against the reference's golden vectors and the CPU oracle (needs a B200).
+
+Tolerance: relative 1e-10 per bin wherever the reference flux exceeds 1e-20
+of that species' maximum; operator patterns bit-exact.
+"""
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from golden_io import light_network, rel_err_on_support
+from oracle import etd2_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return light_network()
+
+
+def _blocks(run):
+    return [s.sl for s in run.spec_man.species_refs]
+
+
+def _solver(run, zi=1.0, **kw):
+    from prince_b200.solvers import UHECRPropagationSolverETD2
+    return UHECRPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, **kw)
+
+
+# --- constant-operator known answers (tests/test_explicit_decay_analytics.py) ----
+def test_const_single_exponential():
+    from prince_b200 import _lib
+    ctx = _lib.Context(0)
+    zg = np.linspace(0.0, 5.0, 1001)
+    x = ctx.integrate_const([-1.0 / 0.7], None, zg, [1.0])
+    np.testing.assert_allclose(x[0], np.exp(-5.0 / 0.7), rtol=1e-10)
+
+
+def test_const_bateman_chain():
+    from prince_b200 import _lib
+    ctx = _lib.Context(0)
+    ta, tb, T = 1.0, 2.5, 6.0
+    zg = np.linspace(0.0, T, 2001)
+    L = sp.csr_matrix(np.array([[0.0, 0.0], [1.0 / ta, 0.0]]))
+    x = ctx.integrate_const([-1 / ta, -1 / tb], L, zg, [1.0, 0.0])
+    np.testing.assert_allclose(x[0], np.exp(-T / ta), rtol=1e-8)
+    np.testing.assert_allclose(x[1], tb / (ta - tb) * (np.exp(-T / ta) - np.exp(-T / tb)), rtol=1e-6)
+
+
+def test_const_chain_matches_reference(golden):
+    from prince_b200 import _lib
+    z, _, _ = golden
+    ctx = _lib.Context(0)
+    L = sp.csr_matrix(np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 0.4, 0.0]]))
+    x = ctx.integrate_const([-1.0, -0.4, 0.0], L, np.linspace(0.0, 6.0, 2001), [1.0, 0.0, 0.0])
+    np.testing.assert_allclose(x, z["chain3_state"], rtol=1e-12)
+
+
+# --- golden light-nuclei network -------------------------------------------------
+CASES = {
+    "plain": (dict(), ["eq"], 1.0, 1e-3, None),
+    "no_pair": (dict(enable_pairprod_losses=False), ["eq"], 1.0, 1e-3, None),
+    "no_adia": (dict(enable_adiabatic_losses=False), ["eq"], 1.0, 1e-3, None),
+    "no_pdiff": (dict(enable_partial_diff_jacobian=False), ["eq"], 1.0, 1e-3, None),
+    "no_photohad": (dict(enable_photohad_losses=False), ["eq"], 1.0, 1e-3, None),
+    "two_src": (dict(), ["auger", "soft"], 1.0, 1e-3, None),
+    "thr": (dict(), ["eq"], 0.5, 2e-3, 1e-3),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_golden_single_rhs(golden, case):
+    z, run, source = golden
+    flags, keys, zi, dz, thr = CASES[case]
+    s = _solver(run, zi, **flags)
+    if thr is not None:
+        s.recomp_z_threshold = thr
+    for k in keys:
+        s.add_source_class(source(k))
+    s.solve(dz=dz)
+    err = rel_err_on_support(s.state, z[f"state_{case}"], _blocks(run))
+    assert err < TOL, (case, err)
+
+
+def test_golden_operator_pattern_and_first_window(golden):
+    z, run, source = golden
+    s = _solver(run)
+    s.add_source_class(source("eq"))
+    s.solve(dz=1e-3)
+    ip, ix = s.operator_pattern()
+    assert np.array_equal(ip, z["M_off_indptr"])
+    assert np.array_equal(ix, z["M_off_indices"])
+    off, diag, kp = s.window_values(0)
+    np.testing.assert_allclose(off, z["M_off_data_z1"], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(diag, z["M_diag_z1"], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(kp, z["kappa_pair_z1"], rtol=1e-13, atol=0)
+
+
+def test_golden_multi_rhs(golden):
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    z, run, source = golden
+    cols = [str(c).split(",") for c in z["multi_columns"]]
+    m = MultiRHSPropagationSolverETD2(initial_z=1.0, final_z=0.0, prince_run=run, K=len(cols))
+    for k, keys in enumerate(cols):
+        for key in keys:
+            m[k].add_source_class(source(key))
+    m.solve(dz=1e-3)
+    assert rel_err_on_support(m.state, z["state_multi"], _blocks(run)) < TOL
+    for k in range(len(cols)):
+        assert np.array_equal(m[k].state, m.state[:, k])
+
+
+def test_golden_decay(golden):
+    from golden_io import light_network as ln
+    z, run, source = ln()   # fresh run: the decay operator is part of the run's device state
+    n = run.dim_states
+    run.decay_operator = (z["lambda_diag"],
+                          sp.csr_matrix((z["lambda_data"], z["lambda_indices"], z["lambda_indptr"]), shape=(n, n)))
+    s = _solver(run, enable_decay=True)
+    s.add_source_class(source("eq"))
+    s.solve(dz=1e-3)
+    assert rel_err_on_support(s.state, z["state_decay"], _blocks(run)) < TOL
+
+
+# --- synthetic networks against the oracle ---------------------------------------
+@pytest.fixture(scope="module")
+def medium_run():
+    from workloads import network_run
+    return network_run(max_mass=16, n_species=60, seed=5)
+
+
+def test_medium_network_plain_vs_oracle(medium_run):
+    from workloads import draw_points, point_source
+    run = medium_run
+    pt = draw_points(run, 1, seed=11, z_range=(0.3, 0.3))[0]
+    src = point_source(run, pt)
+    s = _solver(run, zi=0.3)
+    s.add_source_class(src)
+    s.solve(dz=1e-3)
+    o = O.OracleSolver(run, 0.3, 0.0)
+    ref = o.solve([src], dz=1e-3)
+    assert rel_err_on_support(s.state, ref, _blocks(run)) < TOL
+    ip, ix = s.operator_pattern()
+    assert np.array_equal(ip, o.trace.M_off_first.indptr)
+    assert np.array_equal(ix, o.trace.M_off_first.indices)
+
+
+def test_medium_network_batched_uneven_zmax_vs_oracle(medium_run):
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, point_source
+    run = medium_run
+    K = 40
+    pts = draw_points(run, K, seed=3, z_range=(0.05, 0.3))
+    m = MultiRHSPropagationSolverETD2(initial_z=0.3, final_z=0.0, prince_run=run, K=K)
+    srcs = [point_source(run, p) for p in pts]
+    for k, s in enumerate(srcs):
+        m[k].add_source_class(s)
+    m.solve(dz=1e-3)
+    o = O.OracleSolver(run, 0.3, 0.0, K=K)
+    ref = o.solve([[s] for s in srcs], dz=1e-3)
+    assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
+
+
+def test_full_network_short_range_vs_oracle():
+    from workloads import draw_points, network_run, point_source
+    run = network_run()
+    assert run.dim_states == 33600
+    pt = draw_points(run, 1, seed=5, z_range=(0.05, 0.05))[0]
+    src = point_source(run, pt)
+    s = _solver(run, zi=0.05)
+    s.add_source_class(src)
+    s.solve(dz=1e-3)
+    o = O.OracleSolver(run, 0.05, 0.0)
+    ref = o.solve([src], dz=1e-3)
+    assert rel_err_on_support(s.state, ref, _blocks(run)) < TOL
