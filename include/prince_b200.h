@@ -163,6 +163,12 @@ int pb_integrate_const(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
                        const int64_t* indptr, const int32_t* indices, const double* values,
                        int64_t n_steps, const double* z_grid, double* state);
 
+/* The exp used by the device phi functions, evaluated on n values: a
+ * correctly rounded double-double exp (same operation sequence as the host
+ * form in oracle/crexp.py).  Replaces: the numpy exp of _compute_diag_factors
+ * (src/prince_cr/solvers/etd2.py:355); exposed to test it against exact values. */
+int pb_eval_exp(pb_context* ctx, int64_t n, const double* x, double* y);
+
 /* Timing of the last pb_solve from CUDA events on the context stream (ms):
  * solve_ms  -- whole call on the device, including the state copy-out;
  * device_ms -- photon field, pair losses, fold, split and all steps (inputs resident);

@@ -78,10 +78,14 @@ def window_starts(zg, thr):
     return out
 
 
-def phi_factors(h, d):
-    """eD, phi1, phi2 with the Taylor patches of etd2.py:329-390."""
+def phi_factors(h, d, exp=np.exp):
+    """eD, phi1, phi2 with the Taylor patches of etd2.py:329-390.
+
+    ``exp`` is the exponential: numpy's (as the reference) or the correctly
+    rounded one of ``oracle.crexp`` (as the CUDA path).
+    """
     hD = d * h
-    eD = np.exp(hD)
+    eD = exp(hD)
     a = np.abs(hD)
     m1 = a > PHI1_SMALL
     m2 = a > PHI2_SMALL
@@ -183,7 +187,7 @@ class OracleSolver:
     lists (one per column).  Sources expose ``injection_rate(z)``.
     """
 
-    def __init__(self, run, initial_z, final_z, flags=None, thr=None, K=None, decay=None):
+    def __init__(self, run, initial_z, final_z, flags=None, thr=None, K=None, decay=None, exp="numpy"):
         self.run = run
         self.initial_z = float(initial_z)
         self.final_z = float(final_z)
@@ -201,6 +205,14 @@ class OracleSolver:
         # Explicit decay (propagation.py:1148-1358, 1418-1422, 1479-1482):
         # ``decay = (Lambda_diag, Lambda_off CSR)``, constant over the solve.
         self.L_diag, self.L_off = (None, None) if decay is None else decay
+        # ``exp="cr"`` evaluates the phi functions with the correctly rounded
+        # exp (the CUDA path's); ``"numpy"`` with the host numpy exp (the
+        # reference's, whose rounding depends on the CPU's SIMD level).
+        if exp == "cr":
+            from oracle import crexp
+            self._exp = crexp.exp
+        else:
+            self._exp = np.exp
         self.trace = Trace()
 
     # -- per window --------------------------------------------------------
@@ -291,7 +303,7 @@ class OracleSolver:
         return out
 
     def _step(self, x, h, d, dl, kappa, b):
-        eD, phi1, phi2 = phi_factors(h, d)
+        eD, phi1, phi2 = phi_factors(h, d, self._exp)
         if x.ndim == 2:
             eD, phi1, phi2 = eD[:, None], phi1[:, None], phi2[:, None]
         F_phi = self._apply_F(x, dl, kappa, b)
@@ -306,12 +318,12 @@ class OracleSolver:
         return a + s
 
 
-def integrate_const(state, zg, d, L_off=None):
+def integrate_const(state, zg, d, L_off=None, exp=np.exp):
     """ETD2 with a z-independent operator (etd2.py:478-517 with a constant closure)."""
     x = np.array(state, dtype=np.float64)
     for k in range(len(zg) - 1):
         h = zg[k + 1] - zg[k]
-        eD, phi1, phi2 = phi_factors(h, np.asarray(d, dtype=np.float64))
+        eD, phi1, phi2 = phi_factors(h, np.asarray(d, dtype=np.float64), exp)
 
         def F(v):
             return np.zeros_like(v) if L_off is None else np.asarray(L_off @ v)

@@ -67,6 +67,7 @@ _PROTOS = {
     "pb_get_operator_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
     "pb_get_window": (C.c_int, [_vp, C.c_int32, _d, _d, _d]),
     "pb_integrate_const": (C.c_int, [_vp, C.c_int64, _d, C.c_int64, _i64, _i32, _d, C.c_int64, _d, _d]),
+    "pb_eval_exp": (C.c_int, [_vp, C.c_int64, _d, _d]),
     "pb_last_timing": (C.c_int, [_vp, _d, _d, _d, _i64]),
 }
 
@@ -267,6 +268,14 @@ class Context:
                                              _ptr(zg, C.c_double), _ptr(x, C.c_double))
         self._check(rc, "pb_integrate_const")
         return x
+
+    def eval_exp(self, x):
+        """The device exp of the phi functions on ``x`` (float64 array)."""
+        x = _f64(x)
+        y = np.empty_like(x)
+        self._check(self.lib.pb_eval_exp(self.h, int(x.size), _ptr(x, C.c_double), _ptr(y, C.c_double)),
+                    "pb_eval_exp")
+        return y
 
     def last_timing(self):
         """(solve_ms, device_ms, steps_ms, launches) of the last solve."""

@@ -23,6 +23,7 @@
 
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <math_constants.h>
 
 #include <algorithm>
 #include <cmath>
@@ -110,7 +111,7 @@ struct pb_context {
   // per-solve workspace
   DBuf PT, zwin, rs, kp, keep, pos, dest, m_indptr, m_indices, m_vals, m_diag;
   DBuf s_h, s_dldz, s_hc, s_finj, s_win, s_coeff;
-  DBuf X, A, F;
+  DBuf X, A, F, rowf;
   DBuf scan_tmp;
   size_t scan_tmp_bytes = 0;
   int32_t last_W = 0;
@@ -346,13 +347,105 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
 }
 
 // ---------------------------------------------------------------------------
+// correctly rounded exp (double-double; same operation sequence as oracle/crexp.py)
+//
+// x = k ln2 + r, s = r / 2^10, expm1(s) by a degree-9 Taylor polynomial in
+// double-double, ten squarings E <- 2E + E^2, then (1 + E) 2^k rounded once.
+// Double-double arithmetic after Dekker and Knuth (QD library, Hida/Li/Bailey);
+// every operation is an explicitly rounded intrinsic so the sequence cannot be
+// contracted into FMAs and matches the host form bit for bit.
+// ---------------------------------------------------------------------------
+struct DD {
+  double h, l;
+};
+
+__device__ __forceinline__ DD dd_two_sum(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  const double bb = __dadd_rn(s, -a);
+  return {s, __dadd_rn(__dadd_rn(a, -__dadd_rn(s, -bb)), __dadd_rn(b, -bb))};
+}
+__device__ __forceinline__ DD dd_quick(double a, double b) {
+  const double s = __dadd_rn(a, b);
+  return {s, __dadd_rn(b, -__dadd_rn(s, -a))};
+}
+__device__ __forceinline__ DD dd_two_prod(double a, double b) {
+  const double p = __dmul_rn(a, b);
+  return {p, __fma_rn(a, b, -p)};
+}
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+  DD s = dd_two_sum(a.h, b.h);
+  const DD t = dd_two_sum(a.l, b.l);
+  s.l = __dadd_rn(s.l, t.h);
+  s = dd_quick(s.h, s.l);
+  s.l = __dadd_rn(s.l, t.l);
+  return dd_quick(s.h, s.l);
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+  DD p = dd_two_prod(a.h, b.h);
+  p.l = __dadd_rn(p.l, __dadd_rn(__dmul_rn(a.h, b.l), __dmul_rn(a.l, b.h)));
+  return dd_quick(p.h, p.l);
+}
+
+__constant__ double c_expcoef[9][2] = {
+    {1.0, 0.0},
+    {0.5, 0.0},
+    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+};
+
+__device__ double cr_exp(double x) {
+  if (isnan(x)) return x;
+  if (x > 709.782712893384) return CUDART_INF;
+  if (x < -745.1332191019412) return 0.0;
+  const double ln2_hi = 0x1.62e42fefa39efp-1, ln2_lo = 0x1.abc9e3b39803fp-56;
+  const double k = rint(__dmul_rn(x, 1.4426950408889634));
+  const DD p = dd_two_prod(k, ln2_hi);
+  DD r = dd_two_sum(x, -p.h);
+  r = dd_add(r, DD{-p.l, 0.0});
+  r = dd_add(r, DD{-__dmul_rn(k, ln2_lo), 0.0});
+  const DD s{__dmul_rn(r.h, 0.0009765625), __dmul_rn(r.l, 0.0009765625)};
+  DD t{c_expcoef[8][0], c_expcoef[8][1]};
+#pragma unroll
+  for (int i = 7; i >= 0; --i) {
+    t = dd_mul(t, s);
+    t = dd_add(t, DD{c_expcoef[i][0], c_expcoef[i][1]});
+  }
+  DD e = dd_mul(t, s);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const DD q = dd_mul(e, e);
+    e = dd_add(DD{__dmul_rn(e.h, 2.0), __dmul_rn(e.l, 2.0)}, q);
+  }
+  const DD v = dd_add(e, DD{1.0, 0.0});
+  return ldexp(__dadd_rn(v.h, v.l), (int)k);
+}
+
+__global__ void k_eval_exp(const double* __restrict__ x, double* __restrict__ y, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = cr_exp(x[i]);
+}
+
+// ---------------------------------------------------------------------------
 // ETD2 step kernels
+//
+// Per step, two launches (stage 1 and 2) over the rows; short rows get a warp,
+// rows with more than kLongRow coupling entries a whole CTA.  The per-row
+// factors of a step (kappa, eD, phi1, phi2) are computed once per row by the
+// stage-2 launch of the previous step (k_prep for the first step) into a
+// buffer pair indexed by the step's parity, so the column tiles of the batched
+// kernel never recompute them.
 // ---------------------------------------------------------------------------
 struct StepParams {
   int64_t n;
   int ld;            // leading dimension of the (n x ld) state buffers
   int ncols;         // active columns this step
   int64_t step;
+  int64_t n_steps;
   uint32_t flags;
   const double* h;
   const double* dldz;
@@ -381,6 +474,11 @@ struct StepParams {
   int n_src;
   const int* src_ptr;
   const double* coeff;
+  // per-row step factors, [2][n] each (parity of the step)
+  double* eD;
+  double* phi1;
+  double* phi2;
+  double* kap;
   // states
   const double* src;  // stage 1: x ; stage 2: a
   const double* x;    // stage 1: x
@@ -397,13 +495,13 @@ struct StepScalars {
   bool kap, adia, pair, photohad, inj, decay;
 };
 
-__device__ __forceinline__ StepScalars load_scalars(const StepParams& p) {
+__device__ __forceinline__ StepScalars load_scalars(const StepParams& p, int64_t step) {
   StepScalars s;
-  s.h = p.h[p.step];
-  s.dl = p.dldz[p.step];
-  s.hc = p.hc[p.step];
-  s.finj = p.finj[p.step];
-  s.w = p.win[p.step];
+  s.h = p.h[step];
+  s.dl = p.dldz[step];
+  s.hc = p.hc[step];
+  s.finj = p.finj[step];
+  s.w = p.win[step];
   s.kap = (p.flags & PB_PARTIAL_DIFF) != 0;
   s.adia = (p.flags & PB_ADIABATIC) != 0;
   s.pair = (p.flags & PB_PAIRPROD) != 0 && p.kp != nullptr;
@@ -413,44 +511,46 @@ __device__ __forceinline__ StepScalars load_scalars(const StepParams& p) {
   return s;
 }
 
-// kappa(z) at state r: 0 + H cm2sec E (adiabatic) + kappa_pair (propagation.py:1393-1401)
-__device__ __forceinline__ double kappa_at(const StepParams& p, const StepScalars& s, int64_t r) {
+// phi functions with the Taylor patches of etd2.py:43-46, 329-390
+__device__ __forceinline__ void phi_of(double h, double d, double& eD, double& phi1, double& phi2) {
+  const double hd = __dmul_rn(d, h);
+  const double e = cr_exp(hd);
+  eD = e;
+  const double ahd = fabs(hd);
+  if (ahd > 1e-6) {
+    phi1 = __ddiv_rn(__dadd_rn(e, -1.0), hd);
+  } else {
+    phi1 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 6.0), 0.5), hd), 1.0);
+  }
+  if (ahd > 1e-3) {
+    phi2 = __ddiv_rn(__dadd_rn(__dadd_rn(e, -1.0), -hd), __dmul_rn(hd, hd));
+  } else {
+    phi2 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 24.0), 1.0 / 6.0), hd), 0.5);
+  }
+}
+
+// kappa (propagation.py:1393-1401) and d = dldz (M_diag + kappa D_diag [+ Lambda_diag])
+// (propagation.py:1408-1422) of row r at `step`, then its phi factors.
+__device__ __forceinline__ void row_prep(const StepParams& p, int64_t step, int64_t r) {
+  const StepScalars s = load_scalars(p, step);
   double k = 0.0;
   if (s.adia) k = __dmul_rn(s.hc, p.E[r]);
   if (s.pair) k = __dadd_rn(k, p.kp[(size_t)s.w * p.n + r]);
-  return k;
-}
-
-// diagonal d = dldz (M_diag + kappa D_diag [+ Lambda_diag]) (propagation.py:1408-1422)
-__device__ __forceinline__ double diag_at(const StepParams& p, const StepScalars& s, int64_t r) {
   double d = __dmul_rn(p.m_diag[(size_t)s.w * p.n + r], s.dl);
-  if (s.kap) d = __dadd_rn(d, __dmul_rn(__dmul_rn(kappa_at(p, s, r), p.d_diag[r]), s.dl));
+  if (s.kap) d = __dadd_rn(d, __dmul_rn(__dmul_rn(k, p.d_diag[r]), s.dl));
   if (s.decay) d = __dadd_rn(d, __dmul_rn(p.l_diag[r], s.dl));
-  return d;
+  double e, f1, f2;
+  phi_of(s.h, d, e, f1, f2);
+  const size_t o = (size_t)(step & 1) * p.n + r;
+  p.eD[o] = e;
+  p.phi1[o] = f1;
+  p.phi2[o] = f2;
+  p.kap[o] = k;
 }
 
-struct Phi {
-  double eD, phi1, phi2;
-};
-
-// phi functions with the Taylor patches of etd2.py:43-46, 329-390
-__device__ __forceinline__ Phi phi_of(double h, double d) {
-  Phi o;
-  const double hd = __dmul_rn(d, h);
-  const double e = exp(hd);
-  o.eD = e;
-  const double ahd = fabs(hd);
-  if (ahd > 1e-6) {
-    o.phi1 = __ddiv_rn(__dadd_rn(e, -1.0), hd);
-  } else {
-    o.phi1 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 6.0), 0.5), hd), 1.0);
-  }
-  if (ahd > 1e-3) {
-    o.phi2 = __ddiv_rn(__dadd_rn(__dadd_rn(e, -1.0), -hd), __dmul_rn(hd, hd));
-  } else {
-    o.phi2 = __dadd_rn(__dmul_rn(__dadd_rn(__dmul_rn(hd, 1.0 / 24.0), 1.0 / 6.0), hd), 0.5);
-  }
-  return o;
+__global__ void k_prep(StepParams p) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < p.n) row_prep(p, p.step, r);
 }
 
 // b(z) at (row r, column k): finj * sum_s coeff_s * g_s[r] (propagation.py:363-370, 2476-2488)
@@ -467,22 +567,24 @@ __device__ __forceinline__ double inj_at(const StepParams& p, const StepScalars&
 }
 
 // The rest of apply_F for one (row, column): the FD loss term, the decay term,
-// the dl/dz scale and the injection (propagation.py:1473-1486).
+// the dl/dz scale and the injection (propagation.py:1473-1486).  Sums run in
+// CSR order without contraction, as the host sparse products do.
 __device__ __forceinline__ double finish_F(const StepParams& p, const StepScalars& s, int64_t r,
                                            int k, const double* __restrict__ v, double sM) {
+  const double* kap = p.kap + (size_t)(p.step & 1) * p.n;
   double out = sM;
   if (s.kap) {
     double sD = 0.0;
     for (int64_t j = p.d_indptr[r]; j < p.d_indptr[r + 1]; ++j) {
       const int c = p.d_indices[j];
-      sD += p.d_vals[j] * __dmul_rn(kappa_at(p, s, c), v[(size_t)c * p.ld + k]);
+      sD = __dadd_rn(sD, __dmul_rn(p.d_vals[j], __dmul_rn(kap[c], v[(size_t)c * p.ld + k])));
     }
     out = __dadd_rn(out, sD);
   }
   if (s.decay) {
     double sL = 0.0;
     for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
-      sL += p.l_vals[j] * v[(size_t)p.l_indices[j] * p.ld + k];
+      sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], v[(size_t)p.l_indices[j] * p.ld + k]));
     out = __dadd_rn(out, sL);
   }
   out = __dmul_rn(out, s.dl);
@@ -493,25 +595,30 @@ __device__ __forceinline__ double finish_F(const StepParams& p, const StepScalar
 template <int STAGE>
 __device__ __forceinline__ void row_epilogue(const StepParams& p, const StepScalars& s, int64_t r,
                                              int k, double sM) {
-  const Phi ph = phi_of(s.h, diag_at(p, s, r));
+  const size_t o = (size_t)(p.step & 1) * p.n + r;
   const size_t idx = (size_t)r * p.ld + k;
   const double F = finish_F(p, s, r, k, p.src, sM);
   if (STAGE == 1) {
     // a = eD x + (phi1 F(x)) h  (etd2.py:427-430)
-    const double a = __dadd_rn(__dmul_rn(ph.eD, p.x[idx]), __dmul_rn(__dmul_rn(ph.phi1, F), s.h));
+    const double a = __dadd_rn(__dmul_rn(p.eD[o], p.x[idx]), __dmul_rn(__dmul_rn(p.phi1[o], F), s.h));
     p.a[idx] = a;
     p.f[idx] = F;
   } else {
     // x = a + ((F(a) - F(x)) h) phi2  (etd2.py:435-438)
     const double dF = __dmul_rn(__dadd_rn(F, -p.f[idx]), s.h);
-    p.xout[idx] = __dadd_rn(p.a[idx], __dmul_rn(dF, ph.phi2));
+    p.xout[idx] = __dadd_rn(p.a[idx], __dmul_rn(dF, p.phi2[o]));
   }
+}
+
+// stage 2 of step k prepares the row factors of step k + 1 (one thread per row)
+__device__ __forceinline__ void prep_next(const StepParams& p, int64_t r) {
+  if (p.step + 1 < p.n_steps) row_prep(p, p.step + 1, r);
 }
 
 // Single column: a warp per short row (lanes stride the row), a CTA per long row.
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
-  const StepScalars s = load_scalars(p);
+  const StepScalars s = load_scalars(p, p.step);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double* __restrict__ v = p.src;
   const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
@@ -529,6 +636,7 @@ __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
       double t = 0.0;
       for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
       row_epilogue<STAGE>(p, s, r, 0, t);
+      if (STAGE == 2) prep_next(p, r);
     }
     return;
   }
@@ -540,15 +648,20 @@ __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
     for (int64_t j = p.m_indptr[r] + lane; j < p.m_indptr[r + 1]; j += 32)
       acc += mv[j] * v[p.m_indices[j]];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  if (lane == 0) row_epilogue<STAGE>(p, s, r, 0, acc);
+  if (lane == 0) {
+    row_epilogue<STAGE>(p, s, r, 0, acc);
+    if (STAGE == 2) prep_next(p, r);
+  }
 }
 
 // Many columns: lane = column inside a 32-column tile (blockIdx.y); the row's
 // (value, column) pairs are loaded 32 at a time and broadcast by shuffles, so
-// every gathered state row is one coalesced 256-byte load.
+// every gathered state row is one coalesced 256-byte load.  A lane sums its
+// column in CSR order without contraction (the order of a CSR sparse x dense
+// product on the host).
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
-  const StepScalars s = load_scalars(p);
+  const StepScalars s = load_scalars(p, p.step);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k = blockIdx.y * kColTile + lane;
   const bool active = k < p.ncols;
@@ -572,7 +685,7 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
         for (int q = 0; q < cnt; ++q) {
           const double mq = __shfl_sync(0xffffffffu, mvl, q);
           const int cq = __shfl_sync(0xffffffffu, cl, q);
-          acc += mq * v[(size_t)cq * p.ld + kk];
+          acc = __dadd_rn(acc, __dmul_rn(mq, v[(size_t)cq * p.ld + kk]));
         }
       }
     }
@@ -581,8 +694,9 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
     __syncthreads();
     if (wid == 0) {
       double t = 0.0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i][lane];
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t = __dadd_rn(t, red[i][lane]);
       if (active) row_epilogue<STAGE>(p, s, r, k, t);
+      if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
     }
     return;
   }
@@ -600,11 +714,12 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
       for (int q = 0; q < cnt; ++q) {
         const double mq = __shfl_sync(0xffffffffu, mvl, q);
         const int cq = __shfl_sync(0xffffffffu, cl, q);
-        acc += mq * v[(size_t)cq * p.ld + kk];
+        acc = __dadd_rn(acc, __dmul_rn(mq, v[(size_t)cq * p.ld + kk]));
       }
     }
   }
   if (active) row_epilogue<STAGE>(p, s, r, k, acc);
+  if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
 }
 
 // ---------------------------------------------------------------------------
@@ -697,7 +812,7 @@ void pb_destroy(pb_context* c) {
                   &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos,
                   &c->dest, &c->m_indptr, &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h,
                   &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff, &c->X, &c->A, &c->F,
-                  &c->scan_tmp};
+                  &c->rowf, &c->scan_tmp};
   for (DBuf* b : bufs) b->release();
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
@@ -945,6 +1060,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->X.ensure(sbytes));
   PB_CUDA(c, c->A.ensure(sbytes));
   PB_CUDA(c, c->F.ensure(sbytes));
+  PB_CUDA(c, c->rowf.ensure((size_t)8 * n * sizeof(double)));
   size_t scan_need = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
@@ -1043,14 +1159,25 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   }
   p.a = c->A.as<double>();
   p.f = c->F.as<double>();
+  p.n_steps = S;
+  p.eD = c->rowf.as<double>();
+  p.phi1 = p.eD + 2 * n;
+  p.phi2 = p.eD + 4 * n;
+  p.kap = p.eD + 6 * n;
   const int nshort = (int)c->h_short_rows.size(), nlong = (int)c->h_long_rows.size();
   PB_CUDA(c, cudaEventRecord(c->ev2, st));
+  bool prepared = false;
   for (int64_t k = 0; k < S; ++k) {
     p.step = k;
     p.ncols = a->n_active[k];
     if (p.ncols == 0) {
       // every column is still exactly zero: nothing to advance
       continue;
+    }
+    if (!prepared) {  // row factors of the first active step; later steps get them from stage 2
+      k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
+      ++launches;
+      prepared = true;
     }
     for (int stage = 1; stage <= 2; ++stage) {
       p.src = stage == 1 ? X : c->A.as<double>();
@@ -1153,8 +1280,10 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   cudaStream_t st = c->stream;
   // A constant operator is one window with M_off = L_off, M_diag = d, dl/dz = 1
   // and no losses or injection.
-  DBuf ip, ix, iv, dg, hs, ones, zero_i, X, A, F, rows;
-  auto cleanup = [&]() { for (DBuf* b : {&ip, &ix, &iv, &dg, &hs, &ones, &zero_i, &X, &A, &F, &rows}) b->release(); };
+  DBuf ip, ix, iv, dg, hs, ones, zero_i, X, A, F, rows, rowf;
+  auto cleanup = [&]() {
+    for (DBuf* b : {&ip, &ix, &iv, &dg, &hs, &ones, &zero_i, &X, &A, &F, &rows, &rowf}) b->release();
+  };
   std::vector<double> hv((size_t)std::max<int64_t>(n_steps, 1)), one((size_t)std::max<int64_t>(n_steps, 1), 1.0);
   for (int64_t k = 0; k < n_steps; ++k) hv[k] = z_grid[k + 1] - z_grid[k];
   std::vector<int> zi((size_t)std::max<int64_t>(n_steps, 1), 0), rl((size_t)n);
@@ -1167,7 +1296,8 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
     cleanup();
     return rc;
   }
-  if (A.ensure((size_t)n * sizeof(double)) != cudaSuccess || F.ensure((size_t)n * sizeof(double)) != cudaSuccess) {
+  if (A.ensure((size_t)n * sizeof(double)) != cudaSuccess || F.ensure((size_t)n * sizeof(double)) != cudaSuccess ||
+      rowf.ensure((size_t)8 * n * sizeof(double)) != cudaSuccess) {
     cleanup();
     return fail(c, PB_ERR_CUDA, "pb_integrate_const: allocation failed");
   }
@@ -1191,6 +1321,13 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   p.f = F.as<double>();
   p.rows = rows.as<int>();
   p.nrows = (int)n;
+  p.n_steps = n_steps;
+  p.eD = rowf.as<double>();
+  p.phi1 = p.eD + 2 * n;
+  p.phi2 = p.eD + 4 * n;
+  p.kap = p.eD + 6 * n;
+  p.step = 0;
+  if (n_steps > 0) k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
   for (int64_t k = 0; k < n_steps; ++k) {
     p.step = k;
     p.x = X.as<double>();
@@ -1205,6 +1342,28 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cleanup();
   if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_integrate_const: %s", cudaGetErrorString(e));
+  return PB_OK;
+}
+
+int pb_eval_exp(pb_context* c, int64_t n, const double* x, double* y) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (n < 0 || (n > 0 && (!x || !y))) return fail(c, PB_ERR_ARG, "pb_eval_exp: bad arguments");
+  if (n == 0) return PB_OK;
+  int rc = set_device(c);
+  if (rc) return rc;
+  DBuf dx, dy;
+  if ((rc = upload(c, dx, x, (size_t)n))) return rc;
+  if (dy.ensure((size_t)n * sizeof(double)) != cudaSuccess) {
+    dx.release();
+    return fail(c, PB_ERR_CUDA, "pb_eval_exp: allocation failed");
+  }
+  k_eval_exp<<<blocks_for(n, 256), 256, 0, c->stream>>>(dx.as<double>(), dy.as<double>(), n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  dx.release();
+  dy.release();
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_eval_exp: %s", cudaGetErrorString(e));
   return PB_OK;
 }
 

@@ -29,6 +29,25 @@ def _solver(run, zi=1.0, **kw):
     return UHECRPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, **kw)
 
 
+# --- the device exp -------------------------------------------------------------
+def test_device_exp_is_correctly_rounded():
+    """Bit-exact against exp computed in 60-digit decimal arithmetic, and against
+    the host double-double form used by the oracle."""
+    from decimal import Decimal, getcontext
+    from oracle import crexp
+    from prince_b200 import _lib
+    getcontext().prec = 60
+    rng = np.random.default_rng(3)
+    xs = np.concatenate([-np.exp(rng.uniform(np.log(1e-9), np.log(745), 20000)),
+                         np.exp(rng.uniform(np.log(1e-9), np.log(709), 5000)),
+                         [0.0, 1e-6, -1e-6, 1e-3, -1e-3, -700.0, -745.2, 710.0]])
+    y = _lib.Context(0).eval_exp(xs)
+    exact = np.array([float(Decimal(float(x)).exp()) if -745.13 < x < 709.78 else np.exp(x) for x in xs])
+    normal = np.abs(exact) >= 2.2250738585072014e-308
+    assert np.array_equal(y[normal], exact[normal])
+    assert np.array_equal(y, crexp.exp(xs))
+
+
 # --- constant-operator known answers (tests/test_explicit_decay_analytics.py) ----
 def test_const_single_exponential():
     from prince_b200 import _lib
@@ -139,7 +158,7 @@ def test_medium_network_plain_vs_oracle(medium_run):
     s = _solver(run, zi=0.3)
     s.add_source_class(src)
     s.solve(dz=1e-3)
-    o = O.OracleSolver(run, 0.3, 0.0)
+    o = O.OracleSolver(run, 0.3, 0.0, exp="cr")
     ref = o.solve([src], dz=1e-3)
     assert rel_err_on_support(s.state, ref, _blocks(run)) < TOL
     ip, ix = s.operator_pattern()
@@ -158,7 +177,7 @@ def test_medium_network_batched_uneven_zmax_vs_oracle(medium_run):
     for k, s in enumerate(srcs):
         m[k].add_source_class(s)
     m.solve(dz=1e-3)
-    o = O.OracleSolver(run, 0.3, 0.0, K=K)
+    o = O.OracleSolver(run, 0.3, 0.0, K=K, exp="cr")
     ref = o.solve([[s] for s in srcs], dz=1e-3)
     assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
 
@@ -172,6 +191,6 @@ def test_full_network_short_range_vs_oracle():
     s = _solver(run, zi=0.05)
     s.add_source_class(src)
     s.solve(dz=1e-3)
-    o = O.OracleSolver(run, 0.05, 0.0)
+    o = O.OracleSolver(run, 0.05, 0.0, exp="cr")
     ref = o.solve([src], dz=1e-3)
     assert rel_err_on_support(s.state, ref, _blocks(run)) < TOL

@@ -100,3 +100,16 @@ def test_column_order_and_active_prefix():
     for k in range(0, sched.n_steps, 50):
         assert n_active[k] == np.sum(zmax_sorted >= zs[k])
     assert np.all(np.diff(src_col) >= 0)
+
+
+def test_host_correctly_rounded_exp():
+    """oracle.crexp agrees bit for bit with exp evaluated in 60-digit decimal arithmetic."""
+    from decimal import Decimal, getcontext
+    from oracle import crexp
+
+    getcontext().prec = 60
+    rng = np.random.default_rng(5)
+    xs = np.concatenate([-np.exp(rng.uniform(np.log(1e-9), np.log(708), 4000)),
+                         np.exp(rng.uniform(np.log(1e-9), np.log(709), 1000)), [0.0, 1e-6, -1e-6]])
+    exact = np.array([float(Decimal(float(x)).exp()) for x in xs])
+    assert np.array_equal(crexp.exp(xs), exact)
