@@ -9,7 +9,7 @@
  * Each entry point names the reference interface it replaces (paths inside
  * the PriNCe project).  The reference's ETD2 path is Python, so there is no
  * reference C ABI; the Python binding in prince_b200/_lib.py is the layer a
- * reference backend would call (see INTEGRATION.md).
+ * reference backend would call.
  *
  * Threading: a context is used by one host thread at a time; all device work
  * of a context runs on the context's own stream.
