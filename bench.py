@@ -146,7 +146,7 @@ def run_b200(args, dist, rank, ws, local):
 
     torch.cuda.set_device(local)
     run = network_run()
-    pts = draw_points(run, args.points, seed=1000 + rank)
+    pts = draw_points(run, args.points, seed=1000 + rank, z_range=args.z_range)
     zi = max(p["zmax"] for p in pts)
     solver = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=args.points, device=local)
     for k, p in enumerate(pts):
@@ -271,7 +271,10 @@ def main():
     ap.add_argument("--points", type=int, default=512)
     ap.add_argument("--plain", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--z-range", default="0.5,1.0",
+                    help="z_max range of the source points (smaller cases for profiling)")
     args = ap.parse_args()
+    args.z_range = tuple(float(v) for v in args.z_range.split(","))
 
     if args.impl == "reference":
         return reference_arm(args)
@@ -297,7 +300,7 @@ def reference_arm(args):
     from oracle import cpu_bench
 
     run = network_run()
-    pts = draw_points(run, args.points, seed=1000)
+    pts = draw_points(run, args.points, seed=1000, z_range=args.z_range)
     zi = max(p["zmax"] for p in pts)
     sched = make_schedule(z_grid(zi, 0.0, 1e-3), run.backend.update_rates_z_threshold)
     procs = min(os.cpu_count() or 1, 8)
