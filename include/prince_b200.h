@@ -163,6 +163,35 @@ int pb_integrate_const(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
                        const int64_t* indptr, const int32_t* indices, const double* values,
                        int64_t n_steps, const double* z_grid, double* state);
 
+/* Limits of the static scratch used by pb_integrate_const_noalloc. */
+#define PB_NOALLOC_MAX_STATES 65536
+#define PB_NOALLOC_MAX_STEPS 16384
+
+/* pb_integrate_const for callers that cannot allocate device memory: code
+ * running inside another framework's custom-call or FFI handler (which must
+ * use the buffers it is handed), hosts that reserved all device memory up
+ * front, and code that must not call cudaMalloc while a CUDA graph is being
+ * captured.  No counterpart in the reference (its solvers allocate freely).
+ *
+ * Every pointer is a DEVICE pointer owned by the caller: d (n), the CSR arrays
+ * of L_off (indptr may be NULL when nnz == 0), z_grid (n_steps + 1) and state
+ * (n, advanced in place).  The call allocates and frees nothing: its scratch
+ * (about 6 MB) is one static device array sized for at most
+ * PB_NOALLOC_MAX_STATES states and PB_NOALLOC_MAX_STEPS steps; larger sizes are
+ * rejected with PB_ERR_ARG.  Every GPU that loads the library holds that array
+ * until the process exits.
+ *
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress) and caches it; make that first call before any
+ * stream capture.  All calls share the one array and it keeps the last call's
+ * contents; each call rewrites every part it reads before reading it.  Calls
+ * whose work overlaps on the GPU (other contexts' streams, other host threads)
+ * race on the shared scratch and must be serialised by the caller.  Work runs
+ * on the context's stream; the call returns after it completes. */
+int pb_integrate_const_noalloc(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
+                               const int64_t* indptr, const int32_t* indices, const double* values,
+                               int64_t n_steps, const double* z_grid, double* state);
+
 /* The exp used by the device phi functions, evaluated on n values: a
  * correctly rounded double-double exp (same operation sequence as the host
  * form in oracle/crexp.py).  Replaces: the numpy exp of _compute_diag_factors

@@ -67,6 +67,8 @@ _PROTOS = {
     "pb_get_operator_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
     "pb_get_window": (C.c_int, [_vp, C.c_int32, _d, _d, _d]),
     "pb_integrate_const": (C.c_int, [_vp, C.c_int64, _d, C.c_int64, _i64, _i32, _d, C.c_int64, _d, _d]),
+    "pb_integrate_const_noalloc": (C.c_int, [_vp, C.c_int64, _vp, C.c_int64, _vp, _vp, _vp, C.c_int64, _vp,
+                                              _vp]),
     "pb_eval_exp": (C.c_int, [_vp, C.c_int64, _d, _d]),
     "pb_last_timing": (C.c_int, [_vp, _d, _d, _d, _i64]),
 }
@@ -268,6 +270,14 @@ class Context:
                                              _ptr(zg, C.c_double), _ptr(x, C.c_double))
         self._check(rc, "pb_integrate_const")
         return x
+
+    def integrate_const_noalloc(self, n, d_ptr, nnz, indptr_ptr, indices_ptr, values_ptr, n_steps, z_ptr,
+                                state_ptr):
+        """Allocation-free constant-operator integration; all pointers are device addresses (ints)."""
+        vp = lambda v: None if v is None else C.c_void_p(int(v))
+        self._check(self.lib.pb_integrate_const_noalloc(self.h, int(n), vp(d_ptr), int(nnz), vp(indptr_ptr),
+                                                        vp(indices_ptr), vp(values_ptr), int(n_steps), vp(z_ptr),
+                                                        vp(state_ptr)), "pb_integrate_const_noalloc")
 
     def eval_exp(self, x):
         """The device exp of the phi functions on ``x`` (float64 array)."""

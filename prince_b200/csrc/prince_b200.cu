@@ -31,6 +31,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -551,6 +552,34 @@ __device__ __forceinline__ void row_prep(const StepParams& p, int64_t step, int6
 __global__ void k_prep(StepParams p) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r < p.n) row_prep(p, p.step, r);
+}
+
+// ---------------------------------------------------------------------------
+// Scratch of pb_integrate_const_noalloc: one file-scope device array (every
+// GPU that loads the library holds it until exit).  Layout, in bytes from the
+// start: a and F(x) (n doubles each), the row factors (8 n doubles), the
+// per-step h and dl/dz (s doubles each), the window index (s ints), the row
+// list (n ints) and an all-zero row pointer (n + 1 int64), for n = the
+// state limit and s = the step limit.
+// ---------------------------------------------------------------------------
+constexpr int64_t kNaMaxStates = PB_NOALLOC_MAX_STATES;
+constexpr int64_t kNaMaxSteps = PB_NOALLOC_MAX_STEPS;
+constexpr size_t kNaBytes = (size_t)kNaMaxStates * 10 * sizeof(double) + (size_t)kNaMaxSteps * 2 * sizeof(double) +
+                            (size_t)kNaMaxSteps * sizeof(int) + (size_t)kNaMaxStates * sizeof(int) +
+                            (size_t)(kNaMaxStates + 1) * sizeof(int64_t);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+__global__ void k_noalloc_fill(int64_t n, int64_t n_steps, const double* __restrict__ z, double* __restrict__ h,
+                               double* __restrict__ ones, int* __restrict__ win, int* __restrict__ rows,
+                               int64_t* __restrict__ zero_indptr) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_steps) {
+    h[i] = __dadd_rn(z[i + 1], -z[i]);
+    ones[i] = 1.0;
+    win[i] = 0;
+  }
+  if (i < n) rows[i] = (int)i;
+  if (i <= n) zero_indptr[i] = 0;
 }
 
 // b(z) at (row r, column k): finj * sum_s coeff_s * g_s[r] (propagation.py:363-370, 2476-2488)
@@ -1342,6 +1371,94 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   cleanup();
   if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_integrate_const: %s", cudaGetErrorString(e));
+  return PB_OK;
+}
+
+// No-allocation variant of pb_integrate_const.  The scratch is the static
+// device array g_noalloc_scratch; its device address is looked up with
+// cudaGetSymbolAddress once per device (on that device's first call) and
+// cached.  Nothing here allocates or frees device memory.
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[64] = {nullptr};
+
+int pb_integrate_const_noalloc(pb_context* c, int64_t n, const double* d, int64_t nnz, const int64_t* indptr,
+                               const int32_t* indices, const double* values, int64_t n_steps,
+                               const double* z_grid, double* state) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (n <= 0 || n > kNaMaxStates)
+    return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: n = %lld outside [1, %lld] (static scratch limit)",
+                (long long)n, (long long)kNaMaxStates);
+  if (n_steps < 0 || n_steps > kNaMaxSteps)
+    return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: n_steps = %lld outside [0, %lld] (static scratch limit)",
+                (long long)n_steps, (long long)kNaMaxSteps);
+  if (!d || !z_grid || !state || nnz < 0 || (nnz > 0 && (!indptr || !indices || !values)))
+    return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: bad arguments");
+  if (c->device < 0 || c->device >= 64) return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: device id too large");
+  int rc = set_device(c);
+  if (rc) return rc;
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[c->device]) {
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr)
+        return fail(c, PB_ERR_CUDA, "pb_integrate_const_noalloc: cudaGetSymbolAddress failed: %s",
+                    cudaGetErrorString(e));
+      g_noalloc_addr[c->device] = ptr;
+    }
+    base = static_cast<unsigned char*>(g_noalloc_addr[c->device]);
+  }
+  double* a = reinterpret_cast<double*>(base);
+  double* f = a + kNaMaxStates;
+  double* rowf = f + kNaMaxStates;
+  double* h = rowf + 8 * kNaMaxStates;
+  double* ones = h + kNaMaxSteps;
+  int* win = reinterpret_cast<int*>(ones + kNaMaxSteps);
+  int* rows = win + kNaMaxSteps;
+  int64_t* zero_indptr = reinterpret_cast<int64_t*>(rows + kNaMaxStates);
+  cudaStream_t st = c->stream;
+  const int64_t fill = std::max<int64_t>(n + 1, n_steps);
+  k_noalloc_fill<<<blocks_for(fill, 256), 256, 0, st>>>(n, n_steps, z_grid, h, ones, win, rows, zero_indptr);
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  p.n = n;
+  p.ld = 1;
+  p.ncols = 1;
+  p.flags = PB_PHOTOHAD;
+  p.h = h;
+  p.dldz = ones;
+  p.hc = ones;
+  p.finj = ones;
+  p.win = win;
+  p.m_indptr = nnz > 0 ? indptr : zero_indptr;
+  p.m_indices = indices;
+  p.m_vals = values;
+  p.m_wstride = 0;
+  p.m_diag = d;
+  p.a = a;
+  p.f = f;
+  p.rows = rows;
+  p.nrows = (int)n;
+  p.n_steps = n_steps;
+  p.eD = rowf;
+  p.phi1 = rowf + 2 * n;
+  p.phi2 = rowf + 4 * n;
+  p.kap = rowf + 6 * n;
+  p.step = 0;
+  if (n_steps > 0) k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
+  for (int64_t k = 0; k < n_steps; ++k) {
+    p.step = k;
+    p.x = state;
+    p.xout = state;
+    p.src = state;
+    k_step_plain<1><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    p.src = a;
+    k_step_plain<2><<<blocks_for(n, 8), 256, 0, st>>>(p);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_integrate_const_noalloc: %s", cudaGetErrorString(e));
   return PB_OK;
 }
 
