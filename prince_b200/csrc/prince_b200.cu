@@ -40,9 +40,10 @@
 namespace {
 
 constexpr int kAbiVersion = 1;
-constexpr int kLongRow = 256;      // rows with more coupling entries get a whole CTA
+constexpr int kLongRow = 256;      // rows with more coupling entries are cut into segments
 constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
 constexpr int kColTile = 32;       // state columns per warp in the batched step
+constexpr int kSegLen = 256;       // coupling entries per long-row segment
 
 thread_local std::string g_error;
 
@@ -89,6 +90,9 @@ struct pb_context {
   DBuf cpl_indptr, cpl_indices, cpl_row, cpl_is_diag;
   std::vector<int32_t> h_short_rows, h_long_rows;
   DBuf short_rows, long_rows;
+  // long-row segments over the coupling entries
+  int32_t n_seg = 0;
+  DBuf seg_cb, seg_ce, seg_lr, lr_seg0, lr_nseg, seg_mb, seg_me, partial, counter;
   // fold kernel and photon grid
   DBuf kernel, eph;
   // photon field
@@ -273,6 +277,17 @@ __global__ void k_m_indptr(const int64_t* __restrict__ cpl_indptr, const int* __
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i > n) return;
   m_indptr[i] = pos[cpl_indptr[i]];
+}
+
+// M_off range of each long-row segment from its coupling-entry range: the
+// exclusive prefix count of kept entries maps coupling index -> M_off index.
+__global__ void k_seg_map(const int64_t* __restrict__ cb, const int64_t* __restrict__ ce,
+                          const int* __restrict__ pos, int nseg, int64_t* __restrict__ mb,
+                          int64_t* __restrict__ me) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseg) return;
+  mb[i] = pos[cb[i]];
+  me[i] = pos[ce[i]];
 }
 
 // ---------------------------------------------------------------------------
@@ -486,8 +501,20 @@ struct StepParams {
   double* a;          // stage 1 writes, stage 2 reads
   double* f;          // F(x): stage 1 writes, stage 2 reads
   double* xout;       // stage 2 writes
-  const int* rows;    // short or long row list
+  const int* rows;    // short rows
   int nrows;
+  int nsb;            // blocks of the launch that work on short rows
+  // long rows: segments of at most kSegLen coupling entries
+  const int* seg_lr;        // long-row index of each segment
+  const int64_t* seg_mb;    // M_off range of each segment
+  const int64_t* seg_me;
+  int nseg;
+  const int* lr_row;        // state row of each long row
+  const int* lr_seg0;       // first segment of each long row
+  const int* lr_nseg;       // number of segments of each long row
+  double* partial;          // nseg x ld partial sums
+  int* counter;             // finished segments per (long row, column tile)
+  int ctiles;               // column tiles per long row in `counter`
 };
 
 struct StepScalars {
@@ -644,110 +671,120 @@ __device__ __forceinline__ void prep_next(const StepParams& p, int64_t r) {
   if (p.step + 1 < p.n_steps) row_prep(p, p.step + 1, r);
 }
 
-// Single column: a warp per short row (lanes stride the row), a CTA per long row.
+// Long rows are cut into segments of at most kSegLen coupling entries.  A warp
+// sums one segment into `partial`; the last warp to finish a (row, column tile)
+// -- found with a fence and an atomic ticket, no waiting -- adds the row's
+// partials in segment order and runs the row epilogue.
+__device__ __forceinline__ bool last_of_row(const StepParams& p, int lr, int tile, int lane) {
+  __syncwarp();      // every lane's partial is written before lane 0 publishes the ticket
+  __threadfence();
+  int t = 0;
+  if (lane == 0) t = atomicAdd(&p.counter[(size_t)lr * p.ctiles + tile], 1);
+  t = __shfl_sync(0xffffffffu, t, 0);
+  const bool last = t == p.lr_nseg[lr] - 1;
+  if (last) {
+    __threadfence();
+    if (lane == 0) p.counter[(size_t)lr * p.ctiles + tile] = 0;  // ready for the next launch
+  }
+  return last;
+}
+
+// Single column.  Blocks [0, nsb): a warp per short row, lanes stride the row.
+// Blocks [nsb, ...): a warp per long-row segment.
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
   const StepScalars s = load_scalars(p, p.step);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double* __restrict__ v = p.src;
   const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
-  if (p.nrows < 0) {  // long rows: CTA per row
-    const int64_t r = p.rows[blockIdx.x];
+  if ((int)blockIdx.x < p.nsb) {
+    const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+    if (ri >= p.nrows) return;
+    const int64_t r = p.rows[ri];
     double acc = 0.0;
     if (s.photohad)
-      for (int64_t j = p.m_indptr[r] + threadIdx.x; j < p.m_indptr[r + 1]; j += blockDim.x)
-        acc += mv[j] * v[p.m_indices[j]];
-    __shared__ double red[8];
+      for (int64_t j = p.m_indptr[r] + lane; j < p.m_indptr[r + 1]; j += 32) acc += mv[j] * v[p.m_indices[j]];
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) red[wid] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
-      row_epilogue<STAGE>(p, s, r, 0, t);
+    if (lane == 0) {
+      row_epilogue<STAGE>(p, s, r, 0, acc);
       if (STAGE == 2) prep_next(p, r);
     }
     return;
   }
-  const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
-  if (ri >= p.nrows) return;
-  const int64_t r = p.rows[ri];
+  const int seg = (blockIdx.x - p.nsb) * (blockDim.x >> 5) + wid;
+  if (seg >= p.nseg) return;
   double acc = 0.0;
   if (s.photohad)
-    for (int64_t j = p.m_indptr[r] + lane; j < p.m_indptr[r + 1]; j += 32)
-      acc += mv[j] * v[p.m_indices[j]];
+    for (int64_t j = p.seg_mb[seg] + lane; j < p.seg_me[seg]; j += 32) acc += mv[j] * v[p.m_indices[j]];
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) p.partial[seg] = acc;
+  const int lr = p.seg_lr[seg];
+  if (!last_of_row(p, lr, 0, lane)) return;
   if (lane == 0) {
-    row_epilogue<STAGE>(p, s, r, 0, acc);
+    const int s0 = p.lr_seg0[lr], ns = p.lr_nseg[lr];
+    double t = 0.0;
+    for (int q = 0; q < ns; ++q) t += __ldcg(p.partial + s0 + q);
+    const int64_t r = p.lr_row[lr];
+    row_epilogue<STAGE>(p, s, r, 0, t);
     if (STAGE == 2) prep_next(p, r);
   }
 }
 
-// Many columns: lane = column inside a 32-column tile (blockIdx.y); the row's
-// (value, column) pairs are loaded 32 at a time and broadcast by shuffles, so
-// every gathered state row is one coalesced 256-byte load.  A lane sums its
-// column in CSR order without contraction (the order of a CSR sparse x dense
-// product on the host).
+// Sum of M_off[j] * v[col_j, kk] over j in [j0, j1) for one column per lane:
+// the (value, column) pairs are loaded 32 at a time and broadcast by shuffles,
+// so each gathered state row is one coalesced 256-byte load; the lane adds in
+// CSR order without contraction (the order of a CSR sparse x dense product).
+__device__ __forceinline__ double gather_sum(const double* __restrict__ mv, const int* __restrict__ idx,
+                                             const double* __restrict__ v, int ld, int kk, int64_t j0,
+                                             int64_t j1, int lane) {
+  double acc = 0.0;
+  for (int64_t base = j0; base < j1; base += 32) {
+    const int64_t j = base + lane;
+    const double mvl = (j < j1) ? mv[j] : 0.0;
+    const int cl = (j < j1) ? idx[j] : 0;
+    const int cnt = (int)min((int64_t)32, j1 - base);
+#pragma unroll 4
+    for (int q = 0; q < cnt; ++q) {
+      const double mq = __shfl_sync(0xffffffffu, mvl, q);
+      const int cq = __shfl_sync(0xffffffffu, cl, q);
+      acc = __dadd_rn(acc, __dmul_rn(mq, v[(size_t)cq * ld + kk]));
+    }
+  }
+  return acc;
+}
+
+// Many columns: lane = column inside a 32-column tile (blockIdx.y).  Blocks
+// [0, nsb): a warp per short row; blocks [nsb, ...): a warp per long-row segment.
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
   const StepScalars s = load_scalars(p, p.step);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int k = blockIdx.y * kColTile + lane;
   const bool active = k < p.ncols;
+  const int kk = active ? k : 0;
   const double* __restrict__ v = p.src;
   const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
-  const int kk = active ? k : 0;
-  if (p.nrows < 0) {  // long rows: the CTA's warps split the row
-    const int64_t r = p.rows[blockIdx.x];
-    double acc = 0.0;
-    if (s.photohad) {
-      const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
-      const int64_t len = j1 - j0;
-      const int nw = blockDim.x >> 5;
-      const int64_t chunk = (len + nw - 1) / nw;
-      const int64_t a0 = j0 + wid * chunk, a1 = min(j1, a0 + chunk);
-      for (int64_t base = a0; base < a1; base += 32) {
-        const int64_t j = base + lane;
-        const double mvl = (j < a1) ? mv[j] : 0.0;
-        const int cl = (j < a1) ? p.m_indices[j] : 0;
-        const int cnt = (int)min((int64_t)32, a1 - base);
-        for (int q = 0; q < cnt; ++q) {
-          const double mq = __shfl_sync(0xffffffffu, mvl, q);
-          const int cq = __shfl_sync(0xffffffffu, cl, q);
-          acc = __dadd_rn(acc, __dmul_rn(mq, v[(size_t)cq * p.ld + kk]));
-        }
-      }
-    }
-    __shared__ double red[8][32];
-    red[wid][lane] = acc;
-    __syncthreads();
-    if (wid == 0) {
-      double t = 0.0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t = __dadd_rn(t, red[i][lane]);
-      if (active) row_epilogue<STAGE>(p, s, r, k, t);
-      if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
-    }
+  if ((int)blockIdx.x < p.nsb) {
+    const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+    if (ri >= p.nrows) return;
+    const int64_t r = p.rows[ri];
+    const double acc = s.photohad ? gather_sum(mv, p.m_indices, v, p.ld, kk, p.m_indptr[r], p.m_indptr[r + 1], lane)
+                                  : 0.0;
+    if (active) row_epilogue<STAGE>(p, s, r, k, acc);
+    if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
     return;
   }
-  const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
-  if (ri >= p.nrows) return;
-  const int64_t r = p.rows[ri];
-  double acc = 0.0;
-  if (s.photohad) {
-    const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
-    for (int64_t base = j0; base < j1; base += 32) {
-      const int64_t j = base + lane;
-      const double mvl = (j < j1) ? mv[j] : 0.0;
-      const int cl = (j < j1) ? p.m_indices[j] : 0;
-      const int cnt = (int)min((int64_t)32, j1 - base);
-      for (int q = 0; q < cnt; ++q) {
-        const double mq = __shfl_sync(0xffffffffu, mvl, q);
-        const int cq = __shfl_sync(0xffffffffu, cl, q);
-        acc = __dadd_rn(acc, __dmul_rn(mq, v[(size_t)cq * p.ld + kk]));
-      }
-    }
-  }
-  if (active) row_epilogue<STAGE>(p, s, r, k, acc);
+  const int seg = (blockIdx.x - p.nsb) * (blockDim.x >> 5) + wid;
+  if (seg >= p.nseg) return;
+  const double acc = s.photohad ? gather_sum(mv, p.m_indices, v, p.ld, kk, p.seg_mb[seg], p.seg_me[seg], lane) : 0.0;
+  p.partial[(size_t)seg * p.ld + blockIdx.y * kColTile + lane] = acc;
+  const int lr = p.seg_lr[seg];
+  if (!last_of_row(p, lr, blockIdx.y, lane)) return;
+  const int s0 = p.lr_seg0[lr], ns = p.lr_nseg[lr];
+  double t = 0.0;
+  for (int q = 0; q < ns; ++q) t = __dadd_rn(t, __ldcg(p.partial + (size_t)(s0 + q) * p.ld + blockIdx.y * kColTile + lane));
+  const int64_t r = p.lr_row[lr];
+  if (active) row_epilogue<STAGE>(p, s, r, k, t);
   if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
 }
 
@@ -841,7 +878,8 @@ void pb_destroy(pb_context* c) {
                   &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos,
                   &c->dest, &c->m_indptr, &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h,
                   &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff, &c->X, &c->A, &c->F,
-                  &c->rowf, &c->scan_tmp};
+                  &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0,
+                  &c->lr_nseg, &c->seg_mb, &c->seg_me, &c->partial, &c->counter};
   for (DBuf* b : bufs) b->release();
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
@@ -879,8 +917,26 @@ int pb_set_coupling(pb_context* c, int64_t n, int64_t R, const int64_t* indptr, 
   c->h_short_rows.clear();
   c->h_long_rows.clear();
   for (int64_t i = 0; i < n; ++i) (indptr[i + 1] - indptr[i] > kLongRow ? c->h_long_rows : c->h_short_rows).push_back((int)i);
+  std::vector<int64_t> scb, sce;
+  std::vector<int32_t> slr, l0, ln;
+  for (size_t lr = 0; lr < c->h_long_rows.size(); ++lr) {
+    const int r = c->h_long_rows[lr];
+    l0.push_back((int32_t)scb.size());
+    for (int64_t j = indptr[r]; j < indptr[r + 1]; j += kSegLen) {
+      scb.push_back(j);
+      sce.push_back(std::min<int64_t>(j + kSegLen, indptr[r + 1]));
+      slr.push_back((int32_t)lr);
+    }
+    ln.push_back((int32_t)scb.size() - l0.back());
+  }
+  c->n_seg = (int32_t)scb.size();
   if ((rc = upload(c, c->short_rows, c->h_short_rows.data(), c->h_short_rows.size()))) return rc;
   if ((rc = upload(c, c->long_rows, c->h_long_rows.data(), c->h_long_rows.size()))) return rc;
+  if ((rc = upload(c, c->seg_cb, scb.data(), scb.size()))) return rc;
+  if ((rc = upload(c, c->seg_ce, sce.data(), sce.size()))) return rc;
+  if ((rc = upload(c, c->seg_lr, slr.data(), slr.size()))) return rc;
+  if ((rc = upload(c, c->lr_seg0, l0.data(), l0.size()))) return rc;
+  if ((rc = upload(c, c->lr_nseg, ln.data(), ln.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_coupling = true;
   c->have_kernel = false;
@@ -1090,6 +1146,12 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->A.ensure(sbytes));
   PB_CUDA(c, c->F.ensure(sbytes));
   PB_CUDA(c, c->rowf.ensure((size_t)8 * n * sizeof(double)));
+  const int ctiles = ld / (K == 1 ? 1 : kColTile);
+  const int nlong_rows = (int)c->h_long_rows.size();
+  PB_CUDA(c, c->seg_mb.ensure((size_t)std::max(c->n_seg, 1) * sizeof(int64_t)));
+  PB_CUDA(c, c->seg_me.ensure((size_t)std::max(c->n_seg, 1) * sizeof(int64_t)));
+  PB_CUDA(c, c->partial.ensure((size_t)std::max(c->n_seg, 1) * ld * sizeof(double)));
+  PB_CUDA(c, c->counter.ensure((size_t)std::max(nlong_rows, 1) * ctiles * sizeof(int)));
   size_t scan_need = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
@@ -1126,6 +1188,12 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
                                                   c->m_indices.as<int>());
     k_m_indptr<<<blocks_for(n + 1, 256), 256, 0, st>>>(c->cpl_indptr.as<int64_t>(), c->pos.as<int>(), n,
                                                        c->m_indptr.as<int64_t>());
+    if (c->n_seg > 0) {
+      k_seg_map<<<blocks_for(c->n_seg, 256), 256, 0, st>>>(c->seg_cb.as<int64_t>(), c->seg_ce.as<int64_t>(),
+                                                           c->pos.as<int>(), c->n_seg, c->seg_mb.as<int64_t>(),
+                                                           c->seg_me.as<int64_t>());
+      ++launches;
+    }
     const int kpad = (c->dph + 3) / 4 * 4;
     const size_t smem = (size_t)(kFoldBM + kFoldBN) * (kpad + 4) * sizeof(double);
     k_fold_gemm<<<dim3(blocks_for(R, kFoldBM), blocks_for(W, kFoldBN)), 256, smem, st>>>(
@@ -1134,7 +1202,12 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     launches += 5;
   } else {
     PB_CUDA(c, cudaMemsetAsync(c->m_indptr.p, 0, ((size_t)n + 1) * sizeof(int64_t), st));
+    if (c->n_seg > 0) {
+      PB_CUDA(c, cudaMemsetAsync(c->seg_mb.p, 0, (size_t)c->n_seg * sizeof(int64_t), st));
+      PB_CUDA(c, cudaMemsetAsync(c->seg_me.p, 0, (size_t)c->n_seg * sizeof(int64_t), st));
+    }
   }
+  PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max(nlong_rows, 1) * ctiles * sizeof(int), st));
   PB_CUDA(c, cudaGetLastError());
 
   // ---- ETD2 steps ---------------------------------------------------------
@@ -1193,7 +1266,19 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   p.phi1 = p.eD + 2 * n;
   p.phi2 = p.eD + 4 * n;
   p.kap = p.eD + 6 * n;
-  const int nshort = (int)c->h_short_rows.size(), nlong = (int)c->h_long_rows.size();
+  p.rows = c->short_rows.as<int>();
+  p.nrows = (int)c->h_short_rows.size();
+  p.nsb = (int)blocks_for(p.nrows, 8);
+  p.seg_lr = c->seg_lr.as<int>();
+  p.seg_mb = c->seg_mb.as<int64_t>();
+  p.seg_me = c->seg_me.as<int64_t>();
+  p.nseg = c->n_seg;
+  p.lr_row = c->long_rows.as<int>();
+  p.lr_seg0 = c->lr_seg0.as<int>();
+  p.lr_nseg = c->lr_nseg.as<int>();
+  p.partial = c->partial.as<double>();
+  p.counter = c->counter.as<int>();
+  p.ctiles = ctiles;
   PB_CUDA(c, cudaEventRecord(c->ev2, st));
   bool prepared = false;
   for (int64_t k = 0; k < S; ++k) {
@@ -1213,28 +1298,13 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
       p.x = X;
       p.xout = X;
       const unsigned tiles = K == 1 ? 1u : blocks_for(p.ncols, kColTile);
-      if (nshort > 0) {
-        p.rows = c->short_rows.as<int>();
-        p.nrows = nshort;
-        dim3 grid(blocks_for(nshort, 8), tiles);
-        if (K == 1) {
-          if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
-        } else {
-          if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
-        }
-        ++launches;
+      dim3 grid((unsigned)p.nsb + blocks_for(p.nseg, 8), tiles);
+      if (K == 1) {
+        if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
+      } else {
+        if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
       }
-      if (nlong > 0) {
-        p.rows = c->long_rows.as<int>();
-        p.nrows = -1;
-        dim3 grid(nlong, tiles);
-        if (K == 1) {
-          if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
-        } else {
-          if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
-        }
-        ++launches;
-      }
+      ++launches;
     }
   }
   PB_CUDA(c, cudaGetLastError());
@@ -1350,6 +1420,7 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   p.f = F.as<double>();
   p.rows = rows.as<int>();
   p.nrows = (int)n;
+  p.nsb = (int)blocks_for(n, 8);
   p.n_steps = n_steps;
   p.eD = rowf.as<double>();
   p.phi1 = p.eD + 2 * n;
@@ -1440,6 +1511,7 @@ int pb_integrate_const_noalloc(pb_context* c, int64_t n, const double* d, int64_
   p.f = f;
   p.rows = rows;
   p.nrows = (int)n;
+  p.nsb = (int)blocks_for(n, 8);
   p.n_steps = n_steps;
   p.eD = rowf;
   p.phi1 = rowf + 2 * n;
