@@ -30,6 +30,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -121,6 +122,11 @@ struct pb_context {
   size_t scan_tmp_bytes = 0;
   int32_t last_W = 0;
   bool have_solution = false;
+
+  // CUDA graph of the last solve's device work and the shape it was captured for
+  cudaGraphExec_t graph_exec = nullptr;
+  std::vector<uint64_t> graph_key;
+  int64_t graph_launches = 0;
 
   // timing
   float last_solve_ms = 0.f, last_device_ms = 0.f, last_steps_ms = 0.f;
@@ -689,8 +695,9 @@ __device__ __forceinline__ bool last_of_row(const StepParams& p, int lr, int til
   return last;
 }
 
-// Single column.  Blocks [0, nsb): a warp per short row, lanes stride the row.
-// Blocks [nsb, ...): a warp per long-row segment.
+// Single column.  Blocks [0, nsb): a thread per short row, summing the row in
+// CSR order without contraction (as the host CSR product does).  Blocks
+// [nsb, ...): a warp per long-row segment.
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
   const StepScalars s = load_scalars(p, p.step);
@@ -698,17 +705,17 @@ __global__ void __launch_bounds__(256) k_step_plain(StepParams p) {
   const double* __restrict__ v = p.src;
   const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
   if ((int)blockIdx.x < p.nsb) {
-    const int64_t ri = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+    const int64_t ri = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= p.nrows) return;
     const int64_t r = p.rows[ri];
     double acc = 0.0;
-    if (s.photohad)
-      for (int64_t j = p.m_indptr[r] + lane; j < p.m_indptr[r + 1]; j += 32) acc += mv[j] * v[p.m_indices[j]];
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
-      row_epilogue<STAGE>(p, s, r, 0, acc);
-      if (STAGE == 2) prep_next(p, r);
+    if (s.photohad) {
+      const int64_t j1 = p.m_indptr[r + 1];
+#pragma unroll 4
+      for (int64_t j = p.m_indptr[r]; j < j1; ++j) acc = __dadd_rn(acc, __dmul_rn(mv[j], v[p.m_indices[j]]));
     }
+    row_epilogue<STAGE>(p, s, r, 0, acc);
+    if (STAGE == 2) prep_next(p, r);
     return;
   }
   const int seg = (blockIdx.x - p.nsb) * (blockDim.x >> 5) + wid;
@@ -809,6 +816,7 @@ int set_device(pb_context* c) {
 
 FieldDesc field_desc(const pb_context* c, double scale) {
   FieldDesc f;
+  memset(&f, 0, sizeof(f));  // padding bytes take part in the graph key
   f.n = c->n_comp;
   for (int i = 0; i < 8; ++i) {
     f.kind[i] = i < c->n_comp ? c->comp_kind[i] : 0;
@@ -816,6 +824,16 @@ FieldDesc field_desc(const pb_context* c, double scale) {
   }
   f.scale = scale;
   return f;
+}
+
+std::vector<DBuf*> all_buffers(pb_context* c) {
+  return {&c->cpl_indptr, &c->cpl_indices, &c->cpl_row, &c->cpl_is_diag, &c->short_rows, &c->long_rows, &c->kernel,
+          &c->eph, &c->d_indptr, &c->d_indices, &c->d_vals, &c->d_diag, &c->adia_E, &c->pair_scale, &c->pair_bin,
+          &c->xi, &c->phi_xi2, &c->pair_pg, &c->l_diag, &c->l_indptr, &c->l_indices, &c->l_vals, &c->inj_slot,
+          &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos, &c->dest, &c->m_indptr,
+          &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h, &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff,
+          &c->X, &c->A, &c->F, &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0, &c->lr_nseg,
+          &c->seg_mb, &c->seg_me, &c->partial, &c->counter};
 }
 
 unsigned blocks_for(int64_t work, int per_block) {
@@ -871,16 +889,8 @@ void pb_destroy(pb_context* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  DBuf* bufs[] = {&c->cpl_indptr, &c->cpl_indices, &c->cpl_row, &c->cpl_is_diag, &c->short_rows,
-                  &c->long_rows, &c->kernel, &c->eph, &c->d_indptr, &c->d_indices, &c->d_vals,
-                  &c->d_diag, &c->adia_E, &c->pair_scale, &c->pair_bin, &c->xi, &c->phi_xi2,
-                  &c->pair_pg, &c->l_diag, &c->l_indptr, &c->l_indices, &c->l_vals, &c->inj_slot,
-                  &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos,
-                  &c->dest, &c->m_indptr, &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h,
-                  &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff, &c->X, &c->A, &c->F,
-                  &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0,
-                  &c->lr_nseg, &c->seg_mb, &c->seg_me, &c->partial, &c->counter};
-  for (DBuf* b : bufs) b->release();
+  for (DBuf* b : all_buffers(c)) b->release();
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaEventDestroy(c->ev2);
@@ -1156,8 +1166,24 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
 
+  double* X = c->X.as<double>();
+  if (a->init_state) {
+    if (a->state_on_device) {
+      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
+                                   cudaMemcpyDeviceToDevice, st));
+    } else {
+      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
+                                   cudaMemcpyHostToDevice, st));
+    }
+  } else {
+    PB_CUDA(c, cudaMemsetAsync(X, 0, sbytes, st));
+  }
   const FieldDesc fd = field_desc(c, a->photon_scale);
   int64_t launches = 0;
+  // Everything from here to the end of the last step is enqueued by `enqueue`:
+  // directly, or under stream capture into a CUDA graph that is replayed while
+  // the solve's shape and buffers stay the same.
+  auto enqueue = [&](int64_t& launches) -> int {
   PB_CUDA(c, cudaEventRecord(c->ev0, st));
 
   // ---- photon matrix and pair-loss vectors for every window ---------------
@@ -1211,18 +1237,6 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, cudaGetLastError());
 
   // ---- ETD2 steps ---------------------------------------------------------
-  double* X = c->X.as<double>();
-  if (a->init_state) {
-    if (a->state_on_device) {
-      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
-                                   cudaMemcpyDeviceToDevice, st));
-    } else {
-      PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
-                                   cudaMemcpyHostToDevice, st));
-    }
-  } else {
-    PB_CUDA(c, cudaMemsetAsync(X, 0, sbytes, st));
-  }
   StepParams p;
   memset(&p, 0, sizeof(p));
   p.n = n;
@@ -1268,7 +1282,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   p.kap = p.eD + 6 * n;
   p.rows = c->short_rows.as<int>();
   p.nrows = (int)c->h_short_rows.size();
-  p.nsb = (int)blocks_for(p.nrows, 8);
+  p.nsb = (int)blocks_for(p.nrows, K == 1 ? 256 : 8);   // thread per row (K = 1) or warp per row
   p.seg_lr = c->seg_lr.as<int>();
   p.seg_mb = c->seg_mb.as<int64_t>();
   p.seg_me = c->seg_me.as<int64_t>();
@@ -1309,6 +1323,46 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   }
   PB_CUDA(c, cudaGetLastError());
   PB_CUDA(c, cudaEventRecord(c->ev3, st));
+    return PB_OK;
+  };
+
+  std::vector<uint64_t> key;
+  {
+    auto put = [&](uint64_t v) { key.push_back(v); };
+    put((uint64_t)S); put((uint64_t)W); put((uint64_t)K); put((uint64_t)ld); put(flags); put(inj); put(R);
+    put((uint64_t)c->n_seg); put((uint64_t)c->h_short_rows.size()); put((uint64_t)c->n_cr_bins);
+    const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);
+    for (size_t i = 0; i < sizeof(fd); i += 8) { uint64_t w = 0; memcpy(&w, fb + i, std::min<size_t>(8, sizeof(fd) - i)); put(w); }
+    for (const DBuf* b : all_buffers(c)) put((uint64_t)(uintptr_t)b->p);
+    for (int64_t k = 0; k < S; ++k) put((uint64_t)a->n_active[k]);
+  }
+  static const bool no_graph = getenv("PRINCE_B200_NO_GRAPH") != nullptr;
+  if (no_graph) {
+    if ((rc = enqueue(launches))) return rc;
+  } else {
+    if (!c->graph_exec || c->graph_key != key) {
+      if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+      }
+      PB_CUDA(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      const int rc2 = enqueue(launches);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(st, &g);
+      if (rc2) {
+        if (g) cudaGraphDestroy(g);
+        return rc2;
+      }
+      PB_CUDA(c, e);
+      const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, g, 0);
+      cudaGraphDestroy(g);
+      PB_CUDA(c, ei);
+      c->graph_key = key;
+      c->graph_launches = launches;
+    }
+    PB_CUDA(c, cudaGraphLaunch(c->graph_exec, st));
+    launches = c->graph_launches;
+  }
   if (a->state_on_device) {
     PB_CUDA(c, cudaMemcpy2DAsync(a->state, K * sizeof(double), X, ld * sizeof(double), K * sizeof(double), n,
                                  cudaMemcpyDeviceToDevice, st));
@@ -1420,7 +1474,7 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
   p.f = F.as<double>();
   p.rows = rows.as<int>();
   p.nrows = (int)n;
-  p.nsb = (int)blocks_for(n, 8);
+  p.nsb = (int)blocks_for(n, 256);
   p.n_steps = n_steps;
   p.eD = rowf.as<double>();
   p.phi1 = p.eD + 2 * n;
@@ -1433,9 +1487,9 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
     p.x = X.as<double>();
     p.xout = X.as<double>();
     p.src = X.as<double>();
-    k_step_plain<1><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    k_step_plain<1><<<blocks_for(n, 256), 256, 0, st>>>(p);
     p.src = A.as<double>();
-    k_step_plain<2><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    k_step_plain<2><<<blocks_for(n, 256), 256, 0, st>>>(p);
   }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(state, X.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -1511,7 +1565,7 @@ int pb_integrate_const_noalloc(pb_context* c, int64_t n, const double* d, int64_
   p.f = f;
   p.rows = rows;
   p.nrows = (int)n;
-  p.nsb = (int)blocks_for(n, 8);
+  p.nsb = (int)blocks_for(n, 256);
   p.n_steps = n_steps;
   p.eD = rowf;
   p.phi1 = rowf + 2 * n;
@@ -1524,9 +1578,9 @@ int pb_integrate_const_noalloc(pb_context* c, int64_t n, const double* d, int64_
     p.x = state;
     p.xout = state;
     p.src = state;
-    k_step_plain<1><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    k_step_plain<1><<<blocks_for(n, 256), 256, 0, st>>>(p);
     p.src = a;
-    k_step_plain<2><<<blocks_for(n, 8), 256, 0, st>>>(p);
+    k_step_plain<2><<<blocks_for(n, 256), 256, 0, st>>>(p);
   }
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
