@@ -124,7 +124,7 @@ struct pb_context {
   bool have_solution = false;
 
   // CUDA graph of the last solve's device work and the shape it was captured for
-  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphExec_t graph_exec = nullptr, graph_exec2 = nullptr;
   std::vector<uint64_t> graph_key;
   int64_t graph_launches = 0;
 
@@ -891,6 +891,7 @@ void pb_destroy(pb_context* c) {
   cudaStreamSynchronize(c->stream);
   for (DBuf* b : all_buffers(c)) b->release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph_exec2) cudaGraphExecDestroy(c->graph_exec2);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   cudaEventDestroy(c->ev2);
@@ -1183,8 +1184,9 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   // Everything from here to the end of the last step is enqueued by `enqueue`:
   // directly, or under stream capture into a CUDA graph that is replayed while
   // the solve's shape and buffers stay the same.
+  StepParams p;
+  memset(&p, 0, sizeof(p));
   auto enqueue = [&](int64_t& launches) -> int {
-  PB_CUDA(c, cudaEventRecord(c->ev0, st));
 
   // ---- photon matrix and pair-loss vectors for every window ---------------
   k_photon_matrix<<<blocks_for((int64_t)W * c->dph, 256), 256, 0, st>>>(fd, c->eph.as<double>(), c->dph,
@@ -1237,8 +1239,6 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, cudaGetLastError());
 
   // ---- ETD2 steps ---------------------------------------------------------
-  StepParams p;
-  memset(&p, 0, sizeof(p));
   p.n = n;
   p.ld = ld;
   p.flags = flags;
@@ -1293,7 +1293,9 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   p.partial = c->partial.as<double>();
   p.counter = c->counter.as<int>();
   p.ctiles = ctiles;
-  PB_CUDA(c, cudaEventRecord(c->ev2, st));
+    return PB_OK;
+  };
+  auto enqueue_steps = [&](int64_t& launches) -> int {
   bool prepared = false;
   for (int64_t k = 0; k < S; ++k) {
     p.step = k;
@@ -1322,7 +1324,6 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     }
   }
   PB_CUDA(c, cudaGetLastError());
-  PB_CUDA(c, cudaEventRecord(c->ev3, st));
     return PB_OK;
   };
 
@@ -1336,31 +1337,45 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     for (const DBuf* b : all_buffers(c)) put((uint64_t)(uintptr_t)b->p);
     for (int64_t k = 0; k < S; ++k) put((uint64_t)a->n_active[k]);
   }
+  // Two graphs -- the per-solve operator set-up and the step loop -- with the
+  // timing events recorded on the stream between them.
   static const bool no_graph = getenv("PRINCE_B200_NO_GRAPH") != nullptr;
   if (no_graph) {
+    PB_CUDA(c, cudaEventRecord(c->ev0, st));
     if ((rc = enqueue(launches))) return rc;
+    PB_CUDA(c, cudaEventRecord(c->ev2, st));
+    if ((rc = enqueue_steps(launches))) return rc;
+    PB_CUDA(c, cudaEventRecord(c->ev3, st));
   } else {
-    if (!c->graph_exec || c->graph_key != key) {
-      if (c->graph_exec) {
-        cudaGraphExecDestroy(c->graph_exec);
-        c->graph_exec = nullptr;
+    if (!c->graph_exec || !c->graph_exec2 || c->graph_key != key) {
+      for (cudaGraphExec_t* ge : {&c->graph_exec, &c->graph_exec2})
+        if (*ge) {
+          cudaGraphExecDestroy(*ge);
+          *ge = nullptr;
+        }
+      int64_t l1 = 0, l2 = 0;
+      for (int part = 0; part < 2; ++part) {
+        PB_CUDA(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const int rc2 = part == 0 ? enqueue(l1) : enqueue_steps(l2);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc2) {
+          if (g) cudaGraphDestroy(g);
+          return rc2;
+        }
+        PB_CUDA(c, e);
+        const cudaError_t ei = cudaGraphInstantiate(part == 0 ? &c->graph_exec : &c->graph_exec2, g, 0);
+        cudaGraphDestroy(g);
+        PB_CUDA(c, ei);
       }
-      PB_CUDA(c, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      const int rc2 = enqueue(launches);
-      cudaGraph_t g = nullptr;
-      const cudaError_t e = cudaStreamEndCapture(st, &g);
-      if (rc2) {
-        if (g) cudaGraphDestroy(g);
-        return rc2;
-      }
-      PB_CUDA(c, e);
-      const cudaError_t ei = cudaGraphInstantiate(&c->graph_exec, g, 0);
-      cudaGraphDestroy(g);
-      PB_CUDA(c, ei);
       c->graph_key = key;
-      c->graph_launches = launches;
+      c->graph_launches = l1 + l2;
     }
+    PB_CUDA(c, cudaEventRecord(c->ev0, st));
     PB_CUDA(c, cudaGraphLaunch(c->graph_exec, st));
+    PB_CUDA(c, cudaEventRecord(c->ev2, st));
+    PB_CUDA(c, cudaGraphLaunch(c->graph_exec2, st));
+    PB_CUDA(c, cudaEventRecord(c->ev3, st));
     launches = c->graph_launches;
   }
   if (a->state_on_device) {
@@ -1372,9 +1387,9 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   }
   PB_CUDA(c, cudaEventRecord(c->ev1, st));
   PB_CUDA(c, cudaStreamSynchronize(st));
-  cudaEventElapsedTime(&c->last_solve_ms, c->ev0, c->ev1);
-  cudaEventElapsedTime(&c->last_device_ms, c->ev0, c->ev3);
-  cudaEventElapsedTime(&c->last_steps_ms, c->ev2, c->ev3);
+  PB_CUDA(c, cudaEventElapsedTime(&c->last_solve_ms, c->ev0, c->ev1));
+  PB_CUDA(c, cudaEventElapsedTime(&c->last_device_ms, c->ev0, c->ev3));
+  PB_CUDA(c, cudaEventElapsedTime(&c->last_steps_ms, c->ev2, c->ev3));
   c->last_launches = launches;
   c->last_W = W;
   c->have_solution = true;
