@@ -141,9 +141,25 @@ typedef struct pb_solve_args {
                               init_state != 0), out = state at the final redshift  */
   int32_t init_state;      /* 0: start from zeros                                    */
   int32_t state_on_device; /* 1: `state` is a device pointer                         */
+  int32_t ckpt_every;      /* > 0: keep the state every this many steps for pb_adjoint */
 } pb_solve_args;
 
 int pb_solve(pb_context* ctx, const pb_solve_args* args);
+
+/* Discrete adjoint of the last solve: gradients of L = sum(seed * x_final) with
+ * respect to the injection grids (n_rows x n_src, as passed to pb_set_injection),
+ * the per-step source coefficients (n_steps x n_src) and the photon scale
+ * (one value per column; the scale enters both the rate fold and kappa_pair).
+ * `args` must be the arguments of that solve, which must have set ckpt_every:
+ * the state is recomputed from the checkpoints segment by segment and the
+ * ETD2 step is reversed with the transposed operator
+ * (A^T = dl/dz (M_off^T + diag(kappa) D_off^T + Lambda_off^T)).  Any gradient
+ * pointer may be NULL (no scale gradient: no scale recording).
+ * Replaces: finite differences of the reference solver (no adjoint exists in
+ * the reference; the forward it differentiates is etd2.py:412-439 with
+ * propagation.py:1360-1508). */
+int pb_adjoint(pb_context* ctx, const pb_solve_args* args, const double* seed, int32_t seed_on_device,
+               double* grad_grids, double* grad_coeff, double* grad_scale);
 
 /* Inspection after a solve: the off-diagonal operator pattern built from the
  * first window (split_operator + eliminate_zeros, src/prince_cr/solvers/etd2.py:234-268).

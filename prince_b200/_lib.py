@@ -45,6 +45,7 @@ class SolveArgs(C.Structure):
         ("state", _d),
         ("init_state", C.c_int32),
         ("state_on_device", C.c_int32),
+        ("ckpt_every", C.c_int32),
     ]
 
 
@@ -64,6 +65,7 @@ _PROTOS = {
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
     "pb_set_injection": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _d, C.c_int32, _i32]),
     "pb_solve": (C.c_int, [_vp, C.POINTER(SolveArgs)]),
+    "pb_adjoint": (C.c_int, [_vp, C.POINTER(SolveArgs), _d, C.c_int32, _d, _d, _d]),
     "pb_get_operator_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
     "pb_get_window": (C.c_int, [_vp, C.c_int32, _d, _d, _d]),
     "pb_integrate_const": (C.c_int, [_vp, C.c_int64, _d, C.c_int64, _i64, _i32, _d, C.c_int64, _d, _d]),

@@ -1,0 +1,242 @@
+"""Differentiable batched propagation: a ``torch.autograd.Function`` over the C ABI.
+
+``PropagateFunction.apply(G, coeff, scale, plan)`` propagates K columns and
+returns the z = 0 states ``X`` (n x K).  Its backward runs the device adjoint
+(``pb_adjoint``: checkpointed recomputation, the ETD2 step reversed with the
+transposed operator) and returns gradients for
+
+* ``G``      -- injection grids on the injected state rows (n_rows x n_src),
+* ``coeff``  -- per-step source coefficients norm * evolution(z_k) (n_steps x n_src),
+* ``scale``  -- the photon-density scale shared by the rate fold and the
+  Bethe-Heitler loss (a 0-d tensor).
+
+``SourceBatch`` builds ``G`` and ``coeff`` from per-point parameters with torch
+operations (spectral index, log10 rigidity cutoff, five composition fractions,
+evolution index), so ``torch.autograd`` carries the gradient back to them.
+``group_flux`` is the all-particle flux on the common total-energy grid of
+``UHECRPropagationResult.get_solution_group`` (``propagation.py:135-167``),
+written with torch operations so a flux loss can be differentiated.
+
+The reference has no adjoint; its gradient is obtained by differencing the
+forward solver.  The forward here is the same device solve as
+``MultiRHSPropagationSolverETD2``.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import constants as C
+from .data import EnergyGrid
+from .photonfields import device_components
+from .schedule import make_schedule, z_grid
+from .solvers import DeviceRun
+
+FLAGS_ALL = (_lib.PB_ADIABATIC | _lib.PB_PAIRPROD | _lib.PB_PHOTOHAD | _lib.PB_INJECTION
+             | _lib.PB_PARTIAL_DIFF)
+
+
+class Plan:
+    """Fixed part of a differentiable solve: run, schedule, injected rows, column order."""
+
+    def __init__(self, run, initial_z, n_cols, rows, src_col, first_active, dz=1e-3, device=0,
+                 ckpt_every=32, flags=FLAGS_ALL):
+        self.run = run
+        self.dev = DeviceRun.of(run, device)
+        self.sched = make_schedule(z_grid(initial_z, 0.0, dz), run.backend.update_rates_z_threshold)
+        self.K = int(n_cols)
+        self.rows = np.asarray(rows, dtype=np.int32)
+        self.src_col = np.asarray(src_col, dtype=np.int64)       # user column of each source
+        self.ckpt_every = int(ckpt_every)
+        self.flags = int(flags)
+        first = np.asarray(first_active, dtype=np.int64)         # first active step per user column
+        self.perm = np.argsort(first, kind="stable")             # device column j <- user column perm[j]
+        self.inv = np.empty(self.K, dtype=np.int64)
+        self.inv[self.perm] = np.arange(self.K)
+        self.n_active = np.searchsorted(np.sort(first), np.arange(self.sched.n_steps), side="right").astype(np.int32)
+        self.src_order = np.argsort(self.inv[self.src_col], kind="stable")
+        self.dev_src_col = self.inv[self.src_col][self.src_order].astype(np.int32)
+        self.last_args = None
+
+
+class PropagateFunction(torch.autograd.Function):
+    """X(z=0) = propagate(G, coeff, scale) with a device adjoint as backward."""
+
+    @staticmethod
+    def forward(ctx, G, coeff, scale, plan):
+        ctx_dev = plan.dev.ctx
+        Gd = G.detach().cpu().numpy()[:, plan.src_order]
+        cd = coeff.detach().cpu().numpy()[:, plan.src_order]
+        ctx_dev.set_injection(plan.rows, np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
+        ctx_dev.set_photon_field(device_components(plan.run.photon_field))
+        out = np.zeros((plan.run.dim_states, plan.K))
+        s = float(scale.detach().cpu().item())
+        plan.last_args = (np.ascontiguousarray(cd), s)
+        _solve(ctx_dev, plan, cd, out, s)
+        X = np.empty_like(out)
+        X[:, plan.perm] = out
+        ctx.plan = plan
+        return torch.from_numpy(X).to(G.device)
+
+    @staticmethod
+    def backward(ctx, grad_X):
+        plan = ctx.plan
+        seed = np.ascontiguousarray(grad_X.detach().cpu().numpy()[:, plan.perm], dtype=np.float64)
+        cd, s = plan.last_args
+        gG, gc, gs = _adjoint(plan.dev.ctx, plan, cd, s, seed)
+        gG_user = np.empty_like(gG)
+        gG_user[:, plan.src_order] = gG
+        gc_user = np.empty_like(gc)
+        gc_user[:, plan.src_order] = gc
+        dev = grad_X.device
+        return (torch.from_numpy(gG_user).to(dev), torch.from_numpy(gc_user).to(dev),
+                torch.tensor(float(gs.sum()), dtype=torch.float64, device=dev), None)
+
+
+def _args(plan, coeff, scale, state):
+    import ctypes as Cc
+
+    keep = []
+
+    def f(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return a.ctypes.data_as(Cc.POINTER(Cc.c_double))
+
+    def i(a):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        keep.append(a)
+        return a.ctypes.data_as(Cc.POINTER(Cc.c_int32))
+
+    sc = plan.sched
+    args = _lib.SolveArgs()
+    args.n_steps = sc.n_steps
+    args.n_windows = len(sc.z_window)
+    args.n_cols = plan.K
+    args.flags = plan.flags
+    args.photon_scale = float(scale)
+    args.z_window = f(sc.z_window)
+    args.window = i(sc.window)
+    args.h = f(sc.h)
+    args.dldz = f(sc.dldz)
+    args.hc = f(sc.hc)
+    args.finj = f(sc.finj)
+    args.coeff = f(coeff)
+    args.n_active = i(plan.n_active)
+    args.state = state.ctypes.data_as(Cc.POINTER(Cc.c_double))
+    args.init_state = 0
+    args.state_on_device = 0
+    args.ckpt_every = plan.ckpt_every
+    return args, keep
+
+
+def _solve(ctx, plan, coeff, out, scale):
+    import ctypes as Cc
+
+    args, keep = _args(plan, coeff, scale, out)
+    ctx._check(ctx.lib.pb_solve(ctx.h, Cc.byref(args)), "pb_solve")
+
+
+def _adjoint(ctx, plan, coeff, scale, seed):
+    import ctypes as Cc
+
+    dummy = np.zeros((plan.run.dim_states, plan.K))
+    args, keep = _args(plan, coeff, scale, dummy)
+    n_src = plan.dev_src_col.size
+    gG = np.zeros((plan.rows.size, n_src))
+    gc = np.zeros((plan.sched.n_steps, n_src))
+    gs = np.zeros(plan.K)
+    P = lambda a: a.ctypes.data_as(Cc.POINTER(Cc.c_double))
+    ctx._check(ctx.lib.pb_adjoint(ctx.h, Cc.byref(args), P(seed), 0, P(gG), P(gc), P(gs)), "pb_adjoint")
+    return gG, gc, gs
+
+
+class SourceBatch:
+    """K rigidity-cutoff sources as torch functions of their parameters.
+
+    Per point: ``gamma`` (spectral index), ``lg_rmax`` (log10 R_max / V),
+    ``frac`` (composition weights of ``species``), ``m`` (evolution (1+z)^m),
+    ``z_max`` (fixed, not differentiated).  The spectrum of species (A, Z) on
+    the per-nucleon grid E is ``f A (A E / 1 GeV)^-gamma exp(1 - A E/(Z R_max))``
+    -- ``RigdityCutoffSource`` (``cr_sources.py:182-198``).
+    """
+
+    def __init__(self, run, species, z_max, initial_z, dz=1e-3):
+        self.run = run
+        self.species = [int(p) for p in species]
+        self.z_max = np.asarray(z_max, dtype=np.float64)
+        sm = run.spec_man
+        self.rows = np.concatenate([np.arange(sm.pdgid2sref[p].lidx(), sm.pdgid2sref[p].uidx())
+                                    for p in self.species]).astype(np.int32)
+        E = run.cr_grid.grid
+        self.E = torch.tensor(np.tile(E, len(self.species)), dtype=torch.float64)
+        self.A = torch.tensor(np.repeat([float(sm.pdgid2sref[p].A) for p in self.species], E.size),
+                              dtype=torch.float64)
+        self.Z = torch.tensor(np.repeat([float(sm.pdgid2sref[p].Z) for p in self.species], E.size),
+                              dtype=torch.float64)
+        self.sidx = torch.tensor(np.repeat(np.arange(len(self.species)), E.size))
+        zg = z_grid(initial_z, 0.0, dz)
+        self.zs = torch.tensor(zg[:-1], dtype=torch.float64)
+        K = self.z_max.size
+        live = zg[:-1][:, None] <= self.z_max[None, :]
+        self.live = torch.tensor(live.astype(np.float64))
+        self.first_active = np.array([np.flatnonzero(live[:, k])[0] if live[:, k].any() else zg.size - 1
+                                      for k in range(K)])
+
+    def grids(self, gamma, lg_rmax, frac):
+        """G (n_rows x K) from per-point tensors gamma (K), lg_rmax (K), frac (K x n_species)."""
+        ek = self.A[:, None] * self.E[:, None]
+        rmax = 10.0 ** lg_rmax
+        f = frac.t()[self.sidx]                                   # (rows, K)
+        return f * self.A[:, None] * (ek / 1e9) ** (-gamma[None, :]) * torch.exp(
+            1.0 - ek / (self.Z[:, None] * rmax[None, :]))
+
+    def coefficients(self, m, norm=1.0):
+        """coeff (n_steps x K): norm (1+z_k)^m where z_k <= z_max, else 0."""
+        return norm * (1.0 + self.zs[:, None]) ** m[None, :] * self.live
+
+    def plan(self, initial_z, dz=1e-3, device=0, ckpt_every=32):
+        K = self.z_max.size
+        return Plan(self.run, initial_z, K, self.rows, np.arange(K), self.first_active, dz=dz,
+                    device=device, ckpt_every=ckpt_every)
+
+
+def group_flux(run, X, egrid=None):
+    """All-particle flux of the nuclei on the common total-energy grid (torch, differentiable).
+
+    Per species: total energy A E_i, spectrum state / A, log-log interpolated to
+    the common grid ``EnergyGrid(lo, hi + log10 A_max, 4 bins/decade-multiple)``
+    and summed (``propagation.py:103-167``).  Non-positive states are floored at
+    1e-300 before the logarithm.
+    """
+    sm = run.spec_man
+    cr = run.cr_grid
+    nuclei = [s for s in sm.species_refs if s.is_nucleus]
+    if egrid is None:
+        step = np.log10(cr.grid[1] / cr.grid[0])
+        lo = np.log10(cr.bins[0])
+        hi = np.log10(cr.bins[-1]) + np.log10(max(s.A for s in nuclei))
+        egrid = EnergyGrid(lo, hi, 4.0 / step).grid
+    lge = np.log(egrid)
+    total = torch.zeros((egrid.size, X.shape[1]), dtype=X.dtype, device=X.device)
+    for s in nuclei:
+        le = np.log(s.A * cr.grid)
+        j = np.clip(np.searchsorted(le, lge) - 1, 0, le.size - 2)
+        w = (lge - le[j]) / (le[j + 1] - le[j])
+        inside = (lge >= le[0]) & (lge <= le[-1])
+        y = torch.clamp(X[s.lidx():s.uidx()] / s.A, min=1e-300)
+        ly = torch.log(y)
+        jt = torch.tensor(j, device=X.device)
+        wt = torch.tensor(w, dtype=X.dtype, device=X.device)[:, None]
+        val = torch.exp((1 - wt) * ly[jt] + wt * ly[jt + 1])
+        total = total + val * torch.tensor(inside.astype(np.float64), dtype=X.dtype, device=X.device)[:, None]
+    return torch.tensor(egrid, dtype=X.dtype, device=X.device), total
+
+
+def log_ratio_loss(run, X, target, e_min=10 ** 9.5):
+    """sum over bins with E > e_min of ln(F_k(E) / T(E))^2, per column (K)."""
+    egrid, F = group_flux(run, X)
+    sel = egrid > e_min
+    return ((torch.log(F[sel]) - torch.log(target[sel, None])) ** 2).sum(dim=0)

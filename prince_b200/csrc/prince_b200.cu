@@ -123,6 +123,17 @@ struct pb_context {
   int32_t last_W = 0;
   bool have_solution = false;
 
+  // transposed constant operators (adjoint)
+  DBuf dt_indptr, dt_indices, dt_vals, lt_indptr, lt_indices, lt_vals;
+  DBuf inj_rows, src_col_d, nact;
+  // checkpoints of the last solve and adjoint work buffers
+  DBuf ckpt, lam, lam2, mu, rec_rf, rec_P, rec_Q, rec_sx, dsig, gb_inj, gs, g_out;
+  DBuf erow, tkeys, tvals, skeys, svals, t_indptr, t_indices, t_perm, sort_tmp;
+  int32_t last_ckpt = 0, last_K = 0;
+  int64_t last_S = 0;
+  uint32_t last_flags = 0;
+  double last_scale = 1.0;
+
   // CUDA graph of the last solve's device work and the shape it was captured for
   cudaGraphExec_t graph_exec = nullptr, graph_exec2 = nullptr;
   std::vector<uint64_t> graph_key;
@@ -521,6 +532,17 @@ struct StepParams {
   double* partial;          // nseg x ld partial sums
   int* counter;             // finished segments per (long row, column tile)
   int ctiles;               // column tiles per long row in `counter`
+  // recording for the adjoint (all null in a plain solve)
+  double inv_scale;         // 1 / photon scale
+  double* dsig;             // [2][n] d(d)/d(scale)
+  double* dphi1;            // [2][n] phi1'(h d)
+  double* dphi2;            // [2][n] phi2'(h d)
+  double* rec_rf;           // [rec_len][4][n]: eD, phi1, phi2, kappa of each recorded step
+  double* rec_P;            // [rec_len][n x ld]
+  double* rec_Q;            // [rec_len][n x ld]
+  double* rec_sx;           // n x ld: S x of the current step (stage 1 -> stage 2)
+  int64_t rec_k0;
+  int rec_len;
 };
 
 struct StepScalars {
@@ -563,6 +585,27 @@ __device__ __forceinline__ void phi_of(double h, double d, double& eD, double& p
   }
 }
 
+// phi1'(w) = (e^w - phi1)/w and phi2'(w) = (phi1 - 2 phi2)/w; for |w| < 0.1 their
+// power series sum_n (n+1) w^n/(n+2)! and sum_n (n+1) w^n/(n+3)! (13 terms).
+__device__ __forceinline__ void dphi_of(double w, double e, double f1, double f2, double& d1, double& d2) {
+  if (fabs(w) < 0.1) {
+    double a = 0.0, b = 0.0;
+    double fact2 = 6227020800.0;     // 13!
+    double fact3 = 87178291200.0;    // 14!
+    for (int n = 12; n >= 0; --n) {  // Horner from the top
+      a = a * w + (n + 1) / fact2;
+      b = b * w + (n + 1) / fact3;
+      fact2 /= (n + 2);
+      fact3 /= (n + 3);
+    }
+    d1 = a;
+    d2 = b;
+  } else {
+    d1 = (e - f1) / w;
+    d2 = (f1 - 2.0 * f2) / w;
+  }
+}
+
 // kappa (propagation.py:1393-1401) and d = dldz (M_diag + kappa D_diag [+ Lambda_diag])
 // (propagation.py:1408-1422) of row r at `step`, then its phi factors.
 __device__ __forceinline__ void row_prep(const StepParams& p, int64_t step, int64_t r) {
@@ -580,6 +623,27 @@ __device__ __forceinline__ void row_prep(const StepParams& p, int64_t step, int6
   p.phi1[o] = f1;
   p.phi2[o] = f2;
   p.kap[o] = k;
+  if (p.dsig) {  // derivatives with respect to the photon scale (adjoint record pass)
+    const double md = p.m_diag[(size_t)s.w * p.n + r] * p.inv_scale;
+    double ds = md;
+    if (s.kap && s.pair) ds += (p.kp[(size_t)s.w * p.n + r] * p.inv_scale) * p.d_diag[r];
+    ds *= s.dl;
+    double d1, d2;
+    dphi_of(s.h * d, e, f1, f2, d1, d2);
+    p.dsig[o] = ds;
+    p.dphi1[o] = d1;
+    p.dphi2[o] = d2;
+  }
+  if (p.rec_rf) {
+    const int64_t j = step - p.rec_k0;
+    if (j >= 0 && j < p.rec_len) {
+      double* rf = p.rec_rf + (size_t)j * 4 * p.n;
+      rf[r] = e;
+      rf[p.n + r] = f1;
+      rf[2 * p.n + r] = f2;
+      rf[3 * p.n + r] = k;
+    }
+  }
 }
 
 __global__ void k_prep(StepParams p) {
@@ -654,12 +718,50 @@ __device__ __forceinline__ double finish_F(const StepParams& p, const StepScalar
   return out;
 }
 
+// S v = (1/scale) dl/dz (M_off v + D_off (kappa_pair v)): the derivative of the
+// operator with respect to the photon scale applied to v, from the M_off sum.
+__device__ __forceinline__ double scale_deriv_apply(const StepParams& p, const StepScalars& s, int64_t r, int k,
+                                                    const double* __restrict__ v, double sM) {
+  double out = sM;
+  if (s.kap && s.pair) {
+    const double* kp = p.kp + (size_t)s.w * p.n;
+    double sD = 0.0;
+    for (int64_t j = p.d_indptr[r]; j < p.d_indptr[r + 1]; ++j) {
+      const int c = p.d_indices[j];
+      sD += p.d_vals[j] * (kp[c] * v[(size_t)c * p.ld + k]);
+    }
+    out += sD;
+  }
+  return out * s.dl * p.inv_scale;
+}
+
+template <int STAGE>
+__device__ __forceinline__ void record(const StepParams& p, const StepScalars& s, int64_t r, int k, double sM,
+                                       double F) {
+  const size_t o = (size_t)(p.step & 1) * p.n + r;
+  const size_t idx = (size_t)r * p.ld + k;
+  const int64_t j = p.step - p.rec_k0;
+  if (j < 0 || j >= p.rec_len) return;
+  const size_t ro = (size_t)j * p.n * p.ld + idx;
+  const double h = s.h, ds = p.dsig[o];
+  if (STAGE == 1) {
+    const double Sx = scale_deriv_apply(p, s, r, k, p.src, s.photohad ? sM : 0.0);
+    p.rec_sx[idx] = Sx;
+    p.rec_P[ro] = p.eD[o] * h * ds * p.x[idx] + h * h * p.dphi1[o] * ds * F + h * p.phi1[o] * Sx;
+  } else {
+    const double Sa = scale_deriv_apply(p, s, r, k, p.src, s.photohad ? sM : 0.0);
+    const double dF = F - p.f[idx];
+    p.rec_Q[ro] = h * h * p.dphi2[o] * ds * dF + h * p.phi2[o] * (Sa - p.rec_sx[idx]);
+  }
+}
+
 template <int STAGE>
 __device__ __forceinline__ void row_epilogue(const StepParams& p, const StepScalars& s, int64_t r,
                                              int k, double sM) {
   const size_t o = (size_t)(p.step & 1) * p.n + r;
   const size_t idx = (size_t)r * p.ld + k;
   const double F = finish_F(p, s, r, k, p.src, sM);
+  if (p.rec_P) record<STAGE>(p, s, r, k, sM, F);
   if (STAGE == 1) {
     // a = eD x + (phi1 F(x)) h  (etd2.py:427-430)
     const double a = __dadd_rn(__dmul_rn(p.eD[o], p.x[idx]), __dmul_rn(__dmul_rn(p.phi1[o], F), s.h));
@@ -796,6 +898,178 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// Discrete adjoint of the ETD2 step.  Forward, with A = dl (M_off + D_off diag(kappa)
+// + Lambda_off) frozen over the step:
+//   a = E x + h Phi1 (A x + b),   x' = a + h Phi2 A (a - x).
+// Backward, given lam' = dL/dx':
+//   mu  = lam' + h A^T (Phi2 lam')                    (stage 1; dL/da)
+//   lam = E mu + h A^T (Phi1 mu - Phi2 lam')          (stage 2; dL/dx)
+//   dL/db = h Phi1 mu,
+//   dL/dscale += mu . P + lam' . Q with the recorded P = d a / d scale and
+//   Q = h d(Phi2)/d scale A(a - x) + h Phi2 (dA/d scale)(a - x).
+// A^T = dl (M_off^T + diag(kappa) D_off^T + Lambda_off^T).
+// ---------------------------------------------------------------------------
+struct AdjParams {
+  int64_t n;
+  int ld;
+  int ncols;
+  int64_t step;
+  uint32_t flags;
+  double h, dl;
+  int w;
+  const int64_t* t_indptr;  // M_off^T pattern (rows = columns of M_off)
+  const int* t_indices;
+  const int* t_perm;        // entry of M_off behind each M_off^T entry
+  const double* m_vals;     // window w values of M_off
+  const int64_t* dt_indptr;
+  const int* dt_indices;
+  const double* dt_vals;
+  const int64_t* lt_indptr;
+  const int* lt_indices;
+  const double* lt_vals;
+  const double* rf;         // recorded eD, phi1, phi2, kappa of this step (n each)
+  const double* P;          // recorded sigma vectors of this step or null
+  const double* Q;
+  const double* lam;        // dL/dx'
+  double* mu;               // dL/da
+  double* lam_out;          // dL/dx
+  const int* inj_slot;
+  double* gb_inj;           // n_inj x ld: dL/db of this step on the injected rows, or null
+  double* gs;               // n x ld accumulator of the scale gradient, or null
+};
+
+template <int STAGE>
+__device__ __forceinline__ double adj_v(const AdjParams& a, int c, int k) {
+  const size_t i = (size_t)c * a.ld + k;
+  if (STAGE == 1) return a.rf[2 * a.n + c] * a.lam[i];
+  return a.rf[a.n + c] * a.mu[i] - a.rf[2 * a.n + c] * a.lam[i];
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_adj(AdjParams a) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+  if (r >= a.n) return;
+  const int k = blockIdx.y * kColTile + lane;
+  const bool active = k < a.ncols;
+  const int kk = active ? k : 0;
+  double sM = 0.0;
+  if (a.flags & PB_PHOTOHAD) {
+    const int64_t j0 = a.t_indptr[r], j1 = a.t_indptr[r + 1];
+    for (int64_t base = j0; base < j1; base += 32) {
+      const int64_t j = base + lane;
+      const double mvl = (j < j1) ? a.m_vals[a.t_perm[j]] : 0.0;
+      const int cl = (j < j1) ? a.t_indices[j] : 0;
+      const int cnt = (int)min((int64_t)32, j1 - base);
+      for (int q = 0; q < cnt; ++q) {
+        const double mq = __shfl_sync(0xffffffffu, mvl, q);
+        const int cq = __shfl_sync(0xffffffffu, cl, q);
+        sM += mq * adj_v<STAGE>(a, cq, kk);
+      }
+    }
+  }
+  if (!active) return;
+  double out = sM;
+  if (a.flags & PB_PARTIAL_DIFF) {
+    double sD = 0.0;
+    for (int64_t j = a.dt_indptr[r]; j < a.dt_indptr[r + 1]; ++j) sD += a.dt_vals[j] * adj_v<STAGE>(a, a.dt_indices[j], k);
+    out += a.rf[3 * a.n + r] * sD;
+  }
+  if ((a.flags & PB_DECAY) && a.lt_indptr) {
+    double sL = 0.0;
+    for (int64_t j = a.lt_indptr[r]; j < a.lt_indptr[r + 1]; ++j) sL += a.lt_vals[j] * adj_v<STAGE>(a, a.lt_indices[j], k);
+    out += sL;
+  }
+  out *= a.dl;
+  const size_t idx = (size_t)r * a.ld + k;
+  if (STAGE == 1) {
+    const double mu = a.lam[idx] + a.h * out;
+    a.mu[idx] = mu;
+    if (a.gb_inj) {
+      const int slot = a.inj_slot[r];
+      if (slot >= 0) a.gb_inj[(size_t)slot * a.ld + k] = a.h * a.rf[a.n + r] * mu;
+    }
+    if (a.gs) a.gs[idx] += mu * a.P[idx] + a.lam[idx] * a.Q[idx];
+  } else {
+    a.lam_out[idx] = a.rf[r] * a.mu[idx] + a.h * out;
+  }
+}
+
+// transpose of the M_off pattern: row of every entry, sentinel keys past nnz
+__global__ void k_entry_rows(const int64_t* __restrict__ indptr, int64_t n, int* __restrict__ row) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  if (r >= n) return;
+  for (int64_t j = indptr[r] + (threadIdx.x & 31); j < indptr[r + 1]; j += 32) row[j] = (int)r;
+}
+
+__global__ void k_transpose_keys(const int* __restrict__ indices, const int64_t* __restrict__ indptr, int64_t n,
+                                 int64_t R, int* __restrict__ keys, int* __restrict__ vals) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= R) return;
+  const int64_t nnz = indptr[n];
+  keys[j] = j < nnz ? indices[j] : (int)n;
+  vals[j] = (int)j;
+}
+
+__global__ void k_transpose_finish(const int* __restrict__ skeys, const int* __restrict__ svals,
+                                   const int* __restrict__ erow, int64_t n, int64_t R, int64_t* __restrict__ t_indptr,
+                                   int* __restrict__ t_indices, int* __restrict__ t_perm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i <= n) {  // t_indptr[c] = first sorted position with key >= c
+    int64_t lo = 0, hi = R;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) / 2;
+      if (skeys[mid] < (int)i) lo = mid + 1; else hi = mid;
+    }
+    t_indptr[i] = lo;
+  }
+  if (i < R && skeys[i] < (int)n) {
+    t_perm[i] = svals[i];
+    t_indices[i] = erow[svals[i]];
+  }
+}
+
+// dL/dcoeff[k][s] = finj_k sum_slot G[slot][s] dL/db_k[row(slot)][col(s)] (active steps)
+__global__ void k_grad_coeff(const double* __restrict__ gb, const double* __restrict__ G,
+                             const double* __restrict__ finj, const int* __restrict__ src_col,
+                             const int* __restrict__ n_active, int64_t S, int n_src, int n_inj, int ld,
+                             double* __restrict__ gcoeff) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S * n_src) return;
+  const int64_t k = i / n_src;
+  const int s = (int)(i % n_src), col = src_col[s];
+  double acc = 0.0;
+  if (col < n_active[k]) {
+    const double* g = gb + (size_t)k * n_inj * ld;
+    for (int q = 0; q < n_inj; ++q) acc += G[(size_t)q * n_src + s] * g[(size_t)q * ld + col];
+    acc *= finj[k];
+  }
+  gcoeff[i] = acc;
+}
+
+// dL/dG[slot][s] = sum_k finj_k coeff[k][s] dL/db_k[row(slot)][col(s)] (active steps)
+__global__ void k_grad_grids(const double* __restrict__ gb, const double* __restrict__ coeff,
+                             const double* __restrict__ finj, const int* __restrict__ src_col,
+                             const int* __restrict__ n_active, int64_t S, int n_src, int n_inj, int ld,
+                             double* __restrict__ gG) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n_inj * n_src) return;
+  const int q = (int)(i / n_src), s = (int)(i % n_src), col = src_col[s];
+  double acc = 0.0;
+  for (int64_t k = 0; k < S; ++k)
+    if (col < n_active[k]) acc += finj[k] * coeff[(size_t)k * n_src + s] * gb[((size_t)k * n_inj + q) * ld + col];
+  gG[i] = acc;
+}
+
+__global__ void k_grad_scale(const double* __restrict__ gs, int64_t n, int ld, int K, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  double acc = 0.0;
+  for (int64_t r = 0; r < n; ++r) acc += gs[(size_t)r * ld + k];
+  out[k] = acc;
+}
+
+// ---------------------------------------------------------------------------
 // host helpers
 // ---------------------------------------------------------------------------
 template <class T>
@@ -833,11 +1107,133 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->inj_G, &c->src_ptr, &c->PT, &c->zwin, &c->rs, &c->kp, &c->keep, &c->pos, &c->dest, &c->m_indptr,
           &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h, &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff,
           &c->X, &c->A, &c->F, &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0, &c->lr_nseg,
-          &c->seg_mb, &c->seg_me, &c->partial, &c->counter};
+          &c->seg_mb, &c->seg_me, &c->partial, &c->counter, &c->dt_indptr, &c->dt_indices, &c->dt_vals,
+          &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->nact, &c->ckpt, &c->lam,
+          &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj, &c->gs, &c->g_out,
+          &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
+          &c->sort_tmp};
+}
+
+// Stable CSR transpose (entries of a transposed row keep increasing column order).
+void csr_transpose(int64_t n, int64_t nnz, const int64_t* ip, const int32_t* ix, const double* v,
+                   std::vector<int64_t>& tip, std::vector<int32_t>& tix, std::vector<double>& tv) {
+  tip.assign((size_t)n + 1, 0);
+  for (int64_t j = 0; j < nnz; ++j) tip[(size_t)ix[j] + 1]++;
+  for (int64_t i = 0; i < n; ++i) tip[i + 1] += tip[i];
+  std::vector<int64_t> fill(tip.begin(), tip.end() - 1);
+  tix.assign((size_t)std::max<int64_t>(nnz, 1), 0);
+  tv.assign((size_t)std::max<int64_t>(nnz, 1), 0.0);
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+      const int64_t t = fill[ix[j]]++;
+      tix[t] = (int32_t)r;
+      tv[t] = v[j];
+    }
 }
 
 unsigned blocks_for(int64_t work, int per_block) {
   return (unsigned)((work + per_block - 1) / per_block);
+}
+
+
+// Step parameters of a solve on the context's device buffers.
+void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flags, bool pair, bool inj, int64_t S,
+                      int ctiles) {
+  const int64_t n = c->n;
+  const int64_t mstride = std::max<int64_t>(c->R, 1);
+  p.n = n;
+  p.ld = ld;
+  p.flags = flags;
+  if (!pair) p.flags &= ~PB_PAIRPROD;
+  if (!inj) p.flags &= ~PB_INJECTION;
+  p.h = c->s_h.as<double>();
+  p.dldz = c->s_dldz.as<double>();
+  p.hc = c->s_hc.as<double>();
+  p.finj = c->s_finj.as<double>();
+  p.win = c->s_win.as<int>();
+  p.m_indptr = c->m_indptr.as<int64_t>();
+  p.m_indices = c->m_indices.as<int>();
+  p.m_vals = c->m_vals.as<double>();
+  p.m_wstride = mstride;
+  p.m_diag = c->m_diag.as<double>();
+  p.d_indptr = c->d_indptr.as<int64_t>();
+  p.d_indices = c->d_indices.as<int>();
+  p.d_vals = c->d_vals.as<double>();
+  p.d_diag = c->d_diag.as<double>();
+  p.E = c->adia_E.as<double>();
+  p.kp = pair ? c->kp.as<double>() : nullptr;
+  if ((flags & PB_DECAY) && c->have_decay) {
+    p.l_indptr = c->l_indptr.as<int64_t>();
+    p.l_indices = c->l_indices.as<int>();
+    p.l_vals = c->l_vals.as<double>();
+    p.l_diag = c->l_diag.as<double>();
+  }
+  if (inj) {
+    p.inj_slot = c->inj_slot.as<int>();
+    p.G = c->inj_G.as<double>();
+    p.n_src = c->n_src;
+    p.src_ptr = c->src_ptr.as<int>();
+    p.coeff = c->s_coeff.as<double>();
+  }
+  p.a = c->A.as<double>();
+  p.f = c->F.as<double>();
+  p.n_steps = S;
+  p.eD = c->rowf.as<double>();
+  p.phi1 = p.eD + 2 * n;
+  p.phi2 = p.eD + 4 * n;
+  p.kap = p.eD + 6 * n;
+  p.rows = c->short_rows.as<int>();
+  p.nrows = (int)c->h_short_rows.size();
+  p.nsb = (int)blocks_for(p.nrows, K == 1 ? 256 : 8);   // thread per row (K = 1) or warp per row
+  p.seg_lr = c->seg_lr.as<int>();
+  p.seg_mb = c->seg_mb.as<int64_t>();
+  p.seg_me = c->seg_me.as<int64_t>();
+  p.nseg = c->n_seg;
+  p.lr_row = c->long_rows.as<int>();
+  p.lr_seg0 = c->lr_seg0.as<int>();
+  p.lr_nseg = c->lr_nseg.as<int>();
+  p.partial = c->partial.as<double>();
+  p.counter = c->counter.as<int>();
+  p.ctiles = ctiles;
+}
+
+// Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
+// advanced at step k; a step without active columns is skipped (every column
+// is still exactly zero).  With `ckpt`, the state before every step k with
+// k % every == 0 is copied to checkpoint k / every.  Returns the kernel count.
+int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_active, int64_t k0, int64_t k1,
+                     cudaStream_t st, double* ckpt, int every) {
+  const int64_t n = c->n;
+  double* X = c->X.as<double>();
+  const size_t sbytes = (size_t)n * p.ld * sizeof(double);
+  int64_t launches = 0;
+  bool prepared = false;
+  for (int64_t k = k0; k < k1; ++k) {
+    if (ckpt && every > 0 && k % every == 0)
+      cudaMemcpyAsync(ckpt + (size_t)(k / every) * n * p.ld, X, sbytes, cudaMemcpyDeviceToDevice, st);
+    p.step = k;
+    p.ncols = n_active[k];
+    if (p.ncols == 0) continue;
+    if (!prepared) {  // row factors of the first active step; later steps get them from stage 2
+      k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
+      ++launches;
+      prepared = true;
+    }
+    for (int stage = 1; stage <= 2; ++stage) {
+      p.src = stage == 1 ? X : c->A.as<double>();
+      p.x = X;
+      p.xout = X;
+      const unsigned tiles = K == 1 ? 1u : blocks_for(p.ncols, kColTile);
+      dim3 grid((unsigned)p.nsb + blocks_for(p.nseg, 8), tiles);
+      if (K == 1) {
+        if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
+      } else {
+        if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
+      }
+      ++launches;
+    }
+  }
+  return launches;
 }
 
 }  // namespace
@@ -1014,6 +1410,16 @@ int pb_set_fd_operator(pb_context* c, int64_t nnz, const int64_t* indptr, const 
   if ((rc = upload(c, c->d_indices, indices, (size_t)nnz))) return rc;
   if ((rc = upload(c, c->d_vals, values, (size_t)nnz))) return rc;
   if ((rc = upload(c, c->d_diag, diag, (size_t)c->n))) return rc;
+  {
+    std::vector<int64_t> tip;
+    std::vector<int32_t> tix;
+    std::vector<double> tv;
+    csr_transpose(c->n, nnz, indptr, indices, values, tip, tix, tv);
+    if ((rc = upload(c, c->dt_indptr, tip.data(), tip.size()))) return rc;
+    if ((rc = upload(c, c->dt_indices, tix.data(), tix.size()))) return rc;
+    if ((rc = upload(c, c->dt_vals, tv.data(), tv.size()))) return rc;
+    PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->nnzD = nnz;
   c->have_fd = true;
@@ -1065,6 +1471,16 @@ int pb_set_decay(pb_context* c, const double* diag, int64_t nnz, const int64_t* 
   if ((rc = upload(c, c->l_indptr, indptr, (size_t)c->n + 1))) return rc;
   if ((rc = upload(c, c->l_indices, indices, (size_t)nnz))) return rc;
   if ((rc = upload(c, c->l_vals, values, (size_t)nnz))) return rc;
+  {
+    std::vector<int64_t> tip;
+    std::vector<int32_t> tix;
+    std::vector<double> tv;
+    csr_transpose(c->n, nnz, indptr, indices, values, tip, tix, tv);
+    if ((rc = upload(c, c->lt_indptr, tip.data(), tip.size()))) return rc;
+    if ((rc = upload(c, c->lt_indices, tix.data(), tix.size()))) return rc;
+    if ((rc = upload(c, c->lt_vals, tv.data(), tv.size()))) return rc;
+    PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->nnzL = nnz;
   c->have_decay = true;
@@ -1095,6 +1511,8 @@ int pb_set_injection(pb_context* c, int32_t n_src, int32_t n_rows, const int32_t
   if ((rc = upload(c, c->inj_slot, slot.data(), slot.size()))) return rc;
   if ((rc = upload(c, c->inj_G, grids, (size_t)n_rows * n_src))) return rc;
   if ((rc = upload(c, c->src_ptr, ptr.data(), ptr.size()))) return rc;
+  if ((rc = upload(c, c->inj_rows, rows, (size_t)n_rows))) return rc;
+  if ((rc = upload(c, c->src_col_d, src_col, (size_t)n_src))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->n_src = n_src;
   c->n_inj_rows = n_rows;
@@ -1163,6 +1581,9 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->seg_me.ensure((size_t)std::max(c->n_seg, 1) * sizeof(int64_t)));
   PB_CUDA(c, c->partial.ensure((size_t)std::max(c->n_seg, 1) * ld * sizeof(double)));
   PB_CUDA(c, c->counter.ensure((size_t)std::max(nlong_rows, 1) * ctiles * sizeof(int)));
+  if (a->ckpt_every < 0) return fail(c, PB_ERR_ARG, "pb_solve: ckpt_every must be >= 0");
+  if (a->ckpt_every > 0)
+    PB_CUDA(c, c->ckpt.ensure((size_t)((S + a->ckpt_every - 1) / a->ckpt_every + 1) * n * ld * sizeof(double)));
   size_t scan_need = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
@@ -1238,91 +1659,13 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max(nlong_rows, 1) * ctiles * sizeof(int), st));
   PB_CUDA(c, cudaGetLastError());
 
-  // ---- ETD2 steps ---------------------------------------------------------
-  p.n = n;
-  p.ld = ld;
-  p.flags = flags;
-  if (!pair) p.flags &= ~PB_PAIRPROD;
-  if (!inj) p.flags &= ~PB_INJECTION;
-  p.h = c->s_h.as<double>();
-  p.dldz = c->s_dldz.as<double>();
-  p.hc = c->s_hc.as<double>();
-  p.finj = c->s_finj.as<double>();
-  p.win = c->s_win.as<int>();
-  p.m_indptr = c->m_indptr.as<int64_t>();
-  p.m_indices = c->m_indices.as<int>();
-  p.m_vals = c->m_vals.as<double>();
-  p.m_wstride = mstride;
-  p.m_diag = c->m_diag.as<double>();
-  p.d_indptr = c->d_indptr.as<int64_t>();
-  p.d_indices = c->d_indices.as<int>();
-  p.d_vals = c->d_vals.as<double>();
-  p.d_diag = c->d_diag.as<double>();
-  p.E = c->adia_E.as<double>();
-  p.kp = pair ? c->kp.as<double>() : nullptr;
-  if ((flags & PB_DECAY) && c->have_decay) {
-    p.l_indptr = c->l_indptr.as<int64_t>();
-    p.l_indices = c->l_indices.as<int>();
-    p.l_vals = c->l_vals.as<double>();
-    p.l_diag = c->l_diag.as<double>();
-  }
-  if (inj) {
-    p.inj_slot = c->inj_slot.as<int>();
-    p.G = c->inj_G.as<double>();
-    p.n_src = c->n_src;
-    p.src_ptr = c->src_ptr.as<int>();
-    p.coeff = c->s_coeff.as<double>();
-  }
-  p.a = c->A.as<double>();
-  p.f = c->F.as<double>();
-  p.n_steps = S;
-  p.eD = c->rowf.as<double>();
-  p.phi1 = p.eD + 2 * n;
-  p.phi2 = p.eD + 4 * n;
-  p.kap = p.eD + 6 * n;
-  p.rows = c->short_rows.as<int>();
-  p.nrows = (int)c->h_short_rows.size();
-  p.nsb = (int)blocks_for(p.nrows, K == 1 ? 256 : 8);   // thread per row (K = 1) or warp per row
-  p.seg_lr = c->seg_lr.as<int>();
-  p.seg_mb = c->seg_mb.as<int64_t>();
-  p.seg_me = c->seg_me.as<int64_t>();
-  p.nseg = c->n_seg;
-  p.lr_row = c->long_rows.as<int>();
-  p.lr_seg0 = c->lr_seg0.as<int>();
-  p.lr_nseg = c->lr_nseg.as<int>();
-  p.partial = c->partial.as<double>();
-  p.counter = c->counter.as<int>();
-  p.ctiles = ctiles;
+  // ---- ETD2 step parameters -----------------------------------------------
+  fill_step_params(c, p, K, ld, flags, pair, inj, S, ctiles);
     return PB_OK;
   };
   auto enqueue_steps = [&](int64_t& launches) -> int {
-  bool prepared = false;
-  for (int64_t k = 0; k < S; ++k) {
-    p.step = k;
-    p.ncols = a->n_active[k];
-    if (p.ncols == 0) {
-      // every column is still exactly zero: nothing to advance
-      continue;
-    }
-    if (!prepared) {  // row factors of the first active step; later steps get them from stage 2
-      k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
-      ++launches;
-      prepared = true;
-    }
-    for (int stage = 1; stage <= 2; ++stage) {
-      p.src = stage == 1 ? X : c->A.as<double>();
-      p.x = X;
-      p.xout = X;
-      const unsigned tiles = K == 1 ? 1u : blocks_for(p.ncols, kColTile);
-      dim3 grid((unsigned)p.nsb + blocks_for(p.nseg, 8), tiles);
-      if (K == 1) {
-        if (stage == 1) k_step_plain<1><<<grid, 256, 0, st>>>(p); else k_step_plain<2><<<grid, 256, 0, st>>>(p);
-      } else {
-        if (stage == 1) k_step_multi<1><<<grid, 256, 0, st>>>(p); else k_step_multi<2><<<grid, 256, 0, st>>>(p);
-      }
-      ++launches;
-    }
-  }
+  const int CK = a->ckpt_every;
+  launches += launch_steps(c, p, K, a->n_active, 0, S, st, CK > 0 ? c->ckpt.as<double>() : nullptr, CK);
   PB_CUDA(c, cudaGetLastError());
     return PB_OK;
   };
@@ -1332,6 +1675,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     auto put = [&](uint64_t v) { key.push_back(v); };
     put((uint64_t)S); put((uint64_t)W); put((uint64_t)K); put((uint64_t)ld); put(flags); put(inj); put(R);
     put((uint64_t)c->n_seg); put((uint64_t)c->h_short_rows.size()); put((uint64_t)c->n_cr_bins);
+    put((uint64_t)a->ckpt_every);
     const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);
     for (size_t i = 0; i < sizeof(fd); i += 8) { uint64_t w = 0; memcpy(&w, fb + i, std::min<size_t>(8, sizeof(fd) - i)); put(w); }
     for (const DBuf* b : all_buffers(c)) put((uint64_t)(uintptr_t)b->p);
@@ -1393,6 +1737,189 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   c->last_launches = launches;
   c->last_W = W;
   c->have_solution = true;
+  c->last_ckpt = a->ckpt_every;
+  c->last_S = S;
+  c->last_K = K;
+  c->last_flags = flags;
+  c->last_scale = a->photon_scale;
+  return PB_OK;
+}
+
+int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_t seed_on_device,
+               double* grad_grids, double* grad_coeff, double* grad_scale) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!a || !seed) return fail(c, PB_ERR_ARG, "pb_adjoint: args and seed are required");
+  if (!c->have_solution || c->last_ckpt <= 0)
+    return fail(c, PB_ERR_STATE, "pb_adjoint: run pb_solve with ckpt_every > 0 first");
+  if (a->n_steps != c->last_S || a->n_cols != c->last_K || a->flags != c->last_flags ||
+      a->ckpt_every != c->last_ckpt || a->n_windows != c->last_W || a->photon_scale != c->last_scale)
+    return fail(c, PB_ERR_ARG, "pb_adjoint: arguments differ from the checkpointed solve");
+  const int64_t S = a->n_steps, n = c->n, R = c->R;
+  const int K = a->n_cols, CK = a->ckpt_every;
+  const int ld = K == 1 ? 1 : ((K + kColTile - 1) / kColTile) * kColTile;
+  const uint32_t flags = a->flags;
+  const bool inj = (flags & PB_INJECTION) && c->n_src > 0;
+  const bool pair = (flags & PB_PAIRPROD) && (flags & PB_PARTIAL_DIFF);
+  const bool want_scale = grad_scale != nullptr;
+  const bool want_inj = inj && (grad_grids || grad_coeff);
+  if (want_scale && !(a->photon_scale > 0.0)) return fail(c, PB_ERR_ARG, "pb_adjoint: photon scale must be positive");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  const int64_t mstride = std::max<int64_t>(R, 1);
+  const size_t sb = (size_t)n * ld * sizeof(double);
+
+  // ---- transposed M_off pattern (stable radix sort of the entries by column) --
+  PB_CUDA(c, c->erow.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->tkeys.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->tvals.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->skeys.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->svals.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->t_indptr.ensure(((size_t)n + 1) * sizeof(int64_t)));
+  PB_CUDA(c, c->t_indices.ensure((size_t)mstride * sizeof(int)));
+  PB_CUDA(c, c->t_perm.ensure((size_t)mstride * sizeof(int)));
+  int end_bit = 1;
+  while (((int64_t)1 << end_bit) <= n) ++end_bit;
+  size_t sort_need = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_need, (int*)nullptr, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+                                  (int)mstride, 0, end_bit);
+  PB_CUDA(c, c->sort_tmp.ensure(sort_need));
+  if (R > 0) {
+    k_entry_rows<<<blocks_for(n, 8), 256, 0, st>>>(c->m_indptr.as<int64_t>(), n, c->erow.as<int>());
+    k_transpose_keys<<<blocks_for(R, 256), 256, 0, st>>>(c->m_indices.as<int>(), c->m_indptr.as<int64_t>(), n, R,
+                                                         c->tkeys.as<int>(), c->tvals.as<int>());
+    size_t tb = c->sort_tmp.bytes;
+    PB_CUDA(c, cub::DeviceRadixSort::SortPairs(c->sort_tmp.p, tb, c->tkeys.as<int>(), c->skeys.as<int>(),
+                                               c->tvals.as<int>(), c->svals.as<int>(), (int)R, 0, end_bit, st));
+    k_transpose_finish<<<blocks_for(std::max<int64_t>(R, n + 1), 256), 256, 0, st>>>(
+        c->skeys.as<int>(), c->svals.as<int>(), c->erow.as<int>(), n, R, c->t_indptr.as<int64_t>(),
+        c->t_indices.as<int>(), c->t_perm.as<int>());
+  } else {
+    PB_CUDA(c, cudaMemsetAsync(c->t_indptr.p, 0, ((size_t)n + 1) * sizeof(int64_t), st));
+  }
+  PB_CUDA(c, cudaGetLastError());
+
+  // ---- work buffers ----------------------------------------------------------
+  PB_CUDA(c, c->lam.ensure(sb));
+  PB_CUDA(c, c->lam2.ensure(sb));
+  PB_CUDA(c, c->mu.ensure(sb));
+  PB_CUDA(c, c->rec_rf.ensure((size_t)CK * 4 * n * sizeof(double)));
+  PB_CUDA(c, c->rec_sx.ensure(sb));
+  PB_CUDA(c, c->dsig.ensure((size_t)6 * n * sizeof(double)));
+  if (want_scale) {
+    PB_CUDA(c, c->rec_P.ensure((size_t)CK * sb));
+    PB_CUDA(c, c->rec_Q.ensure((size_t)CK * sb));
+    PB_CUDA(c, c->gs.ensure(sb));
+    PB_CUDA(c, cudaMemsetAsync(c->gs.p, 0, sb, st));
+  }
+  const int n_inj = c->n_inj_rows;
+  if (want_inj) PB_CUDA(c, c->gb_inj.ensure((size_t)std::max<int64_t>(S, 1) * std::max(n_inj, 1) * ld * sizeof(double)));
+  if ((rc = upload(c, c->nact, a->n_active, (size_t)std::max<int64_t>(S, 1)))) return rc;
+  PB_CUDA(c, cudaMemsetAsync(c->lam.p, 0, sb, st));
+  PB_CUDA(c, cudaMemcpy2DAsync(c->lam.p, ld * sizeof(double), seed, K * sizeof(double), K * sizeof(double), n,
+                               seed_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+
+  // ---- forward parameters (recording) and backward sweep per checkpoint segment
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  const int ctiles = ld / (K == 1 ? 1 : kColTile);
+  fill_step_params(c, p, K, ld, flags, pair, inj, S, ctiles);
+  p.inv_scale = 1.0 / a->photon_scale;
+  p.rec_rf = c->rec_rf.as<double>();
+  p.rec_sx = c->rec_sx.as<double>();
+  if (want_scale) {
+    p.dsig = c->dsig.as<double>();
+    p.dphi1 = p.dsig + 2 * n;
+    p.dphi2 = p.dsig + 4 * n;
+    p.rec_P = c->rec_P.as<double>();
+    p.rec_Q = c->rec_Q.as<double>();
+  }
+  double* lam = c->lam.as<double>();
+  double* lam2 = c->lam2.as<double>();
+  const int64_t nseg = (S + CK - 1) / CK;
+  for (int64_t sg = nseg - 1; sg >= 0; --sg) {
+    const int64_t k0 = sg * CK, k1 = std::min<int64_t>(S, k0 + CK);
+    int64_t kf = k0;
+    while (kf < k1 && a->n_active[kf] == 0) ++kf;
+    if (kf == k1) continue;  // no active column in this segment
+    PB_CUDA(c, cudaMemcpyAsync(c->X.p, c->ckpt.as<double>() + (size_t)sg * n * ld, sb, cudaMemcpyDeviceToDevice, st));
+    p.rec_k0 = k0;
+    p.rec_len = (int)(k1 - k0);
+    PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max<size_t>(c->h_long_rows.size(), 1) * ctiles * sizeof(int), st));
+    launch_steps(c, p, K, a->n_active, k0, k1, st, nullptr, 0);
+    for (int64_t k = k1 - 1; k >= kf; --k) {
+      AdjParams q;
+      memset(&q, 0, sizeof(q));
+      q.n = n;
+      q.ld = ld;
+      q.ncols = a->n_active[k];
+      q.step = k;
+      q.flags = p.flags;
+      q.h = a->h[k];
+      q.dl = a->dldz[k];
+      q.w = a->window[k];
+      q.t_indptr = c->t_indptr.as<int64_t>();
+      q.t_indices = c->t_indices.as<int>();
+      q.t_perm = c->t_perm.as<int>();
+      q.m_vals = c->m_vals.as<double>() + (size_t)q.w * mstride;
+      q.dt_indptr = c->dt_indptr.as<int64_t>();
+      q.dt_indices = c->dt_indices.as<int>();
+      q.dt_vals = c->dt_vals.as<double>();
+      if ((flags & PB_DECAY) && c->have_decay) {
+        q.lt_indptr = c->lt_indptr.as<int64_t>();
+        q.lt_indices = c->lt_indices.as<int>();
+        q.lt_vals = c->lt_vals.as<double>();
+      }
+      const size_t j = (size_t)(k - k0);
+      q.rf = c->rec_rf.as<double>() + j * 4 * n;
+      if (want_scale) {
+        q.P = c->rec_P.as<double>() + j * n * ld;
+        q.Q = c->rec_Q.as<double>() + j * n * ld;
+        q.gs = c->gs.as<double>();
+      }
+      q.lam = lam;
+      q.mu = c->mu.as<double>();
+      q.lam_out = lam2;
+      if (want_inj) {
+        q.inj_slot = c->inj_slot.as<int>();
+        q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
+      }
+      dim3 grid(blocks_for(n, 8), K == 1 ? 1u : blocks_for(q.ncols, kColTile));
+      k_adj<1><<<grid, 256, 0, st>>>(q);
+      k_adj<2><<<grid, 256, 0, st>>>(q);
+      std::swap(lam, lam2);
+    }
+    PB_CUDA(c, cudaGetLastError());
+  }
+
+  // ---- gradients ----------------------------------------------------------------
+  if (want_inj) {
+    PB_CUDA(c, c->g_out.ensure((size_t)std::max<int64_t>((int64_t)S * c->n_src, (int64_t)n_inj * c->n_src) * sizeof(double) + 8));
+    if (grad_coeff) {
+      k_grad_coeff<<<blocks_for(S * c->n_src, 256), 256, 0, st>>>(
+          c->gb_inj.as<double>(), c->inj_G.as<double>(), c->s_finj.as<double>(), c->src_col_d.as<int>(),
+          c->nact.as<int>(), S, c->n_src, n_inj, ld, c->g_out.as<double>());
+      PB_CUDA(c, cudaMemcpyAsync(grad_coeff, c->g_out.p, (size_t)S * c->n_src * sizeof(double), cudaMemcpyDeviceToHost, st));
+      PB_CUDA(c, cudaStreamSynchronize(st));
+    }
+    if (grad_grids) {
+      k_grad_grids<<<blocks_for((int64_t)n_inj * c->n_src, 256), 256, 0, st>>>(
+          c->gb_inj.as<double>(), c->s_coeff.as<double>(), c->s_finj.as<double>(), c->src_col_d.as<int>(),
+          c->nact.as<int>(), S, c->n_src, n_inj, ld, c->g_out.as<double>());
+      PB_CUDA(c, cudaMemcpyAsync(grad_grids, c->g_out.p, (size_t)n_inj * c->n_src * sizeof(double), cudaMemcpyDeviceToHost, st));
+      PB_CUDA(c, cudaStreamSynchronize(st));
+    }
+  } else {
+    if (grad_coeff) memset(grad_coeff, 0, (size_t)S * std::max(c->n_src, 0) * sizeof(double));
+    if (grad_grids) memset(grad_grids, 0, (size_t)n_inj * std::max(c->n_src, 0) * sizeof(double));
+  }
+  if (want_scale) {
+    PB_CUDA(c, c->g_out.ensure((size_t)std::max(K, 1) * sizeof(double) + 8));
+    k_grad_scale<<<blocks_for(K, 128), 128, 0, st>>>(c->gs.as<double>(), n, ld, K, c->g_out.as<double>());
+    PB_CUDA(c, cudaMemcpyAsync(grad_scale, c->g_out.p, (size_t)K * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  PB_CUDA(c, cudaGetLastError());
+  PB_CUDA(c, cudaStreamSynchronize(st));
   return PB_OK;
 }
 

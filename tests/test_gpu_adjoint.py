@@ -1,0 +1,168 @@
+"""Adjoint gradients against central finite differences (needs a B200).
+
+Parameters per source point: spectral index, log10 R_max, composition
+fractions, evolution index m; plus the shared photon-density scale.  The
+adjoint gradient must match central differences (h = 1e-5 relative) of the
+GPU forward and of the CPU oracle of the reference solver to 1e-6 relative.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import etd2_oracle as O
+from prince_b200 import adjoint as AD
+from prince_b200 import cr_sources, photonfields as pf
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _params(K, seed, nspec):
+    rng = np.random.default_rng(seed)
+    return dict(gamma=rng.uniform(0.5, 2.2, K), lg_rmax=rng.uniform(9.3, 10.5, K),
+                frac=rng.dirichlet(np.ones(nspec), K), m=rng.uniform(-2, 4, K))
+
+
+def _tensors(p):
+    return {k: torch.tensor(v, dtype=torch.float64, requires_grad=True) for k, v in p.items()}
+
+
+def _forward(sb, plan, t, scale):
+    G = sb.grids(t["gamma"], t["lg_rmax"], t["frac"])
+    coeff = sb.coefficients(t["m"])
+    return AD.PropagateFunction.apply(G, coeff, scale, plan)
+
+
+def _check_fd(fun, t, scale, keys, rel=TOL, h=1e-5, skip_small=1e-12):
+    """Adjoint gradient of fun (via autograd) against central differences."""
+    L = fun(t, scale)
+    L.backward()
+    worst = 0.0
+    for key in keys:
+        base = t[key].detach().clone()
+        g = t[key].grad.detach().numpy()
+        for idx in np.ndindex(base.shape):
+            step = h * max(abs(float(base[idx])), 1e-3)
+            vals = []
+            for sgn in (1, -1):
+                tt = {k: v.detach().clone() for k, v in t.items()}
+                tt[key][idx] += sgn * step
+                with torch.no_grad():
+                    vals.append(float(fun(tt, scale.detach())))
+            fd = (vals[0] - vals[1]) / (2 * step)
+            if abs(fd) < skip_small and abs(g[idx]) < skip_small:
+                continue
+            worst = max(worst, abs(g[idx] - fd) / max(abs(fd), 1e-300))
+    # scale
+    gs = float(scale.grad)
+    s0 = float(scale.detach())
+    step = h * s0
+    with torch.no_grad():
+        tt = {k: v.detach().clone() for k, v in t.items()}
+        lp = float(fun(tt, torch.tensor(s0 + step, dtype=torch.float64)))
+        lm = float(fun(tt, torch.tensor(s0 - step, dtype=torch.float64)))
+    fd = (lp - lm) / (2 * step)
+    worst_scale = abs(gs - fd) / abs(fd)
+    return worst, worst_scale
+
+
+@pytest.fixture(scope="module")
+def light():
+    from workloads import light_run
+    return light_run()
+
+
+def test_adjoint_linear_functional_light(light):
+    run = light
+    species = [2212, 1000020040]
+    K = 3
+    sb = AD.SourceBatch(run, species, z_max=[0.3, 0.24, 0.17], initial_z=0.3)
+    plan = sb.plan(0.3, ckpt_every=8)
+    t = _tensors(_params(K, 1, len(species)))
+    seed = torch.tensor(np.random.default_rng(2).uniform(0.5, 1.5, (run.dim_states, K)))
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    ref = None
+
+    def fun(tt, sc):
+        X = _forward(sb, plan, tt, sc)
+        return (seed * X / 1e20).sum()
+
+    worst, worst_s = _check_fd(fun, t, scale, ["gamma", "lg_rmax", "frac", "m"])
+    assert worst < TOL, worst
+    assert worst_s < TOL, worst_s
+
+
+def test_adjoint_flux_loss_medium_network():
+    from workloads import network_run
+    run = network_run(max_mass=16, n_species=60, seed=5)
+    species = [2212, 1000020040, 1000070140]
+    K = 3
+    sb = AD.SourceBatch(run, species, z_max=[0.2, 0.15, 0.12], initial_z=0.2)
+    plan = sb.plan(0.2, ckpt_every=32)
+    hidden = _tensors(_params(1, 9, len(species)))
+    sbh = AD.SourceBatch(run, species, z_max=[0.2], initial_z=0.2)
+    ph = sbh.plan(0.2)
+    with torch.no_grad():
+        Xt = _forward(sbh, ph, hidden, torch.tensor(1.0, dtype=torch.float64))
+        _, T = AD.group_flux(run, Xt)
+    target = T[:, 0]
+    t = _tensors(_params(K, 4, len(species)))
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+
+    def fun(tt, sc):
+        X = _forward(sb, plan, tt, sc)
+        return AD.log_ratio_loss(run, X, target).sum()
+
+    worst, worst_s = _check_fd(fun, t, scale, ["gamma", "lg_rmax", "frac", "m"])
+    assert worst < TOL, worst
+    assert worst_s < TOL, worst_s
+
+
+def test_adjoint_against_oracle_differences(light):
+    """Gradient of the flux loss vs central differences of the CPU reference solver."""
+    run = light
+    species = [2212, 1000020040]
+    K = 2
+    zmax = [0.15, 0.1]
+    sb = AD.SourceBatch(run, species, z_max=zmax, initial_z=0.15)
+    plan = sb.plan(0.15, ckpt_every=16)
+    p = _params(K, 5, len(species))
+    t = _tensors(p)
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    target = torch.tensor(np.logspace(0, -3, 200), dtype=torch.float64)
+
+    X = _forward(sb, plan, t, scale)
+    eg, F = AD.group_flux(run, X)
+    target = F[:, 0].detach() * 1.3
+    L = AD.log_ratio_loss(run, X, target).sum()
+    L.backward()
+
+    def oracle_loss(pp, s):
+        field = pf.ScaledPhotonField(pf.CMBPhotonSpectrum(), s)
+        run.set_photon_field(field)
+        try:
+            srcs = []
+            for k in range(K):
+                params = {sp: (pp["gamma"][k], 10 ** pp["lg_rmax"][k], float(pp["frac"][k, i]))
+                          for i, sp in enumerate(species)}
+                srcs.append([cr_sources.RigdityCutoffSource(run, norm=1.0, params=params,
+                                                            m=("simple", float(pp["m"][k])), z_max=zmax[k])])
+            Xo = O.OracleSolver(run, 0.15, 0.0, K=K, exp="cr").solve(srcs, dz=1e-3)
+        finally:
+            run.set_photon_field(pf.CMBPhotonSpectrum())
+        return float(AD.log_ratio_loss(run, torch.tensor(Xo), target).sum())
+
+    for key in ("gamma", "m"):
+        for k in range(K):
+            pp = {kk: np.array(v, dtype=np.float64) for kk, v in p.items()}
+            step = 1e-5 * abs(pp[key][k])
+            pp[key][k] += step
+            lp = oracle_loss(pp, 1.0)
+            pp[key][k] -= 2 * step
+            lm = oracle_loss(pp, 1.0)
+            fd = (lp - lm) / (2 * step)
+            g = float(t[key].grad[k])
+            assert abs(g - fd) / abs(fd) < TOL, (key, k, g, fd)
+    fd = (oracle_loss(p, 1 + 1e-5) - oracle_loss(p, 1 - 1e-5)) / 2e-5
+    assert abs(float(scale.grad) - fd) / abs(fd) < TOL, (float(scale.grad), fd)
