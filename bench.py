@@ -203,6 +203,8 @@ def run_b200(args, dist, rank, ws, local):
             pm.append(ps.last_timing[1])
         plain = len(pm) / (sum(pm) / 1e3)
 
+    adj = adjoint_timing(run, pts, zi, local) if args.adjoint else None
+
     pk, pk_kind = _peaks()
     avg_steps_ms = statistics.mean(steps_ms)
     achieved = bytes_solve / (avg_steps_ms / 1e3) / 1e9
@@ -243,9 +245,47 @@ def run_b200(args, dist, rank, ws, local):
         "plain_spectra_per_s": plain,
         "batched_over_plain": (value / ws / plain) if plain else None,
     }
+    if adj:
+        fwd_wall = t_wall / args.steps
+        adj["forward_s"] = fwd_wall
+        adj["adjoint_over_forward"] = adj["adjoint_s"] / fwd_wall
+        adj["gradient_over_forward"] = (adj["forward_ckpt_s"] + adj["adjoint_s"]) / fwd_wall
+        line["adjoint"] = adj
     if clk:
         line["clocks"] = clk
     return line, run, pts, zi, sched
+
+
+def adjoint_timing(run, pts, zi, device):
+    """Gradient of sum(seed * X) for the same points: forward with checkpoints every
+    32 steps plus the device adjoint, against the plain forward time."""
+    import torch
+    from prince_b200 import adjoint as AD
+
+    species = [p for p in pts[0]["species"]]
+    sb = AD.SourceBatch(run, species, z_max=[p["zmax"] for p in pts], initial_z=zi)
+    plan = sb.plan(zi, device=device, ckpt_every=32)
+    t = {"gamma": torch.tensor([p["gamma"] for p in pts], requires_grad=True),
+         "lg_rmax": torch.tensor([np.log10(p["rmax"]) for p in pts], requires_grad=True),
+         "frac": torch.tensor(np.array([p["frac"] for p in pts]), requires_grad=True),
+         "m": torch.tensor([p["m"] for p in pts], requires_grad=True)}
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    seed = torch.ones((run.dim_states, len(pts)), dtype=torch.float64)
+    fwd, bwd = [], []
+    for rep in range(2):
+        G = sb.grids(t["gamma"], t["lg_rmax"], t["frac"])
+        coeff = sb.coefficients(t["m"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X = AD.PropagateFunction.apply(G, coeff, scale, plan)
+        t1 = time.perf_counter()
+        (seed * X).sum().backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        fwd.append(t1 - t0)
+        bwd.append(t2 - t1)
+    return {"points": len(pts), "ckpt_every": 32, "forward_ckpt_s": fwd[-1], "adjoint_s": bwd[-1],
+            "params_per_point": 8, "with_photon_scale": True}
 
 
 def cpu_line(pts, zi, sched, K_total, samples_steps=20, processes=None):
@@ -271,6 +311,7 @@ def main():
     ap.add_argument("--points", type=int, default=512)
     ap.add_argument("--plain", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--adjoint", type=int, default=1, help="also time the adjoint gradient (1/0)")
     ap.add_argument("--z-range", default="0.5,1.0",
                     help="z_max range of the source points (smaller cases for profiling)")
     args = ap.parse_args()
