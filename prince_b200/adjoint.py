@@ -235,8 +235,12 @@ def group_flux(run, X, egrid=None):
     return torch.tensor(egrid, dtype=X.dtype, device=X.device), total
 
 
-def log_ratio_loss(run, X, target, e_min=10 ** 9.5):
-    """sum over bins with E > e_min of ln(F_k(E) / T(E))^2, per column (K)."""
+def log_ratio_loss(run, X, target, e_min=10 ** 9.5, dynamic_range=1e-30):
+    """sum over bins with E > e_min of ln(F_k(E) / T(E))^2, per column (K).
+
+    Bins where the target is below ``dynamic_range`` of its maximum (beyond the
+    end of the spectra) are left out, so the loss stays finite.
+    """
     egrid, F = group_flux(run, X)
-    sel = egrid > e_min
+    sel = (egrid > e_min) & (target > dynamic_range * target.max())
     return ((torch.log(F[sel]) - torch.log(target[sel, None])) ** 2).sum(dim=0)

@@ -2,8 +2,8 @@
 
 Parameters per source point: spectral index, log10 R_max, composition
 fractions, evolution index m; plus the shared photon-density scale.  The
-adjoint gradient must match central differences (h = 1e-5 relative) of the
-GPU forward and of the CPU oracle of the reference solver to 1e-6 relative.
+adjoint gradient must match central differences (step h = 1e-5) of the GPU
+forward and of the CPU oracle of the reference solver to 1e-6 relative.
 """
 
 import numpy as np
@@ -43,7 +43,7 @@ def _check_fd(fun, t, scale, keys, rel=TOL, h=1e-5, skip_small=1e-12):
         base = t[key].detach().clone()
         g = t[key].grad.detach().numpy()
         for idx in np.ndindex(base.shape):
-            step = h * max(abs(float(base[idx])), 1e-3)
+            step = h
             vals = []
             for sgn in (1, -1):
                 tt = {k: v.detach().clone() for k, v in t.items()}
@@ -156,7 +156,7 @@ def test_adjoint_against_oracle_differences(light):
     for key in ("gamma", "m"):
         for k in range(K):
             pp = {kk: np.array(v, dtype=np.float64) for kk, v in p.items()}
-            step = 1e-5 * abs(pp[key][k])
+            step = 1e-5
             pp[key][k] += step
             lp = oracle_loss(pp, 1.0)
             pp[key][k] -= 2 * step
