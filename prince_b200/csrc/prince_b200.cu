@@ -590,8 +590,8 @@ __device__ __forceinline__ void phi_of(double h, double d, double& eD, double& p
 __device__ __forceinline__ void dphi_of(double w, double e, double f1, double f2, double& d1, double& d2) {
   if (fabs(w) < 0.1) {
     double a = 0.0, b = 0.0;
-    double fact2 = 6227020800.0;     // 13!
-    double fact3 = 87178291200.0;    // 14!
+    double fact2 = 87178291200.0;    // (12 + 2)!
+    double fact3 = 1307674368000.0;  // (12 + 3)!
     for (int n = 12; n >= 0; --n) {  // Horner from the top
       a = a * w + (n + 1) / fact2;
       b = b * w + (n + 1) / fact3;
