@@ -208,8 +208,9 @@ def group_flux(run, X, egrid=None):
 
     Per species: total energy A E_i, spectrum state / A, log-log interpolated to
     the common grid ``EnergyGrid(lo, hi + log10 A_max, 4 bins/decade-multiple)``
-    and summed (``propagation.py:103-167``).  Non-positive states are floored at
-    1e-300 before the logarithm.
+    and summed (``propagation.py:103-167``).  States below 1e-30 of the
+    species' maximum (including non-positive ones) are floored at that level
+    before the logarithm.
     """
     sm = run.spec_man
     cr = run.cr_grid
@@ -226,8 +227,11 @@ def group_flux(run, X, egrid=None):
         j = np.clip(np.searchsorted(le, lge) - 1, 0, le.size - 2)
         w = (lge - le[j]) / (le[j + 1] - le[j])
         inside = (lge >= le[0]) & (lge <= le[-1])
-        y = torch.clamp(X[s.lidx():s.uidx()] / s.A, min=1e-300)
-        ly = torch.log(y)
+        y = X[s.lidx():s.uidx()] / s.A
+        # floor at 1e-30 of the species' maximum (per column): values below it are
+        # treated as the floor, so the logarithm and its derivative stay bounded
+        floor = (1e-30 * y.detach().abs().max(dim=0).values).clamp(min=1e-300)
+        ly = torch.log(torch.maximum(y, floor[None, :]))
         jt = torch.tensor(j, device=X.device)
         wt = torch.tensor(w, dtype=X.dtype, device=X.device)[:, None]
         val = torch.exp((1 - wt) * ly[jt] + wt * ly[jt + 1])
