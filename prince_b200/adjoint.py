@@ -230,7 +230,7 @@ def group_flux(run, X, egrid=None):
         y = X[s.lidx():s.uidx()] / s.A
         # floor at 1e-30 of the species' maximum (per column): values below it are
         # treated as the floor, so the logarithm and its derivative stay bounded
-        floor = (1e-30 * y.detach().abs().max(dim=0).values).clamp(min=1e-300)
+        floor = (1e-30 * y.abs().amax(dim=0)).clamp(min=1e-300)
         ly = torch.log(torch.maximum(y, floor[None, :]))
         jt = torch.tensor(j, device=X.device)
         wt = torch.tensor(w, dtype=X.dtype, device=X.device)[:, None]
