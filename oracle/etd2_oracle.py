@@ -22,7 +22,9 @@ Reference files restated here (paths inside the PriNCe project):
 * ``src/prince_cr/solvers/etd2.py:329-439`` -- phi functions and the step;
 * ``src/prince_cr/solvers/partial_diff.py:48-110`` -- FD loss operator;
 * ``src/prince_cr/interaction_rates.py:966-1067`` -- rate fold;
-* ``interaction_rates.py:1202-1210, 1277-1294`` -- loss vectors.
+* ``interaction_rates.py:1202-1210, 1277-1294`` -- loss vectors;
+* ``propagation.py:555-665`` -- EM-cascade step hooks (Bethe-Heitler pair
+  injection, then the cascade transfer of gamma and e+-).
 """
 
 from __future__ import annotations
@@ -187,7 +189,8 @@ class OracleSolver:
     lists (one per column).  Sources expose ``injection_rate(z)``.
     """
 
-    def __init__(self, run, initial_z, final_z, flags=None, thr=None, K=None, decay=None, exp="numpy"):
+    def __init__(self, run, initial_z, final_z, flags=None, thr=None, K=None, decay=None, exp="numpy",
+                 em=None):
         self.run = run
         self.initial_z = float(initial_z)
         self.final_z = float(final_z)
@@ -213,6 +216,15 @@ class OracleSolver:
             self._exp = crexp.exp
         else:
             self._exp = np.exp
+        # Co-evolved EM cascade (propagation.py:555-665): ``em(z)`` returns the
+        # window's (T_gamma, T_electron, R_BH); applied after every step.
+        self.em = em
+        if em is not None:
+            sm = run.spec_man
+            self._em_gamma_sl = sm.pdgid2sref[22].sl
+            self._em_lep_sl = [sm.pdgid2sref[p].sl for p in (11, -11) if p in sm.pdgid2sref]
+            self._em_bh_species = [(sp.sl, float(sp.A)) for sp in sm.species_refs
+                                   if sp.is_nucleus and abs(sp.charge) >= 1]
         self.trace = Trace()
 
     # -- per window --------------------------------------------------------
@@ -236,6 +248,9 @@ class OracleSolver:
             d_M[present] = vec[self.diag_to_M[present]]
             self.d_M = d_M
         self.kappa_pair = _pair_loss(self.run, z) if self.flags.pairprod else None
+        if self.em is not None:
+            self._em_T = self.em(z)
+            self._em_z = float(z)
         if first:
             self.trace.kappa_pair_first = None if self.kappa_pair is None else self.kappa_pair.copy()
         self.trace.windows.append(z)
@@ -288,7 +303,42 @@ class OracleSolver:
             if self.L_diag is not None:
                 d = d + self.L_diag * dl
             x = self._step(x, h, d, dl, kappa, b)
+            if self.em is not None:
+                self._inject_bh_pairs(x, dz)
+                self._apply_em_cascade(x)
         return x
+
+    def _inject_bh_pairs(self, x, dz):
+        """propagation.py:620-665."""
+        Tg, Te, R = self._em_T
+        z = self._em_z
+        E_p = self.run.cr_grid.grid
+        dE = np.gradient(E_p)
+        loss_full = _pair_loss(self.run, z)
+        dl_step = 1e2 * _spc.c * abs(dz) / ((1.0 + z) * hubble(z))
+        w = None
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv_E = np.where(E_p > 0, 1.0 / E_p, 0.0)
+            for sl, A in self._em_bh_species:
+                n_s = x[sl]
+                cw = A * loss_full[sl] * dl_step * inv_E * dE
+                if n_s.ndim == 2:
+                    cw = cw[:, None]
+                term = cw * n_s
+                w = term if w is None else w + term
+        e_src = R @ w
+        for sl in self._em_lep_sl:
+            x[sl] = x[sl] + e_src
+
+    def _apply_em_cascade(self, x):
+        """propagation.py:555-571."""
+        Tg, Te, R = self._em_T
+        ph = np.array(x[self._em_gamma_sl])
+        lep = np.zeros_like(ph)
+        for sl in self._em_lep_sl:
+            lep = lep + x[sl]
+            x[sl] = 0.0
+        x[self._em_gamma_sl] = Tg @ ph + Te @ lep
 
     def _apply_F(self, x, dl, kappa, b):
         out = np.asarray(self.M_off.dot(x))

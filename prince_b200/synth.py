@@ -252,3 +252,56 @@ def full_network_species(max_mass=56, n_species=350, per_isobar=7):
 
     keep = sorted(chart, key=lambda p: (dist(p), p))[: max(n_species - 2, 0)]
     return [2212, 2112] + sorted(keep)
+
+
+def em_cascade_matrices(em_grid, cr_grid, z):
+    """Seeded-free synthetic EM-cascade transfer ``(T_gamma, T_electron, R_BH)`` at redshift z.
+
+    Stand-ins with the shapes and conservation laws of the kinetic cascade
+    transfer and the Bethe-Heitler pair shape (whose construction from cross
+    sections is outside the ETD2 path):
+
+    * photons below the pair-production threshold ``E_abs = 1.1e6 GeV/(1+z)``
+      pass through; above it their energy is re-emitted below ``E_abs`` with
+      a universal cascade spectrum (``E^-1.5`` under ``E_X = 0.04 E_abs``,
+      ``E^-2`` above), energy conserving;
+    * electrons and positrons hand their energy to photons: above ``E_abs``
+      through the same cascade, below it as inverse-Compton photons at
+      ``E_ic = (4/3)(E/m_e)^2 2.7 E_CMB (1+z)`` (capped at E);
+    * ``R_BH[:, j]`` is the per-sign e+- spectrum of a nucleon at ``E_j`` (per
+      nucleon): log-normal around ``4 (m_e/m_p) E_j`` with one decade width,
+      normalised so the pair carries ``E_j``: ``2 sum_i E_i R_ij dE_i = E_j``.
+
+    The state is dN/dE per bin, so energy in bin i is ``E_i n_i dE_i``.
+    """
+    U = C.PRINCE_UNITS
+    E = em_grid.grid
+    dE = em_grid.widths
+    n_em = E.size
+    e_abs = 1.1e6 / (1.0 + z)
+    e_x = 0.04 * e_abs
+    shape = np.where(E < e_x, (E / e_x) ** -1.5, (E / e_x) ** -2.0) * (E < e_abs)
+    norm = np.sum(E * shape * dE)
+    Tg = np.zeros((n_em, n_em))
+    Te = np.zeros((n_em, n_em))
+    e_ic_all = (4.0 / 3.0) * (E / U.m_electron) ** 2 * 2.7 * C.E_CMB * (1.0 + z)
+    for j in range(n_em):
+        if E[j] < e_abs or norm <= 0:
+            Tg[j, j] = 1.0
+        else:
+            Tg[:, j] = shape * (E[j] * dE[j]) / norm
+        if E[j] >= e_abs and norm > 0:
+            Te[:, j] = shape * (E[j] * dE[j]) / norm
+        else:
+            e_ic = min(e_ic_all[j], E[j])
+            i = int(np.clip(np.searchsorted(em_grid.bins, e_ic) - 1, 0, n_em - 1))
+            Te[i, j] = E[j] * dE[j] / (E[i] * dE[i])
+    Ep = cr_grid.grid
+    R = np.zeros((n_em, Ep.size))
+    for j in range(Ep.size):
+        e0 = 4.0 * (U.m_electron / U.m_proton) * Ep[j]
+        g = np.exp(-0.5 * (np.log10(E / e0) / 0.5) ** 2)
+        s = 2.0 * np.sum(E * g * dE)
+        if s > 0:
+            R[:, j] = g * Ep[j] / s
+    return Tg, Te, R

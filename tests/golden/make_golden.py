@@ -4,7 +4,8 @@
 Run in a checkout where the reference source tree is available (default
 ``/root/reference``, override with ``PRINCE_REFERENCE``)::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # light network
+    python tests/golden/make_golden.py --em     # light network + EM cascade
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -22,7 +23,8 @@ It then builds the light-nuclei run (p, n, 2H, 3H, 3He, 4He; 64 bins over
 1e6-1e14 GeV at 8 bins/decade; CMB; z = 1 -> 0, dz = 1e-3) and records the
 inputs the ETD2 path consumes together with the reference's own outputs
 (final states of single- and multi-RHS solves, per-window intermediates).
-The result is ``tests/golden/light_network.npz``.
+The result is ``tests/golden/light_network.npz`` (and, with ``--em``,
+``tests/golden/light_network_em.npz``).
 """
 
 from __future__ import annotations
@@ -297,5 +299,84 @@ def main():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_em():
+    """Light network with the co-evolved EM cascade (gamma, e+-) on the shared grid.
+
+    The per-window cascade transfer and Bethe-Heitler pair shape are supplied by
+    the synthetic stand-ins ``prince_b200.synth.em_cascade_matrices`` (patched
+    into the reference solver's ``_em_transfer_at`` / ``_em_bh_at``); the
+    reference then runs its own step hooks ``_inject_bh_pairs`` and
+    ``_apply_em_cascade`` after every ETD2 step.
+    """
+    _prepare_reference()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from prince_b200 import synth
+    from prince_b200.data import EnergyGrid
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (8, 12, 8)
+    config.em_cascade_grid_lo = 7.0
+    config.photon_grid = (-15, -6, 8)
+    config.tau_dec_threshold = 0.0
+    config.max_mass = 4
+    config.batch_matrix_format = "dense"
+    config.xs_dtype = "float64"
+    config.linear_algebra_backend = "scipy"
+
+    from prince_cr import core, cr_sources
+    from prince_cr.cross_sections.base import CrossSectionBase
+    from prince_cr.solvers import MultiRHSPropagationSolverETD2, UHECRPropagationSolverETD2
+
+    orig = core.PriNCeRun
+
+    def em_run(*a, **k):
+        k.update(enable_em_cascade=True, enable_em_decoupled_grid=False)
+        return orig(*a, **k)
+
+    core.PriNCeRun = em_run
+    run = build(config, CrossSectionBase)
+    core.PriNCeRun = orig
+    ir = run.int_rates
+    grid = run.cr_grid
+    lo, hi = np.log10(grid.bins[0]), np.log10(grid.bins[-1])
+    mine = EnergyGrid(lo, hi, 8)
+    assert np.allclose(mine.grid, grid.grid, rtol=1e-14)
+
+    def patch(s):
+        s._em_transfer_at = lambda z: synth.em_cascade_matrices(mine, mine, float(z))[:2]
+        s._em_bh_at = lambda z: synth.em_cascade_matrices(mine, mine, float(z))[2]
+        return s
+
+    eq = {2212: (2.0, 1e10, 1.0), 1000020040: (2.0, 1e10, 1.0)}
+    soft = {2212: (2.5, 3e10, 1.0)}
+    out = {}
+    out["species"] = np.array(run.spec_man.known_species, dtype=np.int64)
+    out["cr_grid"] = np.array([lo, hi, 8.0])
+    out["ph_grid"] = np.array(config.photon_grid, dtype=np.float64)
+    out["batch_matrix"] = np.asarray(ir._batch_matrix, dtype=np.float64)
+    out["batch_rows"] = np.asarray(ir._batch_rows, dtype=np.int64)
+    out["batch_cols"] = np.asarray(ir._batch_cols, dtype=np.int64)
+    out["cpl_indptr"] = np.asarray(ir.coupling_mat.indptr, dtype=np.int64)
+    out["cpl_indices"] = np.asarray(ir.coupling_mat.indices, dtype=np.int64)
+    s = patch(UHECRPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run))
+    s.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=eq))
+    s.solve(dz=1e-3)
+    out["state_em"] = np.asarray(s.state)
+    m = patch(MultiRHSPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run, K=2))
+    m[0].add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=eq))
+    m[1].add_source_class(cr_sources.SimpleSource(run, norm=1.0, params=soft, m=("simple", 2.0)))
+    m.solve(dz=1e-3)
+    out["state_em_multi"] = np.asarray(m.state)
+    out["src_eq"] = np.array(repr(eq))
+    out["src_soft"] = np.array(repr(soft))
+    path = os.path.join(HERE, "light_network_em.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
-    main()
+    if "--em" in sys.argv:
+        main_em()
+    else:
+        main()

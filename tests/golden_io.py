@@ -59,3 +59,27 @@ def rel_err_on_support(x, ref, species_blocks, floor=1e-20):
             if e.size:
                 worst = max(worst, float(e.max()))
     return worst
+
+
+def light_network_em():
+    """The EM-cascade fixture: run (gamma, e+- on the shared grid) and the
+    synthetic per-window transfer used by the reference run."""
+    from prince_b200 import synth
+    from prince_b200.data import EnergyGrid
+
+    z = dict(np.load(os.path.join(GOLDEN, "light_network_em.npz")))
+    model = FixedKernelModel(z["species"], z["batch_matrix"], z["batch_rows"], z["batch_cols"])
+    run = PriNCeRun(model, photonfields.CMBPhotonSpectrum(), cosmic_ray_grid=tuple(z["cr_grid"]),
+                    photon_grid=tuple(z["ph_grid"]))
+    grid = EnergyGrid(*tuple(z["cr_grid"]))
+
+    def em(zz):
+        return synth.em_cascade_matrices(grid, grid, float(zz))
+
+    def source(key, m="flat"):
+        params = ast.literal_eval(str(z[f"src_{key}"]))
+        if key == "soft":
+            return cr_sources.SimpleSource(run, norm=1.0, params=params, m=("simple", 2.0))
+        return cr_sources.RigdityCutoffSource(run, norm=1.0, params=params)
+
+    return z, run, em, source

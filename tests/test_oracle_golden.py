@@ -156,3 +156,15 @@ def test_single_exponential_known_answer():
     zg = np.linspace(0.0, 5.0, 1001)
     x = O.integrate_const([1.0], zg, [-1.0 / 0.7])
     np.testing.assert_allclose(x[0], np.exp(-5.0 / 0.7), rtol=1e-10)
+
+
+def test_oracle_em_cascade_single_and_multi():
+    """EM step hooks (BH pair injection + cascade transfer) against the reference."""
+    from golden_io import light_network_em
+
+    z, run, em, source = light_network_em()
+    blocks = [s.sl for s in run.spec_man.species_refs]
+    x = O.OracleSolver(run, 0.2, 0.0, em=em).solve([source("eq")], dz=1e-3)
+    assert rel_err_on_support(x, z["state_em"], blocks) < TOL
+    X = O.OracleSolver(run, 0.2, 0.0, K=2, em=em).solve([[source("eq")], [source("soft")]], dz=1e-3)
+    assert rel_err_on_support(X, z["state_em_multi"], blocks) < TOL
