@@ -37,6 +37,7 @@ extern "C" {
 #define PB_INJECTION 8u     /* enable_injection_jacobian    */
 #define PB_PARTIAL_DIFF 16u /* enable_partial_diff_jacobian */
 #define PB_DECAY 32u        /* enable_decay (explicit Lambda operator) */
+#define PB_EM_CASCADE 64u   /* co-evolved EM cascade (run.enable_em_cascade) */
 
 typedef struct pb_context pb_context;
 
@@ -113,6 +114,23 @@ int pb_set_decay(pb_context* ctx, const double* diag, int64_t nnz, const int64_t
  * (propagation.py:363-370, 2476-2488). */
 int pb_set_injection(pb_context* ctx, int32_t n_src, int32_t n_rows, const int32_t* rows,
                      const double* grids, int32_t n_cols, const int32_t* src_col);
+
+/* Co-evolved EM cascade layout: the gamma block (n_em states from gamma_off),
+ * the e- and e+ blocks (offsets, -1 if absent), and the charged nuclei whose
+ * Bethe-Heitler losses feed the pairs: n_bh blocks of n_cr states from
+ * bh_off[s] with mass numbers bh_A[s]; inv_E (1/E) and dE (numpy.gradient of
+ * E) on that nucleon grid.  Replaces: the EM attributes set in
+ * UHECRPropagationSolver.__init__ (src/prince_cr/solvers/propagation.py:270-305). */
+int pb_set_em(pb_context* ctx, int32_t n_em, int64_t gamma_off, int64_t em_off, int64_t ep_off,
+              int32_t n_cr, int32_t n_bh, const int64_t* bh_off, const double* bh_A,
+              const double* inv_E, const double* dE);
+
+/* Per-window EM-cascade data of the next solve: T_gamma and T_electron
+ * (n_windows x n_em x n_em), R_BH (n_windows x n_em x n_cr), row-major, and
+ * dl_step = c |dz| / ((1+z) H(z)) at each window.  Applied after every step
+ * (propagation.py:555-665: _inject_bh_pairs then _apply_em_cascade). */
+int pb_set_em_windows(pb_context* ctx, int32_t n_windows, const double* Tg, const double* Te,
+                      const double* R, const double* dl_step);
 
 /* One solve: the redshift stepping of UHECRPropagationSolverETD2.solve /
  * MultiRHSPropagationSolverETD2.solve (propagation.py:813-890; etd2.py:478-517;

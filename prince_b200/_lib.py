@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libprince_b
 
 PB_OK, PB_ERR_ARG, PB_ERR_STATE, PB_ERR_CUDA, PB_ERR_DEVICE = 0, 1, 2, 3, 4
 PB_ADIABATIC, PB_PAIRPROD, PB_PHOTOHAD, PB_INJECTION, PB_PARTIAL_DIFF, PB_DECAY = 1, 2, 4, 8, 16, 32
+PB_EM_CASCADE = 64
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)
@@ -64,6 +65,9 @@ _PROTOS = {
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
     "pb_set_injection": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _d, C.c_int32, _i32]),
+    "pb_set_em": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, _i64, _d, _d,
+                            _d]),
+    "pb_set_em_windows": (C.c_int, [_vp, C.c_int32, _d, _d, _d, _d]),
     "pb_solve": (C.c_int, [_vp, C.POINTER(SolveArgs)]),
     "pb_adjoint": (C.c_int, [_vp, C.POINTER(SolveArgs), _d, C.c_int32, _d, _d, _d]),
     "pb_get_operator_pattern": (C.c_int, [_vp, _i64, _i64, _i32]),
@@ -198,6 +202,17 @@ class Context:
         self._check(self.lib.pb_set_injection(self.h, int(src_col.size), int(rows.size), _ptr(rows, C.c_int32),
                                               _ptr(grids, C.c_double), int(n_cols), _ptr(src_col, C.c_int32)),
                     "pb_set_injection")
+
+    def set_em(self, n_em, gamma_off, em_off, ep_off, n_cr, bh_off, bh_A, inv_E, dE):
+        bo, ba, ie, de = _i64a(bh_off), _f64(bh_A), _f64(inv_E), _f64(dE)
+        self._check(self.lib.pb_set_em(self.h, int(n_em), int(gamma_off), int(em_off), int(ep_off), int(n_cr),
+                                       int(bo.size), _ptr(bo, C.c_int64), _ptr(ba, C.c_double),
+                                       _ptr(ie, C.c_double), _ptr(de, C.c_double)), "pb_set_em")
+
+    def set_em_windows(self, Tg, Te, R, dl_step):
+        Tg, Te, R, dl = _f64(Tg), _f64(Te), _f64(R), _f64(dl_step)
+        self._check(self.lib.pb_set_em_windows(self.h, int(dl.size), _ptr(Tg, C.c_double), _ptr(Te, C.c_double),
+                                               _ptr(R, C.c_double), _ptr(dl, C.c_double)), "pb_set_em_windows")
 
     # -- solve ----------------------------------------------------------
     def solve(self, sched, flags, n_cols, coeff, n_active, state, photon_scale=1.0, init_state=False,

@@ -43,6 +43,9 @@ class Plan:
 
     def __init__(self, run, initial_z, n_cols, rows, src_col, first_active, dz=1e-3, device=0,
                  ckpt_every=32, flags=FLAGS_ALL):
+        if getattr(run, "enable_em_cascade", False):
+            raise NotImplementedError("the co-evolved EM cascade hook has no adjoint; differentiate a run "
+                                      "without enable_em_cascade")
         self.run = run
         self.dev = DeviceRun.of(run, device)
         self.sched = make_schedule(z_grid(initial_z, 0.0, dz), run.backend.update_rates_z_threshold)

@@ -45,6 +45,7 @@ constexpr int kLongRow = 256;      // rows with more coupling entries are cut in
 constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
 constexpr int kColTile = 32;       // state columns per warp in the batched step
 constexpr int kSegLen = 256;       // coupling entries per long-row segment
+constexpr int kMaxEmBins = 160;    // EM / nucleon bins of the cascade hook (shared-memory tiles)
 
 thread_local std::string g_error;
 
@@ -122,6 +123,14 @@ struct pb_context {
   size_t scan_tmp_bytes = 0;
   int32_t last_W = 0;
   bool have_solution = false;
+  std::vector<int32_t> h_win;   // window of each step of the current solve (host copy)
+
+  // EM cascade
+  bool have_em = false;
+  int32_t em_n = 0, em_ncr = 0, em_nbh = 0, em_W = 0;
+  int64_t em_g = -1, em_m = -1, em_p = -1;
+  DBuf em_bh_off, em_bh_A, em_invE, em_dE, em_Tg, em_Te, em_R;
+  std::vector<double> em_dl;
 
   // transposed constant operators (adjoint)
   DBuf dt_indptr, dt_indices, dt_vals, lt_indptr, lt_indices, lt_vals;
@@ -898,6 +907,75 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// Co-evolved EM cascade, applied after every ETD2 step (propagation.py:555-665):
+//   w      = sum over charged nuclei s of (A_s kappa_pair_s dl_step / E dE) n_s   (per nucleon bin)
+//   e_src  = R_BH(z_w) w                     added to e- and e+
+//   gamma <- T_gamma gamma + T_electron (e- + e+),   e+- <- 0
+// One CTA per 32-column tile (lane = column), the per-column vectors in shared memory.
+// ---------------------------------------------------------------------------
+struct EmParams {
+  int64_t n;
+  int ld;
+  int ncols;
+  int n_em, n_cr, n_bh;
+  int64_t g_off, em_off, ep_off;  // block offsets of gamma, e-, e+ (e+- may be -1)
+  const int64_t* bh_off;          // block offset of each charged nucleus
+  const double* bh_A;
+  const double* invE;             // 1 / E on the nucleon grid
+  const double* dE;               // gradient of E
+  const double* kp;               // kappa_pair of the window (n)
+  double dl_step;
+  const double* Tg;               // n_em x n_em
+  const double* Te;               // n_em x n_em
+  const double* R;                // n_em x n_cr
+  double* X;
+};
+
+__global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
+  extern __shared__ double sm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int k = blockIdx.x * 32 + lane;
+  const bool active = k < e.ncols;
+  const int kk = active ? k : 0;
+  double* wv = sm;                       // n_cr x 32
+  double* gam = wv + (size_t)e.n_cr * 32;  // n_em x 32
+  double* lep = gam + (size_t)e.n_em * 32; // n_em x 32
+  for (int i = wid; i < e.n_cr; i += nw) {
+    double acc = 0.0;
+    for (int s = 0; s < e.n_bh; ++s) {
+      const int64_t row = e.bh_off[s] + i;
+      const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(e.bh_A[s], e.kp[row]), e.dl_step), e.invE[i]), e.dE[i]);
+      const double term = __dmul_rn(cw, e.X[(size_t)row * e.ld + kk]);
+      acc = (s == 0) ? term : __dadd_rn(acc, term);
+    }
+    wv[i * 32 + lane] = acc;
+  }
+  for (int j = wid; j < e.n_em; j += nw) gam[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
+  __syncthreads();
+  for (int j = wid; j < e.n_em; j += nw) {
+    double es = 0.0;
+    for (int i = 0; i < e.n_cr; ++i) es += e.R[(size_t)j * e.n_cr + i] * wv[i * 32 + lane];
+    double l = 0.0;
+    if (e.em_off >= 0) l = __dadd_rn(l, __dadd_rn(e.X[(size_t)(e.em_off + j) * e.ld + kk], es));
+    if (e.ep_off >= 0) l = __dadd_rn(l, __dadd_rn(e.X[(size_t)(e.ep_off + j) * e.ld + kk], es));
+    lep[j * 32 + lane] = l;
+  }
+  __syncthreads();
+  for (int j = wid; j < e.n_em; j += nw) {
+    double tg = 0.0, te = 0.0;
+    for (int i = 0; i < e.n_em; ++i) {
+      tg += e.Tg[(size_t)j * e.n_em + i] * gam[i * 32 + lane];
+      te += e.Te[(size_t)j * e.n_em + i] * lep[i * 32 + lane];
+    }
+    if (active) {
+      e.X[(size_t)(e.g_off + j) * e.ld + k] = __dadd_rn(tg, te);
+      if (e.em_off >= 0) e.X[(size_t)(e.em_off + j) * e.ld + k] = 0.0;
+      if (e.ep_off >= 0) e.X[(size_t)(e.ep_off + j) * e.ld + k] = 0.0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Discrete adjoint of the ETD2 step.  Forward, with A = dl (M_off + D_off diag(kappa)
 // + Lambda_off) frozen over the step:
 //   a = E x + h Phi1 (A x + b),   x' = a + h Phi2 A (a - x).
@@ -1111,7 +1189,7 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->nact, &c->ckpt, &c->lam,
           &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj, &c->gs, &c->g_out,
           &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
-          &c->sort_tmp};
+          &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -1232,6 +1310,32 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       }
       ++launches;
     }
+    if (c->have_em && (p.flags & PB_EM_CASCADE)) {
+      const int w = c->h_win[k];
+      EmParams e;
+      e.n = n;
+      e.ld = p.ld;
+      e.ncols = p.ncols;
+      e.n_em = c->em_n;
+      e.n_cr = c->em_ncr;
+      e.n_bh = c->em_nbh;
+      e.g_off = c->em_g;
+      e.em_off = c->em_m;
+      e.ep_off = c->em_p;
+      e.bh_off = c->em_bh_off.as<int64_t>();
+      e.bh_A = c->em_bh_A.as<double>();
+      e.invE = c->em_invE.as<double>();
+      e.dE = c->em_dE.as<double>();
+      e.kp = c->kp.as<double>() + (size_t)w * n;
+      e.dl_step = c->em_dl[w];
+      e.Tg = c->em_Tg.as<double>() + (size_t)w * c->em_n * c->em_n;
+      e.Te = c->em_Te.as<double>() + (size_t)w * c->em_n * c->em_n;
+      e.R = c->em_R.as<double>() + (size_t)w * c->em_n * c->em_ncr;
+      e.X = X;
+      const size_t smem = (size_t)(c->em_ncr + 2 * c->em_n) * 32 * sizeof(double);
+      k_em_hook<<<blocks_for(p.ncols, 32), 256, smem, st>>>(e);
+      ++launches;
+    }
   }
   return launches;
 }
@@ -1276,6 +1380,12 @@ int pb_create(int device, pb_context** out) {
   if (e != cudaSuccess) {
     pb_destroy(c);
     return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_fold_gemm): %s", cudaGetErrorString(e));
+  }
+  e = cudaFuncSetAttribute(k_em_hook, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           3 * kMaxEmBins * 32 * (int)sizeof(double));
+  if (e != cudaSuccess) {
+    pb_destroy(c);
+    return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_em_hook): %s", cudaGetErrorString(e));
   }
   *out = c;
   return PB_OK;
@@ -1347,7 +1457,8 @@ int pb_set_coupling(pb_context* c, int64_t n, int64_t R, const int64_t* indptr, 
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_coupling = true;
   c->have_kernel = false;
-  c->have_fd = c->have_losses = c->have_decay = false;
+  c->have_fd = c->have_losses = c->have_decay = c->have_em = false;
+  c->em_W = 0;
   c->n_src = 0;
   c->have_solution = false;
   return PB_OK;
@@ -1520,6 +1631,53 @@ int pb_set_injection(pb_context* c, int32_t n_src, int32_t n_rows, const int32_t
   return PB_OK;
 }
 
+int pb_set_em(pb_context* c, int32_t n_em, int64_t gamma_off, int64_t em_off, int64_t ep_off, int32_t n_cr,
+              int32_t n_bh, const int64_t* bh_off, const double* bh_A, const double* inv_E, const double* dE) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_em: set the coupling pattern first");
+  if (n_em < 1 || n_em > kMaxEmBins || n_cr < 1 || n_cr > kMaxEmBins || n_bh < 0 || (n_bh > 0 && (!bh_off || !bh_A)) ||
+      !inv_E || !dE)
+    return fail(c, PB_ERR_ARG, "pb_set_em: bad arguments (bins must be in [1, %d])", kMaxEmBins);
+  if (gamma_off < 0 || gamma_off + n_em > c->n) return fail(c, PB_ERR_ARG, "pb_set_em: gamma block out of range");
+  for (int64_t off : {em_off, ep_off})
+    if (off >= 0 && off + n_em > c->n) return fail(c, PB_ERR_ARG, "pb_set_em: lepton block out of range");
+  for (int s = 0; s < n_bh; ++s)
+    if (bh_off[s] < 0 || bh_off[s] + n_cr > c->n) return fail(c, PB_ERR_ARG, "pb_set_em: nucleus block out of range");
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->em_bh_off, bh_off, (size_t)n_bh))) return rc;
+  if ((rc = upload(c, c->em_bh_A, bh_A, (size_t)n_bh))) return rc;
+  if ((rc = upload(c, c->em_invE, inv_E, (size_t)n_cr))) return rc;
+  if ((rc = upload(c, c->em_dE, dE, (size_t)n_cr))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->em_n = n_em;
+  c->em_ncr = n_cr;
+  c->em_nbh = n_bh;
+  c->em_g = gamma_off;
+  c->em_m = em_off;
+  c->em_p = ep_off;
+  c->have_em = true;
+  c->em_W = 0;
+  return PB_OK;
+}
+
+int pb_set_em_windows(pb_context* c, int32_t n_windows, const double* Tg, const double* Te, const double* R,
+                      const double* dl_step) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_em) return fail(c, PB_ERR_STATE, "pb_set_em_windows: call pb_set_em first");
+  if (n_windows < 1 || !Tg || !Te || !R || !dl_step) return fail(c, PB_ERR_ARG, "pb_set_em_windows: bad arguments");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t nn = (size_t)c->em_n * c->em_n;
+  if ((rc = upload(c, c->em_Tg, Tg, nn * n_windows))) return rc;
+  if ((rc = upload(c, c->em_Te, Te, nn * n_windows))) return rc;
+  if ((rc = upload(c, c->em_R, R, (size_t)c->em_n * c->em_ncr * n_windows))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->em_dl.assign(dl_step, dl_step + n_windows);
+  c->em_W = n_windows;
+  return PB_OK;
+}
+
 int pb_solve(pb_context* c, const pb_solve_args* a) {
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
   if (!a) return fail(c, PB_ERR_ARG, "pb_solve: args is NULL");
@@ -1535,6 +1693,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   if (S > 0 && (!a->z_window || !a->window || !a->h || !a->dldz || !a->hc || !a->finj || !a->n_active))
     return fail(c, PB_ERR_ARG, "pb_solve: schedule arrays missing");
   const bool inj = (flags & PB_INJECTION) && c->n_src > 0;
+  if ((flags & PB_EM_CASCADE) && (!c->have_em || c->em_W != W))
+    return fail(c, PB_ERR_STATE, "pb_solve: EM cascade requested but pb_set_em / pb_set_em_windows (%d windows) missing", W);
   if (inj && c->n_src_cols != K) return fail(c, PB_ERR_ARG, "pb_solve: injection was set for %d columns, solve has %d", c->n_src_cols, K);
   if (inj && S > 0 && !a->coeff) return fail(c, PB_ERR_ARG, "pb_solve: coeff missing");
   for (int64_t k = 0; k < S; ++k) {
@@ -1542,6 +1702,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     if (a->n_active[k] < 0 || a->n_active[k] > K) return fail(c, PB_ERR_ARG, "pb_solve: n_active out of range");
   }
   if ((int64_t)W * c->n >= ((int64_t)1 << 40)) return fail(c, PB_ERR_ARG, "pb_solve: too many windows");
+  c->h_win.assign(a->window, a->window + S);
   int rc = set_device(c);
   if (rc) return rc;
   const int64_t n = c->n;
@@ -1614,7 +1775,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
                                                                           c->zwin.as<double>(), W, c->PT.as<double>());
   ++launches;
   const bool pair = (flags & PB_PAIRPROD) && (flags & PB_PARTIAL_DIFF);
-  if (pair) {
+  if (pair || (flags & PB_EM_CASCADE)) {  // the EM hook reads kappa_pair whatever the loss flags
     k_pair_rate<<<dim3(c->n_cr_bins, W), 128, 0, st>>>(fd, c->pair_pg.as<double>(), c->xi.as<double>(),
                                                        c->phi_xi2.as<double>(), c->n_xi, c->n_cr_bins,
                                                        c->zwin.as<double>(), c->rs.as<double>());
@@ -1676,6 +1837,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)S); put((uint64_t)W); put((uint64_t)K); put((uint64_t)ld); put(flags); put(inj); put(R);
     put((uint64_t)c->n_seg); put((uint64_t)c->h_short_rows.size()); put((uint64_t)c->n_cr_bins);
     put((uint64_t)a->ckpt_every);
+    put((uint64_t)c->em_W);
+    for (double v : c->em_dl) { uint64_t b; memcpy(&b, &v, 8); put(b); }
     const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);
     for (size_t i = 0; i < sizeof(fd); i += 8) { uint64_t w = 0; memcpy(&w, fb + i, std::min<size_t>(8, sizeof(fd) - i)); put(w); }
     for (const DBuf* b : all_buffers(c)) put((uint64_t)(uintptr_t)b->p);
@@ -1754,6 +1917,8 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   if (a->n_steps != c->last_S || a->n_cols != c->last_K || a->flags != c->last_flags ||
       a->ckpt_every != c->last_ckpt || a->n_windows != c->last_W || a->photon_scale != c->last_scale)
     return fail(c, PB_ERR_ARG, "pb_adjoint: arguments differ from the checkpointed solve");
+  if (a->flags & PB_EM_CASCADE)
+    return fail(c, PB_ERR_ARG, "pb_adjoint: the EM cascade hook has no adjoint (solve without PB_EM_CASCADE)");
   const int64_t S = a->n_steps, n = c->n, R = c->R;
   const int K = a->n_cols, CK = a->ckpt_every;
   const int ld = K == 1 ? 1 : ((K + kColTile - 1) / kColTile) * kColTile;

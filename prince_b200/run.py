@@ -194,10 +194,17 @@ class PriNCeRun:
             both grids must share the log step (the kernel construction contract).
         max_mass: keep species with ``A <= max_mass``.
         backend: a ``constants.BackendConfig`` (default backend ``"b200"``).
+        enable_em_cascade: co-evolve gamma and e+- with the nuclei (the
+            reference run's flag of the same name); the EM species share the
+            cosmic-ray grid.
+        em_cascade_model: ``callable(z) -> (T_gamma, T_electron, R_BH)``, the
+            per-redshift cascade transfer and Bethe-Heitler pair shape on that
+            grid, read by the solvers' ``_em_transfer_at`` / ``_em_bh_at``.
     """
 
     def __init__(self, cross_sections, photon_field, cosmic_ray_grid=(3, 14, 8),
-                 photon_grid=(-15, -6, 8), max_mass=np.inf, backend=None, species_list=None):
+                 photon_grid=(-15, -6, 8), max_mass=np.inf, backend=None, species_list=None,
+                 enable_em_cascade=False, em_cascade_model=None):
         self.backend = backend if backend is not None else C.BackendConfig()
         self.cross_sections = cross_sections
         self.photon_field = photon_field
@@ -220,7 +227,9 @@ class PriNCeRun:
         bm, rows, cols = cross_sections.build_kernel(self.cr_grid, self.ph_grid, self.spec_man)
         self.int_rates = PhotoNuclearInteractionRate(self, bm, rows, cols)
         self.em_int_rates = None
-        self.enable_em_cascade = False
+        self.enable_em_cascade = bool(enable_em_cascade)
+        self.em_cascade_model = em_cascade_model
+        self.em_grid = None
         self.spec_man.add_grid("ph", self.ph_grid.d)
 
     def set_photon_field(self, pfield):

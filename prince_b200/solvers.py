@@ -21,6 +21,7 @@ import scipy.sparse as sp
 
 from . import _lib
 from . import constants as C
+from .cosmology import H as _H
 from .cosmology import dldz as _dldz
 from .data import EnergyGrid, is_nucleus
 from .operators import fd_loss_operator, split_diagonal
@@ -188,6 +189,29 @@ class DeviceRun:
             self.ctx.set_decay(diag, None if off is None else sp.csr_matrix(off))
             self.has_decay = True
 
+    def ensure_em(self):
+        """Upload the EM-cascade layout once: gamma / e+- blocks and the charged
+        nuclei feeding Bethe-Heitler pairs (``propagation.py:270-305``)."""
+        if getattr(self, "_em_ready", False):
+            return
+        run = self.run
+        if getattr(run, "em_grid", None) is not None:
+            raise NotImplementedError("EM cascade on a separate (decoupled) EM grid is not supported; "
+                                      "put gamma and e+- on the cosmic-ray grid")
+        sm = run.spec_man
+        if 22 not in sm.pdgid2sref:
+            raise ValueError("enable_em_cascade needs the photon (22) among the run's species")
+        g = sm.pdgid2sref[22]
+        lep = [sm.pdgid2sref[p].lidx() if p in sm.pdgid2sref else -1 for p in (11, -11)]
+        bh = [(s.lidx(), float(s.A)) for s in sm.species_refs if s.is_nucleus and abs(s.charge) >= 1]
+        E = run.cr_grid.grid
+        with np.errstate(divide="ignore"):
+            inv_E = np.where(E > 0, 1.0 / E, 0.0)
+        self.ctx.set_em(g.uidx() - g.lidx(), g.lidx(), lep[0], lep[1], E.size,
+                        np.array([b[0] for b in bh], dtype=np.int64), np.array([b[1] for b in bh]),
+                        inv_E, np.gradient(E))
+        self._em_ready = True
+
     @classmethod
     def of(cls, run, device=0):
         cache = getattr(run, "_b200_device_runs", None)
@@ -252,6 +276,9 @@ class UHECRPropagationSolverETD2:
         self.device = device
         self._dev = DeviceRun.of(prince_run, device)
         self.last_timing = None
+        self.enable_em_cascade = bool(getattr(prince_run, "enable_em_cascade", False))
+        if self.enable_em_cascade:
+            self._dev.ensure_em()
         if enable_decay and not self._dev.has_decay:
             unstable = [s for s in self.spec_man.species_refs if np.isfinite(getattr(s, "lifetime", np.inf))]
             if unstable:
@@ -285,6 +312,37 @@ class UHECRPropagationSolverETD2:
     def close(self):
         pass
 
+    # -- co-evolved EM cascade (propagation.py:540-665) --------------------
+    def _em_model(self, z):
+        model = getattr(self.prince_run, "em_cascade_model", None)
+        if model is None:
+            raise NotImplementedError(
+                "enable_em_cascade needs the run's em_cascade_model(z) -> (T_gamma, T_electron, R_BH), "
+                "or overrides of _em_transfer_at / _em_bh_at")
+        return model(z)
+
+    def _em_transfer_at(self, z):
+        """(T_gamma, T_electron) of the cascade transfer at redshift z."""
+        return tuple(self._em_model(z)[:2])
+
+    def _em_bh_at(self, z):
+        """Bethe-Heitler e+- pair shape R_BH at redshift z."""
+        return self._em_model(z)[2]
+
+    def _em_windows(self, sched, dz):
+        """Per-window T_gamma, T_electron, R_BH and dl_step = c |dz| / ((1+z) H(z)),
+        all at the window's redshift (``_refresh_z_caches`` and
+        ``_inject_bh_pairs``, ``propagation.py:620-665``)."""
+        Tg, Te, R, dl = [], [], [], []
+        for zw in sched.z_window:
+            zw = float(zw)
+            tg, te = self._em_transfer_at(zw)
+            Tg.append(np.asarray(tg, dtype=np.float64))
+            Te.append(np.asarray(te, dtype=np.float64))
+            R.append(np.asarray(self._em_bh_at(zw), dtype=np.float64))
+            dl.append(C.PRINCE_UNITS.c * abs(dz) / ((1.0 + zw) * _H(zw)))
+        return np.stack(Tg), np.stack(Te), np.stack(R), np.array(dl)
+
     # -- solve -----------------------------------------------------------
     def _flags(self):
         f = 0
@@ -300,6 +358,8 @@ class UHECRPropagationSolverETD2:
             f |= _lib.PB_PARTIAL_DIFF
         if self.enable_decay and self._dev.has_decay:
             f |= _lib.PB_DECAY
+        if self.enable_em_cascade:
+            f |= _lib.PB_EM_CASCADE
         return f
 
     def _column_sources(self):
@@ -350,6 +410,8 @@ class UHECRPropagationSolverETD2:
         else:
             flags &= ~_lib.PB_INJECTION
         ctx.set_photon_field(device_components(self.prince_run.photon_field))
+        if flags & _lib.PB_EM_CASCADE:
+            ctx.set_em_windows(*self._em_windows(sched, dz))
         out = np.zeros((self.dim_states, K))
         ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, out, photon_scale=self._photon_scale())
         state = np.empty_like(out)

@@ -69,12 +69,13 @@ def light_network_em():
 
     z = dict(np.load(os.path.join(GOLDEN, "light_network_em.npz")))
     model = FixedKernelModel(z["species"], z["batch_matrix"], z["batch_rows"], z["batch_cols"])
-    run = PriNCeRun(model, photonfields.CMBPhotonSpectrum(), cosmic_ray_grid=tuple(z["cr_grid"]),
-                    photon_grid=tuple(z["ph_grid"]))
     grid = EnergyGrid(*tuple(z["cr_grid"]))
 
     def em(zz):
         return synth.em_cascade_matrices(grid, grid, float(zz))
+
+    run = PriNCeRun(model, photonfields.CMBPhotonSpectrum(), cosmic_ray_grid=tuple(z["cr_grid"]),
+                    photon_grid=tuple(z["ph_grid"]), enable_em_cascade=True, em_cascade_model=em)
 
     def source(key, m="flat"):
         params = ast.literal_eval(str(z[f"src_{key}"]))
