@@ -39,6 +39,12 @@ extern "C" {
 #define PB_DECAY 32u        /* enable_decay (explicit Lambda operator) */
 #define PB_EM_CASCADE 64u   /* co-evolved EM cascade (run.enable_em_cascade) */
 
+/* pb_set_option / pb_get_info keys */
+#define PB_OPT_BATCHED_KERNELS 1 /* 1 (default): bin-blocked kernels for K > 1 when the layout allows; 0: row kernels */
+#define PB_INFO_BLOCKED_LAYOUT 2 /* 1 if pb_set_layout found a pattern the bin-blocked kernels handle */
+#define PB_INFO_LAST_BLOCKED 3   /* 1 if the last pb_solve ran the bin-blocked kernels */
+#define PB_INFO_BAND_SPECIES 4   /* species whose coupling rows leave their energy bin */
+
 typedef struct pb_context pb_context;
 
 /* Version of this ABI (bumped on any signature change). */
@@ -114,6 +120,18 @@ int pb_set_decay(pb_context* ctx, const double* diag, int64_t nnz, const int64_t
  * (propagation.py:363-370, 2476-2488). */
 int pb_set_injection(pb_context* ctx, int32_t n_src, int32_t n_rows, const int32_t* rows,
                      const double* grids, int32_t n_cols, const int32_t* src_col);
+
+/* State layout: species blocks of d energy bins (n = n_species * d), the
+ * SpeciesManager layout on a shared grid (src/prince_cr/data.py:1385-1450).
+ * Classifies the coupling rows into
+ * bin-local rows and band rows for the bin-blocked batched kernels.  No
+ * reference counterpart (the reference multiplies the whole CSR operator). */
+int pb_set_layout(pb_context* ctx, int32_t d);
+
+/* Execution options (PB_OPT_*) and read-only facts (PB_INFO_*) of a context.
+ * No reference counterpart. */
+int pb_set_option(pb_context* ctx, int32_t key, int64_t value);
+int pb_get_info(pb_context* ctx, int32_t key, int64_t* value);
 
 /* Co-evolved EM cascade layout: the gamma block (n_em states from gamma_off),
  * the e- and e+ blocks (offsets, -1 if absent), and the charged nuclei whose

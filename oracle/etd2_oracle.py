@@ -190,7 +190,7 @@ class OracleSolver:
     """
 
     def __init__(self, run, initial_z, final_z, flags=None, thr=None, K=None, decay=None, exp="numpy",
-                 em=None):
+                 em=None, perturb=None):
         self.run = run
         self.initial_z = float(initial_z)
         self.final_z = float(final_z)
@@ -225,6 +225,13 @@ class OracleSolver:
             self._em_lep_sl = [sm.pdgid2sref[p].sl for p in (11, -11) if p in sm.pdgid2sref]
             self._em_bh_species = [(sp.sl, float(sp.A)) for sp in sm.species_refs
                                    if sp.is_nucleus and abs(sp.charge) >= 1]
+        # ``perturb=(delta, seed)`` multiplies every window's operator values
+        # (M_off, its diagonal, kappa_pair) by 1 + delta N(0, 1): a probe of how
+        # far each output bin moves under operator differences of the size
+        # that different math libraries and summation orders produce.
+        self._perturb = None
+        if perturb is not None:
+            self._perturb = (float(perturb[0]), np.random.default_rng(int(perturb[1])))
         self.trace = Trace()
 
     # -- per window --------------------------------------------------------
@@ -248,6 +255,12 @@ class OracleSolver:
             d_M[present] = vec[self.diag_to_M[present]]
             self.d_M = d_M
         self.kappa_pair = _pair_loss(self.run, z) if self.flags.pairprod else None
+        if self._perturb is not None:
+            delta, rng = self._perturb
+            self.M_off.data *= 1.0 + delta * rng.standard_normal(self.M_off.data.size)
+            self.d_M = self.d_M * (1.0 + delta * rng.standard_normal(self.d_M.size))
+            if self.kappa_pair is not None:
+                self.kappa_pair = self.kappa_pair * (1.0 + delta * rng.standard_normal(self.kappa_pair.size))
         if self.em is not None:
             self._em_T = self.em(z)
             self._em_z = float(z)

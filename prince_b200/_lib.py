@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libprince_b
 PB_OK, PB_ERR_ARG, PB_ERR_STATE, PB_ERR_CUDA, PB_ERR_DEVICE = 0, 1, 2, 3, 4
 PB_ADIABATIC, PB_PAIRPROD, PB_PHOTOHAD, PB_INJECTION, PB_PARTIAL_DIFF, PB_DECAY = 1, 2, 4, 8, 16, 32
 PB_EM_CASCADE = 64
+PB_OPT_BATCHED_KERNELS, PB_INFO_BLOCKED_LAYOUT, PB_INFO_LAST_BLOCKED, PB_INFO_BAND_SPECIES = 1, 2, 3, 4
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)
@@ -65,6 +66,9 @@ _PROTOS = {
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
     "pb_set_injection": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _d, C.c_int32, _i32]),
+    "pb_set_layout": (C.c_int, [_vp, C.c_int32]),
+    "pb_set_option": (C.c_int, [_vp, C.c_int32, C.c_int64]),
+    "pb_get_info": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int64)]),
     "pb_set_em": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, _i64, _d, _d,
                             _d]),
     "pb_set_em_windows": (C.c_int, [_vp, C.c_int32, _d, _d, _d, _d]),
@@ -202,6 +206,17 @@ class Context:
         self._check(self.lib.pb_set_injection(self.h, int(src_col.size), int(rows.size), _ptr(rows, C.c_int32),
                                               _ptr(grids, C.c_double), int(n_cols), _ptr(src_col, C.c_int32)),
                     "pb_set_injection")
+
+    def set_layout(self, d):
+        self._check(self.lib.pb_set_layout(self.h, int(d)), "pb_set_layout")
+
+    def set_option(self, key, value):
+        self._check(self.lib.pb_set_option(self.h, int(key), int(value)), "pb_set_option")
+
+    def info(self, key):
+        v = C.c_int64(0)
+        self._check(self.lib.pb_get_info(self.h, int(key), C.byref(v)), "pb_get_info")
+        return int(v.value)
 
     def set_em(self, n_em, gamma_off, em_off, ep_off, n_cr, bh_off, bh_A, inv_E, dE):
         bo, ba, ie, de = _i64a(bh_off), _f64(bh_A), _f64(inv_E), _f64(dE)

@@ -125,6 +125,20 @@ struct pb_context {
   bool have_solution = false;
   std::vector<int32_t> h_win;   // window of each step of the current solve (host copy)
 
+  // bin-blocked batched path (pb_set_layout): species blocks of `lay_d` bins
+  std::vector<int64_t> h_cpl_indptr;
+  std::vector<int32_t> h_cpl_indices;
+  int32_t lay_d = 0, lay_nsp = 0;
+  bool blocked_ok = false;          // the coupling pattern admits the band + slab kernels
+  int32_t band_nb = 0, band_RT = 0, band_J = 0, n_slab_spec = 0;
+  int64_t band_stride = 0;          // band-tile doubles per window
+  DBuf band_slot, band_mask, band_spec, slab_spec, band_vals, band_part, m_sidx;
+  int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
+  bool last_blocked = false;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int num_sms = 148;
+
   // EM cascade
   bool have_em = false;
   int32_t em_n = 0, em_ncr = 0, em_nbh = 0, em_W = 0;
@@ -286,12 +300,14 @@ __global__ void k_fold_first(const double* __restrict__ K, int64_t R, int dph,
 __global__ void k_compact(const int* __restrict__ keep, const int* __restrict__ pos,
                           const int* __restrict__ cpl_indices, const int* __restrict__ is_diag,
                           const int* __restrict__ row, int64_t R, int* __restrict__ dest,
-                          int* __restrict__ diag_row, int* __restrict__ m_indices) {
+                          int* __restrict__ diag_row, int* __restrict__ m_indices, int d,
+                          int* __restrict__ m_sidx) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= R) return;
   if (keep[i]) {
     dest[i] = pos[i];
     m_indices[pos[i]] = cpl_indices[i];
+    if (m_sidx) m_sidx[pos[i]] = cpl_indices[i] / d;
   } else {
     dest[i] = -1;
   }
@@ -322,8 +338,8 @@ __global__ void k_seg_map(const int64_t* __restrict__ cb, const int64_t* __restr
 // axis in shared memory; the epilogue scatters into M_off values / diagonal.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(c0), "+d"(c1)
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
 
@@ -334,7 +350,9 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
                                                    const int* __restrict__ dest,
                                                    const int* __restrict__ diag_row,
                                                    double* __restrict__ mv, int64_t mv_stride,
-                                                   double* __restrict__ md, int64_t n) {
+                                                   double* __restrict__ md, int64_t n,
+                                                   const int* __restrict__ band_slot,
+                                                   double* __restrict__ band, int64_t band_stride) {
   extern __shared__ double smem[];
   const int lda = kpad + 4;  // +4 doubles: 8-row fragments spread over all banks
   double* As = smem;
@@ -375,6 +393,7 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
     if (r >= R) continue;
     const int de = dest[r];
     const int dr = diag_row[r];
+    const int bs = (band_slot && de >= 0) ? band_slot[r] : -1;
 #pragma unroll
     for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
@@ -384,6 +403,7 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
         const double v = acc[mt][nt][i];
         if (de >= 0) mv[(size_t)w * mv_stride + de] = v;
         if (dr >= 0) md[(size_t)w * n + dr] = v;
+        if (bs >= 0) band[(size_t)w * band_stride + bs] = v;
       }
   }
 }
@@ -552,6 +572,20 @@ struct StepParams {
   double* rec_sx;           // n x ld: S x of the current step (stage 1 -> stage 2)
   int64_t rec_k0;
   int rec_len;
+  // bin-blocked batched path
+  int d;                    // bins per species block
+  int nsp;                  // species blocks
+  const int* slab_spec;     // species whose coupling rows are bin-local
+  int n_slab_spec;
+  const int* m_sidx;        // species block of each M_off column
+  const int* band_spec;     // species with cross-bin coupling rows
+  int nb;
+  const double* band_vals;  // [W][nb][nsp][RT][J][32] DMMA A fragments
+  int64_t band_stride;
+  const uint32_t* band_mask;  // [nb][nsp][RT]: k-tiles present per row tile
+  double* band_part;        // [G][nb][d][ld] partial sums of the band rows
+  int ngroups;              // mother-species groups of the band launch
+  int spg;                  // species per group
 };
 
 struct StepScalars {
@@ -907,6 +941,166 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// Bin-blocked batched stage kernels.
+//
+// States are species blocks of d energy bins.  The coupling rows split in two
+// classes (pb_set_layout):
+//  * bin-local rows: every M_off entry couples bin e to bin e of another
+//    species (boost-conserving fragments).  k_slab stages the state slab of one
+//    bin -- all species x 32 columns -- in shared memory and sums each row
+//    from there, so a state value is read from DRAM once per stage instead of
+//    once per coupling entry.
+//  * band rows (species with cross-bin entries: the redistributed nucleons):
+//    their block rows against each mother species form a band of d x d tiles.
+//    k_band multiplies them on the FP64 tensor pipe (DMMA m8n8k4) with the
+//    tiles stored in fragment order per window, split over groups of mother
+//    species into partial sums that k_band_finish adds in group order.
+// k_band runs on a second stream, concurrently with k_slab (they touch
+// disjoint outputs); k_band_finish follows both.
+// ---------------------------------------------------------------------------
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_slab(StepParams p) {
+  extern __shared__ double slab[];
+  const StepScalars s = load_scalars(p, p.step);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int e = blockIdx.x;
+  const int col = blockIdx.y * kColTile + lane;  // < ld: the grid covers the active columns only
+  const bool active = col < p.ncols;
+  if (s.photohad) {
+    const double* __restrict__ v = p.src + (size_t)e * p.ld + col;
+    const size_t sstride = (size_t)p.d * p.ld;
+    for (int q = wid; q < p.nsp; q += nw) slab[q * kColTile + lane] = v[q * sstride];
+    __syncthreads();
+  }
+  const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
+  for (int i = wid; i < p.n_slab_spec; i += nw) {
+    const int64_t r = (int64_t)p.slab_spec[i] * p.d + e;
+    double acc = 0.0;
+    if (s.photohad) {
+      const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
+      for (int64_t base = j0; base < j1; base += 32) {
+        const int64_t j = base + lane;
+        const double mvl = (j < j1) ? mv[j] : 0.0;
+        const int sl = (j < j1) ? p.m_sidx[j] : 0;
+        const int cnt = (int)min((int64_t)32, j1 - base);
+        for (int q = 0; q < cnt; ++q) {
+          const double mq = __shfl_sync(0xffffffffu, mvl, q);
+          const int sq = __shfl_sync(0xffffffffu, sl, q);
+          acc = __dadd_rn(acc, __dmul_rn(mq, slab[sq * kColTile + lane]));
+        }
+      }
+    }
+    if (active) row_epilogue<STAGE>(p, s, r, col, acc);
+    if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
+  }
+}
+
+// Band partial sums.  CTA = (128-column block, mother-species group, band
+// species); warp = 16 columns (two 8-column DMMA tiles) x all d rows of the
+// band species, accumulators in registers (RT row tiles x 2 column tiles).
+// For each mother species the warp walks the 2 RT k-tiles (4 mother bins
+// each): it loads the X fragment of the k-tile once and multiplies it into
+// every row tile whose band holds that k-tile (mask bit set).
+template <int RT, int J>
+__global__ void __launch_bounds__(256, RT <= 12 ? 2 : 1) k_band(StepParams p) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int c0 = blockIdx.x * 128 + wid * 16;
+  if (c0 >= p.ncols) return;  // c0 + 15 < ld: ld is a multiple of 32
+  const int b = blockIdx.z, g = blockIdx.y;
+  const int s0 = g * p.spg, s1 = min(p.nsp, s0 + p.spg);
+  const int d = p.d, ld = p.ld;
+  const int w = p.win[p.step];
+  const double* __restrict__ A = p.band_vals + (size_t)w * p.band_stride;
+  double acc[RT][2][2];
+#pragma unroll
+  for (int rt = 0; rt < RT; ++rt) acc[rt][0][0] = acc[rt][0][1] = acc[rt][1][0] = acc[rt][1][1] = 0.0;
+  const int kr = lane & 3;
+  for (int sp = s0; sp < s1; ++sp) {
+    const double* __restrict__ xs = p.src + (size_t)sp * d * ld + c0 + (lane >> 2);
+    const size_t tb = (size_t)(b * p.nsp + sp) * RT;
+    const double* __restrict__ as = A + tb * J * 32 + lane;
+    uint32_t m[RT];
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) m[rt] = p.band_mask[tb + rt];
+#pragma unroll
+    for (int kt = 0; kt < 2 * RT; ++kt) {
+      const int e = 4 * kt + kr;
+      double b0 = 0.0, b1 = 0.0;
+      if (e < d) {
+        b0 = xs[(size_t)e * ld];
+        b1 = xs[(size_t)e * ld + 8];
+      }
+#pragma unroll
+      for (int rt = 0; rt < RT; ++rt) {
+        const int jj = kt - 2 * rt;
+        if (jj < 0 || jj >= J) continue;
+        if (m[rt] & (1u << jj)) {
+          const double a = as[(rt * J + jj) * 32];
+          dmma884(acc[rt][0][0], acc[rt][0][1], a, b0);
+          dmma884(acc[rt][1][0], acc[rt][1][1], a, b1);
+        }
+      }
+    }
+  }
+  double* __restrict__ P = p.band_part + (size_t)(g * p.nb + b) * d * ld;
+#pragma unroll
+  for (int rt = 0; rt < RT; ++rt) {
+    const int row = 8 * rt + (lane >> 2);
+    if (row >= d) continue;
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+      double2 v;
+      v.x = acc[rt][nt][0];
+      v.y = acc[rt][nt][1];
+      *reinterpret_cast<double2*>(P + (size_t)row * ld + c0 + nt * 8 + kr * 2) = v;
+    }
+  }
+}
+
+// Band rows: add the group partials in group order, then the row epilogue.
+template <int STAGE>
+__global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
+  const StepScalars s = load_scalars(p, p.step);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int rb = blockIdx.x * (blockDim.x >> 5) + wid;
+  if (rb >= p.nb * p.d) return;
+  const int b = rb / p.d, e = rb - b * p.d;
+  const int64_t r = (int64_t)p.band_spec[b] * p.d + e;
+  const int col = blockIdx.y * kColTile + lane;
+  double t = 0.0;
+  for (int g = 0; g < p.ngroups; ++g)
+    t = __dadd_rn(t, p.band_part[((size_t)(g * p.nb + b) * p.d + e) * p.ld + col]);
+  if (col < p.ncols) row_epilogue<STAGE>(p, s, r, col, t);
+  if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
+}
+
+// Instances of k_band: row tiles RT (d <= 8 RT) x k-tiles per row tile J
+// (band offsets up to 4 J - 8 bins).
+using BandKernel = void (*)(StepParams);
+constexpr int kBandRT[] = {4, 8, 12, 16};
+constexpr int kBandJ[] = {5, 9, 13, 17};
+template <int RT>
+BandKernel band_kernel_j(int J) {
+  switch (J) {
+    case 5: return k_band<RT, 5>;
+    case 9: return k_band<RT, 9>;
+    case 13: return k_band<RT, 13>;
+    case 17: return k_band<RT, 17>;
+  }
+  return nullptr;
+}
+BandKernel band_kernel(int RT, int J) {
+  switch (RT) {
+    case 4: return band_kernel_j<4>(J);
+    case 8: return band_kernel_j<8>(J);
+    case 12: return band_kernel_j<12>(J);
+    case 16: return band_kernel_j<16>(J);
+  }
+  return nullptr;
+}
+constexpr int kMaxBandGroups = 64;
+
+// ---------------------------------------------------------------------------
 // Co-evolved EM cascade, applied after every ETD2 step (propagation.py:555-665):
 //   w      = sum over charged nuclei s of (A_s kappa_pair_s dl_step / E dE) n_s   (per nucleon bin)
 //   e_src  = R_BH(z_w) w                     added to e- and e+
@@ -1189,7 +1383,8 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->nact, &c->ckpt, &c->lam,
           &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj, &c->gs, &c->g_out,
           &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
-          &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R};
+          &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
+          &c->band_slot, &c->band_mask, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->m_sidx};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -1273,6 +1468,50 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.partial = c->partial.as<double>();
   p.counter = c->counter.as<int>();
   p.ctiles = ctiles;
+  p.d = c->lay_d;
+  p.nsp = c->lay_nsp;
+  p.slab_spec = c->slab_spec.as<int>();
+  p.n_slab_spec = c->n_slab_spec;
+  p.m_sidx = c->m_sidx.as<int>();
+  p.band_spec = c->band_spec.as<int>();
+  p.nb = c->band_nb;
+  p.band_vals = c->band_vals.as<double>();
+  p.band_stride = c->band_stride;
+  p.band_mask = c->band_mask.as<uint32_t>();
+  p.band_part = c->band_part.as<double>();
+}
+
+// Whether a solve with K columns runs the bin-blocked kernels.
+bool use_blocked(const pb_context* c, int K) { return c->blocked_ok && c->batched_mode == 1 && K > 1; }
+
+// One stage of the bin-blocked path: k_band (second stream) || k_slab, then k_band_finish.
+template <int STAGE>
+int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
+  const bool photohad = (p.flags & PB_PHOTOHAD) != 0;
+  int64_t launches = 0;
+  p.ngroups = 0;
+  p.spg = 1;
+  if (photohad && p.nb > 0) {
+    const int cblocks = (int)blocks_for(p.ncols, 128);
+    const int target = 2 * c->num_sms;
+    int G = std::max(1, std::min({(target + cblocks * p.nb - 1) / (cblocks * p.nb), kMaxBandGroups, p.nsp}));
+    p.spg = (p.nsp + G - 1) / G;
+    p.ngroups = (p.nsp + p.spg - 1) / p.spg;
+    cudaEventRecord(c->ev_fork, st);
+    cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+    band_kernel(c->band_RT, c->band_J)<<<dim3(cblocks, p.ngroups, p.nb), 256, 0, c->stream2>>>(p);
+    cudaEventRecord(c->ev_join, c->stream2);
+    ++launches;
+  }
+  const size_t smem = photohad ? (size_t)p.nsp * kColTile * sizeof(double) : 0;
+  k_slab<STAGE><<<dim3(p.d, blocks_for(p.ncols, kColTile)), 256, smem, st>>>(p);
+  ++launches;
+  if (p.ngroups > 0) cudaStreamWaitEvent(st, c->ev_join, 0);
+  if (p.nb > 0) {
+    k_band_finish<STAGE><<<dim3(blocks_for((int64_t)p.nb * p.d, 8), blocks_for(p.ncols, kColTile)), 256, 0, st>>>(p);
+    ++launches;
+  }
+  return launches;
 }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
@@ -1297,10 +1536,15 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       ++launches;
       prepared = true;
     }
+    const bool blocked = use_blocked(c, K) && !p.rec_P && !p.dsig;
     for (int stage = 1; stage <= 2; ++stage) {
       p.src = stage == 1 ? X : c->A.as<double>();
       p.x = X;
       p.xout = X;
+      if (blocked) {
+        launches += stage == 1 ? launch_blocked_stage<1>(c, p, st) : launch_blocked_stage<2>(c, p, st);
+        continue;
+      }
       const unsigned tiles = K == 1 ? 1u : blocks_for(p.ncols, kColTile);
       dim3 grid((unsigned)p.nsb + blocks_for(p.nseg, 8), tiles);
       if (K == 1) {
@@ -1369,9 +1613,13 @@ int pb_create(int device, pb_context** out) {
     return fail(nullptr, PB_ERR_CUDA, "device %d is sm_%d%d; this build targets sm_100a", device, prop.major, prop.minor);
   pb_context* c = new pb_context();
   c->device = device;
+  c->num_sms = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
-      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess) {
+      cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
     return fail(nullptr, PB_ERR_CUDA, "stream/event creation failed");
   }
@@ -1395,6 +1643,7 @@ void pb_destroy(pb_context* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  if (c->stream2) cudaStreamSynchronize(c->stream2);
   for (DBuf* b : all_buffers(c)) b->release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph_exec2) cudaGraphExecDestroy(c->graph_exec2);
@@ -1402,6 +1651,9 @@ void pb_destroy(pb_context* c) {
   cudaEventDestroy(c->ev1);
   cudaEventDestroy(c->ev2);
   cudaEventDestroy(c->ev3);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->stream2) cudaStreamDestroy(c->stream2);
   cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -1422,6 +1674,10 @@ int pb_set_coupling(pb_context* c, int64_t n, int64_t R, const int64_t* indptr, 
   if (rc) return rc;
   c->n = n;
   c->R = R;
+  c->h_cpl_indptr.assign(indptr, indptr + n + 1);
+  c->h_cpl_indices.assign(indices, indices + R);
+  c->blocked_ok = false;
+  c->lay_d = c->lay_nsp = 0;
   if ((rc = upload(c, c->cpl_indptr, indptr, (size_t)n + 1))) return rc;
   if ((rc = upload(c, c->cpl_indices, indices, (size_t)R))) return rc;
   PB_CUDA(c, c->cpl_row.ensure((size_t)std::max<int64_t>(R, 1) * sizeof(int)));
@@ -1631,6 +1887,107 @@ int pb_set_injection(pb_context* c, int32_t n_src, int32_t n_rows, const int32_t
   return PB_OK;
 }
 
+int pb_set_layout(pb_context* c, int32_t d) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_layout: set the coupling pattern first");
+  if (d <= 0 || c->n % d != 0) return fail(c, PB_ERR_ARG, "pb_set_layout: %lld states are not blocks of %d bins", (long long)c->n, d);
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int64_t n = c->n, R = c->R;
+  const int nsp = (int)(n / d);
+  const std::vector<int64_t>& ip = c->h_cpl_indptr;
+  const std::vector<int32_t>& ix = c->h_cpl_indices;
+  // band species: rows with an off-diagonal entry that leaves the row's bin
+  std::vector<int> band_of(nsp, -1);
+  std::vector<int32_t> bspec, sspec;
+  int lo = 1 << 30, hi = -(1 << 30);
+  for (int sp = 0; sp < nsp; ++sp) {
+    bool band = false;
+    for (int64_t r = (int64_t)sp * d; r < (int64_t)(sp + 1) * d && !band; ++r)
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
+        if (ix[j] != r && ix[j] % d != r % d) { band = true; break; }
+    if (band) {
+      band_of[sp] = (int)bspec.size();
+      bspec.push_back(sp);
+    } else {
+      sspec.push_back(sp);
+    }
+  }
+  for (int32_t sp : bspec)
+    for (int64_t r = (int64_t)sp * d; r < (int64_t)(sp + 1) * d; ++r)
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+        if (ix[j] == r) continue;
+        const int off = ix[j] % d - (int)(r % d);
+        lo = std::min(lo, off);
+        hi = std::max(hi, off);
+      }
+  c->blocked_ok = false;
+  c->lay_d = d;
+  c->lay_nsp = nsp;
+  const size_t slab_bytes = (size_t)nsp * kColTile * sizeof(double);
+  const int RTr = (d + 7) / 8;
+  const int Jr = bspec.empty() ? 1 : (7 + hi) / 4 + 1;
+  int RT = 0, J = 0;
+  for (int v : kBandRT) if (!RT && v >= RTr) RT = v;
+  for (int v : kBandJ) if (!J && v >= Jr) J = v;
+  const bool ok = slab_bytes <= 227 * 1024 && RT > 0 && J > 0 && (bspec.empty() || lo >= 0) &&
+                  (int64_t)bspec.size() * nsp * RT * J * 32 < ((int64_t)1 << 31);
+  if (!ok) return PB_OK;  // the general row kernels stay in use
+  const int nb = (int)bspec.size();
+  std::vector<int32_t> slot((size_t)std::max<int64_t>(R, 1), -1);
+  std::vector<uint32_t> mask((size_t)std::max(nb * nsp * RT, 1), 0u);
+  for (int b = 0; b < nb; ++b)
+    for (int e = 0; e < d; ++e) {
+      const int64_t r = (int64_t)bspec[b] * d + e;
+      const int rt = e / 8;
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+        if (ix[j] == r) continue;
+        const int sp = ix[j] / d, e2 = ix[j] % d;
+        const int jj = e2 / 4 - 2 * rt;
+        const size_t tile = ((size_t)(b * nsp + sp) * RT + rt);
+        slot[j] = (int32_t)((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4));
+        mask[tile] |= 1u << jj;
+      }
+    }
+  if ((rc = upload(c, c->band_slot, slot.data(), slot.size()))) return rc;
+  if ((rc = upload(c, c->band_mask, mask.data(), mask.size()))) return rc;
+  if ((rc = upload(c, c->band_spec, bspec.data(), bspec.size()))) return rc;
+  if ((rc = upload(c, c->slab_spec, sspec.data(), sspec.size()))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_bytes));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_bytes));
+  c->band_nb = nb;
+  c->band_RT = RT;
+  c->band_J = J;
+  c->band_stride = (int64_t)nb * nsp * RT * J * 32;
+  c->n_slab_spec = (int)sspec.size();
+  c->blocked_ok = true;
+  return PB_OK;
+}
+
+int pb_set_option(pb_context* c, int32_t key, int64_t value) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  switch (key) {
+    case PB_OPT_BATCHED_KERNELS:
+      if (value != 0 && value != 1) return fail(c, PB_ERR_ARG, "pb_set_option: batched kernels must be 0 or 1");
+      c->batched_mode = (int32_t)value;
+      return PB_OK;
+  }
+  return fail(c, PB_ERR_ARG, "pb_set_option: unknown key %d", key);
+}
+
+int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!value) return fail(c, PB_ERR_ARG, "pb_get_info: value is NULL");
+  switch (key) {
+    case PB_OPT_BATCHED_KERNELS: *value = c->batched_mode; return PB_OK;
+    case PB_INFO_BLOCKED_LAYOUT: *value = c->blocked_ok ? 1 : 0; return PB_OK;
+    case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
+    case PB_INFO_BAND_SPECIES: *value = c->band_nb; return PB_OK;
+  }
+  return fail(c, PB_ERR_ARG, "pb_get_info: unknown key %d", key);
+}
+
 int pb_set_em(pb_context* c, int32_t n_em, int64_t gamma_off, int64_t em_off, int64_t ep_off, int32_t n_cr,
               int32_t n_bh, const int64_t* bh_off, const double* bh_A, const double* inv_E, const double* dE) {
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
@@ -1745,6 +2102,13 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   if (a->ckpt_every < 0) return fail(c, PB_ERR_ARG, "pb_solve: ckpt_every must be >= 0");
   if (a->ckpt_every > 0)
     PB_CUDA(c, c->ckpt.ensure((size_t)((S + a->ckpt_every - 1) / a->ckpt_every + 1) * n * ld * sizeof(double)));
+  const bool blocked = use_blocked(c, K);
+  if (blocked) {
+    PB_CUDA(c, c->m_sidx.ensure((size_t)mstride * sizeof(int)));
+    PB_CUDA(c, c->band_vals.ensure((size_t)W * std::max<int64_t>(c->band_stride, 1) * sizeof(double)));
+    PB_CUDA(c, c->band_part.ensure((size_t)kMaxBandGroups * std::max(c->band_nb, 1) * c->lay_d * ld * sizeof(double)));
+  }
+  c->last_blocked = blocked;
   size_t scan_need = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
@@ -1788,6 +2152,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   int* dest = c->dest.as<int>();
   int* diag_row = dest + mstride;
   PB_CUDA(c, cudaMemsetAsync(c->m_diag.p, 0, (size_t)W * n * sizeof(double), st));
+  if (blocked && c->band_stride > 0)
+    PB_CUDA(c, cudaMemsetAsync(c->band_vals.p, 0, (size_t)W * c->band_stride * sizeof(double), st));
   if ((flags & PB_PHOTOHAD) && R > 0) {
     k_fold_first<<<blocks_for(R + 1, 8), 256, 0, st>>>(c->kernel.as<double>(), R, c->dph, c->PT.as<double>(),
                                                        c->cpl_is_diag.as<int>(), c->keep.as<int>());
@@ -1795,7 +2161,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, tb, c->keep.as<int>(), c->pos.as<int>(), (int)(R + 1), st));
     k_compact<<<blocks_for(R, 256), 256, 0, st>>>(c->keep.as<int>(), c->pos.as<int>(), c->cpl_indices.as<int>(),
                                                   c->cpl_is_diag.as<int>(), c->cpl_row.as<int>(), R, dest, diag_row,
-                                                  c->m_indices.as<int>());
+                                                  c->m_indices.as<int>(), std::max(c->lay_d, 1),
+                                                  blocked ? c->m_sidx.as<int>() : nullptr);
     k_m_indptr<<<blocks_for(n + 1, 256), 256, 0, st>>>(c->cpl_indptr.as<int64_t>(), c->pos.as<int>(), n,
                                                        c->m_indptr.as<int64_t>());
     if (c->n_seg > 0) {
@@ -1808,7 +2175,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     const size_t smem = (size_t)(kFoldBM + kFoldBN) * (kpad + 4) * sizeof(double);
     k_fold_gemm<<<dim3(blocks_for(R, kFoldBM), blocks_for(W, kFoldBN)), 256, smem, st>>>(
         c->kernel.as<double>(), R, c->dph, kpad, c->PT.as<double>(), W, dest, diag_row, c->m_vals.as<double>(),
-        mstride, c->m_diag.as<double>(), n);
+        mstride, c->m_diag.as<double>(), n, blocked ? c->band_slot.as<int>() : nullptr,
+        blocked ? c->band_vals.as<double>() : nullptr, c->band_stride);
     launches += 5;
   } else {
     PB_CUDA(c, cudaMemsetAsync(c->m_indptr.p, 0, ((size_t)n + 1) * sizeof(int64_t), st));
@@ -1837,6 +2205,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)S); put((uint64_t)W); put((uint64_t)K); put((uint64_t)ld); put(flags); put(inj); put(R);
     put((uint64_t)c->n_seg); put((uint64_t)c->h_short_rows.size()); put((uint64_t)c->n_cr_bins);
     put((uint64_t)a->ckpt_every);
+    put((uint64_t)blocked);
+    put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
     put((uint64_t)c->em_W);
     for (double v : c->em_dl) { uint64_t b; memcpy(&b, &v, 8); put(b); }
     const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);

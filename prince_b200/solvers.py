@@ -170,6 +170,7 @@ class DeviceRun:
         cm = ir.coupling_mat
         self.n = n
         self.ctx.set_coupling(n, cm.indptr, cm.indices)
+        self.ctx.set_layout(run.spec_man.nspec and n // run.spec_man.nspec)
         self.ctx.set_fold_kernel(_dense_kernel(ir._batch_matrix))
         self.ctx.set_photon_grid(ir.e_photon.grid)
         D = fd_loss_operator(run.cr_grid, run.spec_man.nspec)

@@ -61,6 +61,37 @@ def rel_err_on_support(x, ref, species_blocks, floor=1e-20):
     return worst
 
 
+def local_scale_check(x, ref, species_blocks, tol=1e-10, floor=1e-20):
+    """Per-bin parity that tolerates zero crossings of oscillating spectra.
+
+    On the support (``ref > floor`` x the species maximum) every bin is
+    measured twice: strictly, ``|x - ref| / |ref|``, and against its local
+    magnitude, ``|x - ref| / max(|ref|)`` over the bin and its two neighbours.
+    Returns ``(worst local error, bins whose strict error exceeds tol, bins on
+    the support)``.
+    """
+    worst, above, total = 0.0, 0, 0
+    for sl in species_blocks:
+        r, v = ref[sl], x[sl]
+        if r.ndim == 1:
+            r, v = r[:, None], v[:, None]
+        a = np.abs(r)
+        local = a.copy()
+        local[1:] = np.maximum(local[1:], a[:-1])
+        local[:-1] = np.maximum(local[:-1], a[1:])
+        for k in range(r.shape[1]):
+            m = a[:, k].max()
+            if m == 0:
+                continue
+            sel = r[:, k] > floor * m
+            err = np.abs(v[sel, k] - r[sel, k])
+            total += int(sel.sum())
+            above += int(np.count_nonzero(err > tol * a[sel, k]))
+            if err.size:
+                worst = max(worst, float(np.max(err / local[sel, k])))
+    return worst, above, total
+
+
 def light_network_em():
     """The EM-cascade fixture: run (gamma, e+- on the shared grid) and the
     synthetic per-window transfer used by the reference run."""
