@@ -132,7 +132,19 @@ struct pb_context {
   bool blocked_ok = false;          // the coupling pattern admits the band + slab kernels
   int32_t band_nb = 0, band_RT = 0, band_J = 0, n_slab_spec = 0;
   int64_t band_stride = 0;          // band-tile doubles per window
-  DBuf band_slot, band_mask, band_spec, slab_spec, band_vals, band_part, m_sidx;
+  int32_t band_npairs = 0;
+  DBuf band_slot, band_spec, slab_spec, band_vals, band_part;
+  // bin-local rows: coupling entries in bin-major order
+  DBuf slab_rp, slab_sidx, slab_slot, slab_vals;
+  int64_t slab_nent = 0;            // entries per window (with the per-bin alignment padding)
+  int32_t slab_maxbin = 0;          // entries of the largest bin (padded)
+  size_t slab_smem = 0, band_smem = 0;
+  // FD stencil per bin (same in every species block): host copy of D and the table
+  std::vector<int64_t> h_d_indptr;
+  std::vector<int32_t> h_d_indices;
+  std::vector<double> h_d_vals;
+  bool fd_tab_ok = false;
+  DBuf fd_cnt, fd_off, fd_val, fdbuf;
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
@@ -300,14 +312,12 @@ __global__ void k_fold_first(const double* __restrict__ K, int64_t R, int dph,
 __global__ void k_compact(const int* __restrict__ keep, const int* __restrict__ pos,
                           const int* __restrict__ cpl_indices, const int* __restrict__ is_diag,
                           const int* __restrict__ row, int64_t R, int* __restrict__ dest,
-                          int* __restrict__ diag_row, int* __restrict__ m_indices, int d,
-                          int* __restrict__ m_sidx) {
+                          int* __restrict__ diag_row, int* __restrict__ m_indices) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= R) return;
   if (keep[i]) {
     dest[i] = pos[i];
     m_indices[pos[i]] = cpl_indices[i];
-    if (m_sidx) m_sidx[pos[i]] = cpl_indices[i] / d;
   } else {
     dest[i] = -1;
   }
@@ -352,7 +362,9 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
                                                    double* __restrict__ mv, int64_t mv_stride,
                                                    double* __restrict__ md, int64_t n,
                                                    const int* __restrict__ band_slot,
-                                                   double* __restrict__ band, int64_t band_stride) {
+                                                   double* __restrict__ band, int64_t band_stride,
+                                                   const int* __restrict__ slab_slot,
+                                                   double* __restrict__ slab, int64_t slab_stride) {
   extern __shared__ double smem[];
   const int lda = kpad + 4;  // +4 doubles: 8-row fragments spread over all banks
   double* As = smem;
@@ -394,6 +406,7 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
     const int de = dest[r];
     const int dr = diag_row[r];
     const int bs = (band_slot && de >= 0) ? band_slot[r] : -1;
+    const int ss = (slab_slot && de >= 0) ? slab_slot[r] : -1;
 #pragma unroll
     for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
@@ -404,6 +417,7 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
         if (de >= 0) mv[(size_t)w * mv_stride + de] = v;
         if (dr >= 0) md[(size_t)w * n + dr] = v;
         if (bs >= 0) band[(size_t)w * band_stride + bs] = v;
+        if (ss >= 0) slab[2 * ((size_t)w * slab_stride + ss)] = v;  // value half of the packed entry
       }
   }
 }
@@ -577,12 +591,19 @@ struct StepParams {
   int nsp;                  // species blocks
   const int* slab_spec;     // species whose coupling rows are bin-local
   int n_slab_spec;
-  const int* m_sidx;        // species block of each M_off column
+  const int* slab_rp;       // bin-major entry range of each bin-local row ([d][n_slab_spec] + 1)
+  const int* slab_sidx;     // species block of the column of each bin-major entry
+  const double2* slab_ent;  // [W][slab_stride] bin-major entries: (M_off value, slab byte offset of the column)
+  int64_t slab_stride;
+  int slab_maxbin;          // entries of the largest bin (shared-memory sizing)
+  const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
+  const int* fd_off;
+  const double* fd_val;
+  double* fdbuf;            // n x ld: D_off (kappa v) of the stage
   const int* band_spec;     // species with cross-bin coupling rows
   int nb;
-  const double* band_vals;  // [W][nb][nsp][RT][J][32] DMMA A fragments
+  const double* band_vals;  // [W][nsp][band pair][2][RT][J][32] DMMA A fragments
   int64_t band_stride;
-  const uint32_t* band_mask;  // [nb][nsp][RT]: k-tiles present per row tile
   double* band_part;        // [G][nb][d][ld] partial sums of the band rows
   int ngroups;              // mother-species groups of the band launch
   int spg;                  // species per group
@@ -946,118 +967,336 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
 // States are species blocks of d energy bins.  The coupling rows split in two
 // classes (pb_set_layout):
 //  * bin-local rows: every M_off entry couples bin e to bin e of another
-//    species (boost-conserving fragments).  k_slab stages the state slab of one
-//    bin -- all species x 32 columns -- in shared memory and sums each row
-//    from there, so a state value is read from DRAM once per stage instead of
-//    once per coupling entry.
+//    species (boost-conserving fragments).  Their entries are stored
+//    bin-major (all rows of bin e contiguous).  k_slab stages the state slab
+//    of one bin -- all species x 32 columns -- and the bin's entries in shared
+//    memory and sums each row from there, so a state value is read from DRAM
+//    once per stage instead of once per coupling entry.
 //  * band rows (species with cross-bin entries: the redistributed nucleons):
 //    their block rows against each mother species form a band of d x d tiles.
 //    k_band multiplies them on the FP64 tensor pipe (DMMA m8n8k4) with the
 //    tiles stored in fragment order per window, split over groups of mother
 //    species into partial sums that k_band_finish adds in group order.
-// k_band runs on a second stream, concurrently with k_slab (they touch
-// disjoint outputs); k_band_finish follows both.
+// The FD loss term D_off (kappa v) couples neighbouring bins of one species;
+// k_fd evaluates it species-major (one species block per CTA, in shared
+// memory) into fdbuf before the row kernels read it.  A stage is
+// k_band (second stream) || k_fd -> k_slab, then k_band_finish.
 // ---------------------------------------------------------------------------
-template <int STAGE>
-__global__ void __launch_bounds__(256) k_slab(StepParams p) {
-  extern __shared__ double slab[];
-  const StepScalars s = load_scalars(p, p.step);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int e = blockIdx.x;
-  const int col = blockIdx.y * kColTile + lane;  // < ld: the grid covers the active columns only
-  const bool active = col < p.ncols;
-  if (s.photohad) {
-    const double* __restrict__ v = p.src + (size_t)e * p.ld + col;
-    const size_t sstride = (size_t)p.d * p.ld;
-    for (int q = wid; q < p.nsp; q += nw) slab[q * kColTile + lane] = v[q * sstride];
-    __syncthreads();
+constexpr int kFdMax = 4;           // off-diagonal FD stencil entries per row (bin-blocked path)
+constexpr int kSlabThreads = 512;
+constexpr int kMaxBandGroups = 64;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// fdbuf = D_off (kappa v) for every row.  CTA = (species block, 32-column
+// tile): the block's d x 32 states and its kappa go to shared memory, then a
+// thread per (bin, column) adds the stencil terms in CSR order (the stencil of
+// bin e is the same in every species block; it is padded to kFdMax terms
+// with zero weights on the row itself).
+__global__ void __launch_bounds__(256) k_fd(StepParams p) {
+  extern __shared__ double fsm[];
+  const int sp = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int d = p.d, ld = p.ld;
+  const int col = blockIdx.y * kColTile + lane;  // < ld
+  double* vb = fsm;                  // d x 32
+  double* kb = fsm + d * kColTile;   // d
+  const size_t o0 = (size_t)(p.step & 1) * p.n;
+  const double* __restrict__ v = p.src + (size_t)sp * d * ld + blockIdx.y * kColTile;
+  for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
+    const int e = t / (kColTile / 2), c = 2 * (t - e * (kColTile / 2));
+    cp_async16(vb + e * kColTile + c, v + (size_t)e * ld + c);
   }
-  const double* __restrict__ mv = p.m_vals + (size_t)s.w * p.m_wstride;
-  for (int i = wid; i < p.n_slab_spec; i += nw) {
-    const int64_t r = (int64_t)p.slab_spec[i] * p.d + e;
-    double acc = 0.0;
-    if (s.photohad) {
-      const int64_t j0 = p.m_indptr[r], j1 = p.m_indptr[r + 1];
-      for (int64_t base = j0; base < j1; base += 32) {
-        const int64_t j = base + lane;
-        const double mvl = (j < j1) ? mv[j] : 0.0;
-        const int sl = (j < j1) ? p.m_sidx[j] : 0;
-        const int cnt = (int)min((int64_t)32, j1 - base);
-        for (int q = 0; q < cnt; ++q) {
-          const double mq = __shfl_sync(0xffffffffu, mvl, q);
-          const int sq = __shfl_sync(0xffffffffu, sl, q);
-          acc = __dadd_rn(acc, __dmul_rn(mq, slab[sq * kColTile + lane]));
-        }
-      }
-    }
-    if (active) row_epilogue<STAGE>(p, s, r, col, acc);
-    if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
+  cp_async_commit();
+  for (int e = threadIdx.x; e < d; e += blockDim.x) kb[e] = p.kap[o0 + (size_t)sp * d + e];
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int e = wid; e < d; e += blockDim.x >> 5) {
+    const int* fo = p.fd_off + e * kFdMax;
+    const double* fv = p.fd_val + e * kFdMax;
+    double sD = __dmul_rn(fv[0], __dmul_rn(kb[e + fo[0]], vb[(e + fo[0]) * kColTile + lane]));
+#pragma unroll
+    for (int t = 1; t < kFdMax; ++t)
+      sD = __dadd_rn(sD, __dmul_rn(fv[t], __dmul_rn(kb[e + fo[t]], vb[(e + fo[t]) * kColTile + lane])));
+    p.fdbuf[((size_t)sp * d + e) * ld + col] = sD;
   }
 }
 
-// Band partial sums.  CTA = (128-column block, mother-species group, band
-// species); warp = 16 columns (two 8-column DMMA tiles) x all d rows of the
-// band species, accumulators in registers (RT row tiles x 2 column tiles).
-// For each mother species the warp walks the 2 RT k-tiles (4 mother bins
-// each): it loads the X fragment of the k-tile once and multiplies it into
-// every row tile whose band holds that k-tile (mask bit set).
+// k_slab's shared memory: the state slab (nsp x 32), the bin's entries
+// (value, slab byte offset of the column), the row factors (3 x nss) and the
+// int row tables (entry ranges, injection slots, species).
+struct SlabSmem {
+  double* slab;
+  double2* ent;
+  double* fac;
+  int* rp;
+  int* slot;
+  int* spec;
+  __host__ __device__ static size_t bytes(int nsp, int nss, int maxbin) {
+    return ((size_t)nsp * kColTile + 3 * (size_t)nss) * sizeof(double) + (size_t)maxbin * sizeof(double2) +
+           (3 * (size_t)nss + 1) * sizeof(int);
+  }
+  __device__ SlabSmem(double* base, int nsp, int nss, int maxbin) {
+    slab = base;
+    ent = reinterpret_cast<double2*>(slab + (size_t)nsp * kColTile);
+    fac = reinterpret_cast<double*>(ent + maxbin);
+    rp = reinterpret_cast<int*>(fac + 3 * (size_t)nss);
+    slot = rp + nss + 1;
+    spec = slot + nss;
+  }
+};
+
+// Bin-local rows.  CTA = (bin e, 32-column tile), lane = column.  The state
+// slab of bin e and the bin's coupling entries arrive in shared memory by
+// asynchronous copies; a warp then takes rows e-strided (rows are ordered by
+// entry count, longest first), sums each from shared memory and applies the
+// stage update with the FD term from fdbuf (loaded one row ahead).  Offsets
+// into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at launch).
+template <int STAGE>
+__global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
+  extern __shared__ double sm[];
+  const int nss = p.n_slab_spec;
+  const int e = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int col = blockIdx.y * kColTile + lane;  // < ld
+  const bool active = col < p.ncols;
+  const StepScalars s = load_scalars(p, p.step);
+  const size_t o0 = (size_t)(p.step & 1) * p.n;
+  const int ld = p.ld, d = p.d;
+  SlabSmem L(sm, p.nsp, nss, p.slab_maxbin);
+  const double* __restrict__ v = p.src;
+  const int q0 = p.slab_rp[(size_t)e * nss], q1 = p.slab_rp[(size_t)(e + 1) * nss];  // multiples of 4
+  {
+    const double* vs = v + (size_t)e * ld + blockIdx.y * kColTile;
+    for (int t = threadIdx.x; t < p.nsp * (kColTile / 2); t += blockDim.x) {
+      const int q = t / (kColTile / 2), c = 2 * (t - q * (kColTile / 2));
+      cp_async16(L.slab + q * kColTile + c, vs + (size_t)q * d * ld + c);
+    }
+    if (s.photohad) {
+      const double2* me = p.slab_ent + (size_t)s.w * p.slab_stride + q0;
+      for (int t = threadIdx.x; t < q1 - q0; t += blockDim.x) cp_async16(L.ent + t, me + t);
+    }
+    cp_async_commit();
+  }
+  for (int i = threadIdx.x; i < nss; i += blockDim.x) {
+    const int sp = p.slab_spec[i];
+    const int r = sp * d + e;
+    const double a0 = p.eD[o0 + r], a1 = p.phi1[o0 + r], a2 = p.phi2[o0 + r];
+    const int rpi = p.slab_rp[(size_t)e * nss + i] - q0;
+    const int sl = s.inj ? p.inj_slot[r] : -1;
+    L.fac[i] = a0;
+    L.fac[nss + i] = a1;
+    L.fac[2 * nss + i] = a2;
+    L.rp[i] = rpi;
+    L.slot[i] = sl;
+    L.spec[i] = sp;
+  }
+  if (threadIdx.x == 0) L.rp[nss] = q1 - q0;
+  int src0 = 0, src1 = 0;
+  if (s.inj && active) {
+    src0 = p.src_ptr[col];
+    src1 = p.src_ptr[col + 1];
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  const double* __restrict__ fdb = p.fdbuf;
+  const double* __restrict__ fprv = p.f;
+  int i = wid;
+  if (i >= nss) return;
+  // FD term and F(x) of the row, loaded one row ahead
+  int r = L.spec[i] * d + e;
+  double fd = 0.0, fp = 0.0;
+  if (s.kap) fd = fdb[r * ld + col];
+  if (STAGE == 2) fp = fprv[r * ld + col];
+  const double* sl = L.slab + lane;
+  while (true) {
+    const int ni = i + nw;
+    int nr = 0;
+    double nfd = 0.0, nfp = 0.0;
+    if (ni < nss) {
+      nr = L.spec[ni] * d + e;
+      if (s.kap) nfd = fdb[nr * ld + col];
+      if (STAGE == 2) nfp = fprv[nr * ld + col];
+    }
+    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+    if (s.photohad) {
+      const int j1 = L.rp[i + 1];
+      int j = L.rp[i];
+      const char* slb = reinterpret_cast<const char*>(sl);
+      for (; j + 3 < j1; j += 4) {
+        const double2 e0 = L.ent[j], e1 = L.ent[j + 1], e2 = L.ent[j + 2], e3 = L.ent[j + 3];
+        const double x0 = *reinterpret_cast<const double*>(slb + __double2loint(e0.y));
+        const double x1 = *reinterpret_cast<const double*>(slb + __double2loint(e1.y));
+        const double x2 = *reinterpret_cast<const double*>(slb + __double2loint(e2.y));
+        const double x3 = *reinterpret_cast<const double*>(slb + __double2loint(e3.y));
+        acc0 = __fma_rn(e0.x, x0, acc0);
+        acc1 = __fma_rn(e1.x, x1, acc1);
+        acc2 = __fma_rn(e2.x, x2, acc2);
+        acc3 = __fma_rn(e3.x, x3, acc3);
+      }
+      for (; j < j1; ++j) {
+        const double2 en = L.ent[j];
+        acc0 = __fma_rn(en.x, *reinterpret_cast<const double*>(slb + __double2loint(en.y)), acc0);
+      }
+    }
+    if (active) {
+      double out = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
+      if (s.kap) out = __dadd_rn(out, fd);
+      if (s.decay) {
+        double sL = 0.0;
+        for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
+          sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], v[(size_t)p.l_indices[j] * ld + col]));
+        out = __dadd_rn(out, sL);
+      }
+      out = __dmul_rn(out, s.dl);
+      const int slt = L.slot[i];
+      if (slt >= 0 && src1 > src0) {  // injection (rows of injected species only)
+        const double* cf = p.coeff + (size_t)p.step * p.n_src;
+        const double* g = p.G + (size_t)slt * p.n_src;
+        double a = __dmul_rn(cf[src0], g[src0]);
+        for (int q = src0 + 1; q < src1; ++q) a = __dadd_rn(a, __dmul_rn(cf[q], g[q]));
+        out = __dadd_rn(out, __dmul_rn(s.finj, a));
+      }
+      const double own = L.slab[L.spec[i] * kColTile + lane];
+      const int ro = r * ld + col;
+      if (STAGE == 1) {
+        // a = eD x + (phi1 F(x)) h
+        p.a[ro] = __dadd_rn(__dmul_rn(L.fac[i], own), __dmul_rn(__dmul_rn(L.fac[nss + i], out), s.h));
+        p.f[ro] = out;
+      } else {
+        // x = a + ((F(a) - F(x)) h) phi2
+        const double dF = __dmul_rn(__dadd_rn(out, -fp), s.h);
+        p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * nss + i]));
+      }
+    }
+    if (ni >= nss) break;
+    i = ni;
+    r = nr;
+    fd = nfd;
+    fp = nfp;
+  }
+}
+
+// The column half of every window's packed bin-major entries: the byte offset
+// of the column species' row in k_slab's state slab.
+__global__ void k_slab_cols(const int* __restrict__ sidx, int64_t nent, int W, double2* __restrict__ ent) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nent * W) return;
+  ent[t].y = __hiloint2double(0, sidx[t % nent] * kColTile * (int)sizeof(double));
+}
+
+// Stage 2: the row factors of the next step for the bin-local rows (one
+// thread per row; the band rows are prepared by k_band_finish).
+__global__ void k_slab_prep(StepParams p) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)p.n_slab_spec * p.d) return;
+  const int i = (int)(t / p.d), e = (int)(t - (int64_t)i * p.d);
+  prep_next(p, (int64_t)p.slab_spec[i] * p.d + e);
+}
+
+// Band partial sums.  CTA = (64-column block, mother-species group, pair of
+// band species), 8 warps; warp = one 8-column DMMA tile x both band species
+// of the pair x all d rows (accumulators in registers).  Per mother species
+// the CTA copies the pair's A tiles (2 x RT x J fragments, fragment order)
+// into shared memory with cp.async, double-buffered across species; each warp
+// keeps the species' X fragments (2 RT k-tiles of 4 mother bins) in
+// registers, loaded one species ahead.  Every tile of the static band is
+// multiplied: tiles without coupling entries hold zeros and add exact zeros.
 template <int RT, int J>
-__global__ void __launch_bounds__(256, RT <= 12 ? 2 : 1) k_band(StepParams p) {
+__global__ void __launch_bounds__(256, 1) k_band(StepParams p) {
+  extern __shared__ double sm[];
+  constexpr int KT = 2 * RT;
+  constexpr int ABLK = 2 * RT * J * 32;  // doubles of one (species, band pair) block
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int c0 = blockIdx.x * 128 + wid * 16;
-  if (c0 >= p.ncols) return;  // c0 + 15 < ld: ld is a multiple of 32
-  const int b = blockIdx.z, g = blockIdx.y;
+  const int c0 = blockIdx.x * 64 + wid * 8;
+  const bool wact = c0 < p.ncols;  // c0 + 7 < ld: ld is a multiple of 32
+  const int pair = blockIdx.z, g = blockIdx.y;
   const int s0 = g * p.spg, s1 = min(p.nsp, s0 + p.spg);
   const int d = p.d, ld = p.ld;
   const int w = p.win[p.step];
   const double* __restrict__ A = p.band_vals + (size_t)w * p.band_stride;
-  double acc[RT][2][2];
+  const int npairs = gridDim.z;
+  double* As = sm;  // [2][ABLK]
+  auto issue = [&](int sp, int stage) {
+    const double* src = A + ((size_t)sp * npairs + pair) * ABLK;
+    for (int c = threadIdx.x; c < ABLK / 2; c += blockDim.x) cp_async16(As + stage * ABLK + 2 * c, src + 2 * c);
+    cp_async_commit();
+  };
+  double acc[2][RT][2];
 #pragma unroll
-  for (int rt = 0; rt < RT; ++rt) acc[rt][0][0] = acc[rt][0][1] = acc[rt][1][0] = acc[rt][1][1] = 0.0;
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) acc[b][rt][0] = acc[b][rt][1] = 0.0;
   const int kr = lane & 3;
-  for (int sp = s0; sp < s1; ++sp) {
+  double xf[KT], xn[KT];
+  auto load_x = [&](int sp, double (&x)[KT]) {
     const double* __restrict__ xs = p.src + (size_t)sp * d * ld + c0 + (lane >> 2);
-    const size_t tb = (size_t)(b * p.nsp + sp) * RT;
-    const double* __restrict__ as = A + tb * J * 32 + lane;
-    uint32_t m[RT];
 #pragma unroll
-    for (int rt = 0; rt < RT; ++rt) m[rt] = p.band_mask[tb + rt];
-#pragma unroll
-    for (int kt = 0; kt < 2 * RT; ++kt) {
+    for (int kt = 0; kt < KT; ++kt) {
       const int e = 4 * kt + kr;
-      double b0 = 0.0, b1 = 0.0;
-      if (e < d) {
-        b0 = xs[(size_t)e * ld];
-        b1 = xs[(size_t)e * ld + 8];
-      }
-#pragma unroll
-      for (int rt = 0; rt < RT; ++rt) {
-        const int jj = kt - 2 * rt;
-        if (jj < 0 || jj >= J) continue;
-        if (m[rt] & (1u << jj)) {
-          const double a = as[(rt * J + jj) * 32];
-          dmma884(acc[rt][0][0], acc[rt][0][1], a, b0);
-          dmma884(acc[rt][1][0], acc[rt][1][1], a, b1);
-        }
-      }
+      x[kt] = (wact && e < d) ? xs[(size_t)e * ld] : 0.0;
     }
+  };
+  if (s0 < s1) {
+    issue(s0, 0);
+    load_x(s0, xf);
   }
-  double* __restrict__ P = p.band_part + (size_t)(g * p.nb + b) * d * ld;
+  for (int sp = s0; sp < s1; ++sp) {
+    const int stage = (sp - s0) & 1;
+    if (sp + 1 < s1) {
+      issue(sp + 1, stage ^ 1);
+      load_x(sp + 1, xn);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* __restrict__ as = As + stage * ABLK + lane;
+    // consecutive DMMAs go to different accumulators (k-tile outer, row tile inner)
 #pragma unroll
-  for (int rt = 0; rt < RT; ++rt) {
-    const int row = 8 * rt + (lane >> 2);
-    if (row >= d) continue;
+    for (int jj = 0; jj < J; ++jj)
 #pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-      double2 v;
-      v.x = acc[rt][nt][0];
-      v.y = acc[rt][nt][1];
-      *reinterpret_cast<double2*>(P + (size_t)row * ld + c0 + nt * 8 + kr * 2) = v;
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int rt = 0; rt < RT; ++rt) {
+          const int kt = 2 * rt + jj;
+          if (kt >= KT) continue;
+          dmma884(acc[b][rt][0], acc[b][rt][1], as[((b * RT + rt) * J + jj) * 32], xf[kt]);
+        }
+    __syncthreads();  // every warp is done with this stage before it is refilled
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) xf[kt] = xn[kt];
+  }
+  if (!wact) return;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    if (2 * pair + b >= p.nb) continue;
+    double* __restrict__ P = p.band_part + (size_t)(g * p.nb + 2 * pair + b) * d * ld;
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) {
+      const int row = 8 * rt + (lane >> 2);
+      if (row >= d) continue;
+      double2 o;
+      o.x = acc[b][rt][0];
+      o.y = acc[b][rt][1];
+      *reinterpret_cast<double2*>(P + (size_t)row * ld + c0 + kr * 2) = o;
     }
   }
 }
 
-// Band rows: add the group partials in group order, then the row epilogue.
+template <int RT, int J>
+size_t band_smem_bytes() {
+  return (size_t)2 * (2 * RT * J * 32) * sizeof(double);
+}
+
+// Band rows: add the group partials in group order, then the stage update
+// with the FD term from fdbuf.
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
   const StepScalars s = load_scalars(p, p.step);
@@ -1067,10 +1306,30 @@ __global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
   const int b = rb / p.d, e = rb - b * p.d;
   const int64_t r = (int64_t)p.band_spec[b] * p.d + e;
   const int col = blockIdx.y * kColTile + lane;
-  double t = 0.0;
-  for (int g = 0; g < p.ngroups; ++g)
-    t = __dadd_rn(t, p.band_part[((size_t)(g * p.nb + b) * p.d + e) * p.ld + col]);
-  if (col < p.ncols) row_epilogue<STAGE>(p, s, r, col, t);
+  if (col < p.ncols) {
+    double t = 0.0;
+    for (int g = 0; g < p.ngroups; ++g)
+      t = __dadd_rn(t, p.band_part[((size_t)(g * p.nb + b) * p.d + e) * p.ld + col]);
+    const size_t idx = (size_t)r * p.ld + col;
+    double out = t;
+    if (s.kap) out = __dadd_rn(out, p.fdbuf[idx]);
+    if (s.decay) {
+      double sL = 0.0;
+      for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
+        sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], p.src[(size_t)p.l_indices[j] * p.ld + col]));
+      out = __dadd_rn(out, sL);
+    }
+    out = __dmul_rn(out, s.dl);
+    if (s.inj) out = __dadd_rn(out, inj_at(p, s, r, col));
+    const size_t o = (size_t)(p.step & 1) * p.n + r;
+    if (STAGE == 1) {
+      p.a[idx] = __dadd_rn(__dmul_rn(p.eD[o], p.x[idx]), __dmul_rn(__dmul_rn(p.phi1[o], out), s.h));
+      p.f[idx] = out;
+    } else {
+      const double dF = __dmul_rn(__dadd_rn(out, -p.f[idx]), s.h);
+      p.xout[idx] = __dadd_rn(p.a[idx], __dmul_rn(dF, p.phi2[o]));
+    }
+  }
   if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
 }
 
@@ -1079,26 +1338,29 @@ __global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
 using BandKernel = void (*)(StepParams);
 constexpr int kBandRT[] = {4, 8, 12, 16};
 constexpr int kBandJ[] = {5, 9, 13, 17};
+struct BandInstance {
+  BandKernel fn;
+  size_t smem;
+};
 template <int RT>
-BandKernel band_kernel_j(int J) {
+BandInstance band_kernel_j(int J) {
   switch (J) {
-    case 5: return k_band<RT, 5>;
-    case 9: return k_band<RT, 9>;
-    case 13: return k_band<RT, 13>;
-    case 17: return k_band<RT, 17>;
+    case 5: return {k_band<RT, 5>, band_smem_bytes<RT, 5>()};
+    case 9: return {k_band<RT, 9>, band_smem_bytes<RT, 9>()};
+    case 13: return {k_band<RT, 13>, band_smem_bytes<RT, 13>()};
+    case 17: return {k_band<RT, 17>, band_smem_bytes<RT, 17>()};
   }
-  return nullptr;
+  return {nullptr, 0};
 }
-BandKernel band_kernel(int RT, int J) {
+BandInstance band_kernel(int RT, int J) {
   switch (RT) {
     case 4: return band_kernel_j<4>(J);
     case 8: return band_kernel_j<8>(J);
     case 12: return band_kernel_j<12>(J);
     case 16: return band_kernel_j<16>(J);
   }
-  return nullptr;
+  return {nullptr, 0};
 }
-constexpr int kMaxBandGroups = 64;
 
 // ---------------------------------------------------------------------------
 // Co-evolved EM cascade, applied after every ETD2 step (propagation.py:555-665):
@@ -1384,7 +1646,8 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj, &c->gs, &c->g_out,
           &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
           &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
-          &c->band_slot, &c->band_mask, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->m_sidx};
+          &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -1472,43 +1735,65 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.nsp = c->lay_nsp;
   p.slab_spec = c->slab_spec.as<int>();
   p.n_slab_spec = c->n_slab_spec;
-  p.m_sidx = c->m_sidx.as<int>();
+  p.slab_rp = c->slab_rp.as<int>();
+  p.slab_sidx = c->slab_sidx.as<int>();
+  p.slab_ent = c->slab_vals.as<double2>();
+  p.slab_stride = c->slab_nent;
+  p.slab_maxbin = c->slab_maxbin;
+  p.fd_cnt = c->fd_cnt.as<int>();
+  p.fd_off = c->fd_off.as<int>();
+  p.fd_val = c->fd_val.as<double>();
+  p.fdbuf = c->fdbuf.as<double>();
   p.band_spec = c->band_spec.as<int>();
   p.nb = c->band_nb;
   p.band_vals = c->band_vals.as<double>();
   p.band_stride = c->band_stride;
-  p.band_mask = c->band_mask.as<uint32_t>();
   p.band_part = c->band_part.as<double>();
 }
 
 // Whether a solve with K columns runs the bin-blocked kernels.
-bool use_blocked(const pb_context* c, int K) { return c->blocked_ok && c->batched_mode == 1 && K > 1; }
+bool use_blocked(const pb_context* c, int K) {
+  const int64_t ld = ((K + kColTile - 1) / kColTile) * kColTile;
+  return c->blocked_ok && c->fd_tab_ok && c->batched_mode == 1 && K > 1 && c->n * ld < ((int64_t)1 << 31);
+}
 
-// One stage of the bin-blocked path: k_band (second stream) || k_slab, then k_band_finish.
+// One stage of the bin-blocked path: k_band on the second stream, k_fd then
+// k_slab on the launching stream, then k_band_finish (and the next step's row
+// factors of the bin-local rows after stage 2).
 template <int STAGE>
 int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   const bool photohad = (p.flags & PB_PHOTOHAD) != 0;
+  const bool kap = (p.flags & PB_PARTIAL_DIFF) != 0;
   int64_t launches = 0;
   p.ngroups = 0;
   p.spg = 1;
   if (photohad && p.nb > 0) {
-    const int cblocks = (int)blocks_for(p.ncols, 128);
-    const int target = 2 * c->num_sms;
-    int G = std::max(1, std::min({(target + cblocks * p.nb - 1) / (cblocks * p.nb), kMaxBandGroups, p.nsp}));
+    const int cblocks = (int)blocks_for(p.ncols, 64);
+    const int per = cblocks * c->band_npairs;
+    const int G = std::max(1, std::min({(c->num_sms + per - 1) / per, kMaxBandGroups, p.nsp}));
     p.spg = (p.nsp + G - 1) / G;
     p.ngroups = (p.nsp + p.spg - 1) / p.spg;
     cudaEventRecord(c->ev_fork, st);
     cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
-    band_kernel(c->band_RT, c->band_J)<<<dim3(cblocks, p.ngroups, p.nb), 256, 0, c->stream2>>>(p);
+    const BandInstance bi = band_kernel(c->band_RT, c->band_J);
+    bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), 256, bi.smem, c->stream2>>>(p);
     cudaEventRecord(c->ev_join, c->stream2);
     ++launches;
   }
-  const size_t smem = photohad ? (size_t)p.nsp * kColTile * sizeof(double) : 0;
-  k_slab<STAGE><<<dim3(p.d, blocks_for(p.ncols, kColTile)), 256, smem, st>>>(p);
+  const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
+  if (kap) {
+    k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 1) * sizeof(double), st>>>(p);
+    ++launches;
+  }
+  k_slab<STAGE><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
   ++launches;
+  if (STAGE == 2 && p.step + 1 < p.n_steps) {
+    k_slab_prep<<<blocks_for((int64_t)p.n_slab_spec * p.d, 256), 256, 0, st>>>(p);
+    ++launches;
+  }
   if (p.ngroups > 0) cudaStreamWaitEvent(st, c->ev_join, 0);
   if (p.nb > 0) {
-    k_band_finish<STAGE><<<dim3(blocks_for((int64_t)p.nb * p.d, 8), blocks_for(p.ncols, kColTile)), 256, 0, st>>>(p);
+    k_band_finish<STAGE><<<dim3(blocks_for((int64_t)p.nb * p.d, 8), tiles), 256, 0, st>>>(p);
     ++launches;
   }
   return launches;
@@ -1763,6 +2048,45 @@ int pb_set_photon_field(pb_context* c, int32_t n_comp, const int32_t* kinds, con
   return PB_OK;
 }
 
+// Per-bin FD stencil of the bin-blocked kernels: the off-diagonal entries of
+// the FD operator's row e, which must be the same (offsets and values) in
+// every species block; padded to kFdMax terms with zero weights on the row
+// itself.  Sets fd_tab_ok.
+static int build_fd_table(pb_context* c) {
+  c->fd_tab_ok = false;
+  const int d = c->lay_d;
+  if (!c->have_fd || d <= 0 || c->h_d_indptr.size() != (size_t)c->n + 1) return PB_OK;
+  const int nsp = (int)(c->n / d);
+  const std::vector<int64_t>& ip = c->h_d_indptr;
+  const std::vector<int32_t>& ix = c->h_d_indices;
+  const std::vector<double>& dv = c->h_d_vals;
+  std::vector<int32_t> cnt(d, 0), off((size_t)d * kFdMax, 0);
+  std::vector<double> val((size_t)d * kFdMax, 0.0);
+  for (int e = 0; e < d; ++e) {
+    const int64_t n0 = ip[e + 1] - ip[e];
+    if (n0 > kFdMax) return PB_OK;
+    cnt[e] = (int32_t)n0;
+    for (int64_t t = 0; t < n0; ++t) {
+      off[(size_t)e * kFdMax + t] = ix[ip[e] + t] - e;
+      val[(size_t)e * kFdMax + t] = dv[ip[e] + t];
+    }
+    for (int sp = 1; sp < nsp; ++sp) {
+      const int64_t r = (int64_t)sp * d + e;
+      if (ip[r + 1] - ip[r] != n0) return PB_OK;
+      for (int64_t t = 0; t < n0; ++t)
+        if (ix[ip[r] + t] - r != off[(size_t)e * kFdMax + t] || dv[ip[r] + t] != val[(size_t)e * kFdMax + t])
+          return PB_OK;
+    }
+  }
+  int rc;
+  if ((rc = upload(c, c->fd_cnt, cnt.data(), cnt.size()))) return rc;
+  if ((rc = upload(c, c->fd_off, off.data(), off.size()))) return rc;
+  if ((rc = upload(c, c->fd_val, val.data(), val.size()))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->fd_tab_ok = true;
+  return PB_OK;
+}
+
 int pb_set_fd_operator(pb_context* c, int64_t nnz, const int64_t* indptr, const int32_t* indices,
                        const double* values, const double* diag) {
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
@@ -1790,7 +2114,10 @@ int pb_set_fd_operator(pb_context* c, int64_t nnz, const int64_t* indptr, const 
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->nnzD = nnz;
   c->have_fd = true;
-  return PB_OK;
+  c->h_d_indptr.assign(indptr, indptr + c->n + 1);
+  c->h_d_indices.assign(indices, indices + nnz);
+  c->h_d_vals.assign(values, values + nnz);
+  return build_fd_table(c);
 }
 
 int pb_set_losses(pb_context* c, const double* adia_energy, const double* pair_scale, const int32_t* pair_bin,
@@ -1898,7 +2225,6 @@ int pb_set_layout(pb_context* c, int32_t d) {
   const std::vector<int64_t>& ip = c->h_cpl_indptr;
   const std::vector<int32_t>& ix = c->h_cpl_indices;
   // band species: rows with an off-diagonal entry that leaves the row's bin
-  std::vector<int> band_of(nsp, -1);
   std::vector<int32_t> bspec, sspec;
   int lo = 1 << 30, hi = -(1 << 30);
   for (int sp = 0; sp < nsp; ++sp) {
@@ -1906,12 +2232,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
     for (int64_t r = (int64_t)sp * d; r < (int64_t)(sp + 1) * d && !band; ++r)
       for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
         if (ix[j] != r && ix[j] % d != r % d) { band = true; break; }
-    if (band) {
-      band_of[sp] = (int)bspec.size();
-      bspec.push_back(sp);
-    } else {
-      sspec.push_back(sp);
-    }
+    (band ? bspec : sspec).push_back(sp);
   }
   for (int32_t sp : bspec)
     for (int64_t r = (int64_t)sp * d; r < (int64_t)(sp + 1) * d; ++r)
@@ -1921,21 +2242,55 @@ int pb_set_layout(pb_context* c, int32_t d) {
         lo = std::min(lo, off);
         hi = std::max(hi, off);
       }
+  {  // bin-local species by coupling entries, longest rows first (k_slab's warps take rows strided)
+    std::vector<int64_t> cnt(nsp, 0);
+    for (int32_t sp : sspec)
+      for (int64_t r = (int64_t)sp * d; r < (int64_t)(sp + 1) * d; ++r) cnt[sp] += ip[r + 1] - ip[r];
+    std::stable_sort(sspec.begin(), sspec.end(), [&](int32_t a, int32_t b) { return cnt[a] > cnt[b]; });
+  }
   c->blocked_ok = false;
   c->lay_d = d;
   c->lay_nsp = nsp;
-  const size_t slab_bytes = (size_t)nsp * kColTile * sizeof(double);
+  if ((rc = build_fd_table(c))) return rc;
+  const int nb = (int)bspec.size(), nss = (int)sspec.size();
+  const int npairs = (nb + 1) / 2;
   const int RTr = (d + 7) / 8;
   const int Jr = bspec.empty() ? 1 : (7 + hi) / 4 + 1;
   int RT = 0, J = 0;
   for (int v : kBandRT) if (!RT && v >= RTr) RT = v;
   for (int v : kBandJ) if (!J && v >= Jr) J = v;
-  const bool ok = slab_bytes <= 227 * 1024 && RT > 0 && J > 0 && (bspec.empty() || lo >= 0) &&
-                  (int64_t)bspec.size() * nsp * RT * J * 32 < ((int64_t)1 << 31);
+  // bin-local rows: entries in bin-major order (bin, row species, CSR order);
+  // every bin starts on a multiple of 4 entries (16-byte copies of values and columns)
+  std::vector<int32_t> srp((size_t)d * nss + 1, 0), ssidx, sslot((size_t)std::max<int64_t>(R, 1), -1);
+  int32_t maxbin = 0;
+  for (int e = 0; e < d; ++e) {
+    while (ssidx.size() % 4) ssidx.push_back(0);
+    const size_t b0 = ssidx.size();
+    for (int i = 0; i < nss; ++i) {
+      const int64_t r = (int64_t)sspec[i] * d + e;
+      srp[(size_t)e * nss + i] = (int32_t)ssidx.size();
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+        if (ix[j] == r) continue;
+        sslot[j] = (int32_t)ssidx.size();
+        ssidx.push_back(ix[j] / d);
+      }
+    }
+    size_t b1 = ssidx.size();
+    b1 = (b1 + 3) & ~(size_t)3;
+    maxbin = std::max<int32_t>(maxbin, (int32_t)(b1 - b0));
+  }
+  while (ssidx.size() % 4) ssidx.push_back(0);
+  srp[(size_t)d * nss] = (int32_t)ssidx.size();
+  if (ssidx.empty()) ssidx.assign(4, 0);
+  const size_t max_smem = 227 * 1024;
+  const size_t ssm = SlabSmem::bytes(nsp, nss, maxbin);
+  const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0};
+  const bool ok = ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
+                  (size_t)d * (kColTile + 1) * sizeof(double) <= max_smem &&
+                  (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && ssidx.size() < ((size_t)1 << 31);
   if (!ok) return PB_OK;  // the general row kernels stay in use
-  const int nb = (int)bspec.size();
-  std::vector<int32_t> slot((size_t)std::max<int64_t>(R, 1), -1);
-  std::vector<uint32_t> mask((size_t)std::max(nb * nsp * RT, 1), 0u);
+  // band tiles: [species][band pair][2][RT][J][32] DMMA A fragments per window
+  std::vector<int32_t> bslot((size_t)std::max<int64_t>(R, 1), -1);
   for (int b = 0; b < nb; ++b)
     for (int e = 0; e < d; ++e) {
       const int64_t r = (int64_t)bspec[b] * d + e;
@@ -1944,23 +2299,30 @@ int pb_set_layout(pb_context* c, int32_t d) {
         if (ix[j] == r) continue;
         const int sp = ix[j] / d, e2 = ix[j] % d;
         const int jj = e2 / 4 - 2 * rt;
-        const size_t tile = ((size_t)(b * nsp + sp) * RT + rt);
-        slot[j] = (int32_t)((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4));
-        mask[tile] |= 1u << jj;
+        const size_t tile = ((size_t)sp * 2 * npairs + b) * RT + rt;
+        bslot[j] = (int32_t)((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4));
       }
     }
-  if ((rc = upload(c, c->band_slot, slot.data(), slot.size()))) return rc;
-  if ((rc = upload(c, c->band_mask, mask.data(), mask.size()))) return rc;
+  if ((rc = upload(c, c->band_slot, bslot.data(), bslot.size()))) return rc;
   if ((rc = upload(c, c->band_spec, bspec.data(), bspec.size()))) return rc;
   if ((rc = upload(c, c->slab_spec, sspec.data(), sspec.size()))) return rc;
+  if ((rc = upload(c, c->slab_rp, srp.data(), srp.size()))) return rc;
+  if ((rc = upload(c, c->slab_sidx, ssidx.data(), ssidx.size()))) return rc;
+  if ((rc = upload(c, c->slab_slot, sslot.data(), sslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_bytes));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)slab_bytes));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+  PB_CUDA(c, cudaFuncSetAttribute(bi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi.smem));
   c->band_nb = nb;
+  c->band_npairs = npairs;
   c->band_RT = RT;
   c->band_J = J;
-  c->band_stride = (int64_t)nb * nsp * RT * J * 32;
-  c->n_slab_spec = (int)sspec.size();
+  c->band_stride = (int64_t)nsp * 2 * npairs * RT * J * 32;
+  c->n_slab_spec = nss;
+  c->slab_nent = (int64_t)ssidx.size();
+  c->slab_maxbin = maxbin;
+  c->slab_smem = ssm;
+  c->band_smem = bi.smem;
   c->blocked_ok = true;
   return PB_OK;
 }
@@ -1981,7 +2343,7 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
   if (!value) return fail(c, PB_ERR_ARG, "pb_get_info: value is NULL");
   switch (key) {
     case PB_OPT_BATCHED_KERNELS: *value = c->batched_mode; return PB_OK;
-    case PB_INFO_BLOCKED_LAYOUT: *value = c->blocked_ok ? 1 : 0; return PB_OK;
+    case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
     case PB_INFO_BAND_SPECIES: *value = c->band_nb; return PB_OK;
   }
@@ -2104,7 +2466,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, c->ckpt.ensure((size_t)((S + a->ckpt_every - 1) / a->ckpt_every + 1) * n * ld * sizeof(double)));
   const bool blocked = use_blocked(c, K);
   if (blocked) {
-    PB_CUDA(c, c->m_sidx.ensure((size_t)mstride * sizeof(int)));
+    PB_CUDA(c, c->slab_vals.ensure((size_t)W * std::max<int64_t>(c->slab_nent, 1) * sizeof(double2)));
+    PB_CUDA(c, c->fdbuf.ensure(sbytes));
     PB_CUDA(c, c->band_vals.ensure((size_t)W * std::max<int64_t>(c->band_stride, 1) * sizeof(double)));
     PB_CUDA(c, c->band_part.ensure((size_t)kMaxBandGroups * std::max(c->band_nb, 1) * c->lay_d * ld * sizeof(double)));
   }
@@ -2154,6 +2517,12 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, cudaMemsetAsync(c->m_diag.p, 0, (size_t)W * n * sizeof(double), st));
   if (blocked && c->band_stride > 0)
     PB_CUDA(c, cudaMemsetAsync(c->band_vals.p, 0, (size_t)W * c->band_stride * sizeof(double), st));
+  if (blocked && c->slab_nent > 0) {
+    PB_CUDA(c, cudaMemsetAsync(c->slab_vals.p, 0, (size_t)W * c->slab_nent * sizeof(double2), st));
+    k_slab_cols<<<blocks_for((int64_t)W * c->slab_nent, 256), 256, 0, st>>>(c->slab_sidx.as<int>(), c->slab_nent, W,
+                                                                           c->slab_vals.as<double2>());
+    ++launches;
+  }
   if ((flags & PB_PHOTOHAD) && R > 0) {
     k_fold_first<<<blocks_for(R + 1, 8), 256, 0, st>>>(c->kernel.as<double>(), R, c->dph, c->PT.as<double>(),
                                                        c->cpl_is_diag.as<int>(), c->keep.as<int>());
@@ -2161,8 +2530,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, cub::DeviceScan::ExclusiveSum(c->scan_tmp.p, tb, c->keep.as<int>(), c->pos.as<int>(), (int)(R + 1), st));
     k_compact<<<blocks_for(R, 256), 256, 0, st>>>(c->keep.as<int>(), c->pos.as<int>(), c->cpl_indices.as<int>(),
                                                   c->cpl_is_diag.as<int>(), c->cpl_row.as<int>(), R, dest, diag_row,
-                                                  c->m_indices.as<int>(), std::max(c->lay_d, 1),
-                                                  blocked ? c->m_sidx.as<int>() : nullptr);
+                                                  c->m_indices.as<int>());
     k_m_indptr<<<blocks_for(n + 1, 256), 256, 0, st>>>(c->cpl_indptr.as<int64_t>(), c->pos.as<int>(), n,
                                                        c->m_indptr.as<int64_t>());
     if (c->n_seg > 0) {
@@ -2176,7 +2544,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     k_fold_gemm<<<dim3(blocks_for(R, kFoldBM), blocks_for(W, kFoldBN)), 256, smem, st>>>(
         c->kernel.as<double>(), R, c->dph, kpad, c->PT.as<double>(), W, dest, diag_row, c->m_vals.as<double>(),
         mstride, c->m_diag.as<double>(), n, blocked ? c->band_slot.as<int>() : nullptr,
-        blocked ? c->band_vals.as<double>() : nullptr, c->band_stride);
+        blocked ? c->band_vals.as<double>() : nullptr, c->band_stride, blocked ? c->slab_slot.as<int>() : nullptr,
+        blocked ? c->slab_vals.as<double>() : nullptr, c->slab_nent);
     launches += 5;
   } else {
     PB_CUDA(c, cudaMemsetAsync(c->m_indptr.p, 0, ((size_t)n + 1) * sizeof(int64_t), st));
@@ -2207,6 +2576,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)a->ckpt_every);
     put((uint64_t)blocked);
     put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
+    put((uint64_t)c->slab_nent);
     put((uint64_t)c->em_W);
     for (double v : c->em_dl) { uint64_t b; memcpy(&b, &v, 8); put(b); }
     const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);

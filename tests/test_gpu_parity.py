@@ -221,7 +221,10 @@ def test_bin_blocked_agrees_with_row_kernels(medium_run):
         finally:
             _batched_kernels(m, 1)
         out.append(m.state)
-    assert rel_err_on_support(out[1], out[0], _blocks(run)) < 1e-13
+    # the bin-blocked gather uses FMA, the row kernels separate multiply-adds
+    assert rel_err_on_support(out[1], out[0], _blocks(run)) < TOL
+    worst, above, total = local_scale_check(out[1], out[0], _blocks(run), tol=TOL)
+    assert worst < 1e-13, worst
 
 
 def test_full_network_short_range_vs_oracle():
