@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(256) k_fold_gemm(const double* __restrict__ K,
         if (de >= 0) mv[(size_t)w * mv_stride + de] = v;
         if (dr >= 0) md[(size_t)w * n + dr] = v;
         if (bs >= 0) band[(size_t)w * band_stride + bs] = v;
-        if (ss >= 0) slab[2 * ((size_t)w * slab_stride + ss)] = v;  // value half of the packed entry
+        if (ss >= 0) slab[(size_t)w * slab_stride + ss] = v;
       }
   }
 }
@@ -593,7 +593,8 @@ struct StepParams {
   int n_slab_spec;
   const int* slab_rp;       // bin-major entry range of each bin-local row ([d][n_slab_spec] + 1)
   const int* slab_sidx;     // species block of the column of each bin-major entry
-  const double2* slab_ent;  // [W][slab_stride] bin-major entries: (M_off value, slab byte offset of the column)
+  const double* slab_vals;  // [W][slab_stride] M_off values of the bin-major entries
+  const int* slab_offs;     // byte offset in k_slab's state slab of each entry's column
   int64_t slab_stride;
   int slab_maxbin;          // entries of the largest bin (shared-memory sizing)
   const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
@@ -1027,25 +1028,33 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
   }
 }
 
-// k_slab's shared memory: the state slab (nsp x 32), the bin's entries
-// (value, slab byte offset of the column), the row factors (3 x nss) and the
-// int row tables (entry ranges, injection slots, species).
+// k_slab's shared memory: the state slab (nsp x 32), the bin's entry values,
+// the row factors (3 x nss), the per-warp rings of (FD term, F(x)) rows, then
+// the int tables (entry column offsets, entry ranges, injection slots,
+// species).  Every block starts on a 16-byte boundary.
+constexpr int kSlabRing = 4;        // rows of FD term / F(x) in flight per warp
 struct SlabSmem {
   double* slab;
-  double2* ent;
+  double* vals;
   double* fac;
+  double* ring;  // [warp][kSlabRing][2][32]
+  int* offs;
   int* rp;
   int* slot;
   int* spec;
+  __host__ __device__ static size_t al2(size_t x) { return (x + 1) & ~(size_t)1; }
   __host__ __device__ static size_t bytes(int nsp, int nss, int maxbin) {
-    return ((size_t)nsp * kColTile + 3 * (size_t)nss) * sizeof(double) + (size_t)maxbin * sizeof(double2) +
-           (3 * (size_t)nss + 1) * sizeof(int);
+    return ((size_t)nsp * kColTile + maxbin + al2(3 * (size_t)nss) +
+            (size_t)(kSlabThreads / 32) * kSlabRing * 2 * kColTile) * sizeof(double) +
+           ((size_t)maxbin + 3 * (size_t)nss + 1) * sizeof(int);
   }
   __device__ SlabSmem(double* base, int nsp, int nss, int maxbin) {
     slab = base;
-    ent = reinterpret_cast<double2*>(slab + (size_t)nsp * kColTile);
-    fac = reinterpret_cast<double*>(ent + maxbin);
-    rp = reinterpret_cast<int*>(fac + 3 * (size_t)nss);
+    vals = slab + (size_t)nsp * kColTile;
+    fac = vals + maxbin;
+    ring = fac + al2(3 * (size_t)nss);
+    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabRing * 2 * kColTile);
+    rp = offs + maxbin;
     slot = rp + nss + 1;
     spec = slot + nss;
   }
@@ -1055,15 +1064,17 @@ struct SlabSmem {
 // slab of bin e and the bin's coupling entries arrive in shared memory by
 // asynchronous copies; a warp then takes rows e-strided (rows are ordered by
 // entry count, longest first), sums each from shared memory and applies the
-// stage update with the FD term from fdbuf (loaded one row ahead).  Offsets
-// into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at launch).
+// stage update.  The row's FD term (fdbuf) and, in stage 2, F(x) are copied
+// asynchronously kSlabRing rows ahead into the warp's ring.  Offsets into the
+// (n x ld) state buffers are 32-bit (n ld < 2^31, checked at launch).
 template <int STAGE>
 __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
   extern __shared__ double sm[];
   const int nss = p.n_slab_spec;
   const int e = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int col = blockIdx.y * kColTile + lane;  // < ld
+  const int col0 = blockIdx.y * kColTile;
+  const int col = col0 + lane;  // < ld
   const bool active = col < p.ncols;
   const StepScalars s = load_scalars(p, p.step);
   const size_t o0 = (size_t)(p.step & 1) * p.n;
@@ -1072,14 +1083,15 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
   const double* __restrict__ v = p.src;
   const int q0 = p.slab_rp[(size_t)e * nss], q1 = p.slab_rp[(size_t)(e + 1) * nss];  // multiples of 4
   {
-    const double* vs = v + (size_t)e * ld + blockIdx.y * kColTile;
+    const double* vs = v + (size_t)e * ld + col0;
     for (int t = threadIdx.x; t < p.nsp * (kColTile / 2); t += blockDim.x) {
       const int q = t / (kColTile / 2), c = 2 * (t - q * (kColTile / 2));
       cp_async16(L.slab + q * kColTile + c, vs + (size_t)q * d * ld + c);
     }
     if (s.photohad) {
-      const double2* me = p.slab_ent + (size_t)s.w * p.slab_stride + q0;
-      for (int t = threadIdx.x; t < q1 - q0; t += blockDim.x) cp_async16(L.ent + t, me + t);
+      const double* mv = p.slab_vals + (size_t)s.w * p.slab_stride + q0;
+      for (int t = threadIdx.x; t < (q1 - q0) / 2; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
+      for (int t = threadIdx.x; t < (q1 - q0) / 4; t += blockDim.x) cp_async16(L.offs + 4 * t, p.slab_offs + q0 + 4 * t);
     }
     cp_async_commit();
   }
@@ -1105,49 +1117,48 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
   cp_async_wait<0>();
   __syncthreads();
 
-  const double* __restrict__ fdb = p.fdbuf;
-  const double* __restrict__ fprv = p.f;
-  int i = wid;
-  if (i >= nss) return;
-  // FD term and F(x) of the row, loaded one row ahead
-  int r = L.spec[i] * d + e;
-  double fd = 0.0, fp = 0.0;
-  if (s.kap) fd = fdb[r * ld + col];
-  if (STAGE == 2) fp = fprv[r * ld + col];
-  const double* sl = L.slab + lane;
-  while (true) {
-    const int ni = i + nw;
-    int nr = 0;
-    double nfd = 0.0, nfp = 0.0;
-    if (ni < nss) {
-      nr = L.spec[ni] * d + e;
-      if (s.kap) nfd = fdb[nr * ld + col];
-      if (STAGE == 2) nfp = fprv[nr * ld + col];
+  // Ring of the warp's upcoming rows: lanes 0-15 copy the FD row, lanes 16-31
+  // the F(x) row, 16 bytes each; one commit group per row (empty past the end).
+  double* ring = L.ring + (size_t)wid * kSlabRing * 2 * kColTile;
+  const bool need_fd = s.kap, need_f = STAGE == 2;
+  const int h = lane >> 4, c2 = 2 * (lane & 15);
+  auto fetch = [&](int i, int k) {
+    if (i < nss) {
+      const int r = L.spec[i] * d + e;
+      double* dst = ring + ((k % kSlabRing) * 2 + h) * kColTile + c2;
+      if (h == 0 && need_fd) cp_async16(dst, p.fdbuf + r * ld + col0 + c2);
+      if (h == 1 && need_f) cp_async16(dst, p.f + r * ld + col0 + c2);
     }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < kSlabRing; ++k) fetch(wid + k * nw, k);
+  const char* slb = reinterpret_cast<const char*>(L.slab + lane);
+  int k = 0;
+  for (int i = wid; i < nss; i += nw, ++k) {
+    const int r = L.spec[i] * d + e;
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     if (s.photohad) {
       const int j1 = L.rp[i + 1];
       int j = L.rp[i];
-      const char* slb = reinterpret_cast<const char*>(sl);
       for (; j + 3 < j1; j += 4) {
-        const double2 e0 = L.ent[j], e1 = L.ent[j + 1], e2 = L.ent[j + 2], e3 = L.ent[j + 3];
-        const double x0 = *reinterpret_cast<const double*>(slb + __double2loint(e0.y));
-        const double x1 = *reinterpret_cast<const double*>(slb + __double2loint(e1.y));
-        const double x2 = *reinterpret_cast<const double*>(slb + __double2loint(e2.y));
-        const double x3 = *reinterpret_cast<const double*>(slb + __double2loint(e3.y));
-        acc0 = __fma_rn(e0.x, x0, acc0);
-        acc1 = __fma_rn(e1.x, x1, acc1);
-        acc2 = __fma_rn(e2.x, x2, acc2);
-        acc3 = __fma_rn(e3.x, x3, acc3);
+        const double x0 = *reinterpret_cast<const double*>(slb + L.offs[j]);
+        const double x1 = *reinterpret_cast<const double*>(slb + L.offs[j + 1]);
+        const double x2 = *reinterpret_cast<const double*>(slb + L.offs[j + 2]);
+        const double x3 = *reinterpret_cast<const double*>(slb + L.offs[j + 3]);
+        acc0 = __fma_rn(L.vals[j], x0, acc0);
+        acc1 = __fma_rn(L.vals[j + 1], x1, acc1);
+        acc2 = __fma_rn(L.vals[j + 2], x2, acc2);
+        acc3 = __fma_rn(L.vals[j + 3], x3, acc3);
       }
-      for (; j < j1; ++j) {
-        const double2 en = L.ent[j];
-        acc0 = __fma_rn(en.x, *reinterpret_cast<const double*>(slb + __double2loint(en.y)), acc0);
-      }
+      for (; j < j1; ++j) acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
     }
+    cp_async_wait<kSlabRing - 1>();  // this row's copies (issued kSlabRing rows ago) have landed
+    __syncwarp();
+    const double* rs = ring + (k % kSlabRing) * 2 * kColTile;
     if (active) {
       double out = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
-      if (s.kap) out = __dadd_rn(out, fd);
+      if (s.kap) out = __dadd_rn(out, rs[lane]);
       if (s.decay) {
         double sL = 0.0;
         for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
@@ -1171,24 +1182,14 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
         p.f[ro] = out;
       } else {
         // x = a + ((F(a) - F(x)) h) phi2
-        const double dF = __dmul_rn(__dadd_rn(out, -fp), s.h);
+        const double dF = __dmul_rn(__dadd_rn(out, -rs[kColTile + lane]), s.h);
         p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * nss + i]));
       }
     }
-    if (ni >= nss) break;
-    i = ni;
-    r = nr;
-    fd = nfd;
-    fp = nfp;
+    __syncwarp();  // the slot is read before it is refilled
+    fetch(i + kSlabRing * nw, k + kSlabRing);
   }
-}
-
-// The column half of every window's packed bin-major entries: the byte offset
-// of the column species' row in k_slab's state slab.
-__global__ void k_slab_cols(const int* __restrict__ sidx, int64_t nent, int W, double2* __restrict__ ent) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nent * W) return;
-  ent[t].y = __hiloint2double(0, sidx[t % nent] * kColTile * (int)sizeof(double));
+  cp_async_wait<0>();
 }
 
 // Stage 2: the row factors of the next step for the bin-local rows (one
@@ -1737,7 +1738,8 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.n_slab_spec = c->n_slab_spec;
   p.slab_rp = c->slab_rp.as<int>();
   p.slab_sidx = c->slab_sidx.as<int>();
-  p.slab_ent = c->slab_vals.as<double2>();
+  p.slab_vals = c->slab_vals.as<double>();
+  p.slab_offs = c->slab_sidx.as<int>();
   p.slab_stride = c->slab_nent;
   p.slab_maxbin = c->slab_maxbin;
   p.fd_cnt = c->fd_cnt.as<int>();
@@ -2272,7 +2274,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
       for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
         if (ix[j] == r) continue;
         sslot[j] = (int32_t)ssidx.size();
-        ssidx.push_back(ix[j] / d);
+        ssidx.push_back((ix[j] / d) * kColTile * (int32_t)sizeof(double));  // byte offset in k_slab's slab
       }
     }
     size_t b1 = ssidx.size();
@@ -2466,7 +2468,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, c->ckpt.ensure((size_t)((S + a->ckpt_every - 1) / a->ckpt_every + 1) * n * ld * sizeof(double)));
   const bool blocked = use_blocked(c, K);
   if (blocked) {
-    PB_CUDA(c, c->slab_vals.ensure((size_t)W * std::max<int64_t>(c->slab_nent, 1) * sizeof(double2)));
+    PB_CUDA(c, c->slab_vals.ensure((size_t)W * std::max<int64_t>(c->slab_nent, 1) * sizeof(double)));
     PB_CUDA(c, c->fdbuf.ensure(sbytes));
     PB_CUDA(c, c->band_vals.ensure((size_t)W * std::max<int64_t>(c->band_stride, 1) * sizeof(double)));
     PB_CUDA(c, c->band_part.ensure((size_t)kMaxBandGroups * std::max(c->band_nb, 1) * c->lay_d * ld * sizeof(double)));
@@ -2517,12 +2519,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, cudaMemsetAsync(c->m_diag.p, 0, (size_t)W * n * sizeof(double), st));
   if (blocked && c->band_stride > 0)
     PB_CUDA(c, cudaMemsetAsync(c->band_vals.p, 0, (size_t)W * c->band_stride * sizeof(double), st));
-  if (blocked && c->slab_nent > 0) {
-    PB_CUDA(c, cudaMemsetAsync(c->slab_vals.p, 0, (size_t)W * c->slab_nent * sizeof(double2), st));
-    k_slab_cols<<<blocks_for((int64_t)W * c->slab_nent, 256), 256, 0, st>>>(c->slab_sidx.as<int>(), c->slab_nent, W,
-                                                                           c->slab_vals.as<double2>());
-    ++launches;
-  }
+  if (blocked && c->slab_nent > 0)
+    PB_CUDA(c, cudaMemsetAsync(c->slab_vals.p, 0, (size_t)W * c->slab_nent * sizeof(double), st));
   if ((flags & PB_PHOTOHAD) && R > 0) {
     k_fold_first<<<blocks_for(R + 1, 8), 256, 0, st>>>(c->kernel.as<double>(), R, c->dph, c->PT.as<double>(),
                                                        c->cpl_is_diag.as<int>(), c->keep.as<int>());
