@@ -13,7 +13,8 @@ Prints one JSON line (rank 0):
             losses, fold, split and all ETD2 steps);
   e2e    -- spectra/s through the public solver API (host schedule, pinned
             host->device uploads, device->host copy of the result states);
-  roofline -- the ETD2 step kernels against the measured HBM copy bandwidth;
+  roofline -- the dominant stage kernel (re-run alone between CUDA events) against
+              its measured peak; roofline_kernels lists every stage kernel;
   cpu_baseline -- the CPU oracle of the reference algorithm on a bounded sample;
   plain  -- the one-spectrum-per-launch path on the same operator.
 
@@ -187,6 +188,9 @@ def run_b200(args, dist, rank, ws, local):
     value = spectra / t_dev
     e2e = spectra / t_wall
 
+    # per-kernel rooflines (re-runs the last batched solve's final step)
+    kern = kernel_rooflines(solver, run, sched, n_active, rows.size)
+
     # plain path: one spectrum per launch on the same operator
     plain = None
     if args.plain > 0:
@@ -236,11 +240,11 @@ def run_b200(args, dist, rank, ws, local):
             "l2": "state buffers 3 x 138 MB exceed the 126 MB L2 between solves",
         },
         "e2e": {"value": e2e, "unit": "spectra/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk, "unit": "GB/s", "frac": achieved / pk,
-                     "traffic": None, "peak_source": pk_kind,
-                     "kernel": "k_step_multi (ETD2 stage kernels, both row classes)",
-                     "bytes_per_solve": bytes_solve, "step_launches_per_solve": step_launches,
-                     "avg_launch_us": avg_steps_ms * 1e3 / max(step_launches, 1)},
+        "roofline": kern["dominant"] if kern else None,
+        "roofline_kernels": kern["kernels"] if kern else None,
+        "step_stream": {"bytes_per_solve": bytes_solve, "steps_ms_per_solve": avg_steps_ms,
+                        "achieved_gbs": achieved, "peak_gbs": pk, "peak_source": pk_kind,
+                        "note": "whole step loop (all stage kernels, both streams) against the HBM copy peak"},
         "gpu_launches": int(launches),
         "plain_spectra_per_s": plain,
         "batched_over_plain": (value / ws / plain) if plain else None,
@@ -254,6 +258,62 @@ def run_b200(args, dist, rank, ws, local):
     if clk:
         line["clocks"] = clk
     return line, run, pts, zi, sched
+
+
+def kernel_rooflines(solver, run, sched, n_active, n_inj):
+    """Per-kernel rooflines of the bin-blocked stage at full activity.
+
+    The last step of the solve has every column active.  Each kernel of its
+    two stages is re-run alone between CUDA events on the library stream
+    (``pb_profile_stage``); achieved = algorithmic bytes (or useful FP64 flops)
+    per launch / mean launch time.  Algorithmic bytes per launch, K columns,
+    n states, ns bin-local rows, E entries of the bin-local rows:
+      k_fd          read v and kappa, write D_off (kappa v):  16 n K + 8 n
+      k_slab        read v (all rows), entries (12 E), FD term, row factors;
+                    stage 1 writes a and F(x), stage 2 reads F(x), writes x:
+                    8 n K + 12 E + 24 ns K + 24 ns
+      k_band        useful flops 2 nnz_band K on the FP64 tensor pipe (DMMA)
+      k_band_finish read the group partials and the band rows' inputs.
+    """
+    from prince_b200 import _lib
+
+    ctx = solver._dev.ctx
+    if not ctx.info(_lib.PB_INFO_LAST_BLOCKED):
+        return None
+    K = int(n_active[-1])
+    step = int(sched.n_steps - 1)
+    n = run.dim_states
+    ns = ctx.info(_lib.PB_INFO_SLAB_ROWS)
+    nent = ctx.info(_lib.PB_INFO_SLAB_ENTRIES)
+    nnz_band = ctx.info(_lib.PB_INFO_BAND_ENTRIES)
+    t1 = ctx.profile_stage(step, 1, reps=5)
+    t2 = ctx.profile_stage(step, 2, reps=5)
+    ms = [(a + b) / 2 for a, b in zip(t1, t2)]
+    hbm, hbm_kind = _peaks()
+    fp64 = ctx.fp64_peak()
+    kb = {
+        "k_fd": 16.0 * n * K + 8.0 * n,
+        "k_slab": 8.0 * n * K + 12.0 * nent + 24.0 * ns * K + 24.0 * ns,
+    }
+    kernels = []
+    for name, t in (("k_fd", ms[0]), ("k_slab", ms[1])):
+        if t > 0:
+            a = kb[name] / (t * 1e-3) / 1e9
+            kernels.append({"kernel": name, "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
+                            "frac": a / hbm, "traffic": None, "launch_us": t * 1e3,
+                            "algorithmic_bytes": kb[name], "peak_source": hbm_kind})
+    if ms[2] > 0:
+        a = 2.0 * nnz_band * K / (ms[2] * 1e-3) / 1e12
+        kernels.append({"kernel": "k_band", "bound": "tensor", "achieved": a, "peak": fp64, "unit": "TFLOP/s",
+                        "frac": a / fp64, "traffic": None, "launch_us": ms[2] * 1e3,
+                        "algorithmic_flops": 2.0 * nnz_band * K,
+                        "peak_source": "measured FP64 DMMA peak (pb_fp64_peak, register-only kernel)"})
+    if ms[3] > 0:
+        kernels.append({"kernel": "k_band_finish", "launch_us": ms[3] * 1e3})
+    timed = [k for k in kernels if "frac" in k]
+    dominant = dict(max(timed, key=lambda k: k["launch_us"]))
+    dominant["share_of_stage"] = dominant["launch_us"] / (sum(ms) * 1e3)
+    return {"dominant": dominant, "kernels": kernels}
 
 
 def adjoint_timing(run, pts, zi, device):

@@ -44,6 +44,9 @@ extern "C" {
 #define PB_INFO_BLOCKED_LAYOUT 2 /* 1 if pb_set_layout found a pattern the bin-blocked kernels handle */
 #define PB_INFO_LAST_BLOCKED 3   /* 1 if the last pb_solve ran the bin-blocked kernels */
 #define PB_INFO_BAND_SPECIES 4   /* species whose coupling rows leave their energy bin */
+#define PB_INFO_BAND_ENTRIES 5   /* off-diagonal coupling entries of the band rows */
+#define PB_INFO_SLAB_ENTRIES 6   /* off-diagonal coupling entries of the bin-local rows */
+#define PB_INFO_SLAB_ROWS 7      /* bin-local rows */
 
 typedef struct pb_context pb_context;
 
@@ -132,6 +135,18 @@ int pb_set_layout(pb_context* ctx, int32_t d);
  * No reference counterpart. */
 int pb_set_option(pb_context* ctx, int32_t key, int64_t value);
 int pb_get_info(pb_context* ctx, int32_t key, int64_t* value);
+
+/* Measurement aid: re-runs the bin-blocked kernels of one stage (1 or 2) of
+ * step `step` of the last solve, each kernel alone between CUDA events on the
+ * context's stream, and returns the mean of `reps` launches in milliseconds:
+ * ms[0] FD term, ms[1] bin-local rows, ms[2] band partial sums, ms[3] band
+ * rows (0 for a kernel the stage does not run).  Overwrites the stage's
+ * output buffers.  No reference counterpart. */
+int pb_profile_stage(pb_context* ctx, int64_t step, int32_t stage, int32_t reps, double* ms);
+
+/* Measured FP64 tensor-pipe (DMMA) throughput of the device in TFLOP/s, from a
+ * register-only kernel on every SM.  No reference counterpart. */
+int pb_fp64_peak(pb_context* ctx, double* tflops);
 
 /* Co-evolved EM cascade layout: the gamma block (n_em states from gamma_off),
  * the e- and e+ blocks (offsets, -1 if absent), and the charged nuclei whose

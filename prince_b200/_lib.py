@@ -22,6 +22,7 @@ PB_OK, PB_ERR_ARG, PB_ERR_STATE, PB_ERR_CUDA, PB_ERR_DEVICE = 0, 1, 2, 3, 4
 PB_ADIABATIC, PB_PAIRPROD, PB_PHOTOHAD, PB_INJECTION, PB_PARTIAL_DIFF, PB_DECAY = 1, 2, 4, 8, 16, 32
 PB_EM_CASCADE = 64
 PB_OPT_BATCHED_KERNELS, PB_INFO_BLOCKED_LAYOUT, PB_INFO_LAST_BLOCKED, PB_INFO_BAND_SPECIES = 1, 2, 3, 4
+PB_INFO_BAND_ENTRIES, PB_INFO_SLAB_ENTRIES, PB_INFO_SLAB_ROWS = 5, 6, 7
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)
@@ -69,6 +70,8 @@ _PROTOS = {
     "pb_set_layout": (C.c_int, [_vp, C.c_int32]),
     "pb_set_option": (C.c_int, [_vp, C.c_int32, C.c_int64]),
     "pb_get_info": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int64)]),
+    "pb_profile_stage": (C.c_int, [_vp, C.c_int64, C.c_int32, C.c_int32, _d]),
+    "pb_fp64_peak": (C.c_int, [_vp, _d]),
     "pb_set_em": (C.c_int, [_vp, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_int32, C.c_int32, _i64, _d, _d,
                             _d]),
     "pb_set_em_windows": (C.c_int, [_vp, C.c_int32, _d, _d, _d, _d]),
@@ -217,6 +220,18 @@ class Context:
         v = C.c_int64(0)
         self._check(self.lib.pb_get_info(self.h, int(key), C.byref(v)), "pb_get_info")
         return int(v.value)
+
+    def profile_stage(self, step, stage, reps=5):
+        """Per-kernel milliseconds of one stage of the last solve: (fd, slab, band, band_finish)."""
+        out = np.zeros(4)
+        self._check(self.lib.pb_profile_stage(self.h, int(step), int(stage), int(reps), _ptr(out, C.c_double)),
+                    "pb_profile_stage")
+        return tuple(float(v) for v in out)
+
+    def fp64_peak(self):
+        v = np.zeros(1)
+        self._check(self.lib.pb_fp64_peak(self.h, _ptr(v, C.c_double)), "pb_fp64_peak")
+        return float(v[0])
 
     def set_em(self, n_em, gamma_off, em_off, ep_off, n_cr, bh_off, bh_A, inv_E, dE):
         bo, ba, ie, de = _i64a(bh_off), _f64(bh_A), _f64(inv_E), _f64(dE)

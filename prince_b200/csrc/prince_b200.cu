@@ -124,6 +124,8 @@ struct pb_context {
   int32_t last_W = 0;
   bool have_solution = false;
   std::vector<int32_t> h_win;   // window of each step of the current solve (host copy)
+  std::vector<int32_t> h_nact;  // active columns of each step of the last solve (host copy)
+  int64_t band_nnz = 0, slab_nnz = 0;  // coupling entries of the band rows and the bin-local rows
 
   // bin-blocked batched path (pb_set_layout): species blocks of `lay_d` bins
   std::vector<int64_t> h_cpl_indptr;
@@ -2263,6 +2265,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   for (int v : kBandJ) if (!J && v >= Jr) J = v;
   // bin-local rows: entries in bin-major order (bin, row species, CSR order);
   // every bin starts on a multiple of 4 entries (16-byte copies of values and columns)
+  int64_t band_nnz = 0, slab_nnz = 0;
   std::vector<int32_t> srp((size_t)d * nss + 1, 0), ssidx, sslot((size_t)std::max<int64_t>(R, 1), -1);
   int32_t maxbin = 0;
   for (int e = 0; e < d; ++e) {
@@ -2274,6 +2277,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
       for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
         if (ix[j] == r) continue;
         sslot[j] = (int32_t)ssidx.size();
+        ++slab_nnz;
         ssidx.push_back((ix[j] / d) * kColTile * (int32_t)sizeof(double));  // byte offset in k_slab's slab
       }
     }
@@ -2303,6 +2307,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
         const int jj = e2 / 4 - 2 * rt;
         const size_t tile = ((size_t)sp * 2 * npairs + b) * RT + rt;
         bslot[j] = (int32_t)((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4));
+        ++band_nnz;
       }
     }
   if ((rc = upload(c, c->band_slot, bslot.data(), bslot.size()))) return rc;
@@ -2325,7 +2330,105 @@ int pb_set_layout(pb_context* c, int32_t d) {
   c->slab_maxbin = maxbin;
   c->slab_smem = ssm;
   c->band_smem = bi.smem;
+  c->band_nnz = band_nnz;
+  c->slab_nnz = slab_nnz;
   c->blocked_ok = true;
+  return PB_OK;
+}
+
+int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, double* ms) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!ms || reps < 1 || (stage != 1 && stage != 2)) return fail(c, PB_ERR_ARG, "pb_profile_stage: bad arguments");
+  if (!c->have_solution) return fail(c, PB_ERR_STATE, "pb_profile_stage: run pb_solve first");
+  const int K = c->last_K;
+  if (!use_blocked(c, K)) return fail(c, PB_ERR_STATE, "pb_profile_stage: the last solve did not run the bin-blocked kernels");
+  if (step < 0 || step >= c->last_S || c->h_nact[step] == 0) return fail(c, PB_ERR_ARG, "pb_profile_stage: step without active columns");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int ld = ((K + kColTile - 1) / kColTile) * kColTile;
+  const uint32_t flags = c->last_flags;
+  const bool pair = (flags & PB_PAIRPROD) && (flags & PB_PARTIAL_DIFF);
+  const bool inj = (flags & PB_INJECTION) && c->n_src > 0;
+  StepParams p;
+  memset(&p, 0, sizeof(p));
+  fill_step_params(c, p, K, ld, flags, pair, inj, c->last_S, ld / kColTile);
+  p.step = step;
+  p.ncols = c->h_nact[step];
+  p.src = stage == 1 ? c->X.as<double>() : c->A.as<double>();
+  p.x = c->X.as<double>();
+  p.xout = c->X.as<double>();
+  cudaStream_t st = c->stream;
+  const bool photohad = (flags & PB_PHOTOHAD) != 0, kap = (flags & PB_PARTIAL_DIFF) != 0;
+  const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
+  const int cblocks = (int)blocks_for(p.ncols, 64);
+  const int per = cblocks * std::max(c->band_npairs, 1);
+  const int G = std::max(1, std::min({(c->num_sms + per - 1) / per, kMaxBandGroups, p.nsp}));
+  p.spg = (p.nsp + G - 1) / G;
+  p.ngroups = (photohad && p.nb > 0) ? (p.nsp + p.spg - 1) / p.spg : 0;
+  const BandInstance bi = band_kernel(c->band_RT, c->band_J);
+  for (int kk = 0; kk < 4; ++kk) ms[kk] = 0.0;
+  for (int kk = 0; kk < 4; ++kk) {
+    const bool runs = kk == 0 ? kap : kk == 1 ? true : kk == 2 ? p.ngroups > 0 : p.nb > 0;
+    if (!runs) continue;
+    for (int r = -1; r < reps; ++r) {  // one untimed launch first
+      PB_CUDA(c, cudaEventRecord(c->ev0, st));
+      if (kk == 0) k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 1) * sizeof(double), st>>>(p);
+      if (kk == 1) {
+        if (stage == 1) k_slab<1><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
+        else k_slab<2><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
+      }
+      if (kk == 2) bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), 256, bi.smem, st>>>(p);
+      if (kk == 3) {
+        const unsigned gb = (unsigned)blocks_for((int64_t)p.nb * p.d, 8);
+        if (stage == 1) k_band_finish<1><<<dim3(gb, tiles), 256, 0, st>>>(p);
+        else k_band_finish<2><<<dim3(gb, tiles), 256, 0, st>>>(p);
+      }
+      PB_CUDA(c, cudaGetLastError());
+      PB_CUDA(c, cudaEventRecord(c->ev1, st));
+      PB_CUDA(c, cudaEventSynchronize(c->ev1));
+      float t = 0.f;
+      PB_CUDA(c, cudaEventElapsedTime(&t, c->ev0, c->ev1));
+      if (r >= 0) ms[kk] += t / reps;
+    }
+  }
+  return PB_OK;
+}
+
+// FP64 tensor-pipe throughput probe: independent DMMA m8n8k4 chains in registers.
+__global__ void k_fp64_probe(double* out, int iters) {
+  double a = 1.0 + threadIdx.x * 1e-9, b = 1.0 - threadIdx.x * 1e-9;
+  double cc[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) cc[i][0] = cc[i][1] = 0.0;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dmma884(cc[i][0], cc[i][1], a, b);
+  }
+  double sum = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) sum += cc[i][0] + cc[i][1];
+  out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = sum;
+}
+
+int pb_fp64_peak(pb_context* c, double* tflops) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!tflops) return fail(c, PB_ERR_ARG, "pb_fp64_peak: tflops is NULL");
+  int rc = set_device(c);
+  if (rc) return rc;
+  const int blocks = 4 * c->num_sms, threads = 256, iters = 4096;
+  DBuf out;
+  PB_CUDA(c, out.ensure((size_t)blocks * threads * sizeof(double)));
+  cudaStream_t st = c->stream;
+  k_fp64_probe<<<blocks, threads, 0, st>>>(out.as<double>(), 16);
+  PB_CUDA(c, cudaEventRecord(c->ev0, st));
+  k_fp64_probe<<<blocks, threads, 0, st>>>(out.as<double>(), iters);
+  PB_CUDA(c, cudaEventRecord(c->ev1, st));
+  PB_CUDA(c, cudaEventSynchronize(c->ev1));
+  float t = 0.f;
+  PB_CUDA(c, cudaEventElapsedTime(&t, c->ev0, c->ev1));
+  out.release();
+  const double flop = 2.0 * 256 * 8 * (double)iters * ((double)blocks * threads / 32);
+  *tflops = flop / (t * 1e-3) / 1e12;
   return PB_OK;
 }
 
@@ -2348,6 +2451,9 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
     case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
     case PB_INFO_BAND_SPECIES: *value = c->band_nb; return PB_OK;
+    case PB_INFO_BAND_ENTRIES: *value = c->band_nnz; return PB_OK;
+    case PB_INFO_SLAB_ENTRIES: *value = c->slab_nnz; return PB_OK;
+    case PB_INFO_SLAB_ROWS: *value = (int64_t)c->n_slab_spec * c->lay_d; return PB_OK;
   }
   return fail(c, PB_ERR_ARG, "pb_get_info: unknown key %d", key);
 }
@@ -2424,6 +2530,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   }
   if ((int64_t)W * c->n >= ((int64_t)1 << 40)) return fail(c, PB_ERR_ARG, "pb_solve: too many windows");
   c->h_win.assign(a->window, a->window + S);
+  c->h_nact.assign(a->n_active, a->n_active + S);
   int rc = set_device(c);
   if (rc) return rc;
   const int64_t n = c->n;
