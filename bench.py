@@ -260,6 +260,12 @@ def run_b200(args, dist, rank, ws, local):
     return line, run, pts, zi, sched
 
 
+# DRAM bytes per launch (dram__bytes read + write) of each stage kernel in one
+# ncu capture of this workload at K = 512 (bench.py --z-range 0.05,0.05,
+# -s 4 -c 1 per kernel); the capture is repeated after kernel changes.
+NCU_TRAFFIC_K512 = {"k_slab": 533e6, "k_band": 171e6, "k_fd": 227e6}
+
+
 def kernel_rooflines(solver, run, sched, n_active, n_inj):
     """Per-kernel rooflines of the bin-blocked stage at full activity.
 
@@ -300,12 +306,14 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
         if t > 0:
             a = kb[name] / (t * 1e-3) / 1e9
             kernels.append({"kernel": name, "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
-                            "frac": a / hbm, "traffic": None, "launch_us": t * 1e3,
+                            "frac": a / hbm, "traffic": NCU_TRAFFIC_K512.get(name) if K == 512 else None,
+                            "launch_us": t * 1e3,
                             "algorithmic_bytes": kb[name], "peak_source": hbm_kind})
     if ms[2] > 0:
         a = 2.0 * nnz_band * K / (ms[2] * 1e-3) / 1e12
         kernels.append({"kernel": "k_band", "bound": "tensor", "achieved": a, "peak": fp64, "unit": "TFLOP/s",
-                        "frac": a / fp64, "traffic": None, "launch_us": ms[2] * 1e3,
+                        "frac": a / fp64, "traffic": NCU_TRAFFIC_K512["k_band"] if K == 512 else None,
+                        "traffic_unit": "bytes", "launch_us": ms[2] * 1e3,
                         "algorithmic_flops": 2.0 * nnz_band * K,
                         "peak_source": "measured FP64 DMMA peak (pb_fp64_peak, register-only kernel)"})
     if ms[3] > 0:
