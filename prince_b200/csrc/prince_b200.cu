@@ -146,7 +146,7 @@ struct pb_context {
   std::vector<int32_t> h_d_indices;
   std::vector<double> h_d_vals;
   bool fd_tab_ok = false;
-  DBuf fd_cnt, fd_off, fd_val, fdbuf;
+  DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp;
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
@@ -603,6 +603,7 @@ struct StepParams {
   const int* fd_off;
   const double* fd_val;
   double* fdbuf;            // n x ld: D_off (kappa v) of the stage
+  double* fdkp;             // n x ld: D_off (kappa_pair v), adjoint record pass with the photon scale, or null
   const int* band_spec;     // species with cross-bin coupling rows
   int nb;
   const double* band_vals;  // [W][nsp][band pair][2][RT][J][32] DMMA A fragments
@@ -1009,6 +1010,7 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
   const int col = blockIdx.y * kColTile + lane;  // < ld
   double* vb = fsm;                  // d x 32
   double* kb = fsm + d * kColTile;   // d
+  double* kpb = kb + d;              // d: kappa_pair of the window (recording only)
   const size_t o0 = (size_t)(p.step & 1) * p.n;
   const double* __restrict__ v = p.src + (size_t)sp * d * ld + blockIdx.y * kColTile;
   for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
@@ -1017,6 +1019,9 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
   }
   cp_async_commit();
   for (int e = threadIdx.x; e < d; e += blockDim.x) kb[e] = p.kap[o0 + (size_t)sp * d + e];
+  const double* kpw = p.fdkp ? p.kp + (size_t)p.win[p.step] * p.n + (size_t)sp * d : nullptr;
+  if (kpw)
+    for (int e = threadIdx.x; e < d; e += blockDim.x) kpb[e] = kpw[e];
   cp_async_wait<0>();
   __syncthreads();
   for (int e = wid; e < d; e += blockDim.x >> 5) {
@@ -1027,6 +1032,36 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
     for (int t = 1; t < kFdMax; ++t)
       sD = __dadd_rn(sD, __dmul_rn(fv[t], __dmul_rn(kb[e + fo[t]], vb[(e + fo[t]) * kColTile + lane])));
     p.fdbuf[((size_t)sp * d + e) * ld + col] = sD;
+    if (kpw) {  // the photon-scale derivative's FD term, in the order of scale_deriv_apply
+      double sK = 0.0;
+#pragma unroll
+      for (int t = 0; t < kFdMax; ++t) sK += fv[t] * (kpb[e + fo[t]] * vb[(e + fo[t]) * kColTile + lane]);
+      p.fdkp[((size_t)sp * d + e) * ld + col] = sK;
+    }
+  }
+}
+
+// Record pass of the adjoint in the bin-blocked kernels: the photon-scale
+// sensitivities P (stage 1) and Q (stage 2) of one (row, column), as record()
+// computes them, with the M_off sum sM, the stage result F, the own state
+// (x in stage 1) and F(x) (stage 2).
+template <int STAGE>
+__device__ __forceinline__ void record_blocked(const StepParams& p, const StepScalars& s, int64_t r, int k,
+                                               double sM, double F, double own, double fprev) {
+  const int64_t j = p.step - p.rec_k0;
+  if (j < 0 || j >= p.rec_len) return;
+  const size_t o = (size_t)(p.step & 1) * p.n + r;
+  const size_t idx = (size_t)r * p.ld + k;
+  const size_t ro = (size_t)j * p.n * p.ld + idx;
+  const double h = s.h, ds = p.dsig[o];
+  double S = s.photohad ? sM : 0.0;
+  if (s.kap && s.pair) S += p.fdkp[idx];
+  S = S * s.dl * p.inv_scale;
+  if (STAGE == 1) {
+    p.rec_sx[idx] = S;
+    p.rec_P[ro] = p.eD[o] * h * ds * own + h * h * p.dphi1[o] * ds * F + h * p.phi1[o] * S;
+  } else {
+    p.rec_Q[ro] = h * h * p.dphi2[o] * ds * (F - fprev) + h * p.phi2[o] * (S - p.rec_sx[idx]);
   }
 }
 
@@ -1159,7 +1194,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
     __syncwarp();
     const double* rs = ring + (k % kSlabRing) * 2 * kColTile;
     if (active) {
-      double out = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
+      const double sM = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
+      double out = sM;
       if (s.kap) out = __dadd_rn(out, rs[lane]);
       if (s.decay) {
         double sL = 0.0;
@@ -1178,6 +1214,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
       }
       const double own = L.slab[L.spec[i] * kColTile + lane];
       const int ro = r * ld + col;
+      if (p.rec_P) record_blocked<STAGE>(p, s, r, col, sM, out, own, STAGE == 2 ? rs[kColTile + lane] : 0.0);
       if (STAGE == 1) {
         // a = eD x + (phi1 F(x)) h
         p.a[ro] = __dadd_rn(__dmul_rn(L.fac[i], own), __dmul_rn(__dmul_rn(L.fac[nss + i], out), s.h));
@@ -1325,6 +1362,7 @@ __global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
     out = __dmul_rn(out, s.dl);
     if (s.inj) out = __dadd_rn(out, inj_at(p, s, r, col));
     const size_t o = (size_t)(p.step & 1) * p.n + r;
+    if (p.rec_P) record_blocked<STAGE>(p, s, r, col, t, out, p.x[idx], STAGE == 2 ? p.f[idx] : 0.0);
     if (STAGE == 1) {
       p.a[idx] = __dadd_rn(__dmul_rn(p.eD[o], p.x[idx]), __dmul_rn(__dmul_rn(p.phi1[o], out), s.h));
       p.f[idx] = out;
@@ -1650,7 +1688,7 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
           &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf};
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf, &c->fdkp};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -1786,7 +1824,7 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   }
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
   if (kap) {
-    k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 1) * sizeof(double), st>>>(p);
+    k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
     ++launches;
   }
   k_slab<STAGE><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
@@ -1825,7 +1863,7 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       ++launches;
       prepared = true;
     }
-    const bool blocked = use_blocked(c, K) && !p.rec_P && !p.dsig;
+    const bool blocked = use_blocked(c, K) && (!p.rec_P || p.fdkp || !(p.flags & PB_PAIRPROD));
     for (int stage = 1; stage <= 2; ++stage) {
       p.src = stage == 1 ? X : c->A.as<double>();
       p.x = X;
@@ -2292,7 +2330,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   const size_t ssm = SlabSmem::bytes(nsp, nss, maxbin);
   const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0};
   const bool ok = ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
-                  (size_t)d * (kColTile + 1) * sizeof(double) <= max_smem &&
+                  (size_t)d * (kColTile + 2) * sizeof(double) <= max_smem &&
                   (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && ssidx.size() < ((size_t)1 << 31);
   if (!ok) return PB_OK;  // the general row kernels stay in use
   // band tiles: [species][band pair][2][RT][J][32] DMMA A fragments per window
@@ -2372,7 +2410,7 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
     if (!runs) continue;
     for (int r = -1; r < reps; ++r) {  // one untimed launch first
       PB_CUDA(c, cudaEventRecord(c->ev0, st));
-      if (kk == 0) k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 1) * sizeof(double), st>>>(p);
+      if (kk == 0) k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
       if (kk == 1) {
         if (stage == 1) k_slab<1><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
         else k_slab<2><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
@@ -2843,6 +2881,10 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
     p.dphi2 = p.dsig + 4 * n;
     p.rec_P = c->rec_P.as<double>();
     p.rec_Q = c->rec_Q.as<double>();
+    if (use_blocked(c, K) && pair) {  // the bin-blocked record pass needs D_off (kappa_pair v)
+      PB_CUDA(c, c->fdkp.ensure(sb));
+      p.fdkp = c->fdkp.as<double>();
+    }
   }
   double* lam = c->lam.as<double>();
   double* lam2 = c->lam2.as<double>();
