@@ -147,6 +147,13 @@ struct pb_context {
   std::vector<double> h_d_vals;
   bool fd_tab_ok = false;
   DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp;
+  // transposed bin-blocked structures of the adjoint sweep (one band pair)
+  bool blockedT_ok = false, fdT_ok = false;
+  DBuf bandT_slot, slabT_rp, slabT_offs, slabT_slot, bandT_vals, slabT_vals, fdT_cnt, fdT_off, fdT_val;
+  DBuf vbuf, vbuf2, bTbuf, fdTbuf;
+  int64_t slabT_nent = 0;
+  int32_t slabT_maxbin = 0;
+  size_t slabT_smem = 0, bandT_smem = 0;
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
@@ -1473,6 +1480,334 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
 }
 
 // ---------------------------------------------------------------------------
+// Bin-blocked adjoint sweep.  One backward step applies A^T twice (stage 1 to
+// v1 = Phi2 lam', stage 2 to v2 = Phi1 mu - Phi2 lam'), with
+//   A^T v = dl (M_off^T v + diag(kappa) D_off^T v + Lambda_off^T v).
+// M_off^T v splits like the forward product:
+//  * band part: for every mother species s, out_s = sum_N B_{N,s}^T v_N over
+//    the band species N -- k_bandT on DMMA with the transposed tiles; the v_N
+//    fragments stay in registers for all mother species, so no reduction
+//    across species is needed (written to bT);
+//  * bin-local part: mother rows gather from the daughters of the same bin --
+//    k_slabT with the entries in bin-major, mother-grouped order.
+// D_off^T v is k_fdT (species-major, transposed per-bin stencil).  k_slabT's
+// epilogue combines the parts and applies the stage update of the adjoint
+// step; it also writes the next v (v2 after stage 1; after stage 2, v1 of the
+// previous step when its factors are recorded).
+// ---------------------------------------------------------------------------
+constexpr int kFdTMax = 6;          // entries of a column of the FD operator's off-diagonal block
+constexpr int kSlabTRing = 3;       // rows of (band term, FD term, lam'/mu) in flight per warp
+
+struct AdjBlk {
+  int64_t n;
+  int d, nsp, ld, ncols, w, nb, spg;
+  int64_t step;
+  uint32_t flags;
+  double h, dl;
+  const double* v;          // the vector A^T is applied to (n x ld)
+  double* bT;               // n x ld: band part of M_off^T v
+  double* fdT;              // n x ld: D_off^T v
+  const double* bandT;      // [W][band_stride] transposed band tiles
+  int64_t band_stride;
+  const double* slabT;      // [W][slabT_stride] bin-local entries, mother-grouped
+  int64_t slabT_stride;
+  const int* slabT_rp;      // [d][nsp] + 1 entry ranges of the mother rows
+  const int* slabT_offs;    // byte offset of each entry's daughter in the v slab
+  int slabT_maxbin;
+  const int* fdT_cnt;       // per bin: entries of the transposed stencil, row offsets, values
+  const int* fdT_off;
+  const double* fdT_val;
+  const int* band_spec;
+  const double* rf;         // recorded eD, phi1, phi2, kappa of this step (n each)
+  const double* rf_prev;    // recorded factors of the previous step (phi2 used), or null
+  const double* lam;        // dL/dx'
+  double* mu;               // dL/da
+  double* lam_out;          // dL/dx
+  double* vout;             // stage 1: v2; stage 2: v1 of the previous step (if rf_prev)
+  const double* P;          // recorded sensitivities of this step, or null
+  const double* Q;
+  double* gs;
+  const int* inj_slot;
+  double* gb_inj;
+  const int64_t* lt_indptr; // Lambda_off^T, or null
+  const int* lt_indices;
+  const double* lt_vals;
+};
+
+// v1 = Phi2 lam' for the last step of a checkpoint segment
+__global__ void k_adj_v1(const double* __restrict__ phi2, const double* __restrict__ lam, int64_t n, int ld,
+                         int ncols, double* __restrict__ v) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int k = blockIdx.y * kColTile + (threadIdx.x & 31);
+  if (r >= n || k >= ncols) return;
+  const size_t i = (size_t)r * ld + k;
+  v[i] = phi2[r] * lam[i];
+}
+
+// fdT = D_off^T v, species-major (the block of d x 32 states in shared memory).
+__global__ void __launch_bounds__(256) k_fdT(AdjBlk q) {
+  extern __shared__ double fsm[];
+  const int sp = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int d = q.d, ld = q.ld;
+  const int col = blockIdx.y * kColTile + lane;
+  const double* __restrict__ v = q.v + (size_t)sp * d * ld + blockIdx.y * kColTile;
+  for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
+    const int e = t / (kColTile / 2), c = 2 * (t - e * (kColTile / 2));
+    cp_async16(fsm + e * kColTile + c, v + (size_t)e * ld + c);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int e = wid; e < d; e += blockDim.x >> 5) {
+    const int cnt = q.fdT_cnt[e];
+    double s = 0.0;
+    for (int t = 0; t < cnt; ++t)
+      s += q.fdT_val[e * kFdTMax + t] * fsm[(e + q.fdT_off[e * kFdTMax + t]) * kColTile + lane];
+    q.fdT[((size_t)sp * d + e) * ld + col] = s;
+  }
+}
+
+// bT = band part of M_off^T v.  CTA = (64-column block, mother-species group),
+// 8 warps; warp = one 8-column tile.  The warp loads the v fragments of both
+// band species once (k-tiles of 4 daughter bins, shifted by J - 2 so the band
+// below each mother row tile starts at 0); per mother species the CTA copies
+// its transposed tiles into shared memory (double-buffered cp.async) and the
+// warp accumulates RT row tiles of 8 mother bins and writes them out.
+template <int RT, int J>
+__global__ void __launch_bounds__(256, 1) k_bandT(AdjBlk q) {
+  extern __shared__ double sm[];
+  constexpr int KS = J - 2;              // k-tile shift
+  constexpr int KV = 2 * RT + KS;        // v fragments per band species
+  constexpr int ABLK = 2 * RT * J * 32;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int c0 = blockIdx.x * 64 + wid * 8;
+  const bool wact = c0 < q.ncols;
+  const int g = blockIdx.y;
+  const int s0 = g * q.spg, s1 = min(q.nsp, s0 + q.spg);
+  const int d = q.d, ld = q.ld;
+  const double* __restrict__ A = q.bandT + (size_t)q.w * q.band_stride;
+  double* As = sm;
+  auto issue = [&](int sp, int stage) {
+    const double* src = A + (size_t)sp * ABLK;
+    for (int c = threadIdx.x; c < ABLK / 2; c += blockDim.x) cp_async16(As + stage * ABLK + 2 * c, src + 2 * c);
+    cp_async_commit();
+  };
+  const int kr = lane & 3;
+  double vf[2][KV];
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    const bool on = wact && b < q.nb;
+    const double* vs = q.v + (size_t)(on ? q.band_spec[b] : 0) * d * ld + c0 + (lane >> 2);
+#pragma unroll
+    for (int t = 0; t < KV; ++t) {
+      const int e = 4 * (t - KS) + kr;
+      vf[b][t] = (on && e >= 0 && e < d) ? vs[(size_t)e * ld] : 0.0;
+    }
+  }
+  if (s0 < s1) issue(s0, 0);
+  for (int sp = s0; sp < s1; ++sp) {
+    const int stage = (sp - s0) & 1;
+    if (sp + 1 < s1) {
+      issue(sp + 1, stage ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double* __restrict__ as = As + stage * ABLK + lane;
+    double acc[RT][2];
+#pragma unroll
+    for (int mt = 0; mt < RT; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < J; ++jj)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int mt = 0; mt < RT; ++mt)
+          dmma884(acc[mt][0], acc[mt][1], as[((b * RT + mt) * J + jj) * 32], vf[b][2 * mt + jj]);
+    __syncthreads();
+    if (wact) {
+      double* __restrict__ out = q.bT + (size_t)sp * d * ld + c0 + kr * 2;
+#pragma unroll
+      for (int mt = 0; mt < RT; ++mt) {
+        const int row = 8 * mt + (lane >> 2);
+        if (row >= d) continue;
+        double2 o;
+        o.x = acc[mt][0];
+        o.y = acc[mt][1];
+        *reinterpret_cast<double2*>(out + (size_t)row * ld) = o;
+      }
+    }
+  }
+}
+
+template <int RT, int J>
+size_t bandT_smem_bytes() {
+  return (size_t)2 * (2 * RT * J * 32) * sizeof(double);
+}
+
+// k_slabT's shared memory: the v slab (nsp x 32), the bin's entry values, the
+// rings, then the int tables (entry daughter offsets, entry ranges).
+struct SlabTSmem {
+  double* slab;
+  double* vals;
+  double* ring;  // [warp][kSlabTRing][3][32]
+  int* offs;
+  int* rp;
+  __host__ __device__ static size_t bytes(int nsp, int maxbin) {
+    return ((size_t)nsp * kColTile + maxbin + (size_t)(kSlabThreads / 32) * kSlabTRing * 3 * kColTile) *
+               sizeof(double) +
+           ((size_t)maxbin + nsp + 1) * sizeof(int);
+  }
+  __device__ SlabTSmem(double* base, int nsp, int maxbin) {
+    slab = base;
+    vals = slab + (size_t)nsp * kColTile;
+    ring = vals + maxbin;
+    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabTRing * 3 * kColTile);
+    rp = offs + maxbin;
+  }
+};
+
+// Bin-local part of M_off^T v and the adjoint stage update for every row of
+// bin e.  CTA = (bin e, 32-column tile), lane = column; warps take the mother
+// species strided.  The row's band term, FD term and lam' (stage 1) or mu
+// (stage 2) arrive through the warp's cp.async ring.
+template <int STAGE>
+__global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
+  extern __shared__ double sm[];
+  const int nsp = q.nsp, e = blockIdx.x, d = q.d, ld = q.ld;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int col0 = blockIdx.y * kColTile, col = col0 + lane;
+  const bool active = col < q.ncols;
+  SlabTSmem L(sm, nsp, q.slabT_maxbin);
+  const int q0 = q.slabT_rp[(size_t)e * nsp], q1 = q.slabT_rp[(size_t)(e + 1) * nsp];  // multiples of 4
+  const bool photohad = (q.flags & PB_PHOTOHAD) != 0, kap = (q.flags & PB_PARTIAL_DIFF) != 0;
+  {
+    const double* vs = q.v + (size_t)e * ld + col0;
+    for (int t = threadIdx.x; t < nsp * (kColTile / 2); t += blockDim.x) {
+      const int s = t / (kColTile / 2), c = 2 * (t - s * (kColTile / 2));
+      cp_async16(L.slab + s * kColTile + c, vs + (size_t)s * d * ld + c);
+    }
+    if (photohad) {
+      const double* mv = q.slabT + (size_t)q.w * q.slabT_stride + q0;
+      for (int t = threadIdx.x; t < (q1 - q0) / 2; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
+      for (int t = threadIdx.x; t < (q1 - q0) / 4; t += blockDim.x) cp_async16(L.offs + 4 * t, q.slabT_offs + q0 + 4 * t);
+    }
+    cp_async_commit();
+  }
+  for (int i = threadIdx.x; i <= nsp; i += blockDim.x) L.rp[i] = q.slabT_rp[(size_t)e * nsp + i] - q0;
+  cp_async_wait<0>();
+  __syncthreads();
+
+  double* ring = L.ring + (size_t)wid * kSlabTRing * 3 * kColTile;
+  const double* own_src = STAGE == 1 ? q.lam : q.mu;
+  auto fetch = [&](int s, int k) {
+    if (s < nsp && lane < 24) {  // lanes 0-7 band term, 8-15 FD term, 16-23 lam' or mu; 16 bytes each
+      const int r = s * d + e;
+      const int part = lane >> 3, c2 = 4 * (lane & 7);
+      const double* src = part == 0 ? q.bT : part == 1 ? q.fdT : own_src;
+      double* dst = ring + ((k % kSlabTRing) * 3 + part) * kColTile + c2;
+      const bool need = part == 0 || (part == 1 && kap) || part == 2;
+      if (need) {
+        cp_async16(dst, src + (size_t)r * ld + col0 + c2);
+        cp_async16(dst + 2, src + (size_t)r * ld + col0 + c2 + 2);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < kSlabTRing; ++k) fetch(wid + k * nw, k);
+  const char* slb = reinterpret_cast<const char*>(L.slab + lane);
+  int k = 0;
+  for (int s = wid; s < nsp; s += nw, ++k) {
+    const int r = s * d + e;
+    double acc0 = 0.0, acc1 = 0.0;
+    if (photohad) {
+      const int j1 = L.rp[s + 1];
+      int j = L.rp[s];
+      for (; j + 1 < j1; j += 2) {
+        acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
+        acc1 = __fma_rn(L.vals[j + 1], *reinterpret_cast<const double*>(slb + L.offs[j + 1]), acc1);
+      }
+      if (j < j1) acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
+    }
+    cp_async_wait<kSlabTRing - 1>();
+    __syncwarp();
+    const double* rs = ring + (k % kSlabTRing) * 3 * kColTile;
+    if (active) {
+      double out = photohad ? (acc0 + acc1) + rs[lane] : 0.0;
+      if (kap) out += q.rf[3 * q.n + r] * rs[kColTile + lane];
+      if (q.lt_indptr) {
+        double sL = 0.0;
+        for (int64_t j = q.lt_indptr[r]; j < q.lt_indptr[r + 1]; ++j)
+          sL += q.lt_vals[j] * q.v[(size_t)q.lt_indices[j] * ld + col];
+        out += sL;
+      }
+      out *= q.dl;
+      const size_t idx = (size_t)r * ld + col;
+      const double own = rs[2 * kColTile + lane];
+      if (STAGE == 1) {
+        const double lam = own;
+        const double mu = lam + q.h * out;
+        q.mu[idx] = mu;
+        if (q.gb_inj) {
+          const int slot = q.inj_slot[r];
+          if (slot >= 0) q.gb_inj[(size_t)slot * ld + col] = q.h * q.rf[q.n + r] * mu;
+        }
+        if (q.gs) q.gs[idx] += mu * q.P[idx] + lam * q.Q[idx];
+        q.vout[idx] = q.rf[q.n + r] * mu - q.rf[2 * q.n + r] * lam;
+      } else {
+        const double lam = q.rf[r] * own + q.h * out;
+        q.lam_out[idx] = lam;
+        if (q.rf_prev) q.vout[idx] = q.rf_prev[2 * q.n + r] * lam;
+      }
+    }
+    __syncwarp();
+    fetch(s + kSlabTRing * nw, k + kSlabTRing);
+  }
+  cp_async_wait<0>();
+}
+
+using BandTKernel = void (*)(AdjBlk);
+struct BandTInstance {
+  BandTKernel fn;
+  size_t smem;
+};
+template <int RT>
+BandTInstance bandT_kernel_j(int J) {
+  switch (J) {
+    case 5: return {k_bandT<RT, 5>, bandT_smem_bytes<RT, 5>()};
+    case 9: return {k_bandT<RT, 9>, bandT_smem_bytes<RT, 9>()};
+    case 13: return {k_bandT<RT, 13>, bandT_smem_bytes<RT, 13>()};
+    case 17: return {k_bandT<RT, 17>, bandT_smem_bytes<RT, 17>()};
+  }
+  return {nullptr, 0};
+}
+BandTInstance bandT_kernel(int RT, int J) {
+  switch (RT) {
+    case 4: return bandT_kernel_j<4>(J);
+    case 8: return bandT_kernel_j<8>(J);
+    case 12: return bandT_kernel_j<12>(J);
+    case 16: return bandT_kernel_j<16>(J);
+  }
+  return {nullptr, 0};
+}
+
+// transposed copies of the band tiles and the bin-local entries of every window
+__global__ void k_transpose_blocks(const int* __restrict__ bslot, const int* __restrict__ bslotT,
+                                   const int* __restrict__ sslot, const int* __restrict__ sslotT, int64_t R, int W,
+                                   const double* __restrict__ band, double* __restrict__ bandT, int64_t bstride,
+                                   const double* __restrict__ slab, double* __restrict__ slabT, int64_t sstride) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= R) return;
+  const int b = bslot[j], bt = bslotT[j], s = sslot[j], st = sslotT[j];
+  for (int w = 0; w < W; ++w) {
+    if (b >= 0 && bt >= 0) bandT[(size_t)w * bstride + bt] = band[(size_t)w * bstride + b];
+    if (s >= 0 && st >= 0) slabT[(size_t)w * sstride + st] = slab[(size_t)w * sstride + s];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Discrete adjoint of the ETD2 step.  Forward, with A = dl (M_off + D_off diag(kappa)
 // + Lambda_off) frozen over the step:
 //   a = E x + h Phi1 (A x + b),   x' = a + h Phi2 A (a - x).
@@ -1688,7 +2023,9 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
           &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf, &c->fdkp};
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf, &c->fdkp,
+          &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->bandT_vals, &c->slabT_vals,
+          &c->fdT_cnt, &c->fdT_off, &c->fdT_val, &c->vbuf, &c->vbuf2, &c->bTbuf, &c->fdTbuf};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -1839,6 +2176,30 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
     ++launches;
   }
   return launches;
+}
+
+// One stage of the bin-blocked adjoint sweep: k_bandT on the second stream,
+// k_fdT on the launching stream, then k_slabT.
+template <int STAGE>
+void launch_adj_blocked(pb_context* c, AdjBlk& q, cudaStream_t st) {
+  const bool photohad = (q.flags & PB_PHOTOHAD) != 0, kap = (q.flags & PB_PARTIAL_DIFF) != 0;
+  const unsigned tiles = (unsigned)blocks_for(q.ncols, kColTile);
+  bool forked = false;
+  if (photohad && q.nb > 0) {
+    const int cblocks = (int)blocks_for(q.ncols, 64);
+    const int G = std::max(1, std::min({(c->num_sms + cblocks - 1) / cblocks, kMaxBandGroups, q.nsp}));
+    q.spg = (q.nsp + G - 1) / G;
+    const int ngroups = (q.nsp + q.spg - 1) / q.spg;
+    cudaEventRecord(c->ev_fork, st);
+    cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+    const BandTInstance bi = bandT_kernel(c->band_RT, c->band_J);
+    bi.fn<<<dim3(cblocks, ngroups), 256, bi.smem, c->stream2>>>(q);
+    cudaEventRecord(c->ev_join, c->stream2);
+    forked = true;
+  }
+  if (kap) k_fdT<<<dim3(q.nsp, tiles), 256, (size_t)q.d * kColTile * sizeof(double), st>>>(q);
+  if (forked) cudaStreamWaitEvent(st, c->ev_join, 0);
+  k_slabT<STAGE><<<dim3(q.d, tiles), kSlabThreads, c->slabT_smem, st>>>(q);
 }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
@@ -2096,6 +2457,7 @@ int pb_set_photon_field(pb_context* c, int32_t n_comp, const int32_t* kinds, con
 // itself.  Sets fd_tab_ok.
 static int build_fd_table(pb_context* c) {
   c->fd_tab_ok = false;
+  c->fdT_ok = false;
   const int d = c->lay_d;
   if (!c->have_fd || d <= 0 || c->h_d_indptr.size() != (size_t)c->n + 1) return PB_OK;
   const int nsp = (int)(c->n / d);
@@ -2120,12 +2482,30 @@ static int build_fd_table(pb_context* c) {
           return PB_OK;
     }
   }
+  // the transposed stencil: column e of the block receives from rows e + off
+  std::vector<int32_t> tcnt(d, 0), toff((size_t)d * kFdTMax, 0);
+  std::vector<double> tval((size_t)d * kFdTMax, 0.0);
+  bool t_ok = true;
+  for (int e = 0; e < d; ++e)      // row e, in row order, so each column's list is in row order
+    for (int t = 0; t < cnt[e]; ++t) {
+      const int cidx = e + off[(size_t)e * kFdMax + t];
+      if (tcnt[cidx] >= kFdTMax) { t_ok = false; continue; }
+      toff[(size_t)cidx * kFdTMax + tcnt[cidx]] = e - cidx;
+      tval[(size_t)cidx * kFdTMax + tcnt[cidx]] = val[(size_t)e * kFdMax + t];
+      ++tcnt[cidx];
+    }
   int rc;
   if ((rc = upload(c, c->fd_cnt, cnt.data(), cnt.size()))) return rc;
   if ((rc = upload(c, c->fd_off, off.data(), off.size()))) return rc;
   if ((rc = upload(c, c->fd_val, val.data(), val.size()))) return rc;
+  if (t_ok) {
+    if ((rc = upload(c, c->fdT_cnt, tcnt.data(), tcnt.size()))) return rc;
+    if ((rc = upload(c, c->fdT_off, toff.data(), toff.size()))) return rc;
+    if ((rc = upload(c, c->fdT_val, tval.data(), tval.size()))) return rc;
+  }
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->fd_tab_ok = true;
+  c->fdT_ok = t_ok;
   return PB_OK;
 }
 
@@ -2371,6 +2751,64 @@ int pb_set_layout(pb_context* c, int32_t d) {
   c->band_nnz = band_nnz;
   c->slab_nnz = slab_nnz;
   c->blocked_ok = true;
+  // ---- transposed structures of the adjoint sweep (at most one band pair)
+  c->blockedT_ok = false;
+  if (npairs > 1) return PB_OK;
+  std::vector<int32_t> btslot((size_t)std::max<int64_t>(R, 1), -1);
+  for (int b = 0; b < nb; ++b)
+    for (int e = 0; e < d; ++e) {
+      const int64_t r = (int64_t)bspec[b] * d + e;
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+        if (ix[j] == r) continue;
+        const int sp = ix[j] / d, e2 = ix[j] % d;   // mother species and bin
+        const int mt = e2 / 8, jj = e / 4 - 2 * mt + (J - 2);
+        if (jj < 0 || jj >= J) return PB_OK;
+        const size_t tile = ((size_t)sp * 2 + b) * RT + mt;
+        btslot[j] = (int32_t)((tile * J + jj) * 32 + (e2 % 8) * 4 + (e % 4));
+      }
+    }
+  // bin-local entries grouped by mother: (bin, mother species, daughter order)
+  std::vector<std::vector<std::pair<int32_t, int64_t>>> bym(nsp);
+  std::vector<int32_t> trp((size_t)d * nsp + 1, 0), toffs, tslot((size_t)std::max<int64_t>(R, 1), -1);
+  int32_t tmax = 0;
+  for (int e = 0; e < d; ++e) {
+    for (auto& v : bym) v.clear();
+    for (int i = 0; i < nss; ++i) {
+      const int64_t r = (int64_t)sspec[i] * d + e;
+      for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
+        if (ix[j] != r) bym[ix[j] / d].push_back({sspec[i], j});
+    }
+    while (toffs.size() % 4) toffs.push_back(0);
+    const size_t b0 = toffs.size();
+    for (int m = 0; m < nsp; ++m) {
+      trp[(size_t)e * nsp + m] = (int32_t)toffs.size();
+      for (auto& pr : bym[m]) {
+        tslot[pr.second] = (int32_t)toffs.size();
+        toffs.push_back(pr.first * kColTile * (int32_t)sizeof(double));  // byte offset in the v slab
+      }
+    }
+    size_t b1 = (toffs.size() + 3) & ~(size_t)3;
+    tmax = std::max<int32_t>(tmax, (int32_t)(b1 - b0));
+  }
+  while (toffs.size() % 4) toffs.push_back(0);
+  trp[(size_t)d * nsp] = (int32_t)toffs.size();
+  if (toffs.empty()) toffs.assign(4, 0);
+  const size_t tsm = SlabTSmem::bytes(nsp, tmax);
+  const BandTInstance bti = bandT_kernel(RT, J);
+  if (tsm > max_smem || !bti.fn || bti.smem > max_smem || (size_t)d * kColTile * sizeof(double) > max_smem) return PB_OK;
+  if ((rc = upload(c, c->bandT_slot, btslot.data(), btslot.size()))) return rc;
+  if ((rc = upload(c, c->slabT_rp, trp.data(), trp.size()))) return rc;
+  if ((rc = upload(c, c->slabT_offs, toffs.data(), toffs.size()))) return rc;
+  if ((rc = upload(c, c->slabT_slot, tslot.data(), tslot.size()))) return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slabT<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+  PB_CUDA(c, cudaFuncSetAttribute(k_slabT<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+  PB_CUDA(c, cudaFuncSetAttribute(bti.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bti.smem));
+  c->slabT_nent = (int64_t)toffs.size();
+  c->slabT_maxbin = tmax;
+  c->slabT_smem = tsm;
+  c->bandT_smem = bti.smem;
+  c->blockedT_ok = true;
   return PB_OK;
 }
 
@@ -2889,6 +3327,26 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   double* lam = c->lam.as<double>();
   double* lam2 = c->lam2.as<double>();
   const int64_t nseg = (S + CK - 1) / CK;
+  const int W = a->n_windows;
+  // the bin-blocked sweep needs the transposed structures, one band pair and the FD table
+  const bool blockedT = c->blockedT_ok && c->fdT_ok && use_blocked(c, K) && c->last_W == W;
+  if (blockedT) {
+    PB_CUDA(c, c->vbuf.ensure(sb));
+    PB_CUDA(c, c->vbuf2.ensure(sb));
+    PB_CUDA(c, c->bTbuf.ensure(sb));
+    PB_CUDA(c, c->fdTbuf.ensure(sb));
+    PB_CUDA(c, c->bandT_vals.ensure((size_t)W * std::max<int64_t>(c->band_stride, 1) * sizeof(double)));
+    PB_CUDA(c, c->slabT_vals.ensure((size_t)W * std::max<int64_t>(c->slabT_nent, 1) * sizeof(double)));
+    PB_CUDA(c, cudaMemsetAsync(c->bandT_vals.p, 0, (size_t)W * c->band_stride * sizeof(double), st));
+    PB_CUDA(c, cudaMemsetAsync(c->slabT_vals.p, 0, (size_t)W * c->slabT_nent * sizeof(double), st));
+    PB_CUDA(c, cudaMemsetAsync(c->bTbuf.p, 0, sb, st));
+    if (R > 0)
+      k_transpose_blocks<<<blocks_for(R, 256), 256, 0, st>>>(
+          c->band_slot.as<int>(), c->bandT_slot.as<int>(), c->slab_slot.as<int>(), c->slabT_slot.as<int>(), R, W,
+          c->band_vals.as<double>(), c->bandT_vals.as<double>(), c->band_stride, c->slab_vals.as<double>(),
+          c->slabT_vals.as<double>(), c->slab_nent);
+    PB_CUDA(c, cudaGetLastError());
+  }
   for (int64_t sg = nseg - 1; sg >= 0; --sg) {
     const int64_t k0 = sg * CK, k1 = std::min<int64_t>(S, k0 + CK);
     int64_t kf = k0;
@@ -2899,6 +3357,68 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
     p.rec_len = (int)(k1 - k0);
     PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max<size_t>(c->h_long_rows.size(), 1) * ctiles * sizeof(int), st));
     launch_steps(c, p, K, a->n_active, k0, k1, st, nullptr, 0);
+    if (blockedT) {
+      for (int64_t k = k1 - 1; k >= kf; --k) {
+        const size_t j = (size_t)(k - k0);
+        AdjBlk q;
+        memset(&q, 0, sizeof(q));
+        q.n = n;
+        q.d = c->lay_d;
+        q.nsp = c->lay_nsp;
+        q.ld = ld;
+        q.ncols = a->n_active[k];
+        q.w = a->window[k];
+        q.nb = c->band_nb;
+        q.step = k;
+        q.flags = p.flags;
+        q.h = a->h[k];
+        q.dl = a->dldz[k];
+        q.bT = c->bTbuf.as<double>();
+        q.fdT = c->fdTbuf.as<double>();
+        q.bandT = c->bandT_vals.as<double>();
+        q.band_stride = c->band_stride;
+        q.slabT = c->slabT_vals.as<double>();
+        q.slabT_stride = c->slabT_nent;
+        q.slabT_rp = c->slabT_rp.as<int>();
+        q.slabT_offs = c->slabT_offs.as<int>();
+        q.slabT_maxbin = c->slabT_maxbin;
+        q.fdT_cnt = c->fdT_cnt.as<int>();
+        q.fdT_off = c->fdT_off.as<int>();
+        q.fdT_val = c->fdT_val.as<double>();
+        q.band_spec = c->band_spec.as<int>();
+        q.rf = c->rec_rf.as<double>() + j * 4 * n;
+        q.rf_prev = j >= 1 ? c->rec_rf.as<double>() + (j - 1) * 4 * n : nullptr;
+        q.mu = c->mu.as<double>();
+        if ((flags & PB_DECAY) && c->have_decay) {
+          q.lt_indptr = c->lt_indptr.as<int64_t>();
+          q.lt_indices = c->lt_indices.as<int>();
+          q.lt_vals = c->lt_vals.as<double>();
+        }
+        if (want_scale) {
+          q.P = c->rec_P.as<double>() + j * n * ld;
+          q.Q = c->rec_Q.as<double>() + j * n * ld;
+          q.gs = c->gs.as<double>();
+        }
+        if (want_inj) {
+          q.inj_slot = c->inj_slot.as<int>();
+          q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
+        }
+        if (k == k1 - 1)  // v1 of the segment's last step; later steps get it from stage 2
+          k_adj_v1<<<dim3(blocks_for(n, 8), blocks_for(q.ncols, kColTile)), 256, 0, st>>>(
+              q.rf + 2 * n, lam, n, ld, q.ncols, c->vbuf.as<double>());
+        q.v = c->vbuf.as<double>();
+        q.lam = lam;
+        q.vout = c->vbuf2.as<double>();
+        launch_adj_blocked<1>(c, q, st);
+        q.v = c->vbuf2.as<double>();
+        q.vout = c->vbuf.as<double>();
+        q.lam_out = lam2;
+        launch_adj_blocked<2>(c, q, st);
+        std::swap(lam, lam2);
+      }
+      PB_CUDA(c, cudaGetLastError());
+      continue;
+    }
     for (int64_t k = k1 - 1; k >= kf; --k) {
       AdjParams q;
       memset(&q, 0, sizeof(q));

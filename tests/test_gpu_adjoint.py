@@ -180,3 +180,35 @@ def test_adjoint_against_oracle_differences(light):
             assert abs(g - fd) / abs(fd) < TOL, (key, k, g, fd)
     fd = _central(lambda st: oracle_loss(p, 1.0 + st), 1e-5)
     assert abs(float(scale.grad) - fd) / abs(fd) < TOL, (float(scale.grad), fd)
+
+
+def test_blocked_and_row_kernel_adjoints_agree():
+    """The bin-blocked record pass and transposed sweep against the row kernels:
+    37 columns (a partial column tile) of the 60-species network, with the
+    photon scale, switching on at different redshifts."""
+    from prince_b200 import _lib
+    from workloads import network_run
+    run = network_run(max_mass=16, n_species=60, seed=5)
+    species = [2212, 1000020040, 1000070140]
+    K = 37
+    rng = np.random.default_rng(3)
+    sb = AD.SourceBatch(run, species, z_max=list(rng.uniform(0.05, 0.2, K)), initial_z=0.2)
+    plan = sb.plan(0.2, ckpt_every=16)
+    ctx = plan.dev.ctx
+    assert ctx.info(_lib.PB_INFO_BLOCKED_LAYOUT) == 1
+    seed = torch.tensor(rng.uniform(0.5, 1.5, (run.dim_states, K)))
+    grads = []
+    for mode in (0, 1):
+        ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, mode)
+        try:
+            t = _tensors(_params(K, 8, len(species)))
+            scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+            X = _forward(sb, plan, t, scale)
+            assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == mode
+            (seed * X).sum().backward()
+            grads.append([t[k].grad.numpy().copy() for k in ("gamma", "lg_rmax", "frac", "m")] + [float(scale.grad)])
+        finally:
+            ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, 1)
+    for g0, g1 in zip(grads[0], grads[1]):
+        g0, g1 = np.asarray(g0), np.asarray(g1)
+        np.testing.assert_allclose(g1, g0, rtol=1e-9, atol=1e-12 * np.abs(g0).max())
