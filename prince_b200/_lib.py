@@ -49,6 +49,7 @@ class SolveArgs(C.Structure):
         ("init_state", C.c_int32),
         ("state_on_device", C.c_int32),
         ("ckpt_every", C.c_int32),
+        ("out_cols", _i32),
     ]
 
 
@@ -246,9 +247,10 @@ class Context:
 
     # -- solve ----------------------------------------------------------
     def solve(self, sched, flags, n_cols, coeff, n_active, state, photon_scale=1.0, init_state=False,
-              state_ptr=None):
+              state_ptr=None, out_cols=None):
         """Run one solve.  ``state`` is an (n, K) float64 host array (in/out)
-        unless ``state_ptr`` (a device pointer) is given."""
+        unless ``state_ptr`` (a device pointer) is given.  ``out_cols`` (solve
+        column -> output column) orders the returned columns."""
         keep = []
 
         def f(a):
@@ -283,6 +285,8 @@ class Context:
             args.state = _ptr(state, C.c_double)
             args.state_on_device = 0
         args.init_state = 1 if init_state else 0
+        if out_cols is not None:
+            args.out_cols = i(out_cols)
         self._check(self.lib.pb_solve(self.h, C.byref(args)), "pb_solve")
 
     def operator_pattern(self, n):

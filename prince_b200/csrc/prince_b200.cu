@@ -40,7 +40,7 @@
 
 namespace {
 
-constexpr int kAbiVersion = 1;
+constexpr int kAbiVersion = 2;
 constexpr int kLongRow = 256;      // rows with more coupling entries are cut into segments
 constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
 constexpr int kColTile = 32;       // state columns per warp in the batched step
@@ -150,7 +150,7 @@ struct pb_context {
   // transposed bin-blocked structures of the adjoint sweep (one band pair)
   bool blockedT_ok = false, fdT_ok = false;
   DBuf bandT_slot, slabT_rp, slabT_offs, slabT_slot, bandT_vals, slabT_vals, fdT_cnt, fdT_off, fdT_val;
-  DBuf vbuf, vbuf2, bTbuf, fdTbuf;
+  DBuf vbuf, vbuf2, bTbuf, fdTbuf, outcols;
   int64_t slabT_nent = 0;
   int32_t slabT_maxbin = 0;
   size_t slabT_smem = 0, bandT_smem = 0;
@@ -1534,6 +1534,15 @@ struct AdjBlk {
   const double* lt_vals;
 };
 
+// Y[r][cols[j]] = X[r][j]: the final states in the caller's column order (Y is n x K)
+__global__ void k_gather_cols(const double* __restrict__ X, int ld, int64_t n, int K, const int* __restrict__ cols,
+                              double* __restrict__ Y) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int j = blockIdx.y * kColTile + (threadIdx.x & 31);
+  if (r >= n || j >= K) return;
+  Y[(size_t)r * K + cols[j]] = X[(size_t)r * ld + j];
+}
+
 // v1 = Phi2 lam' for the last step of a checkpoint segment
 __global__ void k_adj_v1(const double* __restrict__ phi2, const double* __restrict__ lam, int64_t n, int ld,
                          int ncols, double* __restrict__ v) {
@@ -2025,7 +2034,7 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf, &c->fdkp,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->bandT_vals, &c->slabT_vals,
-          &c->fdT_cnt, &c->fdT_off, &c->fdT_val, &c->vbuf, &c->vbuf2, &c->bTbuf, &c->fdTbuf};
+          &c->fdT_cnt, &c->fdT_off, &c->fdT_val, &c->vbuf, &c->vbuf2, &c->bTbuf, &c->fdTbuf, &c->outcols};
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -3047,6 +3056,9 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->partial.ensure((size_t)std::max(c->n_seg, 1) * ld * sizeof(double)));
   PB_CUDA(c, c->counter.ensure((size_t)std::max(nlong_rows, 1) * ctiles * sizeof(int)));
   if (a->ckpt_every < 0) return fail(c, PB_ERR_ARG, "pb_solve: ckpt_every must be >= 0");
+  if (a->out_cols)
+    for (int j = 0; j < K; ++j)
+      if (a->out_cols[j] < 0 || a->out_cols[j] >= K) return fail(c, PB_ERR_ARG, "pb_solve: out_cols[%d] out of range", j);
   if (a->ckpt_every > 0)
     PB_CUDA(c, c->ckpt.ensure((size_t)((S + a->ckpt_every - 1) / a->ckpt_every + 1) * n * ld * sizeof(double)));
   const bool blocked = use_blocked(c, K);
@@ -3206,12 +3218,16 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, cudaEventRecord(c->ev3, st));
     launches = c->graph_launches;
   }
-  if (a->state_on_device) {
-    PB_CUDA(c, cudaMemcpy2DAsync(a->state, K * sizeof(double), X, ld * sizeof(double), K * sizeof(double), n,
-                                 cudaMemcpyDeviceToDevice, st));
+  const cudaMemcpyKind out_kind = a->state_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (a->out_cols && K > 1) {  // columns in the caller's order, gathered on the device, then one copy
+    if ((rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
+    double* Y = c->F.as<double>();  // F(x) scratch of the steps, n x ld >= n x K
+    k_gather_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(X, ld, n, K, c->outcols.as<int>(), Y);
+    PB_CUDA(c, cudaGetLastError());
+    PB_CUDA(c, cudaMemcpyAsync(a->state, Y, (size_t)n * K * sizeof(double), out_kind, st));
   } else {
     PB_CUDA(c, cudaMemcpy2DAsync(a->state, K * sizeof(double), X, ld * sizeof(double), K * sizeof(double), n,
-                                 cudaMemcpyDeviceToHost, st));
+                                 out_kind, st));
   }
   PB_CUDA(c, cudaEventRecord(c->ev1, st));
   PB_CUDA(c, cudaStreamSynchronize(st));

@@ -413,10 +413,9 @@ class UHECRPropagationSolverETD2:
         ctx.set_photon_field(device_components(self.prince_run.photon_field))
         if flags & _lib.PB_EM_CASCADE:
             ctx.set_em_windows(*self._em_windows(sched, dz))
-        out = np.zeros((self.dim_states, K))
-        ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, out, photon_scale=self._photon_scale())
-        state = np.empty_like(out)
-        state[:, perm] = out
+        state = np.empty((self.dim_states, K))
+        ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, state, photon_scale=self._photon_scale(),
+                  out_cols=perm)
         self.last_timing = ctx.last_timing()
         self._store(state)
         self.result = None

@@ -29,7 +29,7 @@ def test_library_exports_every_header_symbol():
     for name in syms:
         assert hasattr(lib, name), name
     assert set(syms) == set(_lib.exported_symbols())
-    assert lib.pb_abi_version() == 1
+    assert lib.pb_abi_version() == 2
 
 
 def test_context_without_gpu_raises_cleanly():
