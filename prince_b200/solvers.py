@@ -379,26 +379,32 @@ class UHECRPropagationSolverETD2:
         owner = np.array([k for k, c in enumerate(cols) for _ in c], dtype=np.int64)
         zs = zg[:-1]
         coeff = _coefficients(srcs, zs) if srcs else np.zeros((zs.size, 0))
-        grids = np.array([s.injection_grid for s in srcs]) if srcs else np.zeros((0, self.dim_states))
+        grids = [np.asarray(s.injection_grid, dtype=np.float64) for s in srcs]
         use_inj = self.enable_injection_jacobian and len(srcs) > 0
         # first step at which each column receives a non-zero injection
         first = np.full(K, sched.n_steps, dtype=np.int64)
         if use_inj:
-            live = (coeff != 0.0) & np.any(grids != 0.0, axis=1)[None, :]
-            for k in range(K):
-                sel = owner == k
-                if np.any(sel):
-                    hit = np.flatnonzero(np.any(live[:, sel], axis=1))
-                    if hit.size:
-                        first[k] = hit[0]
+            injects = np.array([bool(np.any(g)) for g in grids])
+            live = (coeff != 0.0) & injects[None, :]
+            has = live.any(axis=0)
+            first_src = np.where(has, live.argmax(axis=0), sched.n_steps)
+            np.minimum.at(first, owner, first_src)
         perm = np.argsort(first, kind="stable")          # device column j <- user column perm[j]
         inv = np.empty(K, dtype=np.int64)
         inv[perm] = np.arange(K)
         n_active = np.searchsorted(np.sort(first), np.arange(sched.n_steps), side="right").astype(np.int32)
         src_order = np.argsort(inv[owner], kind="stable") if srcs else np.zeros(0, dtype=np.int64)
         src_col = inv[owner][src_order].astype(np.int32)
-        rows = np.flatnonzero(np.any(grids != 0.0, axis=0)).astype(np.int32) if srcs else np.zeros(0, np.int32)
-        G = np.ascontiguousarray(grids[src_order][:, rows].T) if srcs else np.zeros((0, 0))
+        if srcs:
+            nz = np.zeros(self.dim_states, dtype=bool)
+            for g in grids:
+                nz |= g != 0.0
+            rows = np.flatnonzero(nz).astype(np.int32)
+            G = np.empty((rows.size, len(srcs)))
+            for i, si in enumerate(src_order):
+                G[:, i] = grids[si][rows]
+        else:
+            rows, G = np.zeros(0, np.int32), np.zeros((0, 0))
         return sched, K, coeff[:, src_order] if srcs else coeff, rows, G, src_col, n_active, perm, use_inj
 
     def solve(self, dz=1e-3, verbose=False, summary=False, progressbar=False):
