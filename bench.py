@@ -107,7 +107,9 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def _dist():
+def _dist(backend=None):
+    """(dist, rank, world size, local rank) under torchrun; (None, 0, 1, 0) alone.
+    The backend is NCCL on GPUs (gloo for host-side tests)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws <= 1:
         return None, 0, 1, 0
@@ -115,29 +117,34 @@ def _dist():
     import torch.distributed as dist
     from datetime import timedelta
 
+    backend = backend or os.environ.get("PB_DIST_BACKEND", "nccl")
     rank = int(os.environ["RANK"])
     local = int(os.environ.get("LOCAL_RANK", rank))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group(backend, timeout=timedelta(seconds=60))
     return dist, rank, ws, local
 
 
 def _max_over_ranks(dist, local, vals):
+    """Element-wise maximum over ranks (the device times of the slowest rank)."""
     if dist is None:
         return vals
     import torch
 
-    t = torch.tensor(vals, dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return t.tolist()
 
 
-def step_bytes(n, nnz_m, n_inj, n_act):
-    """Algorithmic HBM bytes of one ETD2 step (both stages) with n_act columns:
-    state traffic 48 n K (read x, write a and F(x); read a and F(x), write x),
-    the operator twice (8 B value + 4 B column per entry, 4 B row pointer),
-    8 per-row FP64 vectors and the injection rows read in both stages."""
-    return 48.0 * n * n_act + 2 * (12.0 * nnz_m + 4.0 * (n + 1)) + 8.0 * n * 8 + 16.0 * n_inj * n_act
+def rank_points(run, points, rank, z_range):
+    """The source points of one rank: every rank propagates its own seeded batch."""
+    from workloads import draw_points
+
+    return draw_points(run, points, seed=1000 + rank, z_range=z_range)
 
 
 def run_b200(args, dist, rank, ws, local):
@@ -147,7 +154,7 @@ def run_b200(args, dist, rank, ws, local):
 
     torch.cuda.set_device(local)
     run = network_run()
-    pts = draw_points(run, args.points, seed=1000 + rank, z_range=args.z_range)
+    pts = rank_points(run, args.points, rank, args.z_range)
     zi = max(p["zmax"] for p in pts)
     solver = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=args.points, device=local)
     for k, p in enumerate(pts):
