@@ -140,6 +140,14 @@ def _max_over_ranks(dist, local, vals):
     return t.tolist()
 
 
+def step_bytes(n, nnz_m, n_inj, n_act):
+    """Algorithmic HBM bytes of one ETD2 step (both stages) with n_act columns:
+    state traffic 48 n K (read x, write a and F(x); read a and F(x), write x),
+    the operator twice (8 B value + 4 B column per entry, 4 B row pointer),
+    8 per-row FP64 vectors and the injection rows read in both stages."""
+    return 48.0 * n * n_act + 2 * (12.0 * nnz_m + 4.0 * (n + 1)) + 8.0 * n * 8 + 16.0 * n_inj * n_act
+
+
 def rank_points(run, points, rank, z_range):
     """The source points of one rank: every rank propagates its own seeded batch."""
     from workloads import draw_points
