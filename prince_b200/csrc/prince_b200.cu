@@ -1496,7 +1496,8 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
 // previous step when its factors are recorded).
 // ---------------------------------------------------------------------------
 constexpr int kFdTMax = 6;          // entries of a column of the FD operator's off-diagonal block
-constexpr int kSlabTRing = 3;       // rows of (band term, FD term, lam'/mu) in flight per warp
+constexpr int kSlabTRing = 3;       // rows of (band term, FD term, lam'/mu, P, Q) in flight per warp
+constexpr int kSlabTParts = 5;
 
 struct AdjBlk {
   int64_t n;
@@ -1526,7 +1527,7 @@ struct AdjBlk {
   double* vout;             // stage 1: v2; stage 2: v1 of the previous step (if rf_prev)
   const double* P;          // recorded sensitivities of this step, or null
   const double* Q;
-  double* gs;
+  double* gs;               // d x ld: photon-scale gradient, summed over the rows of each bin
   const int* inj_slot;
   double* gb_inj;
   const int64_t* lt_indptr; // Lambda_off^T, or null
@@ -1664,7 +1665,7 @@ struct SlabTSmem {
   int* offs;
   int* rp;
   __host__ __device__ static size_t bytes(int nsp, int maxbin) {
-    return ((size_t)nsp * kColTile + maxbin + (size_t)(kSlabThreads / 32) * kSlabTRing * 3 * kColTile) *
+    return ((size_t)nsp * kColTile + maxbin + (size_t)(kSlabThreads / 32) * kSlabTRing * kSlabTParts * kColTile) *
                sizeof(double) +
            ((size_t)maxbin + nsp + 1) * sizeof(int);
   }
@@ -1672,7 +1673,7 @@ struct SlabTSmem {
     slab = base;
     vals = slab + (size_t)nsp * kColTile;
     ring = vals + maxbin;
-    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabTRing * 3 * kColTile);
+    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabTRing * kSlabTParts * kColTile);
     rp = offs + maxbin;
   }
 };
@@ -1708,22 +1709,29 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
   cp_async_wait<0>();
   __syncthreads();
 
-  double* ring = L.ring + (size_t)wid * kSlabTRing * 3 * kColTile;
+  double* ring = L.ring + (size_t)wid * kSlabTRing * kSlabTParts * kColTile;
   const double* own_src = STAGE == 1 ? q.lam : q.mu;
+  const bool want_pq = STAGE == 1 && q.gs;
+  // lanes 0-7 band term (and Q), 8-15 FD term, 16-23 lam' or mu, 24-31 P; 2 x 16 bytes each
+  auto copy_part = [&](int r, int k, int part, const double* src, int c2) {
+    double* dst = ring + ((k % kSlabTRing) * kSlabTParts + part) * kColTile + c2;
+    const size_t o = (size_t)r * ld + col0 + c2;
+    cp_async16(dst, src + o);
+    cp_async16(dst + 2, src + o + 2);
+  };
   auto fetch = [&](int s, int k) {
-    if (s < nsp && lane < 24) {  // lanes 0-7 band term, 8-15 FD term, 16-23 lam' or mu; 16 bytes each
+    if (s < nsp) {
       const int r = s * d + e;
       const int part = lane >> 3, c2 = 4 * (lane & 7);
-      const double* src = part == 0 ? q.bT : part == 1 ? q.fdT : own_src;
-      double* dst = ring + ((k % kSlabTRing) * 3 + part) * kColTile + c2;
-      const bool need = part == 0 || (part == 1 && kap) || part == 2;
-      if (need) {
-        cp_async16(dst, src + (size_t)r * ld + col0 + c2);
-        cp_async16(dst + 2, src + (size_t)r * ld + col0 + c2 + 2);
-      }
+      if (part == 0) copy_part(r, k, 0, q.bT, c2);
+      if (part == 1 && kap) copy_part(r, k, 1, q.fdT, c2);
+      if (part == 2) copy_part(r, k, 2, own_src, c2);
+      if (part == 3 && want_pq) copy_part(r, k, 3, q.P, c2);
+      if (part == 0 && want_pq) copy_part(r, k, 4, q.Q, c2);
     }
     cp_async_commit();
   };
+  double gsa = 0.0;  // this lane's column of the photon-scale gradient over the warp's rows
 #pragma unroll
   for (int k = 0; k < kSlabTRing; ++k) fetch(wid + k * nw, k);
   const char* slb = reinterpret_cast<const char*>(L.slab + lane);
@@ -1742,7 +1750,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
     }
     cp_async_wait<kSlabTRing - 1>();
     __syncwarp();
-    const double* rs = ring + (k % kSlabTRing) * 3 * kColTile;
+    const double* rs = ring + (k % kSlabTRing) * kSlabTParts * kColTile;
     if (active) {
       double out = photohad ? (acc0 + acc1) + rs[lane] : 0.0;
       if (kap) out += q.rf[3 * q.n + r] * rs[kColTile + lane];
@@ -1763,7 +1771,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
           const int slot = q.inj_slot[r];
           if (slot >= 0) q.gb_inj[(size_t)slot * ld + col] = q.h * q.rf[q.n + r] * mu;
         }
-        if (q.gs) q.gs[idx] += mu * q.P[idx] + lam * q.Q[idx];
+        if (want_pq) gsa += mu * rs[3 * kColTile + lane] + lam * rs[4 * kColTile + lane];
         q.vout[idx] = q.rf[q.n + r] * mu - q.rf[2 * q.n + r] * lam;
       } else {
         const double lam = q.rf[r] * own + q.h * out;
@@ -1775,6 +1783,17 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
     fetch(s + kSlabTRing * nw, k + kSlabTRing);
   }
   cp_async_wait<0>();
+  if (want_pq) {  // the warps' sums for each column, added to the bin's row of gs
+    __syncthreads();
+    double* red = L.slab;  // the slab is no longer read
+    red[wid * kColTile + lane] = gsa;
+    __syncthreads();
+    if (threadIdx.x < kColTile && col0 + (int)threadIdx.x < q.ncols) {
+      double t = 0.0;
+      for (int w = 0; w < nw; ++w) t += red[w * kColTile + threadIdx.x];
+      q.gs[(size_t)e * ld + col0 + threadIdx.x] += t;
+    }
+  }
 }
 
 using BandTKernel = void (*)(AdjBlk);
@@ -3503,7 +3522,8 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   }
   if (want_scale) {
     PB_CUDA(c, c->g_out.ensure((size_t)std::max(K, 1) * sizeof(double) + 8));
-    k_grad_scale<<<blocks_for(K, 128), 128, 0, st>>>(c->gs.as<double>(), n, ld, K, c->g_out.as<double>());
+    k_grad_scale<<<blocks_for(K, 128), 128, 0, st>>>(c->gs.as<double>(), blockedT ? (int64_t)c->lay_d : n, ld, K,
+                                                       c->g_out.as<double>());
     PB_CUDA(c, cudaMemcpyAsync(grad_scale, c->g_out.p, (size_t)K * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   PB_CUDA(c, cudaGetLastError());
