@@ -1072,6 +1072,48 @@ __device__ __forceinline__ void record_blocked(const StepParams& p, const StepSc
   }
 }
 
+// The record inputs of one (row, column), loaded before the row's sum so
+// their latency overlaps it: the scale derivatives, the step factors, the FD
+// term with kappa_pair and (stage 2) the stage-1 S x.
+struct RecIn {
+  double ds, d12, f0, f1, kp, sx;
+  bool on;
+};
+template <int STAGE>
+__device__ __forceinline__ RecIn rec_load(const StepParams& p, const StepScalars& s, int64_t r, int k) {
+  RecIn in{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
+  const int64_t j = p.step - p.rec_k0;
+  if (j < 0 || j >= p.rec_len) return in;
+  const size_t o = (size_t)(p.step & 1) * p.n + r;
+  const size_t idx = (size_t)r * p.ld + k;
+  in.on = true;
+  in.ds = p.dsig[o];
+  in.d12 = STAGE == 1 ? p.dphi1[o] : p.dphi2[o];
+  in.f0 = STAGE == 1 ? p.eD[o] : p.phi2[o];
+  in.f1 = p.phi1[o];
+  if (s.kap && s.pair) in.kp = p.fdkp[idx];
+  if (STAGE == 2) in.sx = p.rec_sx[idx];
+  return in;
+}
+// record_blocked with preloaded inputs (same arithmetic)
+template <int STAGE>
+__device__ __forceinline__ void record_pre(const StepParams& p, const StepScalars& s, int64_t r, int k, double sM,
+                                           double F, double own, double fprev, const RecIn& in) {
+  if (!in.on) return;
+  const size_t idx = (size_t)r * p.ld + k;
+  const size_t ro = (size_t)(p.step - p.rec_k0) * p.n * p.ld + idx;
+  const double h = s.h, ds = in.ds;
+  double S = s.photohad ? sM : 0.0;
+  if (s.kap && s.pair) S += in.kp;
+  S = S * s.dl * p.inv_scale;
+  if (STAGE == 1) {
+    p.rec_sx[idx] = S;
+    p.rec_P[ro] = in.f0 * h * ds * own + h * h * in.d12 * ds * F + h * in.f1 * S;
+  } else {
+    p.rec_Q[ro] = h * h * in.d12 * ds * (F - fprev) + h * in.f0 * (S - in.sx);
+  }
+}
+
 // k_slab's shared memory: the state slab (nsp x 32), the bin's entry values,
 // the row factors (3 x nss), the per-warp rings of (FD term, F(x)) rows, then
 // the int tables (entry column offsets, entry ranges, injection slots,
@@ -1181,6 +1223,8 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
   int k = 0;
   for (int i = wid; i < nss; i += nw, ++k) {
     const int r = L.spec[i] * d + e;
+    RecIn rin{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
+    if (p.rec_P) rin = rec_load<STAGE>(p, s, r, col);
     double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
     if (s.photohad) {
       const int j1 = L.rp[i + 1];
@@ -1221,7 +1265,7 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
       }
       const double own = L.slab[L.spec[i] * kColTile + lane];
       const int ro = r * ld + col;
-      if (p.rec_P) record_blocked<STAGE>(p, s, r, col, sM, out, own, STAGE == 2 ? rs[kColTile + lane] : 0.0);
+      if (p.rec_P) record_pre<STAGE>(p, s, r, col, sM, out, own, STAGE == 2 ? rs[kColTile + lane] : 0.0, rin);
       if (STAGE == 1) {
         // a = eD x + (phi1 F(x)) h
         p.a[ro] = __dadd_rn(__dmul_rn(L.fac[i], own), __dmul_rn(__dmul_rn(L.fac[nss + i], out), s.h));
