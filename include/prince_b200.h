@@ -195,8 +195,9 @@ typedef struct pb_solve_args {
   int32_t ckpt_every;      /* > 0: keep the state every this many steps for pb_adjoint */
   const int32_t* out_cols; /* NULL, or n_cols: output column of each solve column (a
                               permutation); the final states are gathered on the
-                              device into that order.  The initial state is read
-                              in solve-column order. */
+                              device into that order, and pb_adjoint reads its
+                              seed in that order.  The initial state is read in
+                              solve-column order. */
 } pb_solve_args;
 
 int pb_solve(pb_context* ctx, const pb_solve_args* args);

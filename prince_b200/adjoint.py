@@ -74,19 +74,17 @@ class PropagateFunction(torch.autograd.Function):
         cd = coeff.detach().cpu().numpy()[:, plan.src_order]
         ctx_dev.set_injection(plan.rows, np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
         ctx_dev.set_photon_field(device_components(plan.run.photon_field))
-        out = np.zeros((plan.run.dim_states, plan.K))
+        X = np.empty((plan.run.dim_states, plan.K))  # filled in the caller's column order
         s = float(scale.detach().cpu().item())
         plan.last_args = (np.ascontiguousarray(cd), s)
-        _solve(ctx_dev, plan, cd, out, s)
-        X = np.empty_like(out)
-        X[:, plan.perm] = out
+        _solve(ctx_dev, plan, cd, X, s)
         ctx.plan = plan
         return torch.from_numpy(X).to(G.device)
 
     @staticmethod
     def backward(ctx, grad_X):
         plan = ctx.plan
-        seed = np.ascontiguousarray(grad_X.detach().cpu().numpy()[:, plan.perm], dtype=np.float64)
+        seed = np.ascontiguousarray(grad_X.detach().cpu().numpy(), dtype=np.float64)  # caller's column order
         cd, s = plan.last_args
         gG, gc, gs = _adjoint(plan.dev.ctx, plan, cd, s, seed)
         gG_user = np.empty_like(gG)
@@ -132,6 +130,7 @@ def _args(plan, coeff, scale, state):
     args.init_state = 0
     args.state_on_device = 0
     args.ckpt_every = plan.ckpt_every
+    args.out_cols = i(plan.perm)  # solve column -> caller column, for the states and the seed
     return args, keep
 
 
@@ -145,7 +144,7 @@ def _solve(ctx, plan, coeff, out, scale):
 def _adjoint(ctx, plan, coeff, scale, seed):
     import ctypes as Cc
 
-    dummy = np.zeros((plan.run.dim_states, plan.K))
+    dummy = np.zeros(1)  # the adjoint reads no state through args
     args, keep = _args(plan, coeff, scale, dummy)
     n_src = plan.dev_src_col.size
     gG = np.zeros((plan.rows.size, n_src))

@@ -1588,6 +1588,15 @@ __global__ void k_gather_cols(const double* __restrict__ X, int ld, int64_t n, i
   Y[(size_t)r * K + cols[j]] = X[(size_t)r * ld + j];
 }
 
+// lam[r][j] = S[r][cols[j]]: a seed given in the caller's column order, in solve order (S is n x K)
+__global__ void k_pick_cols(const double* __restrict__ S, int64_t n, int K, const int* __restrict__ cols,
+                            double* __restrict__ lam, int ld) {
+  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int j = blockIdx.y * kColTile + (threadIdx.x & 31);
+  if (r >= n || j >= K) return;
+  lam[(size_t)r * ld + j] = S[(size_t)r * K + cols[j]];
+}
+
 // v1 = Phi2 lam' for the last step of a checkpoint segment
 __global__ void k_adj_v1(const double* __restrict__ phi2, const double* __restrict__ lam, int64_t n, int ld,
                          int ncols, double* __restrict__ v) {
@@ -2082,7 +2091,8 @@ FieldDesc field_desc(const pb_context* c, double scale) {
   return f;
 }
 
-std::vector<DBuf*> all_buffers(pb_context* c) {
+// Buffers the forward solve reads or writes (the two captured graphs point into these).
+std::vector<DBuf*> solve_buffers(pb_context* c) {
   return {&c->cpl_indptr, &c->cpl_indices, &c->cpl_row, &c->cpl_is_diag, &c->short_rows, &c->long_rows, &c->kernel,
           &c->eph, &c->d_indptr, &c->d_indices, &c->d_vals, &c->d_diag, &c->adia_E, &c->pair_scale, &c->pair_bin,
           &c->xi, &c->phi_xi2, &c->pair_pg, &c->l_diag, &c->l_indptr, &c->l_indices, &c->l_vals, &c->inj_slot,
@@ -2090,14 +2100,22 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
           &c->m_indices, &c->m_vals, &c->m_diag, &c->s_h, &c->s_dldz, &c->s_hc, &c->s_finj, &c->s_win, &c->s_coeff,
           &c->X, &c->A, &c->F, &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0, &c->lr_nseg,
           &c->seg_mb, &c->seg_me, &c->partial, &c->counter, &c->dt_indptr, &c->dt_indices, &c->dt_vals,
-          &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->nact, &c->ckpt, &c->lam,
-          &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj, &c->gs, &c->g_out,
-          &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr, &c->t_indices, &c->t_perm,
-          &c->sort_tmp, &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
+          &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
+          &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf, &c->fdkp,
-          &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->bandT_vals, &c->slabT_vals,
-          &c->fdT_cnt, &c->fdT_off, &c->fdT_val, &c->vbuf, &c->vbuf2, &c->bTbuf, &c->fdTbuf, &c->outcols};
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
+          &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val};
+}
+
+// Every device buffer: the solve's and the adjoint's scratch.
+std::vector<DBuf*> all_buffers(pb_context* c) {
+  std::vector<DBuf*> b = solve_buffers(c);
+  for (DBuf* x : {&c->nact, &c->lam, &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj,
+                  &c->gs, &c->g_out, &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr,
+                  &c->t_indices, &c->t_perm, &c->sort_tmp, &c->fdkp, &c->bandT_vals, &c->slabT_vals, &c->vbuf,
+                  &c->vbuf2, &c->bTbuf, &c->fdTbuf, &c->outcols})
+    b.push_back(x);
+  return b;
 }
 
 // Stable CSR transpose (entries of a transposed row keep increasing column order).
@@ -3237,7 +3255,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     for (double v : c->em_dl) { uint64_t b; memcpy(&b, &v, 8); put(b); }
     const unsigned char* fb = reinterpret_cast<const unsigned char*>(&fd);
     for (size_t i = 0; i < sizeof(fd); i += 8) { uint64_t w = 0; memcpy(&w, fb + i, std::min<size_t>(8, sizeof(fd) - i)); put(w); }
-    for (const DBuf* b : all_buffers(c)) put((uint64_t)(uintptr_t)b->p);
+    for (const DBuf* b : solve_buffers(c)) put((uint64_t)(uintptr_t)b->p);  // adjoint scratch is not in the graphs
     for (int64_t k = 0; k < S; ++k) put((uint64_t)a->n_active[k]);
   }
   // Two graphs -- the per-solve operator set-up and the step loop -- with the
@@ -3381,8 +3399,20 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   if (want_inj) PB_CUDA(c, c->gb_inj.ensure((size_t)std::max<int64_t>(S, 1) * std::max(n_inj, 1) * ld * sizeof(double)));
   if ((rc = upload(c, c->nact, a->n_active, (size_t)std::max<int64_t>(S, 1)))) return rc;
   PB_CUDA(c, cudaMemsetAsync(c->lam.p, 0, sb, st));
-  PB_CUDA(c, cudaMemcpy2DAsync(c->lam.p, ld * sizeof(double), seed, K * sizeof(double), K * sizeof(double), n,
+  if (a->out_cols && K > 1) {  // the seed in the caller's column order: one copy, then a gather on the device
+    for (int j = 0; j < K; ++j)
+      if (a->out_cols[j] < 0 || a->out_cols[j] >= K) return fail(c, PB_ERR_ARG, "pb_adjoint: out_cols[%d] out of range", j);
+    if ((rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
+    PB_CUDA(c, c->F.ensure(sb));
+    PB_CUDA(c, cudaMemcpyAsync(c->F.p, seed, (size_t)n * K * sizeof(double),
                                seed_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    k_pick_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(c->F.as<double>(), n, K,
+                                                                               c->outcols.as<int>(), c->lam.as<double>(), ld);
+    PB_CUDA(c, cudaGetLastError());
+  } else {
+    PB_CUDA(c, cudaMemcpy2DAsync(c->lam.p, ld * sizeof(double), seed, K * sizeof(double), K * sizeof(double), n,
+                                 seed_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  }
 
   // ---- forward parameters (recording) and backward sweep per checkpoint segment
   StepParams p;
