@@ -137,9 +137,9 @@ struct pb_context {
   int32_t band_npairs = 0;
   DBuf band_slot, band_spec, slab_spec, band_vals, band_part;
   // bin-local rows: coupling entries in bin-major order
-  DBuf slab_rp, slab_sidx, slab_slot, slab_vals;
-  int64_t slab_nent = 0;            // entries per window (with the per-bin alignment padding)
-  int32_t slab_maxbin = 0;          // entries of the largest bin (padded)
+  DBuf slab_rp, slab_sidx, slab_slot, slab_vals, slab_pairs, slab_wrp;  // slab_rp: quad base per bin; slab_sidx: quads
+  int64_t slab_nent = 0;            // value slots per window (4 per quad)
+  int32_t slab_maxbin = 0;          // quads of the largest bin
   size_t slab_smem = 0, band_smem = 0;
   // FD stencil per bin (same in every species block): host copy of D and the table
   std::vector<int64_t> h_d_indptr;
@@ -600,12 +600,14 @@ struct StepParams {
   int nsp;                  // species blocks
   const int* slab_spec;     // species whose coupling rows are bin-local
   int n_slab_spec;
-  const int* slab_rp;       // bin-major entry range of each bin-local row ([d][n_slab_spec] + 1)
-  const int* slab_sidx;     // species block of the column of each bin-major entry
-  const double* slab_vals;  // [W][slab_stride] M_off values of the bin-major entries
-  const int* slab_offs;     // byte offset in k_slab's state slab of each entry's column
+  const int* slab_qbase;    // [d + 1] first entry quad of each bin (even)
+  const unsigned long long* slab_q;  // per quad: the 4 entries' mother species, 16 bits each
+  const int4* slab_pairs;   // row pairs of k_slab's warps: species A, B (-1: none), q0 << 16 | quads of A, of B
+  const int* slab_wrp;      // [d][kSlabWarps + 1] first pair of each warp of a bin's CTA
+  const double* slab_vals;  // [W][slab_stride] M_off values of the quads (4 per quad, zero padding)
   int64_t slab_stride;
-  int slab_maxbin;          // entries of the largest bin (shared-memory sizing)
+  int slab_maxq;            // quads of the largest bin (shared-memory sizing)
+  int slab_maxp;            // row pairs of the largest bin
   const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
   const int* fd_off;
   const double* fd_val;
@@ -1114,87 +1116,111 @@ __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalar
   }
 }
 
-// k_slab's shared memory: the state slab (nsp x 32), the bin's entry values,
-// the row factors (3 x nss), the per-warp rings of (FD term, F(x)) rows, then
-// the int tables (entry column offsets, entry ranges, injection slots,
-// species).  Every block starts on a 16-byte boundary.
-constexpr int kSlabRing = 4;        // rows of FD term / F(x) in flight per warp
+// k_slab's shared memory: the state slab of one bin (nsp x 16 columns), the
+// bin's entry values (4 per quad), mother species (4 x 16 bits per quad), row
+// pairs and the row factors (eD, phi1, phi2) of each pair slot.  Every block
+// starts on a 16-byte boundary (the quad count of a bin is even).
+constexpr int kSlabCols = 16;       // state columns of a k_slab CTA (a half-warp per row)
+constexpr int kSlabWarps = 8;       // two CTAs per SM
+constexpr int kSlabPre = 4;         // row pairs whose FD term and F(x) a warp loads ahead
 struct SlabSmem {
   double* slab;
   double* vals;
-  double* fac;
-  double* ring;  // [warp][kSlabRing][2][32]
-  int* offs;
-  int* rp;
-  int* slot;
-  int* spec;
-  __host__ __device__ static size_t al2(size_t x) { return (x + 1) & ~(size_t)1; }
-  __host__ __device__ static size_t bytes(int nsp, int nss, int maxbin) {
-    return ((size_t)nsp * kColTile + maxbin + al2(3 * (size_t)nss) +
-            (size_t)(kSlabThreads / 32) * kSlabRing * 2 * kColTile) * sizeof(double) +
-           ((size_t)maxbin + 3 * (size_t)nss + 1) * sizeof(int);
+  unsigned long long* sidx;
+  int4* pairs;
+  double* fac;  // [3][2 maxp]
+  __host__ __device__ static size_t bytes(int nsp, int maxq, int maxp) {
+    return (size_t)nsp * kSlabCols * sizeof(double) + (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) +
+           (size_t)maxp * (sizeof(int4) + 6 * sizeof(double));
   }
-  __device__ SlabSmem(double* base, int nsp, int nss, int maxbin) {
+  __device__ SlabSmem(double* base, int nsp, int maxq, int maxp) {
     slab = base;
-    vals = slab + (size_t)nsp * kColTile;
-    fac = vals + maxbin;
-    ring = fac + al2(3 * (size_t)nss);
-    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabRing * 2 * kColTile);
-    rp = offs + maxbin;
-    slot = rp + nss + 1;
-    spec = slot + nss;
+    vals = slab + (size_t)nsp * kSlabCols;
+    sidx = reinterpret_cast<unsigned long long*>(vals + (size_t)maxq * 4);
+    pairs = reinterpret_cast<int4*>(sidx + maxq);
+    fac = reinterpret_cast<double*>(pairs + maxp);
   }
 };
 
-// Bin-local rows.  CTA = (bin e, 32-column tile), lane = column.  The state
-// slab of bin e and the bin's coupling entries arrive in shared memory by
-// asynchronous copies; a warp then takes rows e-strided (rows are ordered by
-// entry count, longest first), sums each from shared memory and applies the
-// stage update.  The row's FD term (fdbuf) and, in stage 2, F(x) are copied
-// asynchronously kSlabRing rows ahead into the warp's ring.  Offsets into the
-// (n x ld) state buffers are 32-bit (n ld < 2^31, checked at launch).
-template <int STAGE>
-__global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+
+// Bin-local rows.  CTA = (bin e, 16-column tile); a half-warp owns a row, its
+// lane c owns column col0 + c.  The state slab of bin e, the bin's entry quads,
+// its row pairs and their row factors arrive in shared memory by asynchronous
+// copies; a warp then walks its row pairs (balanced over the warps when the
+// layout is built), sums each row from shared memory (four accumulators, one
+// per quad position) and applies the stage update.  The row's FD term
+// (fdbuf), F(x) in stage 2 and its injection slot are loaded kSlabPre pairs
+// ahead into registers.  REC: the adjoint's record pass (P / Q sensitivities).
+// Offsets into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at
+// launch).
+template <int STAGE, bool REC>
+__global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParams p) {
   extern __shared__ double sm[];
-  const int nss = p.n_slab_spec;
   const int e = blockIdx.x;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int col0 = blockIdx.y * kColTile;
-  const int col = col0 + lane;  // < ld
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int half = lane >> 4, c = lane & 15;
+  const int col0 = blockIdx.y * kSlabCols;
+  const int col = col0 + c;  // < ld
   const bool active = col < p.ncols;
   const StepScalars s = load_scalars(p, p.step);
   const size_t o0 = (size_t)(p.step & 1) * p.n;
   const int ld = p.ld, d = p.d;
-  SlabSmem L(sm, p.nsp, nss, p.slab_maxbin);
-  const double* __restrict__ v = p.src;
-  const int q0 = p.slab_rp[(size_t)e * nss], q1 = p.slab_rp[(size_t)(e + 1) * nss];  // multiples of 4
+  SlabSmem L(sm, p.nsp, p.slab_maxq, p.slab_maxp);
+  const int qb = p.slab_qbase[e], nqb = p.slab_qbase[e + 1] - qb;
+  const int pb0 = p.slab_wrp[e * (kSlabWarps + 1)], npb = p.slab_wrp[e * (kSlabWarps + 1) + kSlabWarps] - pb0;
+  const int fs = 2 * p.slab_maxp;  // stride of the three row-factor arrays
   {
-    const double* vs = v + (size_t)e * ld + col0;
-    for (int t = threadIdx.x; t < p.nsp * (kColTile / 2); t += blockDim.x) {
-      const int q = t / (kColTile / 2), c = 2 * (t - q * (kColTile / 2));
-      cp_async16(L.slab + q * kColTile + c, vs + (size_t)q * d * ld + c);
+    const double* vs = p.src + (size_t)e * ld + col0;
+    for (int t = threadIdx.x; t < p.nsp * (kSlabCols / 2); t += blockDim.x) {
+      const int q = t / (kSlabCols / 2), cc = 2 * (t - q * (kSlabCols / 2));
+      cp_async16(L.slab + q * kSlabCols + cc, vs + (size_t)q * d * ld + cc);
     }
     if (s.photohad) {
-      const double* mv = p.slab_vals + (size_t)s.w * p.slab_stride + q0;
-      for (int t = threadIdx.x; t < (q1 - q0) / 2; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
-      for (int t = threadIdx.x; t < (q1 - q0) / 4; t += blockDim.x) cp_async16(L.offs + 4 * t, p.slab_offs + q0 + 4 * t);
+      const double* mv = p.slab_vals + (size_t)s.w * p.slab_stride + (size_t)qb * 4;
+      for (int t = threadIdx.x; t < 2 * nqb; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
+      const unsigned long long* mq = p.slab_q + qb;
+      for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
+    }
+    for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, p.slab_pairs + pb0 + t);
+    for (int t = threadIdx.x; t < 2 * npb; t += blockDim.x) {
+      const int4 pr = __ldg(p.slab_pairs + pb0 + (t >> 1));
+      const int sp = (t & 1) ? pr.y : pr.x;
+      if (sp < 0) continue;
+      const size_t r = o0 + (size_t)sp * d + e;
+      cp_async8(L.fac + t, p.eD + r);
+      cp_async8(L.fac + fs + t, p.phi1 + r);
+      cp_async8(L.fac + 2 * fs + t, p.phi2 + r);
     }
     cp_async_commit();
   }
-  for (int i = threadIdx.x; i < nss; i += blockDim.x) {
-    const int sp = p.slab_spec[i];
-    const int r = sp * d + e;
-    const double a0 = p.eD[o0 + r], a1 = p.phi1[o0 + r], a2 = p.phi2[o0 + r];
-    const int rpi = p.slab_rp[(size_t)e * nss + i] - q0;
-    const int sl = s.inj ? p.inj_slot[r] : -1;
-    L.fac[i] = a0;
-    L.fac[nss + i] = a1;
-    L.fac[2 * nss + i] = a2;
-    L.rp[i] = rpi;
-    L.slot[i] = sl;
-    L.spec[i] = sp;
-  }
-  if (threadIdx.x == 0) L.rp[nss] = q1 - q0;
+  const int w0 = p.slab_wrp[e * (kSlabWarps + 1) + wid], w1 = p.slab_wrp[e * (kSlabWarps + 1) + wid + 1];
+  const bool need_fd = s.kap, need_f = STAGE == 2;
+  double fdr[kSlabPre], fxr[kSlabPre];
+  int slr[kSlabPre];
+  // the FD term, F(x) and injection slot of pair pi's row (staged: the pair
+  // comes from shared memory; the first pairs are read from global memory)
+#define PB_SLAB_LOAD(U, PI, PR)                                              \
+  do {                                                                       \
+    fdr[U] = 0.0;                                                            \
+    fxr[U] = 0.0;                                                            \
+    slr[U] = -1;                                                             \
+    if ((PI) < w1) {                                                         \
+      const int4 pr_ = (PR);                                                 \
+      const int sp_ = half ? pr_.y : pr_.x;                                  \
+      if (sp_ >= 0) {                                                        \
+        const int r_ = sp_ * d + e;                                          \
+        if (need_fd) fdr[U] = p.fdbuf[r_ * ld + col];                        \
+        if (need_f) fxr[U] = p.f[r_ * ld + col];                             \
+        if (s.inj) slr[U] = p.inj_slot[r_];                                  \
+      }                                                                      \
+    }                                                                        \
+  } while (0)
+#pragma unroll
+  for (int u = 0; u < kSlabPre; ++u) PB_SLAB_LOAD(u, w0 + u, __ldg(p.slab_pairs + w0 + u));
   int src0 = 0, src1 = 0;
   if (s.inj && active) {
     src0 = p.src_ptr[col];
@@ -1203,83 +1229,72 @@ __global__ void __launch_bounds__(kSlabThreads, 1) k_slab(StepParams p) {
   cp_async_wait<0>();
   __syncthreads();
 
-  // Ring of the warp's upcoming rows: lanes 0-15 copy the FD row, lanes 16-31
-  // the F(x) row, 16 bytes each; one commit group per row (empty past the end).
-  double* ring = L.ring + (size_t)wid * kSlabRing * 2 * kColTile;
-  const bool need_fd = s.kap, need_f = STAGE == 2;
-  const int h = lane >> 4, c2 = 2 * (lane & 15);
-  auto fetch = [&](int i, int k) {
-    if (i < nss) {
-      const int r = L.spec[i] * d + e;
-      double* dst = ring + ((k % kSlabRing) * 2 + h) * kColTile + c2;
-      if (h == 0 && need_fd) cp_async16(dst, p.fdbuf + r * ld + col0 + c2);
-      if (h == 1 && need_f) cp_async16(dst, p.f + r * ld + col0 + c2);
-    }
-    cp_async_commit();
-  };
+  const char* slb = reinterpret_cast<const char*>(L.slab + c);
+  const double2* vq = reinterpret_cast<const double2*>(L.vals);
+  for (int pb = w0; pb < w1; pb += kSlabPre) {
 #pragma unroll
-  for (int k = 0; k < kSlabRing; ++k) fetch(wid + k * nw, k);
-  const char* slb = reinterpret_cast<const char*>(L.slab + lane);
-  int k = 0;
-  for (int i = wid; i < nss; i += nw, ++k) {
-    const int r = L.spec[i] * d + e;
-    RecIn rin{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
-    if (p.rec_P) rin = rec_load<STAGE>(p, s, r, col);
-    double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-    if (s.photohad) {
-      const int j1 = L.rp[i + 1];
-      int j = L.rp[i];
-      for (; j + 3 < j1; j += 4) {
-        const double x0 = *reinterpret_cast<const double*>(slb + L.offs[j]);
-        const double x1 = *reinterpret_cast<const double*>(slb + L.offs[j + 1]);
-        const double x2 = *reinterpret_cast<const double*>(slb + L.offs[j + 2]);
-        const double x3 = *reinterpret_cast<const double*>(slb + L.offs[j + 3]);
-        acc0 = __fma_rn(L.vals[j], x0, acc0);
-        acc1 = __fma_rn(L.vals[j + 1], x1, acc1);
-        acc2 = __fma_rn(L.vals[j + 2], x2, acc2);
-        acc3 = __fma_rn(L.vals[j + 3], x3, acc3);
+    for (int u = 0; u < kSlabPre; ++u) {
+      const int pi = pb + u;
+      if (pi >= w1) break;
+      const int4 pr = L.pairs[pi - pb0];
+      const int sp = half ? pr.y : pr.x;
+      const int qq = half ? pr.w : pr.z;
+      const int r = sp * d + e;
+      RecIn rin{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
+      if (REC && sp >= 0) rin = rec_load<STAGE>(p, s, r, col);
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+      if (sp >= 0 && s.photohad) {
+        const int q0 = qq >> 16, q1 = q0 + (qq & 0xffff);
+        for (int q = q0; q < q1; ++q) {
+          const double2 va = vq[2 * q], vb = vq[2 * q + 1];
+          const unsigned long long m = L.sidx[q];
+          const double x0 = *reinterpret_cast<const double*>(slb + (((unsigned)m & 0xffffu) << 7));
+          const double x1 = *reinterpret_cast<const double*>(slb + (((unsigned)(m >> 16) & 0xffffu) << 7));
+          const double x2 = *reinterpret_cast<const double*>(slb + (((unsigned)(m >> 32) & 0xffffu) << 7));
+          const double x3 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 48) << 7));
+          acc0 = __fma_rn(va.x, x0, acc0);
+          acc1 = __fma_rn(va.y, x1, acc1);
+          acc2 = __fma_rn(vb.x, x2, acc2);
+          acc3 = __fma_rn(vb.y, x3, acc3);
+        }
       }
-      for (; j < j1; ++j) acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
+      if (sp >= 0 && active) {
+        const double sM = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
+        double out = sM;
+        if (s.kap) out = __dadd_rn(out, fdr[u]);
+        if (s.decay) {
+          double sL = 0.0;
+          for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
+            sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], p.src[(size_t)p.l_indices[j] * ld + col]));
+          out = __dadd_rn(out, sL);
+        }
+        out = __dmul_rn(out, s.dl);
+        if (slr[u] >= 0 && src1 > src0) {  // injection (rows of injected species only)
+          const double* cf = p.coeff + (size_t)p.step * p.n_src;
+          const double* g = p.G + (size_t)slr[u] * p.n_src;
+          double a = __dmul_rn(cf[src0], g[src0]);
+          for (int q = src0 + 1; q < src1; ++q) a = __dadd_rn(a, __dmul_rn(cf[q], g[q]));
+          out = __dadd_rn(out, __dmul_rn(s.finj, a));
+        }
+        const double own = L.slab[sp * kSlabCols + c];
+        const int slot = 2 * (pi - pb0) + half;
+        const int ro = r * ld + col;
+        if (REC) record_pre<STAGE>(p, s, r, col, sM, out, own, fxr[u], rin);
+        if (STAGE == 1) {
+          // a = eD x + (phi1 F(x)) h
+          p.a[ro] = __dadd_rn(__dmul_rn(L.fac[slot], own), __dmul_rn(__dmul_rn(L.fac[fs + slot], out), s.h));
+          p.f[ro] = out;
+        } else {
+          // x = a + ((F(a) - F(x)) h) phi2
+          const double dF = __dmul_rn(__dadd_rn(out, -fxr[u]), s.h);
+          p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * fs + slot]));
+        }
+      }
+      const int pn = pi + kSlabPre;
+      PB_SLAB_LOAD(u, pn, L.pairs[pn - pb0]);
     }
-    cp_async_wait<kSlabRing - 1>();  // this row's copies (issued kSlabRing rows ago) have landed
-    __syncwarp();
-    const double* rs = ring + (k % kSlabRing) * 2 * kColTile;
-    if (active) {
-      const double sM = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
-      double out = sM;
-      if (s.kap) out = __dadd_rn(out, rs[lane]);
-      if (s.decay) {
-        double sL = 0.0;
-        for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
-          sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], v[(size_t)p.l_indices[j] * ld + col]));
-        out = __dadd_rn(out, sL);
-      }
-      out = __dmul_rn(out, s.dl);
-      const int slt = L.slot[i];
-      if (slt >= 0 && src1 > src0) {  // injection (rows of injected species only)
-        const double* cf = p.coeff + (size_t)p.step * p.n_src;
-        const double* g = p.G + (size_t)slt * p.n_src;
-        double a = __dmul_rn(cf[src0], g[src0]);
-        for (int q = src0 + 1; q < src1; ++q) a = __dadd_rn(a, __dmul_rn(cf[q], g[q]));
-        out = __dadd_rn(out, __dmul_rn(s.finj, a));
-      }
-      const double own = L.slab[L.spec[i] * kColTile + lane];
-      const int ro = r * ld + col;
-      if (p.rec_P) record_pre<STAGE>(p, s, r, col, sM, out, own, STAGE == 2 ? rs[kColTile + lane] : 0.0, rin);
-      if (STAGE == 1) {
-        // a = eD x + (phi1 F(x)) h
-        p.a[ro] = __dadd_rn(__dmul_rn(L.fac[i], own), __dmul_rn(__dmul_rn(L.fac[nss + i], out), s.h));
-        p.f[ro] = out;
-      } else {
-        // x = a + ((F(a) - F(x)) h) phi2
-        const double dF = __dmul_rn(__dadd_rn(out, -rs[kColTile + lane]), s.h);
-        p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * nss + i]));
-      }
-    }
-    __syncwarp();  // the slot is read before it is refilled
-    fetch(i + kSlabRing * nw, k + kSlabRing);
   }
-  cp_async_wait<0>();
+#undef PB_SLAB_LOAD
 }
 
 // Stage 2: the row factors of the next step for the bin-local rows (one
@@ -1878,13 +1893,14 @@ BandTInstance bandT_kernel(int RT, int J) {
 __global__ void k_transpose_blocks(const int* __restrict__ bslot, const int* __restrict__ bslotT,
                                    const int* __restrict__ sslot, const int* __restrict__ sslotT, int64_t R, int W,
                                    const double* __restrict__ band, double* __restrict__ bandT, int64_t bstride,
-                                   const double* __restrict__ slab, double* __restrict__ slabT, int64_t sstride) {
+                                   const double* __restrict__ slab, int64_t sstride, double* __restrict__ slabT,
+                                   int64_t tstride) {
   const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= R) return;
   const int b = bslot[j], bt = bslotT[j], s = sslot[j], st = sslotT[j];
   for (int w = 0; w < W; ++w) {
     if (b >= 0 && bt >= 0) bandT[(size_t)w * bstride + bt] = band[(size_t)w * bstride + b];
-    if (s >= 0 && st >= 0) slabT[(size_t)w * sstride + st] = slab[(size_t)w * sstride + s];
+    if (s >= 0 && st >= 0) slabT[(size_t)w * tstride + st] = slab[(size_t)w * sstride + s];
   }
 }
 
@@ -2103,7 +2119,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val};
 }
 
@@ -2203,12 +2219,14 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.nsp = c->lay_nsp;
   p.slab_spec = c->slab_spec.as<int>();
   p.n_slab_spec = c->n_slab_spec;
-  p.slab_rp = c->slab_rp.as<int>();
-  p.slab_sidx = c->slab_sidx.as<int>();
+  p.slab_qbase = c->slab_rp.as<int>();
+  p.slab_q = c->slab_sidx.as<unsigned long long>();
+  p.slab_pairs = c->slab_pairs.as<int4>();
+  p.slab_wrp = c->slab_wrp.as<int>();
   p.slab_vals = c->slab_vals.as<double>();
-  p.slab_offs = c->slab_sidx.as<int>();
   p.slab_stride = c->slab_nent;
-  p.slab_maxbin = c->slab_maxbin;
+  p.slab_maxq = c->slab_maxbin;
+  p.slab_maxp = (c->n_slab_spec + 1) / 2;
   p.fd_cnt = c->fd_cnt.as<int>();
   p.fd_off = c->fd_off.as<int>();
   p.fd_val = c->fd_val.as<double>();
@@ -2254,7 +2272,9 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
     k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
     ++launches;
   }
-  k_slab<STAGE><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
+  const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
+  if (p.rec_P) k_slab<STAGE, true><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
+  else k_slab<STAGE, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
   ++launches;
   if (STAGE == 2 && p.step + 1 < p.n_steps) {
     k_slab_prep<<<blocks_for((int64_t)p.n_slab_spec * p.d, 256), 256, 0, st>>>(p);
@@ -2771,37 +2791,78 @@ int pb_set_layout(pb_context* c, int32_t d) {
   int RT = 0, J = 0;
   for (int v : kBandRT) if (!RT && v >= RTr) RT = v;
   for (int v : kBandJ) if (!J && v >= Jr) J = v;
-  // bin-local rows: entries in bin-major order (bin, row species, CSR order);
-  // every bin starts on a multiple of 4 entries (16-byte copies of values and columns)
+  // bin-local rows, per bin: rows ordered by entry quads (longest first) and
+  // paired for the two half-warps of a warp; pairs spread over k_slab's warps
+  // longest-processing-time first; each row's entries in CSR order in quads of
+  // 4 (zero values pad the last quad); every bin starts on an even quad.
   int64_t band_nnz = 0, slab_nnz = 0;
-  std::vector<int32_t> srp((size_t)d * nss + 1, 0), ssidx, sslot((size_t)std::max<int64_t>(R, 1), -1);
+  std::vector<int32_t> qbase((size_t)d + 1, 0), wrp((size_t)d * (kSlabWarps + 1), 0), spairs;
+  std::vector<unsigned long long> squad;
+  std::vector<int32_t> sslot((size_t)std::max<int64_t>(R, 1), -1);
   int32_t maxbin = 0;
-  for (int e = 0; e < d; ++e) {
-    while (ssidx.size() % 4) ssidx.push_back(0);
-    const size_t b0 = ssidx.size();
-    for (int i = 0; i < nss; ++i) {
-      const int64_t r = (int64_t)sspec[i] * d + e;
-      srp[(size_t)e * nss + i] = (int32_t)ssidx.size();
-      for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
-        if (ix[j] == r) continue;
-        sslot[j] = (int32_t)ssidx.size();
-        ++slab_nnz;
-        ssidx.push_back((ix[j] / d) * kColTile * (int32_t)sizeof(double));  // byte offset in k_slab's slab
+  bool quads_fit = nsp < (1 << 16);
+  {
+    std::vector<int32_t> nq(nss), order(nss);
+    std::vector<std::vector<int32_t>> wl(kSlabWarps);
+    std::vector<int64_t> load(kSlabWarps);
+    for (int e = 0; e < d; ++e) {
+      qbase[e] = (int32_t)squad.size();
+      for (int i = 0; i < nss; ++i) {
+        const int64_t r = (int64_t)sspec[i] * d + e;
+        int64_t cnt = 0;
+        for (int64_t j = ip[r]; j < ip[r + 1]; ++j) cnt += ix[j] != r;
+        nq[i] = (int32_t)((cnt + 3) / 4);
+        order[i] = i;
       }
+      std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return nq[a] > nq[b]; });
+      for (auto& v : wl) v.clear();
+      std::fill(load.begin(), load.end(), 0);
+      for (int k = 0; k < nss; k += 2) {  // pair k/2 = rows order[k], order[k + 1]
+        const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        wl[w].push_back(k);
+        load[w] += nq[order[k]] + 1;
+      }
+      for (int w = 0; w < kSlabWarps; ++w) {
+        wrp[(size_t)e * (kSlabWarps + 1) + w] = (int32_t)(spairs.size() / 4);
+        for (int k : wl[w]) {
+          int32_t pr[4] = {-1, -1, 0, 0};
+          for (int hf = 0; hf < 2; ++hf) {
+            if (k + hf >= nss) continue;
+            const int i = order[k + hf];
+            const int64_t r = (int64_t)sspec[i] * d + e;
+            const int64_t q0 = (int64_t)squad.size() - qbase[e];
+            int t = 0, pad_sp = sspec[i];
+            for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
+              if (ix[j] == r) continue;
+              if (t == 0) pad_sp = ix[j] / d;
+              if (t % 4 == 0) squad.push_back(0);
+              squad.back() |= (unsigned long long)(ix[j] / d) << (16 * (t % 4));
+              sslot[j] = (int32_t)((squad.size() - 1) * 4 + t % 4);
+              ++slab_nnz;
+              ++t;
+            }
+            for (; t % 4; ++t) squad.back() |= (unsigned long long)pad_sp << (16 * (t % 4));
+            if (q0 >= (1 << 15) || nq[i] >= (1 << 16)) quads_fit = false;
+            pr[hf] = sspec[i];
+            pr[2 + hf] = (int32_t)((q0 << 16) | nq[i]);
+          }
+          spairs.insert(spairs.end(), pr, pr + 4);
+        }
+      }
+      wrp[(size_t)e * (kSlabWarps + 1) + kSlabWarps] = (int32_t)(spairs.size() / 4);
+      if ((squad.size() - qbase[e]) % 2) squad.push_back(0);
+      maxbin = std::max<int32_t>(maxbin, (int32_t)(squad.size() - qbase[e]));
     }
-    size_t b1 = ssidx.size();
-    b1 = (b1 + 3) & ~(size_t)3;
-    maxbin = std::max<int32_t>(maxbin, (int32_t)(b1 - b0));
+    qbase[d] = (int32_t)squad.size();
+    if (squad.empty()) squad.assign(2, 0);
+    if (spairs.empty()) spairs.assign(4, -1);
   }
-  while (ssidx.size() % 4) ssidx.push_back(0);
-  srp[(size_t)d * nss] = (int32_t)ssidx.size();
-  if (ssidx.empty()) ssidx.assign(4, 0);
   const size_t max_smem = 227 * 1024;
-  const size_t ssm = SlabSmem::bytes(nsp, nss, maxbin);
+  const size_t ssm = SlabSmem::bytes(nsp, maxbin, (nss + 1) / 2);
   const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0};
-  const bool ok = ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
+  const bool ok = quads_fit && ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
                   (size_t)d * (kColTile + 2) * sizeof(double) <= max_smem &&
-                  (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && ssidx.size() < ((size_t)1 << 31);
+                  (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && squad.size() < ((size_t)1 << 29);
   if (!ok) return PB_OK;  // the general row kernels stay in use
   // band tiles: [species][band pair][2][RT][J][32] DMMA A fragments per window
   std::vector<int32_t> bslot((size_t)std::max<int64_t>(R, 1), -1);
@@ -2821,12 +2882,17 @@ int pb_set_layout(pb_context* c, int32_t d) {
   if ((rc = upload(c, c->band_slot, bslot.data(), bslot.size()))) return rc;
   if ((rc = upload(c, c->band_spec, bspec.data(), bspec.size()))) return rc;
   if ((rc = upload(c, c->slab_spec, sspec.data(), sspec.size()))) return rc;
-  if ((rc = upload(c, c->slab_rp, srp.data(), srp.size()))) return rc;
-  if ((rc = upload(c, c->slab_sidx, ssidx.data(), ssidx.size()))) return rc;
+  if ((rc = upload(c, c->slab_rp, qbase.data(), qbase.size()))) return rc;
+  if ((rc = upload(c, c->slab_sidx, squad.data(), squad.size()))) return rc;
+  if ((rc = upload(c, c->slab_pairs, spairs.data(), spairs.size()))) return rc;
+  if ((rc = upload(c, c->slab_wrp, wrp.data(), wrp.size()))) return rc;
   if ((rc = upload(c, c->slab_slot, sslot.data(), sslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slab<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slab<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+  for (const void* fn : {(const void*)k_slab<1, false>, (const void*)k_slab<2, false>, (const void*)k_slab<1, true>,
+                         (const void*)k_slab<2, true>}) {
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+  }
   PB_CUDA(c, cudaFuncSetAttribute(bi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi.smem));
   c->band_nb = nb;
   c->band_npairs = npairs;
@@ -2834,7 +2900,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   c->band_J = J;
   c->band_stride = (int64_t)nsp * 2 * npairs * RT * J * 32;
   c->n_slab_spec = nss;
-  c->slab_nent = (int64_t)ssidx.size();
+  c->slab_nent = (int64_t)squad.size() * 4;
   c->slab_maxbin = maxbin;
   c->slab_smem = ssm;
   c->band_smem = bi.smem;
@@ -2940,8 +3006,9 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
       PB_CUDA(c, cudaEventRecord(c->ev0, st));
       if (kk == 0) k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
       if (kk == 1) {
-        if (stage == 1) k_slab<1><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
-        else k_slab<2><<<dim3(p.d, tiles), kSlabThreads, c->slab_smem, st>>>(p);
+        const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
+        if (stage == 1) k_slab<1, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
+        else k_slab<2, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
       }
       if (kk == 2) bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), 256, bi.smem, st>>>(p);
       if (kk == 3) {
@@ -3453,7 +3520,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
       k_transpose_blocks<<<blocks_for(R, 256), 256, 0, st>>>(
           c->band_slot.as<int>(), c->bandT_slot.as<int>(), c->slab_slot.as<int>(), c->slabT_slot.as<int>(), R, W,
           c->band_vals.as<double>(), c->bandT_vals.as<double>(), c->band_stride, c->slab_vals.as<double>(),
-          c->slabT_vals.as<double>(), c->slab_nent);
+          c->slab_nent, c->slabT_vals.as<double>(), c->slabT_nent);
     PB_CUDA(c, cudaGetLastError());
   }
   for (int64_t sg = nseg - 1; sg >= 0; --sg) {
