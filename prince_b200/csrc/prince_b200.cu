@@ -137,7 +137,8 @@ struct pb_context {
   int32_t band_npairs = 0;
   DBuf band_slot, band_spec, slab_spec, band_vals, band_part;
   // bin-local rows: coupling entries in bin-major order
-  DBuf slab_rp, slab_sidx, slab_slot, slab_vals, slab_pairs, slab_wrp;  // slab_rp: quad base per bin; slab_sidx: quads
+  DBuf slab_rp, slab_sidx, slab_slot, slab_vals, slab_pairs, slab_wrp, slab_rowslot, slab_fac;
+  int64_t slab_nslots = 0;          // pair slots over all bins (two per pair)  // slab_rp: quad base per bin; slab_sidx: quads
   int64_t slab_nent = 0;            // value slots per window (4 per quad)
   int32_t slab_maxbin = 0;          // quads of the largest bin
   size_t slab_smem = 0, band_smem = 0;
@@ -530,6 +531,7 @@ struct StepParams {
   int ld;            // leading dimension of the (n x ld) state buffers
   int ncols;         // active columns this step
   int64_t step;
+  int step_w;        // rate window of this step (k_slab's entry values), set with step
   int64_t n_steps;
   uint32_t flags;
   const double* h;
@@ -608,6 +610,9 @@ struct StepParams {
   int64_t slab_stride;
   int slab_maxq;            // quads of the largest bin (shared-memory sizing)
   int slab_maxp;            // row pairs of the largest bin
+  const int* slab_rowslot;  // [n] pair slot of each bin-local row (-1: other rows)
+  double* slab_fac;         // [2][3][slab_nslots] eD, phi1, phi2 of the bin-local rows in pair-slot order
+  int64_t slab_nslots;
   const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
   const int* fd_off;
   const double* fd_val;
@@ -700,6 +705,15 @@ __device__ __forceinline__ void row_prep(const StepParams& p, int64_t step, int6
   p.phi1[o] = f1;
   p.phi2[o] = f2;
   p.kap[o] = k;
+  if (p.slab_rowslot) {  // k_slab stages the factors of a bin's rows as three contiguous runs
+    const int sl = p.slab_rowslot[r];
+    if (sl >= 0) {
+      double* fc = p.slab_fac + (size_t)(step & 1) * 3 * p.slab_nslots + sl;
+      fc[0] = e;
+      fc[p.slab_nslots] = f1;
+      fc[2 * p.slab_nslots] = f2;
+    }
+  }
   if (p.dsig) {  // derivatives with respect to the photon scale (adjoint record pass)
     const double md = p.m_diag[(size_t)s.w * p.n + r] * p.inv_scale;
     double ds = md;
@@ -1142,15 +1156,10 @@ struct SlabSmem {
   }
 };
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
-}
-
 // Bin-local rows.  CTA = (bin e, 16-column tile); a half-warp owns a row, its
 // lane c owns column col0 + c.  The state slab of bin e, the bin's entry quads,
-// its row pairs and their row factors arrive in shared memory by asynchronous
-// copies; a warp then walks its row pairs (balanced over the warps when the
+// its row pairs and their row factors (written in pair-slot order by the row
+// preparation) arrive in shared memory by asynchronous copies; a warp then walks its row pairs (balanced over the warps when the
 // layout is built), sums each row from shared memory (four accumulators, one
 // per quad position) and applies the stage update.  The row's FD term
 // (fdbuf), F(x) in stage 2 and its injection slot are loaded kSlabPre pairs
@@ -1180,20 +1189,16 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
       cp_async16(L.slab + q * kSlabCols + cc, vs + (size_t)q * d * ld + cc);
     }
     if (s.photohad) {
-      const double* mv = p.slab_vals + (size_t)s.w * p.slab_stride + (size_t)qb * 4;
+      const double* mv = p.slab_vals + (size_t)p.step_w * p.slab_stride + (size_t)qb * 4;
       for (int t = threadIdx.x; t < 2 * nqb; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
       const unsigned long long* mq = p.slab_q + qb;
       for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
     }
     for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, p.slab_pairs + pb0 + t);
-    for (int t = threadIdx.x; t < 2 * npb; t += blockDim.x) {
-      const int4 pr = __ldg(p.slab_pairs + pb0 + (t >> 1));
-      const int sp = (t & 1) ? pr.y : pr.x;
-      if (sp < 0) continue;
-      const size_t r = o0 + (size_t)sp * d + e;
-      cp_async8(L.fac + t, p.eD + r);
-      cp_async8(L.fac + fs + t, p.phi1 + r);
-      cp_async8(L.fac + 2 * fs + t, p.phi2 + r);
+    const double* fc = p.slab_fac + (size_t)(p.step & 1) * 3 * p.slab_nslots + 2 * (size_t)pb0;
+    for (int t = threadIdx.x; t < 3 * npb; t += blockDim.x) {  // 2 npb slots per factor, 16 bytes a copy
+      const int k = t / npb, u = t - k * npb;
+      cp_async16(L.fac + k * fs + 2 * u, fc + (size_t)k * p.slab_nslots + 2 * u);
     }
     cp_async_commit();
   }
@@ -2119,7 +2124,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val};
 }
 
@@ -2227,6 +2232,9 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.slab_stride = c->slab_nent;
   p.slab_maxq = c->slab_maxbin;
   p.slab_maxp = (c->n_slab_spec + 1) / 2;
+  p.slab_rowslot = c->blocked_ok ? c->slab_rowslot.as<int>() : nullptr;
+  p.slab_fac = c->slab_fac.as<double>();
+  p.slab_nslots = c->slab_nslots;
   p.fd_cnt = c->fd_cnt.as<int>();
   p.fd_off = c->fd_off.as<int>();
   p.fd_val = c->fd_val.as<double>();
@@ -2327,6 +2335,7 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
     if (ckpt && every > 0 && k % every == 0)
       cudaMemcpyAsync(ckpt + (size_t)(k / every) * n * p.ld, X, sbytes, cudaMemcpyDeviceToDevice, st);
     p.step = k;
+    p.step_w = c->h_win[k];
     p.ncols = n_active[k];
     if (p.ncols == 0) continue;
     if (!prepared) {  // row factors of the first active step; later steps get them from stage 2
@@ -2798,7 +2807,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   int64_t band_nnz = 0, slab_nnz = 0;
   std::vector<int32_t> qbase((size_t)d + 1, 0), wrp((size_t)d * (kSlabWarps + 1), 0), spairs;
   std::vector<unsigned long long> squad;
-  std::vector<int32_t> sslot((size_t)std::max<int64_t>(R, 1), -1);
+  std::vector<int32_t> sslot((size_t)std::max<int64_t>(R, 1), -1), rowslot((size_t)n, -1);
   int32_t maxbin = 0;
   bool quads_fit = nsp < (1 << 16);
   {
@@ -2845,6 +2854,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
             if (q0 >= (1 << 15) || nq[i] >= (1 << 16)) quads_fit = false;
             pr[hf] = sspec[i];
             pr[2 + hf] = (int32_t)((q0 << 16) | nq[i]);
+            rowslot[r] = (int32_t)(spairs.size() / 2 + hf);  // pair index * 2 + half
           }
           spairs.insert(spairs.end(), pr, pr + 4);
         }
@@ -2886,6 +2896,10 @@ int pb_set_layout(pb_context* c, int32_t d) {
   if ((rc = upload(c, c->slab_sidx, squad.data(), squad.size()))) return rc;
   if ((rc = upload(c, c->slab_pairs, spairs.data(), spairs.size()))) return rc;
   if ((rc = upload(c, c->slab_wrp, wrp.data(), wrp.size()))) return rc;
+  if ((rc = upload(c, c->slab_rowslot, rowslot.data(), rowslot.size()))) return rc;
+  c->slab_nslots = (int64_t)(spairs.size() / 2);
+  PB_CUDA(c, c->slab_fac.ensure((size_t)2 * 3 * c->slab_nslots * sizeof(double)));
+  PB_CUDA(c, cudaMemsetAsync(c->slab_fac.p, 0, (size_t)2 * 3 * c->slab_nslots * sizeof(double), c->stream));
   if ((rc = upload(c, c->slab_slot, sslot.data(), sslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   for (const void* fn : {(const void*)k_slab<1, false>, (const void*)k_slab<2, false>, (const void*)k_slab<1, true>,
@@ -2985,6 +2999,7 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
   memset(&p, 0, sizeof(p));
   fill_step_params(c, p, K, ld, flags, pair, inj, c->last_S, ld / kColTile);
   p.step = step;
+  p.step_w = c->h_win[step];
   p.ncols = c->h_nact[step];
   p.src = stage == 1 ? c->X.as<double>() : c->A.as<double>();
   p.x = c->X.as<double>();
