@@ -147,7 +147,8 @@ struct pb_context {
   std::vector<int32_t> h_d_indices;
   std::vector<double> h_d_vals;
   bool fd_tab_ok = false;
-  DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp;
+  DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp, fd_dense;
+  bool fd_dense_ok = false;         // the stencil fits k_fd_dense's halo
   // transposed bin-blocked structures of the adjoint sweep (one band pair)
   bool blockedT_ok = false, fdT_ok = false;
   DBuf bandT_slot, slabT_rp, slabT_offs, slabT_slot, bandT_vals, slabT_vals, fdT_cnt, fdT_off, fdT_val;
@@ -616,6 +617,7 @@ struct StepParams {
   const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
   const int* fd_off;
   const double* fd_val;
+  const double* fd_dense;   // [d][kFdDenseW] stencil weights of offsets -kFdHalo..kFdHalo (k_fd_dense)
   double* fdbuf;            // n x ld: D_off (kappa v) of the stage
   double* fdkp;             // n x ld: D_off (kappa_pair v), adjoint record pass with the photon scale, or null
   const int* band_spec;     // species with cross-bin coupling rows
@@ -1010,6 +1012,9 @@ __global__ void __launch_bounds__(256) k_step_multi(StepParams p) {
 // k_band (second stream) || k_fd -> k_slab, then k_band_finish.
 // ---------------------------------------------------------------------------
 constexpr int kFdMax = 4;           // off-diagonal FD stencil entries per row (bin-blocked path)
+constexpr int kFdHalo = 3;          // k_fd_dense: stencil offsets within +-kFdHalo bins
+constexpr int kFdDenseW = 8;        // dense weights per bin (2 kFdHalo + 1, padded to 16 bytes)
+constexpr int kFdChunk = 12;        // k_fd_dense: bins per warp pass
 constexpr int kSlabThreads = 512;
 constexpr int kMaxBandGroups = 64;
 
@@ -1060,6 +1065,59 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
 #pragma unroll
       for (int t = 0; t < kFdMax; ++t) sK += fv[t] * (kpb[e + fo[t]] * vb[(e + fo[t]) * kColTile + lane]);
       p.fdkp[((size_t)sp * d + e) * ld + col] = sK;
+    }
+  }
+}
+
+// fdbuf = D_off (kappa v), register-blocked.  CTA = (species block, 32-column
+// tile), lane = column: the block's d x 32 states, its kappa and the dense
+// stencil weights go to shared memory; a warp then takes kFdChunk consecutive
+// bins, holds kappa x of those bins and kFdHalo neighbours on each side in
+// registers (zeros outside the block) and applies the dense stencil in
+// ascending offset order.  The zero weights of absent offsets add exact zeros,
+// so every row's sum equals the CSR-order sum of k_fd.
+__global__ void __launch_bounds__(256) k_fd_dense(StepParams p) {
+  extern __shared__ double fsm[];
+  const int sp = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int d = p.d, ld = p.ld;
+  const int col = blockIdx.y * kColTile + lane;  // < ld
+  double* vb = fsm;                              // d x 32
+  double* wt = vb + (size_t)d * kColTile;        // d x kFdDenseW
+  double* kb = wt + (size_t)d * kFdDenseW;       // d
+  const size_t o0 = (size_t)(p.step & 1) * p.n + (size_t)sp * d;
+  const double* __restrict__ v = p.src + (size_t)sp * d * ld + blockIdx.y * kColTile;
+  for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
+    const int e = t / (kColTile / 2), c = 2 * (t - e * (kColTile / 2));
+    cp_async16(vb + e * kColTile + c, v + (size_t)e * ld + c);
+  }
+  for (int t = threadIdx.x; t < d * (kFdDenseW / 2); t += blockDim.x) cp_async16(wt + 2 * t, p.fd_dense + 2 * t);
+  cp_async_commit();
+  for (int e = threadIdx.x; e < d; e += blockDim.x) kb[e] = p.kap[o0 + e];
+  cp_async_wait<0>();
+  __syncthreads();
+  double* __restrict__ out = p.fdbuf + (size_t)sp * d * ld + col;
+  constexpr int U = kFdChunk + 2 * kFdHalo;
+  for (int c0 = wid * kFdChunk; c0 < d; c0 += (blockDim.x >> 5) * kFdChunk) {
+    double u[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = c0 - kFdHalo + i;
+      u[i] = (e >= 0 && e < d) ? __dmul_rn(kb[e], vb[e * kColTile + lane]) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < kFdChunk; ++i) {
+      const int e = c0 + i;
+      if (e >= d) break;
+      const double2* w2 = reinterpret_cast<const double2*>(wt + e * kFdDenseW);
+      const double2 wa = w2[0], wb = w2[1], wc = w2[2], wd = w2[3];
+      double sD = __dmul_rn(wa.x, u[i]);
+      sD = __dadd_rn(sD, __dmul_rn(wa.y, u[i + 1]));
+      sD = __dadd_rn(sD, __dmul_rn(wb.x, u[i + 2]));
+      sD = __dadd_rn(sD, __dmul_rn(wb.y, u[i + 3]));
+      sD = __dadd_rn(sD, __dmul_rn(wc.x, u[i + 4]));
+      sD = __dadd_rn(sD, __dmul_rn(wc.y, u[i + 5]));
+      sD = __dadd_rn(sD, __dmul_rn(wd.x, u[i + 6]));
+      out[(size_t)e * ld] = sD;
     }
   }
 }
@@ -2124,7 +2182,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fdbuf,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val};
 }
 
@@ -2238,6 +2296,7 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.fd_cnt = c->fd_cnt.as<int>();
   p.fd_off = c->fd_off.as<int>();
   p.fd_val = c->fd_val.as<double>();
+  p.fd_dense = c->fd_dense.as<double>();
   p.fdbuf = c->fdbuf.as<double>();
   p.band_spec = c->band_spec.as<int>();
   p.nb = c->band_nb;
@@ -2277,7 +2336,9 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   }
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
   if (kap) {
-    k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
+    if (c->fd_dense_ok && !p.fdkp)
+      k_fd_dense<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + kFdDenseW + 1) * sizeof(double), st>>>(p);
+    else k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
     ++launches;
   }
   const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
@@ -2613,7 +2674,28 @@ static int build_fd_table(pb_context* c) {
       tval[(size_t)cidx * kFdTMax + tcnt[cidx]] = val[(size_t)e * kFdMax + t];
       ++tcnt[cidx];
     }
+  // dense form for k_fd_dense: weights of offsets -kFdHalo..kFdHalo per bin (zeros
+  // where the stencil has no term), usable when the terms are in ascending
+  // offset order within the halo
+  std::vector<double> dense((size_t)d * kFdDenseW, 0.0);
+  bool dense_ok = true;
+  for (int e = 0; e < d && dense_ok; ++e)
+    for (int t = 0; t < cnt[e]; ++t) {
+      const int o = off[(size_t)e * kFdMax + t];
+      if (o < -kFdHalo || o > kFdHalo || o == 0 || (t > 0 && o <= off[(size_t)e * kFdMax + t - 1])) {
+        dense_ok = false;
+        break;
+      }
+      dense[(size_t)e * kFdDenseW + o + kFdHalo] = val[(size_t)e * kFdMax + t];
+    }
+  // k_fd_dense's shared memory stays within the default 48 KB dynamic limit
+  dense_ok = dense_ok && (size_t)d * (kColTile + kFdDenseW + 1) * sizeof(double) <= 48 * 1024;
   int rc;
+  c->fd_dense_ok = false;
+  if (dense_ok) {
+    if ((rc = upload(c, c->fd_dense, dense.data(), dense.size()))) return rc;
+    c->fd_dense_ok = true;
+  }
   if ((rc = upload(c, c->fd_cnt, cnt.data(), cnt.size()))) return rc;
   if ((rc = upload(c, c->fd_off, off.data(), off.size()))) return rc;
   if ((rc = upload(c, c->fd_val, val.data(), val.size()))) return rc;
@@ -3019,7 +3101,11 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
     if (!runs) continue;
     for (int r = -1; r < reps; ++r) {  // one untimed launch first
       PB_CUDA(c, cudaEventRecord(c->ev0, st));
-      if (kk == 0) k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
+      if (kk == 0) {
+        if (c->fd_dense_ok)
+          k_fd_dense<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + kFdDenseW + 1) * sizeof(double), st>>>(p);
+        else k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
+      }
       if (kk == 1) {
         const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
         if (stage == 1) k_slab<1, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
