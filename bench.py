@@ -278,7 +278,7 @@ def run_b200(args, dist, rank, ws, local):
 # DRAM bytes per launch (dram__bytes read + write) of each stage kernel in one
 # ncu capture of this workload at K = 512 (bench.py --z-range 0.05,0.05,
 # -s 4 -c 1 per kernel); the capture is repeated after kernel changes.
-NCU_TRAFFIC_K512 = {"k_slab": 533e6, "k_band": 171e6, "k_fd": 227e6}
+NCU_TRAFFIC_K512 = {"k_slab": 524e6, "k_band": 170e6, "k_fd_dense": 228e6, "k_fd": 227e6}
 
 
 def kernel_rooflines(solver, run, sched, n_active, n_inj):
@@ -289,7 +289,8 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
     (``pb_profile_stage``); achieved = algorithmic bytes (or useful FP64 flops)
     per launch / mean launch time.  Algorithmic bytes per launch, K columns,
     n states, ns bin-local rows, E entries of the bin-local rows:
-      k_fd          read v and kappa, write D_off (kappa v):  16 n K + 8 n
+      k_fd_dense    read v and kappa, write D_off (kappa v):  16 n K + 8 n
+                    (k_fd, the table-driven form, where the stencil does not fit)
       k_slab        read v (all rows), entries (12 E), FD term, row factors;
                     stage 1 writes a and F(x), stage 2 reads F(x), writes x:
                     8 n K + 12 E + 24 ns K + 24 ns
@@ -312,12 +313,13 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
     ms = [(a + b) / 2 for a, b in zip(t1, t2)]
     hbm, hbm_kind = _peaks()
     fp64 = ctx.fp64_peak()
+    fd_name = "k_fd_dense" if ctx.info(_lib.PB_INFO_FD_DENSE) else "k_fd"
     kb = {
-        "k_fd": 16.0 * n * K + 8.0 * n,
+        fd_name: 16.0 * n * K + 8.0 * n,
         "k_slab": 8.0 * n * K + 12.0 * nent + 24.0 * ns * K + 24.0 * ns,
     }
     kernels = []
-    for name, t in (("k_fd", ms[0]), ("k_slab", ms[1])):
+    for name, t in ((fd_name, ms[0]), ("k_slab", ms[1])):
         if t > 0:
             a = kb[name] / (t * 1e-3) / 1e9
             kernels.append({"kernel": name, "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",

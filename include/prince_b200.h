@@ -47,6 +47,7 @@ extern "C" {
 #define PB_INFO_BAND_ENTRIES 5   /* off-diagonal coupling entries of the band rows */
 #define PB_INFO_SLAB_ENTRIES 6   /* off-diagonal coupling entries of the bin-local rows */
 #define PB_INFO_SLAB_ROWS 7      /* bin-local rows */
+#define PB_INFO_FD_DENSE 8       /* 1 if the forward FD term runs the register-blocked dense stencil */
 
 typedef struct pb_context pb_context;
 

@@ -604,7 +604,7 @@ struct StepParams {
   const int* slab_spec;     // species whose coupling rows are bin-local
   int n_slab_spec;
   const int* slab_qbase;    // [d + 1] first entry quad of each bin (even)
-  const unsigned long long* slab_q;  // per quad: the 4 entries' mother species, 16 bits each
+  const unsigned long long* slab_q;  // per quad: byte offsets of the 4 entries' mother rows in k_slab's slab, 16 bits each
   const int4* slab_pairs;   // row pairs of k_slab's warps: species A, B (-1: none), q0 << 16 | quads of A, of B
   const int* slab_wrp;      // [d][kSlabWarps + 1] first pair of each warp of a bin's CTA
   const double* slab_vals;  // [W][slab_stride] M_off values of the quads (4 per quad, zero padding)
@@ -1189,7 +1189,7 @@ __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalar
 }
 
 // k_slab's shared memory: the state slab of one bin (nsp x 16 columns), the
-// bin's entry values (4 per quad), mother species (4 x 16 bits per quad), row
+// bin's entry values (4 per quad), mother-row byte offsets (4 x 16 bits per quad), row
 // pairs and the row factors (eD, phi1, phi2) of each pair slot.  Every block
 // starts on a 16-byte boundary (the quad count of a bin is even).
 constexpr int kSlabCols = 16;       // state columns of a k_slab CTA (a half-warp per row)
@@ -1308,13 +1308,14 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
       double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
       if (sp >= 0 && s.photohad) {
         const int q0 = qq >> 16, q1 = q0 + (qq & 0xffff);
+#pragma unroll 2
         for (int q = q0; q < q1; ++q) {
           const double2 va = vq[2 * q], vb = vq[2 * q + 1];
           const unsigned long long m = L.sidx[q];
-          const double x0 = *reinterpret_cast<const double*>(slb + (((unsigned)m & 0xffffu) << 7));
-          const double x1 = *reinterpret_cast<const double*>(slb + (((unsigned)(m >> 16) & 0xffffu) << 7));
-          const double x2 = *reinterpret_cast<const double*>(slb + (((unsigned)(m >> 32) & 0xffffu) << 7));
-          const double x3 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 48) << 7));
+          const double x0 = *reinterpret_cast<const double*>(slb + ((unsigned)m & 0xffffu));
+          const double x1 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 16) & 0xffffu));
+          const double x2 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 32) & 0xffffu));
+          const double x3 = *reinterpret_cast<const double*>(slb + (unsigned)(m >> 48));
           acc0 = __fma_rn(va.x, x0, acc0);
           acc1 = __fma_rn(va.y, x1, acc1);
           acc2 = __fma_rn(vb.x, x2, acc2);
@@ -2891,7 +2892,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   std::vector<unsigned long long> squad;
   std::vector<int32_t> sslot((size_t)std::max<int64_t>(R, 1), -1), rowslot((size_t)n, -1);
   int32_t maxbin = 0;
-  bool quads_fit = nsp < (1 << 16);
+  bool quads_fit = (size_t)nsp * kSlabCols * sizeof(double) <= (1 << 16);  // 16-bit slab byte offsets
   {
     std::vector<int32_t> nq(nss), order(nss);
     std::vector<std::vector<int32_t>> wl(kSlabWarps);
@@ -2927,12 +2928,12 @@ int pb_set_layout(pb_context* c, int32_t d) {
               if (ix[j] == r) continue;
               if (t == 0) pad_sp = ix[j] / d;
               if (t % 4 == 0) squad.push_back(0);
-              squad.back() |= (unsigned long long)(ix[j] / d) << (16 * (t % 4));
+              squad.back() |= (unsigned long long)((ix[j] / d) * kSlabCols * sizeof(double)) << (16 * (t % 4));
               sslot[j] = (int32_t)((squad.size() - 1) * 4 + t % 4);
               ++slab_nnz;
               ++t;
             }
-            for (; t % 4; ++t) squad.back() |= (unsigned long long)pad_sp << (16 * (t % 4));
+            for (; t % 4; ++t) squad.back() |= (unsigned long long)(pad_sp * kSlabCols * sizeof(double)) << (16 * (t % 4));
             if (q0 >= (1 << 15) || nq[i] >= (1 << 16)) quads_fit = false;
             pr[hf] = sspec[i];
             pr[2 + hf] = (int32_t)((q0 << 16) | nq[i]);
@@ -3188,6 +3189,7 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
     case PB_INFO_BAND_ENTRIES: *value = c->band_nnz; return PB_OK;
     case PB_INFO_SLAB_ENTRIES: *value = c->slab_nnz; return PB_OK;
     case PB_INFO_SLAB_ROWS: *value = (int64_t)c->n_slab_spec * c->lay_d; return PB_OK;
+    case PB_INFO_FD_DENSE: *value = c->fd_dense_ok ? 1 : 0; return PB_OK;
   }
   return fail(c, PB_ERR_ARG, "pb_get_info: unknown key %d", key);
 }
