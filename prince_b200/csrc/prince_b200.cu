@@ -1075,7 +1075,9 @@ __global__ void __launch_bounds__(256) k_fd(StepParams p) {
 // bins, holds kappa x of those bins and kFdHalo neighbours on each side in
 // registers (zeros outside the block) and applies the dense stencil in
 // ascending offset order.  The zero weights of absent offsets add exact zeros,
-// so every row's sum equals the CSR-order sum of k_fd.
+// so every row's sum equals the CSR-order sum of k_fd.  KP: the adjoint's
+// record pass also needs D_off (kappa_pair v) of the step's window (fdkp).
+template <bool KP>
 __global__ void __launch_bounds__(256) k_fd_dense(StepParams p) {
   extern __shared__ double fsm[];
   const int sp = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1084,6 +1086,7 @@ __global__ void __launch_bounds__(256) k_fd_dense(StepParams p) {
   double* vb = fsm;                              // d x 32
   double* wt = vb + (size_t)d * kColTile;        // d x kFdDenseW
   double* kb = wt + (size_t)d * kFdDenseW;       // d
+  double* kpb = kb + d;                          // d: kappa_pair of the window (KP)
   const size_t o0 = (size_t)(p.step & 1) * p.n + (size_t)sp * d;
   const double* __restrict__ v = p.src + (size_t)sp * d * ld + blockIdx.y * kColTile;
   for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
@@ -1093,31 +1096,37 @@ __global__ void __launch_bounds__(256) k_fd_dense(StepParams p) {
   for (int t = threadIdx.x; t < d * (kFdDenseW / 2); t += blockDim.x) cp_async16(wt + 2 * t, p.fd_dense + 2 * t);
   cp_async_commit();
   for (int e = threadIdx.x; e < d; e += blockDim.x) kb[e] = p.kap[o0 + e];
+  if (KP)
+    for (int e = threadIdx.x; e < d; e += blockDim.x) kpb[e] = p.kp[(size_t)p.step_w * p.n + (size_t)sp * d + e];
   cp_async_wait<0>();
   __syncthreads();
-  double* __restrict__ out = p.fdbuf + (size_t)sp * d * ld + col;
   constexpr int U = kFdChunk + 2 * kFdHalo;
   for (int c0 = wid * kFdChunk; c0 < d; c0 += (blockDim.x >> 5) * kFdChunk) {
-    double u[U];
+#pragma unroll 1
+    for (int pass = 0; pass < (KP ? 2 : 1); ++pass) {  // pass 1: kappa_pair into fdkp
+      const double* kk = pass ? kpb : kb;
+      double* __restrict__ out = (pass ? p.fdkp : p.fdbuf) + (size_t)sp * d * ld + col;
+      double u[U];
 #pragma unroll
-    for (int i = 0; i < U; ++i) {
-      const int e = c0 - kFdHalo + i;
-      u[i] = (e >= 0 && e < d) ? __dmul_rn(kb[e], vb[e * kColTile + lane]) : 0.0;
-    }
+      for (int i = 0; i < U; ++i) {
+        const int e = c0 - kFdHalo + i;
+        u[i] = (e >= 0 && e < d) ? __dmul_rn(kk[e], vb[e * kColTile + lane]) : 0.0;
+      }
 #pragma unroll
-    for (int i = 0; i < kFdChunk; ++i) {
-      const int e = c0 + i;
-      if (e >= d) break;
-      const double2* w2 = reinterpret_cast<const double2*>(wt + e * kFdDenseW);
-      const double2 wa = w2[0], wb = w2[1], wc = w2[2], wd = w2[3];
-      double sD = __dmul_rn(wa.x, u[i]);
-      sD = __dadd_rn(sD, __dmul_rn(wa.y, u[i + 1]));
-      sD = __dadd_rn(sD, __dmul_rn(wb.x, u[i + 2]));
-      sD = __dadd_rn(sD, __dmul_rn(wb.y, u[i + 3]));
-      sD = __dadd_rn(sD, __dmul_rn(wc.x, u[i + 4]));
-      sD = __dadd_rn(sD, __dmul_rn(wc.y, u[i + 5]));
-      sD = __dadd_rn(sD, __dmul_rn(wd.x, u[i + 6]));
-      out[(size_t)e * ld] = sD;
+      for (int i = 0; i < kFdChunk; ++i) {
+        const int e = c0 + i;
+        if (e >= d) break;
+        const double2* w2 = reinterpret_cast<const double2*>(wt + e * kFdDenseW);
+        const double2 wa = w2[0], wb = w2[1], wc = w2[2], wd = w2[3];
+        double sD = __dmul_rn(wa.x, u[i]);
+        sD = __dadd_rn(sD, __dmul_rn(wa.y, u[i + 1]));
+        sD = __dadd_rn(sD, __dmul_rn(wb.x, u[i + 2]));
+        sD = __dadd_rn(sD, __dmul_rn(wb.y, u[i + 3]));
+        sD = __dadd_rn(sD, __dmul_rn(wc.x, u[i + 4]));
+        sD = __dadd_rn(sD, __dmul_rn(wc.y, u[i + 5]));
+        sD = __dadd_rn(sD, __dmul_rn(wd.x, u[i + 6]));
+        out[(size_t)e * ld] = sD;
+      }
     }
   }
 }
@@ -1221,11 +1230,12 @@ struct SlabSmem {
 // layout is built), sums each row from shared memory (four accumulators, one
 // per quad position) and applies the stage update.  The row's FD term
 // (fdbuf), F(x) in stage 2 and its injection slot are loaded kSlabPre pairs
-// ahead into registers.  REC: the adjoint's record pass (P / Q sensitivities).
+// ahead into registers.  REC: the adjoint's record pass (P / Q sensitivities);
+// its row and (row, column) inputs are loaded with the others, a pair less ahead.
 // Offsets into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at
 // launch).
 template <int STAGE, bool REC>
-__global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParams p) {
+__global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   extern __shared__ double sm[];
   const int e = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1262,8 +1272,13 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
   }
   const int w0 = p.slab_wrp[e * (kSlabWarps + 1) + wid], w1 = p.slab_wrp[e * (kSlabWarps + 1) + wid + 1];
   const bool need_fd = s.kap, need_f = STAGE == 2;
-  double fdr[kSlabPre], fxr[kSlabPre];
-  int slr[kSlabPre];
+  constexpr int PRE = REC ? kSlabPre - 1 : kSlabPre;  // the record inputs take registers too
+  double fdr[PRE], fxr[PRE];
+  int slr[PRE];
+  // record pass: dsigma and phi1' / phi2' of the row, D_off (kappa_pair v) and S x of (row, column)
+  const int64_t rj = p.step - p.rec_k0;
+  const bool rec_on = REC && rj >= 0 && rj < p.rec_len;
+  double rds[PRE], rd12[PRE], rkp[PRE], rsx[PRE];
   // the FD term, F(x) and injection slot of pair pi's row (staged: the pair
   // comes from shared memory; the first pairs are read from global memory)
 #define PB_SLAB_LOAD(U, PI, PR)                                              \
@@ -1279,11 +1294,17 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
         if (need_fd) fdr[U] = p.fdbuf[r_ * ld + col];                        \
         if (need_f) fxr[U] = p.f[r_ * ld + col];                             \
         if (s.inj) slr[U] = p.inj_slot[r_];                                  \
+        if (rec_on) {                                                        \
+          rds[U] = p.dsig[o0 + r_];                                          \
+          rd12[U] = STAGE == 1 ? p.dphi1[o0 + r_] : p.dphi2[o0 + r_];        \
+          rkp[U] = (s.kap && s.pair) ? p.fdkp[r_ * ld + col] : 0.0;          \
+          rsx[U] = STAGE == 2 ? p.rec_sx[r_ * ld + col] : 0.0;               \
+        }                                                                    \
       }                                                                      \
     }                                                                        \
   } while (0)
 #pragma unroll
-  for (int u = 0; u < kSlabPre; ++u) PB_SLAB_LOAD(u, w0 + u, __ldg(p.slab_pairs + w0 + u));
+  for (int u = 0; u < PRE; ++u) PB_SLAB_LOAD(u, w0 + u, __ldg(p.slab_pairs + w0 + u));
   int src0 = 0, src1 = 0;
   if (s.inj && active) {
     src0 = p.src_ptr[col];
@@ -1294,17 +1315,15 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
 
   const char* slb = reinterpret_cast<const char*>(L.slab + c);
   const double2* vq = reinterpret_cast<const double2*>(L.vals);
-  for (int pb = w0; pb < w1; pb += kSlabPre) {
+  for (int pb = w0; pb < w1; pb += PRE) {
 #pragma unroll
-    for (int u = 0; u < kSlabPre; ++u) {
+    for (int u = 0; u < PRE; ++u) {
       const int pi = pb + u;
       if (pi >= w1) break;
       const int4 pr = L.pairs[pi - pb0];
       const int sp = half ? pr.y : pr.x;
       const int qq = half ? pr.w : pr.z;
       const int r = sp * d + e;
-      RecIn rin{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
-      if (REC && sp >= 0) rin = rec_load<STAGE>(p, s, r, col);
       double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
       if (sp >= 0 && s.photohad) {
         const int q0 = qq >> 16, q1 = q0 + (qq & 0xffff);
@@ -1343,7 +1362,11 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
         const double own = L.slab[sp * kSlabCols + c];
         const int slot = 2 * (pi - pb0) + half;
         const int ro = r * ld + col;
-        if (REC) record_pre<STAGE>(p, s, r, col, sM, out, own, fxr[u], rin);
+        if (rec_on) {
+          const RecIn rin{rds[u], rd12[u], STAGE == 1 ? L.fac[slot] : L.fac[2 * fs + slot], L.fac[fs + slot], rkp[u],
+                          rsx[u], true};
+          record_pre<STAGE>(p, s, r, col, sM, out, own, fxr[u], rin);
+        }
         if (STAGE == 1) {
           // a = eD x + (phi1 F(x)) h
           p.a[ro] = __dadd_rn(__dmul_rn(L.fac[slot], own), __dmul_rn(__dmul_rn(L.fac[fs + slot], out), s.h));
@@ -1354,7 +1377,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, REC ? 1 : 2) k_slab(StepParam
           p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * fs + slot]));
         }
       }
-      const int pn = pi + kSlabPre;
+      const int pn = pi + PRE;
       PB_SLAB_LOAD(u, pn, L.pairs[pn - pb0]);
     }
   }
@@ -2337,8 +2360,9 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   }
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
   if (kap) {
-    if (c->fd_dense_ok && !p.fdkp)
-      k_fd_dense<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + kFdDenseW + 1) * sizeof(double), st>>>(p);
+    const size_t fsmem = (size_t)p.d * (kColTile + kFdDenseW + 2) * sizeof(double);
+    if (c->fd_dense_ok && p.fdkp) k_fd_dense<true><<<dim3(p.nsp, tiles), 256, fsmem, st>>>(p);
+    else if (c->fd_dense_ok) k_fd_dense<false><<<dim3(p.nsp, tiles), 256, fsmem, st>>>(p);
     else k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
     ++launches;
   }
@@ -2690,7 +2714,7 @@ static int build_fd_table(pb_context* c) {
       dense[(size_t)e * kFdDenseW + o + kFdHalo] = val[(size_t)e * kFdMax + t];
     }
   // k_fd_dense's shared memory stays within the default 48 KB dynamic limit
-  dense_ok = dense_ok && (size_t)d * (kColTile + kFdDenseW + 1) * sizeof(double) <= 48 * 1024;
+  dense_ok = dense_ok && (size_t)d * (kColTile + kFdDenseW + 2) * sizeof(double) <= 48 * 1024;
   int rc;
   c->fd_dense_ok = false;
   if (dense_ok) {
@@ -3104,7 +3128,7 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
       PB_CUDA(c, cudaEventRecord(c->ev0, st));
       if (kk == 0) {
         if (c->fd_dense_ok)
-          k_fd_dense<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + kFdDenseW + 1) * sizeof(double), st>>>(p);
+          k_fd_dense<false><<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + kFdDenseW + 2) * sizeof(double), st>>>(p);
         else k_fd<<<dim3(p.nsp, tiles), 256, (size_t)p.d * (kColTile + 2) * sizeof(double), st>>>(p);
       }
       if (kk == 1) {
