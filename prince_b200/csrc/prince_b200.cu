@@ -152,6 +152,7 @@ struct pb_context {
   // transposed bin-blocked structures of the adjoint sweep (one band pair)
   bool blockedT_ok = false, fdT_ok = false;
   DBuf bandT_slot, slabT_rp, slabT_offs, slabT_slot, bandT_vals, slabT_vals, fdT_cnt, fdT_off, fdT_val;
+  DBuf slabT_pairs, slabT_wrp;  // slabT_rp: quad base per bin; slabT_offs: quads
   DBuf vbuf, vbuf2, bTbuf, fdTbuf, outcols;
   int64_t slabT_nent = 0;
   int32_t slabT_maxbin = 0;
@@ -1015,7 +1016,6 @@ constexpr int kFdMax = 4;           // off-diagonal FD stencil entries per row (
 constexpr int kFdHalo = 3;          // k_fd_dense: stencil offsets within +-kFdHalo bins
 constexpr int kFdDenseW = 8;        // dense weights per bin (2 kFdHalo + 1, padded to 16 bytes)
 constexpr int kFdChunk = 12;        // k_fd_dense: bins per warp pass
-constexpr int kSlabThreads = 512;
 constexpr int kMaxBandGroups = 64;
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -1642,8 +1642,6 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
 // previous step when its factors are recorded).
 // ---------------------------------------------------------------------------
 constexpr int kFdTMax = 6;          // entries of a column of the FD operator's off-diagonal block
-constexpr int kSlabTRing = 3;       // rows of (band term, FD term, lam'/mu, P, Q) in flight per warp
-constexpr int kSlabTParts = 5;
 
 struct AdjBlk {
   int64_t n;
@@ -1656,11 +1654,14 @@ struct AdjBlk {
   double* fdT;              // n x ld: D_off^T v
   const double* bandT;      // [W][band_stride] transposed band tiles
   int64_t band_stride;
-  const double* slabT;      // [W][slabT_stride] bin-local entries, mother-grouped
+  const double* slabT;      // [W][slabT_stride] bin-local entries by mother row, in quads (zero padding)
   int64_t slabT_stride;
-  const int* slabT_rp;      // [d][nsp] + 1 entry ranges of the mother rows
-  const int* slabT_offs;    // byte offset of each entry's daughter in the v slab
-  int slabT_maxbin;
+  const int* slabT_qbase;   // [d + 1] first quad of each bin (even)
+  const unsigned long long* slabT_q;  // per quad: byte offsets of the 4 daughters' rows in the v slab, 16 bits each
+  const int4* slabT_pairs;  // mother-row pairs of k_slabT's warps (as k_slab's row pairs)
+  const int* slabT_wrp;     // [d][kSlabWarps + 1] first pair of each warp of a bin's CTA
+  int slabT_maxq;           // quads of the largest bin
+  int slabT_maxp;           // row pairs of a bin
   const int* fdT_cnt;       // per bin: entries of the transposed stencil, row offsets, values
   const int* fdT_off;
   const double* fdT_val;
@@ -1811,141 +1812,161 @@ size_t bandT_smem_bytes() {
   return (size_t)2 * (2 * RT * J * 32) * sizeof(double);
 }
 
-// k_slabT's shared memory: the v slab (nsp x 32), the bin's entry values, the
-// rings, then the int tables (entry daughter offsets, entry ranges).
+// k_slabT's shared memory: the v slab of one bin (nsp x 16 columns), the bin's
+// entry values (4 per quad), daughter-row byte offsets (4 x 16 bits per quad)
+// and mother-row pairs.  Every block starts on a 16-byte boundary.
+constexpr int kSlabTPre = 3;        // row pairs whose inputs a warp loads ahead
 struct SlabTSmem {
   double* slab;
   double* vals;
-  double* ring;  // [warp][kSlabTRing][3][32]
-  int* offs;
-  int* rp;
-  __host__ __device__ static size_t bytes(int nsp, int maxbin) {
-    return ((size_t)nsp * kColTile + maxbin + (size_t)(kSlabThreads / 32) * kSlabTRing * kSlabTParts * kColTile) *
-               sizeof(double) +
-           ((size_t)maxbin + nsp + 1) * sizeof(int);
+  unsigned long long* sidx;
+  int4* pairs;
+  __host__ __device__ static size_t bytes(int nsp, int maxq, int maxp) {
+    return (size_t)nsp * kSlabCols * sizeof(double) + (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) +
+           (size_t)maxp * sizeof(int4);
   }
-  __device__ SlabTSmem(double* base, int nsp, int maxbin) {
+  __device__ SlabTSmem(double* base, int nsp, int maxq) {
     slab = base;
-    vals = slab + (size_t)nsp * kColTile;
-    ring = vals + maxbin;
-    offs = reinterpret_cast<int*>(ring + (size_t)(kSlabThreads / 32) * kSlabTRing * kSlabTParts * kColTile);
-    rp = offs + maxbin;
+    vals = slab + (size_t)nsp * kSlabCols;
+    sidx = reinterpret_cast<unsigned long long*>(vals + (size_t)maxq * 4);
+    pairs = reinterpret_cast<int4*>(sidx + maxq);
   }
 };
 
 // Bin-local part of M_off^T v and the adjoint stage update for every row of
-// bin e.  CTA = (bin e, 32-column tile), lane = column; warps take the mother
-// species strided.  The row's band term, FD term and lam' (stage 1) or mu
-// (stage 2) arrive through the warp's cp.async ring.
+// bin e.  CTA = (bin e, 16-column tile); a half-warp owns a mother row, its
+// lane c owns column col0 + c.  The v slab of bin e, the bin's entry quads and
+// row pairs arrive by asynchronous copies; each row is summed from shared
+// memory (four accumulators, one per quad position).  The row's band term, FD
+// term, lam' (stage 1) or mu (stage 2), P and Q, and its recorded factors are
+// loaded kSlabTPre pairs ahead into registers.  Stage 1 reduces the
+// photon-scale gradient of the bin's rows inside the CTA.
 template <int STAGE>
-__global__ void __launch_bounds__(kSlabThreads, 1) k_slabT(AdjBlk q) {
+__global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slabT(AdjBlk q) {
   extern __shared__ double sm[];
   const int nsp = q.nsp, e = blockIdx.x, d = q.d, ld = q.ld;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int col0 = blockIdx.y * kColTile, col = col0 + lane;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int half = lane >> 4, c = lane & 15;
+  const int col0 = blockIdx.y * kSlabCols, col = col0 + c;  // col < ld
   const bool active = col < q.ncols;
-  SlabTSmem L(sm, nsp, q.slabT_maxbin);
-  const int q0 = q.slabT_rp[(size_t)e * nsp], q1 = q.slabT_rp[(size_t)(e + 1) * nsp];  // multiples of 4
+  SlabTSmem L(sm, nsp, q.slabT_maxq);
+  const int qb = q.slabT_qbase[e], nqb = q.slabT_qbase[e + 1] - qb;
+  const int pb0 = q.slabT_wrp[e * (kSlabWarps + 1)], npb = q.slabT_wrp[e * (kSlabWarps + 1) + kSlabWarps] - pb0;
   const bool photohad = (q.flags & PB_PHOTOHAD) != 0, kap = (q.flags & PB_PARTIAL_DIFF) != 0;
   {
     const double* vs = q.v + (size_t)e * ld + col0;
-    for (int t = threadIdx.x; t < nsp * (kColTile / 2); t += blockDim.x) {
-      const int s = t / (kColTile / 2), c = 2 * (t - s * (kColTile / 2));
-      cp_async16(L.slab + s * kColTile + c, vs + (size_t)s * d * ld + c);
+    for (int t = threadIdx.x; t < nsp * (kSlabCols / 2); t += blockDim.x) {
+      const int sp = t / (kSlabCols / 2), cc = 2 * (t - sp * (kSlabCols / 2));
+      cp_async16(L.slab + sp * kSlabCols + cc, vs + (size_t)sp * d * ld + cc);
     }
     if (photohad) {
-      const double* mv = q.slabT + (size_t)q.w * q.slabT_stride + q0;
-      for (int t = threadIdx.x; t < (q1 - q0) / 2; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
-      for (int t = threadIdx.x; t < (q1 - q0) / 4; t += blockDim.x) cp_async16(L.offs + 4 * t, q.slabT_offs + q0 + 4 * t);
+      const double* mv = q.slabT + (size_t)q.w * q.slabT_stride + (size_t)qb * 4;
+      for (int t = threadIdx.x; t < 2 * nqb; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
+      const unsigned long long* mq = q.slabT_q + qb;
+      for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
     }
+    for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, q.slabT_pairs + pb0 + t);
     cp_async_commit();
   }
-  for (int i = threadIdx.x; i <= nsp; i += blockDim.x) L.rp[i] = q.slabT_rp[(size_t)e * nsp + i] - q0;
+  const int w0 = q.slabT_wrp[e * (kSlabWarps + 1) + wid], w1 = q.slabT_wrp[e * (kSlabWarps + 1) + wid + 1];
+  const double* own_src = STAGE == 1 ? q.lam : q.mu;
+  const bool want_pq = STAGE == 1 && q.gs;
+  constexpr int PRE = kSlabTPre;
+  // per pair slot: band term, FD term, own (lam' or mu), P, Q; kappa and the
+  // row factors (stage 1: phi1, phi2; stage 2: eD, phi2 of the previous step)
+  double rb[PRE], rfd[PRE], rown[PRE], rp[PRE], rq[PRE], rk[PRE], rf1[PRE], rf2[PRE];
+  int rsl[PRE];
+#define PB_SLABT_LOAD(U, PI, PR)                                                 \
+  do {                                                                           \
+    if ((PI) < w1) {                                                             \
+      const int4 pr_ = (PR);                                                     \
+      const int sp_ = half ? pr_.y : pr_.x;                                      \
+      if (sp_ >= 0) {                                                            \
+        const int r_ = sp_ * d + e;                                              \
+        const size_t ix_ = (size_t)r_ * ld + col;                                \
+        rb[U] = photohad ? q.bT[ix_] : 0.0;                                      \
+        rfd[U] = kap ? q.fdT[ix_] : 0.0;                                         \
+        rown[U] = own_src[ix_];                                                  \
+        rp[U] = want_pq ? q.P[ix_] : 0.0;                                        \
+        rq[U] = want_pq ? q.Q[ix_] : 0.0;                                        \
+        rk[U] = kap ? q.rf[3 * q.n + r_] : 0.0;                                  \
+        rf1[U] = STAGE == 1 ? q.rf[q.n + r_] : q.rf[r_];                         \
+        rf2[U] = STAGE == 1 ? q.rf[2 * q.n + r_] : (q.rf_prev ? q.rf_prev[2 * q.n + r_] : 0.0); \
+        rsl[U] = (STAGE == 1 && q.gb_inj) ? q.inj_slot[r_] : -1;                 \
+      }                                                                          \
+    }                                                                            \
+  } while (0)
+#pragma unroll
+  for (int u = 0; u < PRE; ++u) PB_SLABT_LOAD(u, w0 + u, __ldg(q.slabT_pairs + w0 + u));
   cp_async_wait<0>();
   __syncthreads();
 
-  double* ring = L.ring + (size_t)wid * kSlabTRing * kSlabTParts * kColTile;
-  const double* own_src = STAGE == 1 ? q.lam : q.mu;
-  const bool want_pq = STAGE == 1 && q.gs;
-  // lanes 0-7 band term (and Q), 8-15 FD term, 16-23 lam' or mu, 24-31 P; 2 x 16 bytes each
-  auto copy_part = [&](int r, int k, int part, const double* src, int c2) {
-    double* dst = ring + ((k % kSlabTRing) * kSlabTParts + part) * kColTile + c2;
-    const size_t o = (size_t)r * ld + col0 + c2;
-    cp_async16(dst, src + o);
-    cp_async16(dst + 2, src + o + 2);
-  };
-  auto fetch = [&](int s, int k) {
-    if (s < nsp) {
-      const int r = s * d + e;
-      const int part = lane >> 3, c2 = 4 * (lane & 7);
-      if (part == 0) copy_part(r, k, 0, q.bT, c2);
-      if (part == 1 && kap) copy_part(r, k, 1, q.fdT, c2);
-      if (part == 2) copy_part(r, k, 2, own_src, c2);
-      if (part == 3 && want_pq) copy_part(r, k, 3, q.P, c2);
-      if (part == 0 && want_pq) copy_part(r, k, 4, q.Q, c2);
-    }
-    cp_async_commit();
-  };
-  double gsa = 0.0;  // this lane's column of the photon-scale gradient over the warp's rows
+  double gsa = 0.0;  // this lane's column of the photon-scale gradient over its rows
+  const char* slb = reinterpret_cast<const char*>(L.slab + c);
+  const double2* vq = reinterpret_cast<const double2*>(L.vals);
+  for (int pb = w0; pb < w1; pb += PRE) {
 #pragma unroll
-  for (int k = 0; k < kSlabTRing; ++k) fetch(wid + k * nw, k);
-  const char* slb = reinterpret_cast<const char*>(L.slab + lane);
-  int k = 0;
-  for (int s = wid; s < nsp; s += nw, ++k) {
-    const int r = s * d + e;
-    double acc0 = 0.0, acc1 = 0.0;
-    if (photohad) {
-      const int j1 = L.rp[s + 1];
-      int j = L.rp[s];
-      for (; j + 1 < j1; j += 2) {
-        acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
-        acc1 = __fma_rn(L.vals[j + 1], *reinterpret_cast<const double*>(slb + L.offs[j + 1]), acc1);
-      }
-      if (j < j1) acc0 = __fma_rn(L.vals[j], *reinterpret_cast<const double*>(slb + L.offs[j]), acc0);
-    }
-    cp_async_wait<kSlabTRing - 1>();
-    __syncwarp();
-    const double* rs = ring + (k % kSlabTRing) * kSlabTParts * kColTile;
-    if (active) {
-      double out = photohad ? (acc0 + acc1) + rs[lane] : 0.0;
-      if (kap) out += q.rf[3 * q.n + r] * rs[kColTile + lane];
-      if (q.lt_indptr) {
-        double sL = 0.0;
-        for (int64_t j = q.lt_indptr[r]; j < q.lt_indptr[r + 1]; ++j)
-          sL += q.lt_vals[j] * q.v[(size_t)q.lt_indices[j] * ld + col];
-        out += sL;
-      }
-      out *= q.dl;
-      const size_t idx = (size_t)r * ld + col;
-      const double own = rs[2 * kColTile + lane];
-      if (STAGE == 1) {
-        const double lam = own;
-        const double mu = lam + q.h * out;
-        q.mu[idx] = mu;
-        if (q.gb_inj) {
-          const int slot = q.inj_slot[r];
-          if (slot >= 0) q.gb_inj[(size_t)slot * ld + col] = q.h * q.rf[q.n + r] * mu;
+    for (int u = 0; u < PRE; ++u) {
+      const int pi = pb + u;
+      if (pi >= w1) break;
+      const int4 pr = L.pairs[pi - pb0];
+      const int sp = half ? pr.y : pr.x;
+      const int qq = half ? pr.w : pr.z;
+      const int r = sp * d + e;
+      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
+      if (sp >= 0 && photohad) {
+        const int qa = qq >> 16, qz = qa + (qq & 0xffff);
+#pragma unroll 2
+        for (int k = qa; k < qz; ++k) {
+          const double2 va = vq[2 * k], vb = vq[2 * k + 1];
+          const unsigned long long m = L.sidx[k];
+          const double x0 = *reinterpret_cast<const double*>(slb + ((unsigned)m & 0xffffu));
+          const double x1 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 16) & 0xffffu));
+          const double x2 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 32) & 0xffffu));
+          const double x3 = *reinterpret_cast<const double*>(slb + (unsigned)(m >> 48));
+          acc0 = __fma_rn(va.x, x0, acc0);
+          acc1 = __fma_rn(va.y, x1, acc1);
+          acc2 = __fma_rn(vb.x, x2, acc2);
+          acc3 = __fma_rn(vb.y, x3, acc3);
         }
-        if (want_pq) gsa += mu * rs[3 * kColTile + lane] + lam * rs[4 * kColTile + lane];
-        q.vout[idx] = q.rf[q.n + r] * mu - q.rf[2 * q.n + r] * lam;
-      } else {
-        const double lam = q.rf[r] * own + q.h * out;
-        q.lam_out[idx] = lam;
-        if (q.rf_prev) q.vout[idx] = q.rf_prev[2 * q.n + r] * lam;
       }
+      if (sp >= 0 && active) {
+        double out = photohad ? ((acc0 + acc1) + (acc2 + acc3)) + rb[u] : 0.0;
+        if (kap) out += rk[u] * rfd[u];
+        if (q.lt_indptr) {
+          double sL = 0.0;
+          for (int64_t j = q.lt_indptr[r]; j < q.lt_indptr[r + 1]; ++j)
+            sL += q.lt_vals[j] * q.v[(size_t)q.lt_indices[j] * ld + col];
+          out += sL;
+        }
+        out *= q.dl;
+        const size_t idx = (size_t)r * ld + col;
+        if (STAGE == 1) {
+          const double lam = rown[u];
+          const double mu = lam + q.h * out;
+          q.mu[idx] = mu;
+          if (rsl[u] >= 0) q.gb_inj[(size_t)rsl[u] * ld + col] = q.h * rf1[u] * mu;
+          if (want_pq) gsa += mu * rp[u] + lam * rq[u];
+          q.vout[idx] = rf1[u] * mu - rf2[u] * lam;
+        } else {
+          const double lam = rf1[u] * rown[u] + q.h * out;
+          q.lam_out[idx] = lam;
+          if (q.rf_prev) q.vout[idx] = rf2[u] * lam;
+        }
+      }
+      const int pn = pi + PRE;
+      PB_SLABT_LOAD(u, pn, L.pairs[pn - pb0]);
     }
-    __syncwarp();
-    fetch(s + kSlabTRing * nw, k + kSlabTRing);
   }
-  cp_async_wait<0>();
-  if (want_pq) {  // the warps' sums for each column, added to the bin's row of gs
+#undef PB_SLABT_LOAD
+  if (want_pq) {  // the half-warps' sums for each column, added to the bin's row of gs
     __syncthreads();
     double* red = L.slab;  // the slab is no longer read
-    red[wid * kColTile + lane] = gsa;
+    red[threadIdx.x] = gsa;
     __syncthreads();
-    if (threadIdx.x < kColTile && col0 + (int)threadIdx.x < q.ncols) {
+    if (threadIdx.x < kSlabCols && col0 + (int)threadIdx.x < q.ncols) {
       double t = 0.0;
-      for (int w = 0; w < nw; ++w) t += red[w * kColTile + threadIdx.x];
+      for (int h = 0; h < 2 * kSlabWarps; ++h) t += red[h * kSlabCols + threadIdx.x];
       q.gs[(size_t)e * ld + col0 + threadIdx.x] += t;
     }
   }
@@ -2207,7 +2228,8 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdbuf,
-          &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val};
+          &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
+          &c->slabT_pairs, &c->slabT_wrp};
 }
 
 // Every device buffer: the solve's and the adjoint's scratch.
@@ -2403,7 +2425,7 @@ void launch_adj_blocked(pb_context* c, AdjBlk& q, cudaStream_t st) {
   }
   if (kap) k_fdT<<<dim3(q.nsp, tiles), 256, (size_t)q.d * kColTile * sizeof(double), st>>>(q);
   if (forked) cudaStreamWaitEvent(st, c->ev_join, 0);
-  k_slabT<STAGE><<<dim3(q.d, tiles), kSlabThreads, c->slabT_smem, st>>>(q);
+  k_slabT<STAGE><<<dim3(q.d, (unsigned)blocks_for(q.ncols, kSlabCols)), kSlabWarps * 32, c->slabT_smem, st>>>(q);
 }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
@@ -3044,44 +3066,90 @@ int pb_set_layout(pb_context* c, int32_t d) {
         btslot[j] = (int32_t)((tile * J + jj) * 32 + (e2 % 8) * 4 + (e % 4));
       }
     }
-  // bin-local entries grouped by mother: (bin, mother species, daughter order)
+  // transposed bin-local rows (mothers), per bin: every species is a row; its
+  // daughter entries in the order (daughter species in k_slab's species order,
+  // CSR order), in quads of 4 (daughter slab byte offsets, zero values pad the
+  // last quad); rows paired for k_slabT's half-warps and the pairs spread over
+  // its warps longest-processing-time first; every bin starts on an even quad.
   std::vector<std::vector<std::pair<int32_t, int64_t>>> bym(nsp);
-  std::vector<int32_t> trp((size_t)d * nsp + 1, 0), toffs, tslot((size_t)std::max<int64_t>(R, 1), -1);
+  std::vector<int32_t> tqbase((size_t)d + 1, 0), twrp((size_t)d * (kSlabWarps + 1), 0), tpairs;
+  std::vector<unsigned long long> tquad;
+  std::vector<int32_t> tslot((size_t)std::max<int64_t>(R, 1), -1);
   int32_t tmax = 0;
-  for (int e = 0; e < d; ++e) {
-    for (auto& v : bym) v.clear();
-    for (int i = 0; i < nss; ++i) {
-      const int64_t r = (int64_t)sspec[i] * d + e;
-      for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
-        if (ix[j] != r) bym[ix[j] / d].push_back({sspec[i], j});
-    }
-    while (toffs.size() % 4) toffs.push_back(0);
-    const size_t b0 = toffs.size();
-    for (int m = 0; m < nsp; ++m) {
-      trp[(size_t)e * nsp + m] = (int32_t)toffs.size();
-      for (auto& pr : bym[m]) {
-        tslot[pr.second] = (int32_t)toffs.size();
-        toffs.push_back(pr.first * kColTile * (int32_t)sizeof(double));  // byte offset in the v slab
+  bool tq_fit = (size_t)nsp * kSlabCols * sizeof(double) <= (1 << 16);
+  {
+    std::vector<int32_t> nqm(nsp), order(nsp);
+    std::vector<std::vector<int32_t>> wl(kSlabWarps);
+    std::vector<int64_t> load(kSlabWarps);
+    for (int e = 0; e < d; ++e) {
+      for (auto& v : bym) v.clear();
+      for (int i = 0; i < nss; ++i) {
+        const int64_t r = (int64_t)sspec[i] * d + e;
+        for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
+          if (ix[j] != r) bym[ix[j] / d].push_back({sspec[i], j});
       }
+      tqbase[e] = (int32_t)tquad.size();
+      for (int m = 0; m < nsp; ++m) {
+        nqm[m] = (int32_t)((bym[m].size() + 3) / 4);
+        order[m] = m;
+      }
+      std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return nqm[a] > nqm[b]; });
+      for (auto& v : wl) v.clear();
+      std::fill(load.begin(), load.end(), 0);
+      for (int k = 0; k < nsp; k += 2) {
+        const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        wl[w].push_back(k);
+        load[w] += nqm[order[k]] + 1;
+      }
+      for (int w = 0; w < kSlabWarps; ++w) {
+        twrp[(size_t)e * (kSlabWarps + 1) + w] = (int32_t)(tpairs.size() / 4);
+        for (int k : wl[w]) {
+          int32_t pr[4] = {-1, -1, 0, 0};
+          for (int hf = 0; hf < 2; ++hf) {
+            if (k + hf >= nsp) continue;
+            const int m = order[k + hf];
+            const int64_t q0 = (int64_t)tquad.size() - tqbase[e];
+            int t = 0;
+            const unsigned long long pad = bym[m].empty() ? 0ull : (unsigned long long)bym[m][0].first * kSlabCols * sizeof(double);
+            for (auto& dj : bym[m]) {
+              if (t % 4 == 0) tquad.push_back(0);
+              tquad.back() |= ((unsigned long long)dj.first * kSlabCols * sizeof(double)) << (16 * (t % 4));
+              tslot[dj.second] = (int32_t)((tquad.size() - 1) * 4 + t % 4);
+              ++t;
+            }
+            for (; t % 4; ++t) tquad.back() |= pad << (16 * (t % 4));
+            if (q0 >= (1 << 15) || nqm[m] >= (1 << 16)) tq_fit = false;
+            pr[hf] = m;
+            pr[2 + hf] = (int32_t)((q0 << 16) | nqm[m]);
+          }
+          tpairs.insert(tpairs.end(), pr, pr + 4);
+        }
+      }
+      twrp[(size_t)e * (kSlabWarps + 1) + kSlabWarps] = (int32_t)(tpairs.size() / 4);
+      if ((tquad.size() - tqbase[e]) % 2) tquad.push_back(0);
+      tmax = std::max<int32_t>(tmax, (int32_t)(tquad.size() - tqbase[e]));
     }
-    size_t b1 = (toffs.size() + 3) & ~(size_t)3;
-    tmax = std::max<int32_t>(tmax, (int32_t)(b1 - b0));
+    tqbase[d] = (int32_t)tquad.size();
+    if (tquad.empty()) tquad.assign(2, 0);
   }
-  while (toffs.size() % 4) toffs.push_back(0);
-  trp[(size_t)d * nsp] = (int32_t)toffs.size();
-  if (toffs.empty()) toffs.assign(4, 0);
-  const size_t tsm = SlabTSmem::bytes(nsp, tmax);
+  if (!tq_fit) return PB_OK;
+  // at least one double per thread: stage 1 reduces the gradient over the slab's space
+  const size_t tsm = std::max(SlabTSmem::bytes(nsp, tmax, (nsp + 1) / 2), (size_t)kSlabWarps * 32 * sizeof(double));
   const BandTInstance bti = bandT_kernel(RT, J);
   if (tsm > max_smem || !bti.fn || bti.smem > max_smem || (size_t)d * kColTile * sizeof(double) > max_smem) return PB_OK;
   if ((rc = upload(c, c->bandT_slot, btslot.data(), btslot.size()))) return rc;
-  if ((rc = upload(c, c->slabT_rp, trp.data(), trp.size()))) return rc;
-  if ((rc = upload(c, c->slabT_offs, toffs.data(), toffs.size()))) return rc;
+  if ((rc = upload(c, c->slabT_rp, tqbase.data(), tqbase.size()))) return rc;
+  if ((rc = upload(c, c->slabT_offs, tquad.data(), tquad.size()))) return rc;
+  if ((rc = upload(c, c->slabT_pairs, tpairs.data(), tpairs.size()))) return rc;
+  if ((rc = upload(c, c->slabT_wrp, twrp.data(), twrp.size()))) return rc;
   if ((rc = upload(c, c->slabT_slot, tslot.data(), tslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slabT<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
-  PB_CUDA(c, cudaFuncSetAttribute(k_slabT<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+  for (const void* fn : {(const void*)k_slabT<1>, (const void*)k_slabT<2>}) {
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
+  }
   PB_CUDA(c, cudaFuncSetAttribute(bti.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bti.smem));
-  c->slabT_nent = (int64_t)toffs.size();
+  c->slabT_nent = (int64_t)tquad.size() * 4;
   c->slabT_maxbin = tmax;
   c->slabT_smem = tsm;
   c->bandT_smem = bti.smem;
@@ -3682,9 +3750,12 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
         q.band_stride = c->band_stride;
         q.slabT = c->slabT_vals.as<double>();
         q.slabT_stride = c->slabT_nent;
-        q.slabT_rp = c->slabT_rp.as<int>();
-        q.slabT_offs = c->slabT_offs.as<int>();
-        q.slabT_maxbin = c->slabT_maxbin;
+        q.slabT_qbase = c->slabT_rp.as<int>();
+        q.slabT_q = c->slabT_offs.as<unsigned long long>();
+        q.slabT_pairs = c->slabT_pairs.as<int4>();
+        q.slabT_wrp = c->slabT_wrp.as<int>();
+        q.slabT_maxq = c->slabT_maxbin;
+        q.slabT_maxp = (c->lay_nsp + 1) / 2;
         q.fdT_cnt = c->fdT_cnt.as<int>();
         q.fdT_off = c->fdT_off.as<int>();
         q.fdT_val = c->fdT_val.as<double>();
