@@ -47,12 +47,17 @@ class CosmicRaySource(metaclass=ABCMeta):
 
     def _compute_injection_grid(self):
         self.injection_grid = np.zeros(self.dim_states)
+        blocks = []
         for pid in self.pdgids:
             sref = self.spec_man.pdgid2sref[int(pid)]
             with np.errstate(divide="ignore", over="ignore", invalid="ignore"):
                 self.injection_grid[sref.sl] = self.injection_spectrum(
                     int(pid), self.cr_grid, self.params[int(pid)]
                 )
+            blocks.append(np.arange(sref.sl.start, sref.sl.stop))
+        # states with a non-zero injection (only the injected species' blocks are written)
+        idx = np.unique(np.concatenate(blocks)) if blocks else np.zeros(0, dtype=np.int64)
+        self.injection_support = idx[self.injection_grid[idx] != 0.0]
 
     def injection_rate(self, z):
         """``norm * evolution(z) * injection_grid`` on the state grid."""

@@ -232,14 +232,16 @@ class DeviceRun:
 # ---------------------------------------------------------------------------
 def _coefficients(sources, zs):
     """(n_steps, n_src) table of norm * evolution(z_k) per source."""
-    out = np.zeros((zs.size, len(sources)))
-    for i, s in enumerate(sources):
+    if not sources:
+        return np.zeros((zs.size, 0))
+    cols = []
+    for s in sources:
         if hasattr(s, "evolution_array"):
             ev = s.evolution_array(zs)
         else:
             ev = np.array([s.evolution(z) for z in zs])
-        out[:, i] = s.norm * ev
-    return out
+        cols.append(s.norm * np.asarray(ev, dtype=np.float64))
+    return np.stack(cols, axis=1)
 
 
 class UHECRPropagationSolverETD2:
@@ -380,11 +382,14 @@ class UHECRPropagationSolverETD2:
         zs = zg[:-1]
         coeff = _coefficients(srcs, zs) if srcs else np.zeros((zs.size, 0))
         grids = [np.asarray(s.injection_grid, dtype=np.float64) for s in srcs]
+        # injected states of each source (sources of this package record them when they build their grid)
+        support = [s.injection_support if getattr(s, "injection_support", None) is not None else np.flatnonzero(g)
+                   for s, g in zip(srcs, grids)]
         use_inj = self.enable_injection_jacobian and len(srcs) > 0
         # first step at which each column receives a non-zero injection
         first = np.full(K, sched.n_steps, dtype=np.int64)
         if use_inj:
-            injects = np.array([bool(np.any(g)) for g in grids])
+            injects = np.array([sp.size > 0 for sp in support])
             live = (coeff != 0.0) & injects[None, :]
             has = live.any(axis=0)
             first_src = np.where(has, live.argmax(axis=0), sched.n_steps)
@@ -396,13 +401,8 @@ class UHECRPropagationSolverETD2:
         src_order = np.argsort(inv[owner], kind="stable") if srcs else np.zeros(0, dtype=np.int64)
         src_col = inv[owner][src_order].astype(np.int32)
         if srcs:
-            nz = np.zeros(self.dim_states, dtype=bool)
-            for g in grids:
-                nz |= g != 0.0
-            rows = np.flatnonzero(nz).astype(np.int32)
-            G = np.empty((rows.size, len(srcs)))
-            for i, si in enumerate(src_order):
-                G[:, i] = grids[si][rows]
+            rows = np.unique(np.concatenate(support)).astype(np.int32)
+            G = np.stack([grids[si][rows] for si in src_order], axis=1)
         else:
             rows, G = np.zeros(0, np.int32), np.zeros((0, 0))
         return sched, K, coeff[:, src_order] if srcs else coeff, rows, G, src_col, n_active, perm, use_inj
