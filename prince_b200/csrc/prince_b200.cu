@@ -21,6 +21,7 @@
 //   src/prince_cr/interaction_rates.py:966-1067 (fold), 1277-1294 (pair loss).
 // The data layout, the kernels and the launch structure are this project's own.
 
+#include <cuda.h>  // CUtensorMap (the encoder is reached through cudaGetDriverEntryPoint)
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 #include <math_constants.h>
@@ -158,10 +159,16 @@ struct pb_context {
   int32_t slabT_maxbin = 0;
   size_t slabT_smem = 0, bandT_smem = 0;
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
+  int32_t tma_mode = 1;             // 1: k_slab stages by TMA when tensor maps can be encoded; 0: cp.async
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int num_sms = 148;
+  DBuf tmaps;                       // [2] CUtensorMap of X and A for k_slab's TMA staging (64-byte aligned)
+  bool tma_ok = false;              // tmaps hold maps of the current X / A / ld
+  bool last_tma = false;            // the last solve staged k_slab by TMA
+  const void* tma_key[3] = {nullptr, nullptr, nullptr};
+  DBuf d_err;                       // int: a bounded wait of a kernel gave up
 
   // EM cascade
   bool have_em = false;
@@ -534,6 +541,8 @@ struct StepParams {
   int ncols;         // active columns this step
   int64_t step;
   int step_w;        // rate window of this step (k_slab's entry values), set with step
+  const CUtensorMap* tmap_src;  // k_slab: tensor map of src for the TMA staging, or null (cp.async staging)
+  int* err;          // set to a nonzero code when a bounded wait gives up
   int64_t n_steps;
   uint32_t flags;
   const double* h;
@@ -1026,6 +1035,47 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// mbarrier and bulk-copy helpers of the TMA staging (CTA-local barrier, no cluster)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `phase` of the barrier, giving up after `tries` polls.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned phase, long long tries) {
+  for (long long i = 0; i < tries; ++i)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+// Tiled 3-D tensor load (x = column, y = bin, z = species) into shared memory.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+// Contiguous bulk copy (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+constexpr long long kWaitTries = 1ll << 24;  // polls of a bounded wait (well above any staging time)
+constexpr int kErrStagingWait = 1;           // err code: a k_slab CTA's staging wait gave up
+
 // fdbuf = D_off (kappa v) for every row.  CTA = (species block, 32-column
 // tile): the block's d x 32 states and its kappa go to shared memory, then a
 // thread per (bin, column) adds the stencil terms in CSR order (the stencil of
@@ -1210,16 +1260,23 @@ struct SlabSmem {
   unsigned long long* sidx;
   int4* pairs;
   double* fac;  // [3][2 maxp]
+  unsigned long long* bar;  // the TMA staging barrier
+  // species rows of the slab, padded to whole TMA boxes of at most 256 species
+  __host__ __device__ static int nbox(int nsp) { return (nsp + 255) / 256; }
+  __host__ __device__ static int box_rows(int nsp) { return (nsp + nbox(nsp) - 1) / nbox(nsp); }
+  __host__ __device__ static int rows(int nsp) { return nbox(nsp) * box_rows(nsp); }
   __host__ __device__ static size_t bytes(int nsp, int maxq, int maxp) {
-    return (size_t)nsp * kSlabCols * sizeof(double) + (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) +
-           (size_t)maxp * (sizeof(int4) + 6 * sizeof(double));
+    return (size_t)rows(nsp) * kSlabCols * sizeof(double) +
+           (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) + (size_t)maxp * (sizeof(int4) + 6 * sizeof(double)) +
+           sizeof(unsigned long long);
   }
   __device__ SlabSmem(double* base, int nsp, int maxq, int maxp) {
     slab = base;
-    vals = slab + (size_t)nsp * kSlabCols;
+    vals = slab + (size_t)rows(nsp) * kSlabCols;
     sidx = reinterpret_cast<unsigned long long*>(vals + (size_t)maxq * 4);
     pairs = reinterpret_cast<int4*>(sidx + maxq);
     fac = reinterpret_cast<double*>(pairs + maxp);
+    bar = reinterpret_cast<unsigned long long*>(fac + 6 * (size_t)maxp);
   }
 };
 
@@ -1236,7 +1293,7 @@ struct SlabSmem {
 // launch).
 template <int STAGE, bool REC>
 __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(128) double sm[];  // TMA boxes land at 128-byte boundaries
   const int e = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int half = lane >> 4, c = lane & 15;
@@ -1250,20 +1307,41 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   const int qb = p.slab_qbase[e], nqb = p.slab_qbase[e + 1] - qb;
   const int pb0 = p.slab_wrp[e * (kSlabWarps + 1)], npb = p.slab_wrp[e * (kSlabWarps + 1) + kSlabWarps] - pb0;
   const int fs = 2 * p.slab_maxp;  // stride of the three row-factor arrays
-  {
+  unsigned long long* stage_bar = L.bar;
+  const double* mv = p.slab_vals + (size_t)p.step_w * p.slab_stride + (size_t)qb * 4;
+  const double* fc = p.slab_fac + (size_t)(p.step & 1) * 3 * p.slab_nslots + 2 * (size_t)pb0;
+  if (p.tmap_src) {  // TMA: the slab as tensor boxes, the rest as bulk copies, one barrier
+    if (threadIdx.x == 0) mbar_init(stage_bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nb = SlabSmem::nbox(p.nsp), br = SlabSmem::box_rows(p.nsp);
+      unsigned bytes = (unsigned)(nb * br * kSlabCols * sizeof(double)) + (unsigned)(npb * sizeof(int4)) +
+                       (unsigned)(6 * npb * sizeof(double));
+      if (s.photohad) bytes += (unsigned)(nqb * (4 * sizeof(double) + sizeof(unsigned long long)));
+      mbar_expect_tx(stage_bar, bytes);
+      for (int b = 0; b < nb; ++b) tma_load_3d(L.slab + (size_t)b * br * kSlabCols, p.tmap_src, col0, e, b * br, stage_bar);
+      if (s.photohad && nqb > 0) {
+        bulk_load(L.vals, mv, (unsigned)(nqb * 4 * sizeof(double)), stage_bar);
+        bulk_load(L.sidx, p.slab_q + qb, (unsigned)(nqb * sizeof(unsigned long long)), stage_bar);
+      }
+      if (npb > 0) {
+        bulk_load(L.pairs, p.slab_pairs + pb0, (unsigned)(npb * sizeof(int4)), stage_bar);
+        for (int k = 0; k < 3; ++k)
+          bulk_load(L.fac + k * fs, fc + (size_t)k * p.slab_nslots, (unsigned)(2 * npb * sizeof(double)), stage_bar);
+      }
+    }
+  } else {
     const double* vs = p.src + (size_t)e * ld + col0;
     for (int t = threadIdx.x; t < p.nsp * (kSlabCols / 2); t += blockDim.x) {
       const int q = t / (kSlabCols / 2), cc = 2 * (t - q * (kSlabCols / 2));
       cp_async16(L.slab + q * kSlabCols + cc, vs + (size_t)q * d * ld + cc);
     }
     if (s.photohad) {
-      const double* mv = p.slab_vals + (size_t)p.step_w * p.slab_stride + (size_t)qb * 4;
       for (int t = threadIdx.x; t < 2 * nqb; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
       const unsigned long long* mq = p.slab_q + qb;
       for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
     }
     for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, p.slab_pairs + pb0 + t);
-    const double* fc = p.slab_fac + (size_t)(p.step & 1) * 3 * p.slab_nslots + 2 * (size_t)pb0;
     for (int t = threadIdx.x; t < 3 * npb; t += blockDim.x) {  // 2 npb slots per factor, 16 bytes a copy
       const int k = t / npb, u = t - k * npb;
       cp_async16(L.fac + k * fs + 2 * u, fc + (size_t)k * p.slab_nslots + 2 * u);
@@ -1310,7 +1388,15 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
     src0 = p.src_ptr[col];
     src1 = p.src_ptr[col + 1];
   }
-  cp_async_wait<0>();
+  if (p.tmap_src) {
+    if (!mbar_wait_bounded(stage_bar, 0, kWaitTries)) {  // the copies did not land: report and leave
+      if (threadIdx.x == 0) atomicExch(p.err, kErrStagingWait);
+      mbar_wait_bounded(stage_bar, 0, kWaitTries);
+      return;
+    }
+  } else {
+    cp_async_wait<0>();
+  }
   __syncthreads();
 
   const char* slb = reinterpret_cast<const char*>(L.slab + c);
@@ -2229,7 +2315,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
-          &c->slabT_pairs, &c->slabT_wrp};
+          &c->slabT_pairs, &c->slabT_wrp, &c->tmaps, &c->d_err};
 }
 
 // Every device buffer: the solve's and the adjoint's scratch.
@@ -2351,6 +2437,69 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.band_part = c->band_part.as<double>();
 }
 
+// cuTensorMapEncodeTiled, reached through the runtime (no link against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  });
+  return fn;
+}
+
+// Tensor maps of X and A as (column, bin, species) for k_slab's TMA staging:
+// box = 16 columns x 1 bin x box_rows species.  Leaves tma_ok false (cp.async
+// staging) when TMA is switched off, the encoder is missing or a map is refused.
+int ensure_tmaps(pb_context* c, bool blocked, int ld) {
+  const bool want = blocked && c->tma_mode == 1 && ld % kSlabCols == 0;
+  if (want && c->tma_ok && c->tma_key[0] == c->X.p && c->tma_key[1] == c->A.p &&
+      c->tma_key[2] == reinterpret_cast<const void*>((intptr_t)ld))
+    return PB_OK;
+  c->tma_ok = false;
+  if (!want) return PB_OK;
+  const EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) return PB_OK;
+  const int d = c->lay_d, nsp = c->lay_nsp;
+  CUtensorMap maps[2];
+  for (int k = 0; k < 2; ++k) {
+    const cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)d, (cuuint64_t)nsp};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld * sizeof(double), (cuuint64_t)d * ld * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)kSlabCols, 1u, (cuuint32_t)SlabSmem::box_rows(nsp)};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    if (enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, k == 0 ? c->X.p : c->A.p, dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return PB_OK;
+  }
+  PB_CUDA(c, c->tmaps.ensure(sizeof(maps)));
+  PB_CUDA(c, cudaMemcpy(c->tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
+  c->tma_key[0] = c->X.p;
+  c->tma_key[1] = c->A.p;
+  c->tma_key[2] = reinterpret_cast<const void*>((intptr_t)ld);
+  c->tma_ok = true;
+  return PB_OK;
+}
+
+// Reports a bounded wait that gave up inside a kernel of the last enqueued work.
+int check_wait_flag(pb_context* c, const char* who) {
+  int herr = 0;
+  PB_CUDA(c, cudaMemcpy(&herr, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr) return fail(c, PB_ERR_CUDA, "%s: a k_slab CTA gave up waiting for its staging copies (code %d)", who, herr);
+  return PB_OK;
+}
+
+// The k_slab staging of a stage: the tensor map of its source, or null.
+const CUtensorMap* stage_tmap(const pb_context* c, int stage) {
+  return c->tma_ok ? reinterpret_cast<const CUtensorMap*>(c->tmaps.p) + (stage == 1 ? 0 : 1) : nullptr;
+}
+
 // Whether a solve with K columns runs the bin-blocked kernels.
 bool use_blocked(const pb_context* c, int K) {
   const int64_t ld = ((K + kColTile - 1) / kColTile) * kColTile;
@@ -2456,6 +2605,8 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       p.src = stage == 1 ? X : c->A.as<double>();
       p.x = X;
       p.xout = X;
+      p.tmap_src = blocked ? stage_tmap(c, stage) : nullptr;
+      p.err = c->d_err.as<int>();
       if (blocked) {
         launches += stage == 1 ? launch_blocked_stage<1>(c, p, st) : launch_blocked_stage<2>(c, p, st);
         continue;
@@ -3179,6 +3330,9 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
   p.src = stage == 1 ? c->X.as<double>() : c->A.as<double>();
   p.x = c->X.as<double>();
   p.xout = c->X.as<double>();
+  p.tmap_src = stage_tmap(c, stage);
+  PB_CUDA(c, c->d_err.ensure(sizeof(int)));
+  p.err = c->d_err.as<int>();
   cudaStream_t st = c->stream;
   const bool photohad = (flags & PB_PHOTOHAD) != 0, kap = (flags & PB_PARTIAL_DIFF) != 0;
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
@@ -3266,6 +3420,10 @@ int pb_set_option(pb_context* c, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(c, PB_ERR_ARG, "pb_set_option: batched kernels must be 0 or 1");
       c->batched_mode = (int32_t)value;
       return PB_OK;
+    case PB_OPT_TMA_STAGING:
+      if (value != 0 && value != 1) return fail(c, PB_ERR_ARG, "pb_set_option: TMA staging must be 0 or 1");
+      c->tma_mode = (int32_t)value;
+      return PB_OK;
   }
   return fail(c, PB_ERR_ARG, "pb_set_option: unknown key %d", key);
 }
@@ -3275,6 +3433,8 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
   if (!value) return fail(c, PB_ERR_ARG, "pb_get_info: value is NULL");
   switch (key) {
     case PB_OPT_BATCHED_KERNELS: *value = c->batched_mode; return PB_OK;
+    case PB_OPT_TMA_STAGING: *value = c->tma_mode; return PB_OK;
+    case PB_INFO_LAST_TMA: *value = c->last_tma ? 1 : 0; return PB_OK;
     case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
     case PB_INFO_BAND_SPECIES: *value = c->band_nb; return PB_OK;
@@ -3412,6 +3572,10 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     PB_CUDA(c, c->band_part.ensure((size_t)kMaxBandGroups * std::max(c->band_nb, 1) * c->lay_d * ld * sizeof(double)));
   }
   c->last_blocked = blocked;
+  PB_CUDA(c, c->d_err.ensure(sizeof(int)));
+  if ((rc = ensure_tmaps(c, blocked, ld))) return rc;
+  c->last_tma = blocked && c->tma_ok;
+  PB_CUDA(c, cudaMemsetAsync(c->d_err.p, 0, sizeof(int), st));
   size_t scan_need = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, scan_need, (int*)nullptr, (int*)nullptr, (int)(R + 1));
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
@@ -3511,6 +3675,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)c->n_seg); put((uint64_t)c->h_short_rows.size()); put((uint64_t)c->n_cr_bins);
     put((uint64_t)a->ckpt_every);
     put((uint64_t)blocked);
+    put((uint64_t)(blocked && c->tma_ok));
     put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
     put((uint64_t)c->slab_nent);
     put((uint64_t)c->em_W);
@@ -3574,6 +3739,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   }
   PB_CUDA(c, cudaEventRecord(c->ev1, st));
   PB_CUDA(c, cudaStreamSynchronize(st));
+  if ((rc = check_wait_flag(c, "pb_solve"))) return rc;
   PB_CUDA(c, cudaEventElapsedTime(&c->last_solve_ms, c->ev0, c->ev1));
   PB_CUDA(c, cudaEventElapsedTime(&c->last_device_ms, c->ev0, c->ev3));
   PB_CUDA(c, cudaEventElapsedTime(&c->last_steps_ms, c->ev2, c->ev3));
@@ -3611,6 +3777,8 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   int rc = set_device(c);
   if (rc) return rc;
   cudaStream_t st = c->stream;
+  PB_CUDA(c, c->d_err.ensure(sizeof(int)));
+  PB_CUDA(c, cudaMemsetAsync(c->d_err.p, 0, sizeof(int), st));
   const int64_t mstride = std::max<int64_t>(R, 1);
   const size_t sb = (size_t)n * ld * sizeof(double);
 
@@ -3867,7 +4035,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   }
   PB_CUDA(c, cudaGetLastError());
   PB_CUDA(c, cudaStreamSynchronize(st));
-  return PB_OK;
+  return check_wait_flag(c, "pb_adjoint");
 }
 
 int pb_get_operator_pattern(pb_context* c, int64_t* nnz, int64_t* indptr, int32_t* indices) {

@@ -194,6 +194,32 @@ def test_medium_network_batched_uneven_zmax_vs_oracle(medium_run, mode):
     assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
 
 
+def test_tma_and_cp_async_staging_agree_bitwise(medium_run):
+    """The bin-local kernel stages the same bytes by TMA (tensor maps, bulk
+    copies, one mbarrier) or by cp.async; the states must be identical."""
+    from prince_b200 import _lib
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, point_source
+    run = medium_run
+    K = 37
+    pts = draw_points(run, K, seed=8, z_range=(0.05, 0.2))
+    m = MultiRHSPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run, K=K)
+    for k, p in enumerate(pts):
+        m[k].add_source_class(point_source(run, p))
+    ctx = m._dev.ctx
+    states = {}
+    try:
+        for mode in (1, 0):
+            ctx.set_option(_lib.PB_OPT_TMA_STAGING, mode)
+            m.solve(dz=1e-3)
+            assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == 1
+            assert ctx.info(_lib.PB_INFO_LAST_TMA) == mode
+            states[mode] = m.state.copy()
+    finally:
+        ctx.set_option(_lib.PB_OPT_TMA_STAGING, 1)
+    assert np.array_equal(states[0], states[1])
+
+
 def test_layout_classification(golden, medium_run):
     from prince_b200 import _lib
     from prince_b200.solvers import DeviceRun
