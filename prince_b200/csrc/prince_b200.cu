@@ -1252,8 +1252,8 @@ __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalar
 // pairs and the row factors (eD, phi1, phi2) of each pair slot.  Every block
 // starts on a 16-byte boundary (the quad count of a bin is even).
 constexpr int kSlabCols = 16;       // state columns of a k_slab CTA (a half-warp per row)
-constexpr int kSlabWarps = 8;       // two CTAs per SM
-constexpr int kSlabPre = 4;         // row pairs whose FD term and F(x) a warp loads ahead
+constexpr int kSlabWarps = 16;      // two CTAs per SM: 32 warps hide the gather's latencies (64 registers)
+constexpr int kSlabPre = 3;         // row pairs whose FD term and F(x) a warp loads ahead
 struct SlabSmem {
   double* slab;
   double* vals;
@@ -1745,7 +1745,7 @@ struct AdjBlk {
   const int* slabT_qbase;   // [d + 1] first quad of each bin (even)
   const unsigned long long* slabT_q;  // per quad: byte offsets of the 4 daughters' rows in the v slab, 16 bits each
   const int4* slabT_pairs;  // mother-row pairs of k_slabT's warps (as k_slab's row pairs)
-  const int* slabT_wrp;     // [d][kSlabWarps + 1] first pair of each warp of a bin's CTA
+  const int* slabT_wrp;     // [d][kSlabTWarps + 1] first pair of each warp of a bin's CTA
   int slabT_maxq;           // quads of the largest bin
   int slabT_maxp;           // row pairs of a bin
   const int* fdT_cnt;       // per bin: entries of the transposed stencil, row offsets, values
@@ -1902,6 +1902,7 @@ size_t bandT_smem_bytes() {
 // entry values (4 per quad), daughter-row byte offsets (4 x 16 bits per quad)
 // and mother-row pairs.  Every block starts on a 16-byte boundary.
 constexpr int kSlabTPre = 3;        // row pairs whose inputs a warp loads ahead
+constexpr int kSlabTWarps = 8;      // two CTAs per SM
 struct SlabTSmem {
   double* slab;
   double* vals;
@@ -1928,7 +1929,7 @@ struct SlabTSmem {
 // loaded kSlabTPre pairs ahead into registers.  Stage 1 reduces the
 // photon-scale gradient of the bin's rows inside the CTA.
 template <int STAGE>
-__global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slabT(AdjBlk q) {
+__global__ void __launch_bounds__(kSlabTWarps * 32, 2) k_slabT(AdjBlk q) {
   extern __shared__ double sm[];
   const int nsp = q.nsp, e = blockIdx.x, d = q.d, ld = q.ld;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1937,7 +1938,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slabT(AdjBlk q) {
   const bool active = col < q.ncols;
   SlabTSmem L(sm, nsp, q.slabT_maxq);
   const int qb = q.slabT_qbase[e], nqb = q.slabT_qbase[e + 1] - qb;
-  const int pb0 = q.slabT_wrp[e * (kSlabWarps + 1)], npb = q.slabT_wrp[e * (kSlabWarps + 1) + kSlabWarps] - pb0;
+  const int pb0 = q.slabT_wrp[e * (kSlabTWarps + 1)], npb = q.slabT_wrp[e * (kSlabTWarps + 1) + kSlabTWarps] - pb0;
   const bool photohad = (q.flags & PB_PHOTOHAD) != 0, kap = (q.flags & PB_PARTIAL_DIFF) != 0;
   {
     const double* vs = q.v + (size_t)e * ld + col0;
@@ -1954,7 +1955,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slabT(AdjBlk q) {
     for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, q.slabT_pairs + pb0 + t);
     cp_async_commit();
   }
-  const int w0 = q.slabT_wrp[e * (kSlabWarps + 1) + wid], w1 = q.slabT_wrp[e * (kSlabWarps + 1) + wid + 1];
+  const int w0 = q.slabT_wrp[e * (kSlabTWarps + 1) + wid], w1 = q.slabT_wrp[e * (kSlabTWarps + 1) + wid + 1];
   const double* own_src = STAGE == 1 ? q.lam : q.mu;
   const bool want_pq = STAGE == 1 && q.gs;
   constexpr int PRE = kSlabTPre;
@@ -2052,7 +2053,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slabT(AdjBlk q) {
     __syncthreads();
     if (threadIdx.x < kSlabCols && col0 + (int)threadIdx.x < q.ncols) {
       double t = 0.0;
-      for (int h = 0; h < 2 * kSlabWarps; ++h) t += red[h * kSlabCols + threadIdx.x];
+      for (int h = 0; h < 2 * kSlabTWarps; ++h) t += red[h * kSlabCols + threadIdx.x];
       q.gs[(size_t)e * ld + col0 + threadIdx.x] += t;
     }
   }
@@ -2574,7 +2575,7 @@ void launch_adj_blocked(pb_context* c, AdjBlk& q, cudaStream_t st) {
   }
   if (kap) k_fdT<<<dim3(q.nsp, tiles), 256, (size_t)q.d * kColTile * sizeof(double), st>>>(q);
   if (forked) cudaStreamWaitEvent(st, c->ev_join, 0);
-  k_slabT<STAGE><<<dim3(q.d, (unsigned)blocks_for(q.ncols, kSlabCols)), kSlabWarps * 32, c->slabT_smem, st>>>(q);
+  k_slabT<STAGE><<<dim3(q.d, (unsigned)blocks_for(q.ncols, kSlabCols)), kSlabTWarps * 32, c->slabT_smem, st>>>(q);
 }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
@@ -3223,15 +3224,15 @@ int pb_set_layout(pb_context* c, int32_t d) {
   // last quad); rows paired for k_slabT's half-warps and the pairs spread over
   // its warps longest-processing-time first; every bin starts on an even quad.
   std::vector<std::vector<std::pair<int32_t, int64_t>>> bym(nsp);
-  std::vector<int32_t> tqbase((size_t)d + 1, 0), twrp((size_t)d * (kSlabWarps + 1), 0), tpairs;
+  std::vector<int32_t> tqbase((size_t)d + 1, 0), twrp((size_t)d * (kSlabTWarps + 1), 0), tpairs;
   std::vector<unsigned long long> tquad;
   std::vector<int32_t> tslot((size_t)std::max<int64_t>(R, 1), -1);
   int32_t tmax = 0;
   bool tq_fit = (size_t)nsp * kSlabCols * sizeof(double) <= (1 << 16);
   {
     std::vector<int32_t> nqm(nsp), order(nsp);
-    std::vector<std::vector<int32_t>> wl(kSlabWarps);
-    std::vector<int64_t> load(kSlabWarps);
+    std::vector<std::vector<int32_t>> wl(kSlabTWarps);
+    std::vector<int64_t> load(kSlabTWarps);
     for (int e = 0; e < d; ++e) {
       for (auto& v : bym) v.clear();
       for (int i = 0; i < nss; ++i) {
@@ -3252,8 +3253,8 @@ int pb_set_layout(pb_context* c, int32_t d) {
         wl[w].push_back(k);
         load[w] += nqm[order[k]] + 1;
       }
-      for (int w = 0; w < kSlabWarps; ++w) {
-        twrp[(size_t)e * (kSlabWarps + 1) + w] = (int32_t)(tpairs.size() / 4);
+      for (int w = 0; w < kSlabTWarps; ++w) {
+        twrp[(size_t)e * (kSlabTWarps + 1) + w] = (int32_t)(tpairs.size() / 4);
         for (int k : wl[w]) {
           int32_t pr[4] = {-1, -1, 0, 0};
           for (int hf = 0; hf < 2; ++hf) {
@@ -3276,7 +3277,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
           tpairs.insert(tpairs.end(), pr, pr + 4);
         }
       }
-      twrp[(size_t)e * (kSlabWarps + 1) + kSlabWarps] = (int32_t)(tpairs.size() / 4);
+      twrp[(size_t)e * (kSlabTWarps + 1) + kSlabTWarps] = (int32_t)(tpairs.size() / 4);
       if ((tquad.size() - tqbase[e]) % 2) tquad.push_back(0);
       tmax = std::max<int32_t>(tmax, (int32_t)(tquad.size() - tqbase[e]));
     }
@@ -3285,7 +3286,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   }
   if (!tq_fit) return PB_OK;
   // at least one double per thread: stage 1 reduces the gradient over the slab's space
-  const size_t tsm = std::max(SlabTSmem::bytes(nsp, tmax, (nsp + 1) / 2), (size_t)kSlabWarps * 32 * sizeof(double));
+  const size_t tsm = std::max(SlabTSmem::bytes(nsp, tmax, (nsp + 1) / 2), (size_t)kSlabTWarps * 32 * sizeof(double));
   const BandTInstance bti = bandT_kernel(RT, J);
   if (tsm > max_smem || !bti.fn || bti.smem > max_smem || (size_t)d * kColTile * sizeof(double) > max_smem) return PB_OK;
   if ((rc = upload(c, c->bandT_slot, btslot.data(), btslot.size()))) return rc;
