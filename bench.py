@@ -278,7 +278,7 @@ def run_b200(args, dist, rank, ws, local):
 # DRAM bytes per launch (dram__bytes read + write) of each stage kernel in one
 # ncu capture of this workload at K = 512 (bench.py --z-range 0.05,0.05,
 # -s 4 -c 1 per kernel); the capture is repeated after kernel changes.
-NCU_TRAFFIC_K512 = {"k_slab": 524e6, "k_band": 170e6, "k_fd_dense": 228e6, "k_fd": 227e6}
+NCU_TRAFFIC_K512 = {"k_slab": 525e6, "k_band": 170e6, "k_fd_dense": 228e6, "k_fd": 227e6}
 
 
 def kernel_rooflines(solver, run, sched, n_active, n_inj):
