@@ -1205,29 +1205,13 @@ __device__ __forceinline__ void record_blocked(const StepParams& p, const StepSc
   }
 }
 
-// The record inputs of one (row, column), loaded before the row's sum so
-// their latency overlaps it: the scale derivatives, the step factors, the FD
-// term with kappa_pair and (stage 2) the stage-1 S x.
+// The record inputs of one (row, column), loaded by k_slab with the row's
+// other inputs ahead of its sum: the scale derivatives, the step factors, the
+// FD term with kappa_pair and (stage 2) the stage-1 S x.
 struct RecIn {
   double ds, d12, f0, f1, kp, sx;
   bool on;
 };
-template <int STAGE>
-__device__ __forceinline__ RecIn rec_load(const StepParams& p, const StepScalars& s, int64_t r, int k) {
-  RecIn in{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, false};
-  const int64_t j = p.step - p.rec_k0;
-  if (j < 0 || j >= p.rec_len) return in;
-  const size_t o = (size_t)(p.step & 1) * p.n + r;
-  const size_t idx = (size_t)r * p.ld + k;
-  in.on = true;
-  in.ds = p.dsig[o];
-  in.d12 = STAGE == 1 ? p.dphi1[o] : p.dphi2[o];
-  in.f0 = STAGE == 1 ? p.eD[o] : p.phi2[o];
-  in.f1 = p.phi1[o];
-  if (s.kap && s.pair) in.kp = p.fdkp[idx];
-  if (STAGE == 2) in.sx = p.rec_sx[idx];
-  return in;
-}
 // record_blocked with preloaded inputs (same arithmetic)
 template <int STAGE>
 __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalars& s, int64_t r, int k, double sM,
@@ -1901,8 +1885,8 @@ size_t bandT_smem_bytes() {
 // k_slabT's shared memory: the v slab of one bin (nsp x 16 columns), the bin's
 // entry values (4 per quad), daughter-row byte offsets (4 x 16 bits per quad)
 // and mother-row pairs.  Every block starts on a 16-byte boundary.
-constexpr int kSlabTPre = 3;        // row pairs whose inputs a warp loads ahead
-constexpr int kSlabTWarps = 8;      // two CTAs per SM
+constexpr int kSlabTPre = 2;        // row pairs whose inputs a warp loads ahead
+constexpr int kSlabTWarps = 12;     // two CTAs per SM (80 registers)
 struct SlabTSmem {
   double* slab;
   double* vals;
