@@ -148,8 +148,9 @@ struct pb_context {
   std::vector<int32_t> h_d_indices;
   std::vector<double> h_d_vals;
   bool fd_tab_ok = false;
-  DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp, fd_dense;
+  DBuf fd_cnt, fd_off, fd_val, fdbuf, fdkp, fd_dense, fdT_dense;
   bool fd_dense_ok = false;         // the stencil fits k_fd_dense's halo
+  bool fdT_dense_ok = false;        // the transposed stencil fits k_fdT_dense's halo
   // transposed bin-blocked structures of the adjoint sweep (one band pair)
   bool blockedT_ok = false, fdT_ok = false;
   DBuf bandT_slot, slabT_rp, slabT_offs, slabT_slot, bandT_vals, slabT_vals, fdT_cnt, fdT_off, fdT_val;
@@ -1735,6 +1736,7 @@ struct AdjBlk {
   const int* fdT_cnt;       // per bin: entries of the transposed stencil, row offsets, values
   const int* fdT_off;
   const double* fdT_val;
+  const double* fdT_dense;  // [d][kFdDenseW] transposed weights of offsets -kFdHalo..kFdHalo, or null
   const int* band_spec;
   const double* rf;         // recorded eD, phi1, phi2, kappa of this step (n each)
   const double* rf_prev;    // recorded factors of the previous step (phi2 used), or null
@@ -1800,6 +1802,54 @@ __global__ void __launch_bounds__(256) k_fdT(AdjBlk q) {
     for (int t = 0; t < cnt; ++t)
       s += q.fdT_val[e * kFdTMax + t] * fsm[(e + q.fdT_off[e * kFdTMax + t]) * kColTile + lane];
     q.fdT[((size_t)sp * d + e) * ld + col] = s;
+  }
+}
+
+// fdT = D_off^T v, register-blocked like k_fd_dense (no kappa): the block's
+// d x 32 states and the dense transposed weights in shared memory, a warp
+// holds kFdChunk bins plus a kFdHalo halo per side in registers.  The terms
+// are fused multiply-adds in ascending offset order from zero, so absent
+// offsets (zero weights) leave each sum as k_fdT forms it.
+__global__ void __launch_bounds__(256) k_fdT_dense(AdjBlk q) {
+  extern __shared__ double fsm[];
+  const int sp = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int d = q.d, ld = q.ld;
+  const int col = blockIdx.y * kColTile + lane;
+  double* vb = fsm;                        // d x 32
+  double* wt = vb + (size_t)d * kColTile;  // d x kFdDenseW
+  const double* __restrict__ v = q.v + (size_t)sp * d * ld + blockIdx.y * kColTile;
+  for (int t = threadIdx.x; t < d * (kColTile / 2); t += blockDim.x) {
+    const int e = t / (kColTile / 2), c = 2 * (t - e * (kColTile / 2));
+    cp_async16(vb + e * kColTile + c, v + (size_t)e * ld + c);
+  }
+  for (int t = threadIdx.x; t < d * (kFdDenseW / 2); t += blockDim.x) cp_async16(wt + 2 * t, q.fdT_dense + 2 * t);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  double* __restrict__ out = q.fdT + (size_t)sp * d * ld + col;
+  constexpr int U = kFdChunk + 2 * kFdHalo;
+  for (int c0 = wid * kFdChunk; c0 < d; c0 += (blockDim.x >> 5) * kFdChunk) {
+    double u[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int e = c0 - kFdHalo + i;
+      u[i] = (e >= 0 && e < d) ? vb[e * kColTile + lane] : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < kFdChunk; ++i) {
+      const int e = c0 + i;
+      if (e >= d) break;
+      const double2* w2 = reinterpret_cast<const double2*>(wt + e * kFdDenseW);
+      const double2 wa = w2[0], wb = w2[1], wc = w2[2], wd = w2[3];
+      double sT = __fma_rn(wa.x, u[i], 0.0);
+      sT = __fma_rn(wa.y, u[i + 1], sT);
+      sT = __fma_rn(wb.x, u[i + 2], sT);
+      sT = __fma_rn(wb.y, u[i + 3], sT);
+      sT = __fma_rn(wc.x, u[i + 4], sT);
+      sT = __fma_rn(wc.y, u[i + 5], sT);
+      sT = __fma_rn(wd.x, u[i + 6], sT);
+      out[(size_t)e * ld] = sT;
+    }
   }
 }
 
@@ -2298,7 +2348,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdbuf,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
           &c->slabT_pairs, &c->slabT_wrp, &c->tmaps, &c->d_err};
 }
@@ -2557,7 +2607,10 @@ void launch_adj_blocked(pb_context* c, AdjBlk& q, cudaStream_t st) {
     cudaEventRecord(c->ev_join, c->stream2);
     forked = true;
   }
-  if (kap) k_fdT<<<dim3(q.nsp, tiles), 256, (size_t)q.d * kColTile * sizeof(double), st>>>(q);
+  if (kap && c->fdT_dense_ok)
+    k_fdT_dense<<<dim3(q.nsp, tiles), 256, (size_t)q.d * (kColTile + kFdDenseW) * sizeof(double), st>>>(q);
+  else if (kap)
+    k_fdT<<<dim3(q.nsp, tiles), 256, (size_t)q.d * kColTile * sizeof(double), st>>>(q);
   if (forked) cudaStreamWaitEvent(st, c->ev_join, 0);
   k_slabT<STAGE><<<dim3(q.d, (unsigned)blocks_for(q.ncols, kSlabCols)), kSlabTWarps * 32, c->slabT_smem, st>>>(q);
 }
@@ -2882,6 +2935,24 @@ static int build_fd_table(pb_context* c) {
   if ((rc = upload(c, c->fd_cnt, cnt.data(), cnt.size()))) return rc;
   if ((rc = upload(c, c->fd_off, off.data(), off.size()))) return rc;
   if ((rc = upload(c, c->fd_val, val.data(), val.size()))) return rc;
+  // dense form of the transposed stencil for k_fdT_dense (column lists are in
+  // row order, i.e. ascending offsets)
+  std::vector<double> tdense((size_t)d * kFdDenseW, 0.0);
+  bool tdense_ok = t_ok && (size_t)d * (kColTile + kFdDenseW) * sizeof(double) <= 48 * 1024;
+  for (int e = 0; e < d && tdense_ok; ++e)
+    for (int t = 0; t < tcnt[e]; ++t) {
+      const int o = toff[(size_t)e * kFdTMax + t];
+      if (o < -kFdHalo || o > kFdHalo || o == 0 || (t > 0 && o <= toff[(size_t)e * kFdTMax + t - 1])) {
+        tdense_ok = false;
+        break;
+      }
+      tdense[(size_t)e * kFdDenseW + o + kFdHalo] = tval[(size_t)e * kFdTMax + t];
+    }
+  c->fdT_dense_ok = false;
+  if (tdense_ok) {
+    if ((rc = upload(c, c->fdT_dense, tdense.data(), tdense.size()))) return rc;
+    c->fdT_dense_ok = true;
+  }
   if (t_ok) {
     if ((rc = upload(c, c->fdT_cnt, tcnt.data(), tcnt.size()))) return rc;
     if ((rc = upload(c, c->fdT_off, toff.data(), toff.size()))) return rc;
@@ -3912,6 +3983,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
         q.fdT_cnt = c->fdT_cnt.as<int>();
         q.fdT_off = c->fdT_off.as<int>();
         q.fdT_val = c->fdT_val.as<double>();
+        q.fdT_dense = c->fdT_dense.as<double>();
         q.band_spec = c->band_spec.as<int>();
         q.rf = c->rec_rf.as<double>() + j * 4 * n;
         q.rf_prev = j >= 1 ? c->rec_rf.as<double>() + (j - 1) * 4 * n : nullptr;
