@@ -2526,7 +2526,7 @@ int ensure_tmaps(pb_context* c, bool blocked, int ld) {
 int check_wait_flag(pb_context* c, const char* who) {
   int herr = 0;
   PB_CUDA(c, cudaMemcpy(&herr, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (herr) return fail(c, PB_ERR_CUDA, "%s: a k_slab CTA gave up waiting for its staging copies (code %d)", who, herr);
+  if (herr) return fail(c, PB_ERR_DEVICE, "%s: a k_slab CTA gave up waiting for its staging copies (code %d)", who, herr);
   return PB_OK;
 }
 

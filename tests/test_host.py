@@ -32,6 +32,19 @@ def test_library_exports_every_header_symbol():
     assert lib.pb_abi_version() == 2
 
 
+def test_header_constants_match_the_binding():
+    """Every PB_* constant of the header has the same value in the ctypes binding."""
+    from prince_b200 import _lib
+    text = open(os.path.join(ROOT, "include", "prince_b200.h")).read()
+    consts = dict(re.findall(r"^#define\s+(PB_[A-Z_0-9]+)\s+(\d+)u?\b", text, flags=re.M))
+    assert "PB_OPT_TMA_STAGING" in consts and "PB_INFO_LAST_TMA" in consts
+    for name, value in consts.items():
+        if name.startswith("PB_NOALLOC"):
+            continue
+        assert hasattr(_lib, name), name
+        assert getattr(_lib, name) == int(value), name
+
+
 def test_context_without_gpu_raises_cleanly():
     from prince_b200 import _lib
 
