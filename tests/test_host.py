@@ -86,6 +86,25 @@ def test_vectorised_evolution_matches_scalar():
         np.testing.assert_allclose(vec, ref, rtol=5e-16, atol=0)
 
 
+def test_batched_coefficients_match_per_source_evolution():
+    """The broadcast (1 + z)^m table equals each source's own evolution_array bit for bit."""
+    from prince_b200 import cr_sources
+    from prince_b200.solvers import _coefficients
+    from workloads import light_run
+    run = light_run()
+    rng = np.random.default_rng(4)
+    zs = S.z_grid(0.9, 0.0, 1e-3)[:-1]
+    srcs = []
+    for k in range(40):
+        m = ("simple", float(rng.uniform(-3, 5))) if k % 4 else ("simple", 2.0) if k % 8 == 0 else "flat"
+        srcs.append(cr_sources.RigdityCutoffSource(run, norm=float(rng.uniform(0.5, 2.0)),
+                                                   params={2212: (2.0, 1e10, 1.0)}, m=m,
+                                                   z_max=None if k % 5 == 0 else float(rng.uniform(0.1, 0.9))))
+    table = _coefficients(srcs, zs)
+    for i, s in enumerate(srcs):
+        assert np.array_equal(table[:, i], s.norm * s.evolution_array(zs)), i
+
+
 def test_column_order_and_active_prefix():
     """Columns are stepped in the order they switch on; the active set is a prefix."""
     from prince_b200.solvers import MultiRHSPropagationSolverETD2
