@@ -313,7 +313,9 @@ class UHECRPropagationSolverETD2:
         return f * self.list_of_sources[0].injection_rate(z)
 
     def close(self):
-        pass
+        """Reference API (``propagation.py:708``).  The device buffers belong to the
+        run's ``DeviceRun`` (shared by every solver of the run on that device and
+        released with it), so a solver holds nothing to free."""
 
     # -- co-evolved EM cascade (propagation.py:540-665) --------------------
     def _em_model(self, z):
