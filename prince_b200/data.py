@@ -70,6 +70,7 @@ class EnergyGrid:
     """
 
     def __init__(self, lower, upper, bins_dec):
+        self.lower, self.upper, self.bins_dec = lower, upper, bins_dec
         self.bins = np.logspace(lower, upper, int((upper - lower) * bins_dec + 1))
         self.grid = 0.5 * (self.bins[1:] + self.bins[:-1])
         self.widths = self.bins[1:] - self.bins[:-1]

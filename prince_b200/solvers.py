@@ -8,8 +8,8 @@ vectors, the rate fold, the operator split and the ETD2 steps all run on the
 GPU through the C ABI; the host evaluates only the scalar schedule (z grid,
 windows, dl/dz, source evolution) and moves the state.
 
-``UHECRPropagationResult`` is the reference result container
-(``propagation.py:34-192``).
+The result container ``UHECRPropagationResult`` lives in
+``prince_b200.results`` and is re-exported here.
 """
 
 from __future__ import annotations
@@ -23,126 +23,10 @@ from . import _lib
 from . import constants as C
 from .cosmology import H as _H
 from .cosmology import dldz as _dldz
-from .data import EnergyGrid, is_nucleus
 from .operators import fd_loss_operator, split_diagonal
 from .photonfields import device_components
+from .results import UHECRPropagationResult  # noqa: F401  (reference API location)
 from .schedule import make_schedule, z_grid
-
-
-# ---------------------------------------------------------------------------
-# result container
-# ---------------------------------------------------------------------------
-class UHECRPropagationResult:
-    """State vector plus grid and species table; spectra per species or group."""
-
-    def __init__(self, state, egrid, spec_man):
-        self.spec_man = spec_man
-        self.egrid = egrid
-        self.state = state
-
-    def to_dict(self):
-        return {"egrid": self.egrid, "state": self.state, "known_spec": self.known_species}
-
-    @classmethod
-    def from_dict(cls, dic):
-        from .data import SpeciesManager
-
-        egrid = dic["egrid"]
-        return cls(dic["state"], egrid, SpeciesManager(dic["known_spec"], egrid.size))
-
-    @property
-    def known_species(self):
-        return self.spec_man.known_species
-
-    def __add__(self, other):
-        if not np.array_equal(self.egrid, other.egrid):
-            raise Exception("Cannot add Propagation Results, they are defined in different energy grids!")
-        if not np.array_equal(self.known_species, other.known_species):
-            raise Exception("Cannot add Propagation Results, have different species managers!")
-        return UHECRPropagationResult(self.state + other.state, self.egrid, self.spec_man)
-
-    def __mul__(self, number):
-        if not np.isscalar(number):
-            raise Exception(
-                "Can only multiply result by scalar number, got type {:} instead!".format(type(number)))
-        return UHECRPropagationResult(self.state * number, self.egrid, self.spec_man)
-
-    def get_solution(self, pdg_id):
-        """Spectrum in energy per nucleon."""
-        spec = self.spec_man.pdgid2sref[pdg_id]
-        return self.egrid, self.state[spec.lidx():spec.uidx()]
-
-    def get_solution_scale(self, pdg_id, epow=0):
-        """Spectrum in total energy, times E^epow."""
-        spec = self.spec_man.pdgid2sref[pdg_id]
-        egrid = spec.A * self.egrid
-        return egrid, egrid ** epow * self.state[spec.lidx():spec.uidx()] / spec.A
-
-    def _check_id_grid(self, pdg_ids, egrid):
-        if egrid is None:
-            max_mass = max(s.A for s in self.spec_man.species_refs)
-            emin_log, emax_log, nbins = self._grid_triple()
-            emax_log = np.log10(max_mass) + emax_log
-            com_egrid = EnergyGrid(emin_log, emax_log, nbins * 4).grid
-        else:
-            com_egrid = egrid
-        if isinstance(pdg_ids, list):
-            pass
-        elif pdg_ids == "CR":
-            pdg_ids = [s for s in self.known_species if is_nucleus(s)]
-        elif pdg_ids == "nu":
-            pdg_ids = [s for s in self.known_species if s in (12, -12, 14, -14, 16, -16)]
-        elif pdg_ids == "all":
-            pdg_ids = self.known_species
-        elif isinstance(pdg_ids, tuple):
-            select, vmin, vmax = pdg_ids
-            pdg_ids = [s for s in self.known_species if vmin <= select(s) <= vmax]
-        return pdg_ids, com_egrid
-
-    def _grid_triple(self):
-        """(log10 lo edge, log10 hi edge, bins/decade) recovered from the centres."""
-        g = np.asarray(self.egrid)
-        step = np.log10(g[1] / g[0])
-        ratio = 10 ** step
-        lo_edge = 2 * g[0] / (1 + ratio)
-        hi_edge = lo_edge * ratio ** g.size
-        return (float(np.round(np.log10(lo_edge), 9)), float(np.round(np.log10(hi_edge), 9)),
-                float(np.round(1.0 / step, 9)))
-
-    def _collect_interpolated_spectra(self, pdg_ids, epow, egrid=None):
-        pdg_ids, com_egrid = self._check_id_grid(pdg_ids, egrid)
-        spectra = np.zeros((len(pdg_ids), com_egrid.size))
-        for idx, pid in enumerate(pdg_ids):
-            curr_egrid, curr_spec = self.get_solution_scale(pid, epow)
-            mask = curr_spec > 0.0
-            if np.count_nonzero(mask) > 0:
-                res = np.exp(np.interp(np.log(com_egrid), np.log(curr_egrid[mask]), np.log(curr_spec[mask]),
-                                       left=np.nan, right=np.nan))
-            else:
-                res = np.zeros_like(com_egrid)
-            spectra[idx] = np.nan_to_num(res)
-        return pdg_ids, com_egrid, spectra
-
-    def get_solution_group(self, pdg_ids, epow=3, egrid=None):
-        """Summed spectrum (total energy) of a group of species."""
-        _, com_egrid, spectra = self._collect_interpolated_spectra(pdg_ids, epow, egrid)
-        return com_egrid, spectra.sum(axis=0)
-
-    def get_lnA(self, pdg_ids, egrid=None):
-        """Mean and variance of ln A versus total energy."""
-        pdg_ids, com_egrid, spectra = self._collect_interpolated_spectra(pdg_ids, 0, egrid)
-        lnA = np.array([np.log(self.spec_man.pdgid2sref[el].A) for el in pdg_ids])
-        total = spectra.sum(axis=0)
-        with np.errstate(invalid="ignore", divide="ignore"):
-            average = (lnA[:, None] * spectra).sum(axis=0) / total
-            variance = (lnA[:, None] ** 2 * spectra).sum(axis=0) / total - average ** 2
-        return com_egrid, average, variance
-
-    def get_energy_density(self, pdg_id):
-        from scipy.integrate import trapezoid
-
-        A = self.spec_man.pdgid2sref[pdg_id].A
-        return trapezoid(A * self.egrid * self.get_solution(pdg_id)[1], self.egrid)
 
 
 # ---------------------------------------------------------------------------
@@ -297,7 +181,7 @@ class UHECRPropagationSolverETD2:
     @property
     def res(self):
         if self.result is None:
-            self.result = UHECRPropagationResult(self.state, self.egrid, self.spec_man)
+            self.result = UHECRPropagationResult(self.state, self.egrid, self.spec_man, self.prince_run.cr_grid)
         return self.result
 
     def add_source_class(self, source_instance):
@@ -463,7 +347,8 @@ class _MultiRHSView:
 
     @property
     def res(self):
-        return UHECRPropagationResult(self.state, self.parent.egrid, self.parent.spec_man)
+        return UHECRPropagationResult(self.state, self.parent.egrid, self.parent.spec_man,
+                                      self.parent.prince_run.cr_grid)
 
 
 class MultiRHSPropagationSolverETD2(UHECRPropagationSolverETD2):

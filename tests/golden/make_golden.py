@@ -1,11 +1,12 @@
 #!/usr/bin/env python
 """Generate the golden vectors of the ETD2 path by running the PriNCe reference.
 
-Run in a checkout where the reference source tree is available (default
-``/root/reference``, override with ``PRINCE_REFERENCE``)::
+Run it with ``PRINCE_REFERENCE`` set to a checkout of the PriNCe reference
+source tree (the directory that holds ``src/prince_cr``)::
 
-    python tests/golden/make_golden.py          # light network
-    python tests/golden/make_golden.py --em     # light network + EM cascade
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py        # light network
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --em   # light network + EM cascade
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --groups  # result post-processing
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -25,6 +26,11 @@ inputs the ETD2 path consumes together with the reference's own outputs
 (final states of single- and multi-RHS solves, per-window intermediates).
 The result is ``tests/golden/light_network.npz`` (and, with ``--em``,
 ``tests/golden/light_network_em.npz``).
+
+``--groups`` feeds states of ``light_network.npz`` (and variants with
+non-positive bins inside and at the ends of the spectra) to the reference's
+own ``UHECRPropagationResult`` and records ``get_solution_group``,
+``get_lnA`` and ``get_solution_scale`` in ``tests/golden/result_groups.npz``.
 """
 
 from __future__ import annotations
@@ -38,10 +44,12 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PRINCE_REFERENCE", "/root/reference")
+REF = os.environ.get("PRINCE_REFERENCE")
 
 
 def _prepare_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "src", "prince_cr")):
+        raise SystemExit("set PRINCE_REFERENCE to the PriNCe source tree (the directory holding src/prince_cr)")
     tmp = tempfile.mkdtemp(prefix="prince_golden_")
     shutil.copytree(os.path.join(REF, "src", "prince_cr"), os.path.join(tmp, "prince_cr"))
     os.chmod(os.path.join(tmp, "prince_cr", "data"), 0o755)
@@ -375,8 +383,59 @@ def main_em():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_groups():
+    """The reference's result post-processing on recorded states."""
+    _prepare_reference()
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (6, 14, 8)
+    from prince_cr.data import EnergyGrid as RefGrid
+    from prince_cr.data import SpeciesManager as RefSpeciesManager
+    from prince_cr.solvers import UHECRPropagationResult as RefResult
+
+    z = dict(np.load(os.path.join(HERE, "light_network.npz")))
+    egrid = RefGrid(*config.cosmic_ray_grid).grid
+    species = [int(p) for p in z["species"]]
+    sm = RefSpeciesManager(species, egrid.size)
+    rng = np.random.default_rng(17)
+    mixed = np.array(z["state_two_src"])
+    d = egrid.size
+    for i in range(len(species)):
+        blk = mixed[i * d:(i + 1) * d]
+        interior = rng.choice(np.arange(3, d - 3), 6, replace=False)
+        blk[interior[:3]] *= -1.0
+        blk[interior[3:]] = 0.0
+        blk[:2] = -abs(blk[:2])
+        blk[-1] = 0.0
+    states = {"plain": z["state_plain"], "two_src": z["state_two_src"], "mixed": mixed}
+    for k in range(z["state_multi"].shape[1]):
+        states[f"multi{k}"] = z["state_multi"][:, k]
+    out = {"species": np.array(species, dtype=np.int64), "cr_grid": np.array(config.cosmic_ray_grid)}
+    custom = np.logspace(6.2, 14.4, 57)
+    out["custom_grid"] = custom
+    for name, st in states.items():
+        res = RefResult(np.array(st), egrid, sm)
+        out[f"{name}_state"] = np.array(st)
+        g, f = res.get_solution_group("CR", epow=3)
+        out["common_grid"] = g
+        out[f"{name}_CR_e3"] = f
+        out[f"{name}_CR_e0"] = res.get_solution_group("CR", epow=0)[1]
+        out[f"{name}_heavy_e2"] = res.get_solution_group([1000020030, 1000020040, 1000010030], epow=2)[1]
+        out[f"{name}_custom_e3"] = res.get_solution_group("all", epow=3, egrid=custom)[1]
+        _, mean, var = res.get_lnA("CR")
+        out[f"{name}_lnA_mean"] = mean
+        out[f"{name}_lnA_var"] = var
+        out[f"{name}_He4_scale_e1"] = res.get_solution_scale(1000020040, epow=1)[1]
+    path = os.path.join(HERE, "result_groups.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     if "--em" in sys.argv:
         main_em()
+    elif "--groups" in sys.argv:
+        main_groups()
     else:
         main()
