@@ -155,6 +155,21 @@ def rank_points(run, points, rank, z_range):
     return draw_points(run, points, seed=1000 + rank, z_range=z_range)
 
 
+def workload_config(run, sched, points, ws, nnz_m):
+    """The ``config`` object of both arms' lines."""
+    return {
+        "workload": WORKLOAD,
+        "points_per_gpu": points,
+        "n_states": run.dim_states,
+        "coupling_entries": int(run.int_rates._batch_matrix.shape[0]),
+        "offdiag_nnz": int(nnz_m),
+        "n_steps": sched.n_steps,
+        "n_windows": int(len(sched.z_window)),
+        "parallelism": f"replicas x{ws} (columns sharded, no collective)",
+        "l2": "state buffers 3 x 138 MB exceed the 126 MB L2 between solves",
+    }
+
+
 def run_b200(args, dist, rank, ws, local):
     import torch
     from prince_b200.solvers import MultiRHSPropagationSolverETD2, UHECRPropagationSolverETD2
@@ -243,17 +258,7 @@ def run_b200(args, dist, rank, ws, local):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded synthetic photo-nuclear model and source points)",
-        "config": {
-            "workload": WORKLOAD,
-            "points_per_gpu": args.points,
-            "n_states": n,
-            "coupling_entries": int(run.int_rates._batch_matrix.shape[0]),
-            "offdiag_nnz": nnz_m,
-            "n_steps": sched.n_steps,
-            "n_windows": int(len(sched.z_window)),
-            "parallelism": f"replicas x{ws} (columns sharded, no collective)",
-            "l2": "state buffers 3 x 138 MB exceed the 126 MB L2 between solves",
-        },
+        "config": workload_config(run, sched, args.points, ws, nnz_m),
         "e2e": {"value": e2e, "unit": "spectra/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": kern["dominant"] if kern else None,
         "roofline_kernels": kern["kernels"] if kern else None,
@@ -268,7 +273,7 @@ def run_b200(args, dist, rank, ws, local):
         fwd_wall = t_wall / args.steps
         adj["forward_s"] = fwd_wall
         adj["adjoint_over_forward"] = adj["adjoint_s"] / fwd_wall
-        adj["gradient_over_forward"] = (adj["forward_ckpt_s"] + adj["adjoint_s"]) / fwd_wall
+        adj["gradient_over_forward"] = adj["gradient_s"] / fwd_wall
         line["adjoint"] = adj
     if clk:
         line["clocks"] = clk
@@ -342,49 +347,80 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
 
 
 def adjoint_timing(run, pts, zi, device):
-    """Gradient of sum(seed * X) for the same points: forward with checkpoints every
-    32 steps plus the device adjoint, against the plain forward time."""
+    """Gradient of the flux loss of all points (config 4): the squared log-ratio of
+    each point's z = 0 all-particle flux to a target flux from one hidden
+    parameter point, summed over bins above 10^9.5 GeV.  Timed: the
+    forward with checkpoints every 32 steps (parameters -> grids on the host,
+    states on the device), the loss on the device, and the backward (device
+    adjoint plus the parameter chain rule), against the plain forward time."""
     import torch
     from prince_b200 import adjoint as AD
+    from workloads import draw_points
 
     species = [p for p in pts[0]["species"]]
+
+    def tensors(ps, grad=True):
+        return {"gamma": torch.tensor([p["gamma"] for p in ps], requires_grad=grad),
+                "lg_rmax": torch.tensor([np.log10(p["rmax"]) for p in ps], requires_grad=grad),
+                "frac": torch.tensor(np.array([p["frac"] for p in ps]), requires_grad=grad),
+                "m": torch.tensor([p["m"] for p in ps], requires_grad=grad)}
+
+    hidden = draw_points(run, 1, seed=4242, z_range=(1.0, 1.0))
+    sbh = AD.SourceBatch(run, species, z_max=[hidden[0]["zmax"]], initial_z=hidden[0]["zmax"])
+    th = tensors(hidden, grad=False)
+    with torch.no_grad():
+        Xh = AD.PropagateFunction.apply(sbh.grids(th["gamma"], th["lg_rmax"], th["frac"]),
+                                        sbh.coefficients(th["m"]), torch.tensor(1.0, dtype=torch.float64),
+                                        sbh.plan(hidden[0]["zmax"], device=device))
+        target = AD.group_flux(run, Xh)[1][:, 0]
     sb = AD.SourceBatch(run, species, z_max=[p["zmax"] for p in pts], initial_z=zi)
     plan = sb.plan(zi, device=device, ckpt_every=32)
-    t = {"gamma": torch.tensor([p["gamma"] for p in pts], requires_grad=True),
-         "lg_rmax": torch.tensor([np.log10(p["rmax"]) for p in pts], requires_grad=True),
-         "frac": torch.tensor(np.array([p["frac"] for p in pts]), requires_grad=True),
-         "m": torch.tensor([p["m"] for p in pts], requires_grad=True)}
+    t = tensors(pts)
     scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
-    seed = torch.ones((run.dim_states, len(pts)), dtype=torch.float64)
-    fwd, bwd = [], []
+    fwd, bwd, tot = [], [], []
     for rep in range(2):
-        G = sb.grids(t["gamma"], t["lg_rmax"], t["frac"])
-        coeff = sb.coefficients(t["m"])
+        for v in list(t.values()) + [scale]:
+            v.grad = None
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        G = sb.grids(t["gamma"], t["lg_rmax"], t["frac"])
+        coeff = sb.coefficients(t["m"])
         X = AD.PropagateFunction.apply(G, coeff, scale, plan)
+        loss = AD.log_ratio_loss(run, X, target).sum()
+        torch.cuda.synchronize()
         t1 = time.perf_counter()
-        (seed * X).sum().backward()
+        loss.backward()
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         fwd.append(t1 - t0)
         bwd.append(t2 - t1)
-    return {"points": len(pts), "ckpt_every": 32, "forward_ckpt_s": fwd[-1], "adjoint_s": bwd[-1],
-            "params_per_point": 8, "with_photon_scale": True}
+        tot.append(t2 - t0)
+    grads_finite = all(bool(torch.isfinite(v.grad).all()) for v in list(t.values()) + [scale])
+    return {"points": len(pts), "ckpt_every": 32, "loss": "sum_k sum_{E>10^9.5 GeV} ln(F_k/T)^2",
+            "forward_ckpt_s": fwd[-1], "adjoint_s": bwd[-1], "gradient_s": tot[-1],
+            "params_per_point": 8, "with_photon_scale": True, "grads_finite": grads_finite}
 
 
-def cpu_line(pts, zi, sched, K_total, samples_steps=20, processes=None):
+CPU_SAMPLE_STEPS = 20   # two rate windows at dz = 1e-3 and the 0.01 refresh threshold
+
+
+def cpu_line(pts, zi, sched, processes=None, sampler=None):
+    """The CPU oracle of the reference solver on a bounded sample of this workload."""
     from oracle import cpu_bench
 
-    procs = processes or min(os.cpu_count() or 1, 8)
-    k_sample = min(len(pts), 2 * procs)
-    samples = cpu_bench.measure("network_run", pts[:k_sample], zi, 1e-3, samples_steps, 0.01, processes=procs)
-    rate, t_full = cpu_bench.extrapolate(samples, K_total, sched.n_steps, len(sched.z_window))
-    return {"value": rate, "unit": "spectra/s", "cores": procs, "kind": "port",
-            "sample": (f"CPU oracle of the reference solver (scipy SpMM + numpy fold), {procs} processes x "
-                       f"{k_sample // procs} columns x {samples_steps} steps from z={zi:.3f} incl. the window fold; "
-                       f"extrapolated linearly in columns to {K_total} columns x {sched.n_steps} steps, "
-                       f"{len(sched.z_window)} windows (t_full={t_full:.1f} s)")}
+    own = sampler is None
+    if own:
+        sampler = cpu_bench.Sampler("network_run", pts, zi, 1e-3, 0.01,
+                                    processes or cpu_bench.default_processes())
+    try:
+        samples, wall = sampler.sample(CPU_SAMPLE_STEPS)
+    finally:
+        if own:
+            sampler.close()
+    rate, t_full = cpu_bench.extrapolate(samples, sched.n_steps, len(sched.z_window))
+    return {"value": rate, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": "port",
+            "sample": cpu_bench.describe(sampler, CPU_SAMPLE_STEPS, sched.n_steps, len(sched.z_window), t_full),
+            "sample_wall_s": wall}
 
 
 def main():
@@ -408,7 +444,7 @@ def main():
     dist, rank, ws, local = _dist()
     line, run, pts, zi, sched = run_b200(args, dist, rank, ws, local)
     if rank == 0 and ws == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_line(pts, zi, sched, args.points)
+        line["cpu_baseline"] = cpu_line(pts, zi, sched)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -417,38 +453,56 @@ def main():
 
 
 def reference_arm(args):
+    """The reference's CPU algorithm (its restatement in ``oracle/``) on the host cores.
+
+    Each step is one bounded sample of the workload (every column, 20 redshift
+    steps, window refreshes timed apart) by the same sampler as the GPU arm's
+    ``cpu_baseline``; ``value`` is the mean extrapolated full-solve throughput
+    over the timed steps and ``ms_per_step`` the mean wall time of one sample.
+    """
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from prince_b200.schedule import make_schedule, z_grid
-    from workloads import draw_points, network_run
+    from workloads import network_run
     from oracle import cpu_bench
 
+    from oracle import etd2_oracle as O
+
     run = network_run()
-    pts = draw_points(run, args.points, seed=1000, z_range=args.z_range)
+    pts = rank_points(run, args.points, 0, args.z_range)
     zi = max(p["zmax"] for p in pts)
     sched = make_schedule(z_grid(zi, 0.0, 1e-3), run.backend.update_rates_z_threshold)
-    procs = min(os.cpu_count() or 1, 8)
-    k_sample = min(args.points, 2 * procs)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        samples = cpu_bench.measure("network_run", pts[:k_sample], zi, 1e-3, 10, 0.01, processes=procs)
-        rate, _ = cpu_bench.extrapolate(samples, args.points, sched.n_steps, len(sched.z_window))
-        if i >= args.warmup:
-            vals.append(rate)
+    probe = O.OracleSolver(run, zi, 0.0, K=1)
+    probe._refresh(zi, first=True)    # the off-diagonal pattern of the first window
+    config = workload_config(run, sched, args.points, ws, probe.M_off.nnz)
+    del run, probe
+    sampler = cpu_bench.Sampler("network_run", pts, zi, 1e-3, 0.01, cpu_bench.default_processes())
+    vals, walls = [], []
+    try:
+        for i in range(args.warmup + args.steps):
+            samples, wall = sampler.sample(CPU_SAMPLE_STEPS)
+            rate, t_full = cpu_bench.extrapolate(samples, sched.n_steps, len(sched.z_window))
+            if i >= args.warmup:
+                vals.append(rate)
+                walls.append(wall)
+    finally:
+        sampler.close()
     value = statistics.mean(vals)
     line = {
         "metric": METRIC, "value": value, "unit": "spectra/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "warmup": args.warmup, "ms_per_step": statistics.mean(walls) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded synthetic photo-nuclear model and source points)",
-        "config": {"workload": WORKLOAD, "points_per_gpu": args.points, "n_states": run.dim_states},
+        "config": config,
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": procs, "kind": "port",
-                         "sample": (f"per step: {procs} processes x {k_sample // procs} columns x 10 z-steps of the "
-                                    f"CPU oracle incl. a window fold, extrapolated to {args.points} columns x "
-                                    f"{sched.n_steps} steps")},
+        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": "port",
+                         "sample": "per step: " + cpu_bench.describe(sampler, CPU_SAMPLE_STEPS, sched.n_steps,
+                                                                     len(sched.z_window), t_full),
+                         "spread": [min(vals), max(vals)]},
         "e2e": {"value": value, "unit": "spectra/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_note": "a step is one bounded CPU sample; ms_per_step is its wall time",
     }
     print(json.dumps(line), flush=True)
 
