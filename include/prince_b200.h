@@ -50,6 +50,9 @@ extern "C" {
 #define PB_INFO_FD_DENSE 8       /* 1 if the forward FD term runs the register-blocked dense stencil */
 #define PB_OPT_TMA_STAGING 9     /* 1 (default): bin-local kernel stages by TMA (tensor maps); 0: cp.async */
 #define PB_INFO_LAST_TMA 10      /* 1 if the last pb_solve staged the bin-local kernel by TMA */
+#define PB_OPT_STAGING_WAIT_TRIES 11 /* polls of k_slab's bounded staging wait before it gives up and the solve
+                                     returns PB_ERR_DEVICE (default 2^24; < 0 restores it; 0 gives up at
+                                     once, which tests the error path). The CTA still drains its copies. */
 
 typedef struct pb_context pb_context;
 
@@ -243,26 +246,35 @@ int pb_integrate_const(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
 #define PB_NOALLOC_MAX_STEPS 16384
 
 /* pb_integrate_const for callers that cannot allocate device memory: code
- * running inside another framework's custom-call or FFI handler (which must
- * use the buffers it is handed), hosts that reserved all device memory up
- * front, and code that must not call cudaMalloc while a CUDA graph is being
- * captured.  No counterpart in the reference (its solvers allocate freely).
+ * running inside another framework's custom-call or FFI handler, which may
+ * only use the buffers it is handed, and hosts that reserved all device memory
+ * up front, where a cudaMalloc would fail or take memory the host already
+ * promised elsewhere.  No counterpart in the reference (its solvers allocate
+ * freely).
  *
  * Every pointer is a DEVICE pointer owned by the caller: d (n), the CSR arrays
- * of L_off (indptr may be NULL when nnz == 0), z_grid (n_steps + 1) and state
- * (n, advanced in place).  The call allocates and frees nothing: its scratch
- * (about 6 MB) is one static device array sized for at most
- * PB_NOALLOC_MAX_STATES states and PB_NOALLOC_MAX_STEPS steps; larger sizes are
- * rejected with PB_ERR_ARG.  Every GPU that loads the library holds that array
- * until the process exits.
+ * of L_off (indptr n + 1 int64, indices and values nnz each; indptr may be
+ * NULL when nnz == 0), z_grid (n_steps + 1) and state (n, advanced in place).
+ * Before any step, a check kernel verifies that indptr[0] = 0, that indptr
+ * never decreases, that indptr[n] = nnz and that every column index lies in
+ * [0, n); a malformed CSR is rejected with PB_ERR_ARG and nothing else runs.
+ * The buffers themselves must hold the sizes above: the library cannot check
+ * a device allocation's extent.
+ *
+ * The call allocates and frees nothing: its scratch (about 6 MB) is one static
+ * device array sized for at most PB_NOALLOC_MAX_STATES states and
+ * PB_NOALLOC_MAX_STEPS steps; larger sizes are rejected with PB_ERR_ARG.  Every
+ * GPU that loads the library holds that array until the process exits.
  *
  * The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress) and caches it; make that first call before any
- * stream capture.  All calls share the one array and it keeps the last call's
- * contents; each call rewrites every part it reads before reading it.  Calls
- * whose work overlaps on the GPU (other contexts' streams, other host threads)
- * race on the shared scratch and must be serialised by the caller.  Work runs
- * on the context's stream; the call returns after it completes. */
+ * (cudaGetSymbolAddress) and caches it for the life of the process, which
+ * assumes the device's primary context is never reset (cudaDeviceReset)
+ * while the library is loaded.  All calls share the one array and it keeps the
+ * last call's contents; each call rewrites every part it reads before reading
+ * it.  Calls whose work overlaps on the GPU (other contexts' streams, other host
+ * threads) race on the shared scratch and must be serialised by the caller.
+ * Work runs on the context's stream, and the call synchronises that stream
+ * before it returns. */
 int pb_integrate_const_noalloc(pb_context* ctx, int64_t n, const double* d, int64_t nnz,
                                const int64_t* indptr, const int32_t* indices, const double* values,
                                int64_t n_steps, const double* z_grid, double* state);

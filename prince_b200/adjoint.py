@@ -29,7 +29,6 @@ import torch
 
 from . import _lib
 from . import constants as C
-from .data import EnergyGrid
 from .photonfields import device_components
 from .schedule import make_schedule, z_grid
 from .solvers import DeviceRun
@@ -61,11 +60,19 @@ class Plan:
         self.n_active = np.searchsorted(np.sort(first), np.arange(self.sched.n_steps), side="right").astype(np.int32)
         self.src_order = np.argsort(self.inv[self.src_col], kind="stable")
         self.dev_src_col = self.inv[self.src_col][self.src_order].astype(np.int32)
+        self.device = int(device)
         self.last_args = None
 
 
 class PropagateFunction(torch.autograd.Function):
-    """X(z=0) = propagate(G, coeff, scale) with a device adjoint as backward."""
+    """X(z=0) = propagate(G, coeff, scale) with a device adjoint as backward.
+
+    ``X`` is returned as a tensor on the plan's GPU, written there by the solve
+    (no host round trip), and the backward hands the incoming gradient of
+    ``X`` to the adjoint as a device pointer.  ``G`` and ``coeff`` (a few MB at
+    the A <= 56 network) are staged through the host; their gradients are
+    returned on ``G``'s device.
+    """
 
     @staticmethod
     def forward(ctx, G, coeff, scale, plan):
@@ -74,29 +81,35 @@ class PropagateFunction(torch.autograd.Function):
         cd = coeff.detach().cpu().numpy()[:, plan.src_order]
         ctx_dev.set_injection(plan.rows, np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
         ctx_dev.set_photon_field(device_components(plan.run.photon_field))
-        X = np.empty((plan.run.dim_states, plan.K))  # filled in the caller's column order
+        dev = torch.device("cuda", plan.device)
+        X = torch.empty((plan.run.dim_states, plan.K), dtype=torch.float64, device=dev)  # caller's column order
         s = float(scale.detach().cpu().item())
         plan.last_args = (np.ascontiguousarray(cd), s)
-        _solve(ctx_dev, plan, cd, X, s)
+        torch.cuda.current_stream(dev).synchronize()
+        _solve(ctx_dev, plan, cd, X, s)   # returns after the library stream completed
         ctx.plan = plan
-        return torch.from_numpy(X).to(G.device)
+        ctx.in_device = G.device
+        return X
 
     @staticmethod
     def backward(ctx, grad_X):
         plan = ctx.plan
-        seed = np.ascontiguousarray(grad_X.detach().cpu().numpy(), dtype=np.float64)  # caller's column order
+        dev = torch.device("cuda", plan.device)
+        seed = grad_X.detach().to(device=dev, dtype=torch.float64).contiguous()  # caller's column order
+        torch.cuda.current_stream(dev).synchronize()
         cd, s = plan.last_args
         gG, gc, gs = _adjoint(plan.dev.ctx, plan, cd, s, seed)
         gG_user = np.empty_like(gG)
         gG_user[:, plan.src_order] = gG
         gc_user = np.empty_like(gc)
         gc_user[:, plan.src_order] = gc
-        dev = grad_X.device
-        return (torch.from_numpy(gG_user).to(dev), torch.from_numpy(gc_user).to(dev),
-                torch.tensor(float(gs.sum()), dtype=torch.float64, device=dev), None)
+        out = ctx.in_device
+        return (torch.from_numpy(gG_user).to(out), torch.from_numpy(gc_user).to(out),
+                torch.tensor(float(gs.sum()), dtype=torch.float64, device=out), None)
 
 
 def _args(plan, coeff, scale, state):
+    """Solve arguments; ``state`` is a host array or a CUDA tensor (written in place)."""
     import ctypes as Cc
 
     keep = []
@@ -126,9 +139,13 @@ def _args(plan, coeff, scale, state):
     args.finj = f(sc.finj)
     args.coeff = f(coeff)
     args.n_active = i(plan.n_active)
-    args.state = state.ctypes.data_as(Cc.POINTER(Cc.c_double))
+    if isinstance(state, torch.Tensor):
+        args.state = Cc.cast(Cc.c_void_p(state.data_ptr()), Cc.POINTER(Cc.c_double))
+        args.state_on_device = 1
+    else:
+        args.state = state.ctypes.data_as(Cc.POINTER(Cc.c_double))
+        args.state_on_device = 0
     args.init_state = 0
-    args.state_on_device = 0
     args.ckpt_every = plan.ckpt_every
     args.out_cols = i(plan.perm)  # solve column -> caller column, for the states and the seed
     return args, keep
@@ -142,6 +159,7 @@ def _solve(ctx, plan, coeff, out, scale):
 
 
 def _adjoint(ctx, plan, coeff, scale, seed):
+    """Device adjoint; ``seed`` is a contiguous CUDA tensor (n x K, caller's column order)."""
     import ctypes as Cc
 
     dummy = np.zeros(1)  # the adjoint reads no state through args
@@ -151,7 +169,8 @@ def _adjoint(ctx, plan, coeff, scale, seed):
     gc = np.zeros((plan.sched.n_steps, n_src))
     gs = np.zeros(plan.K)
     P = lambda a: a.ctypes.data_as(Cc.POINTER(Cc.c_double))
-    ctx._check(ctx.lib.pb_adjoint(ctx.h, Cc.byref(args), P(seed), 0, P(gG), P(gc), P(gs)), "pb_adjoint")
+    seed_p = Cc.cast(Cc.c_void_p(seed.data_ptr()), Cc.POINTER(Cc.c_double))
+    ctx._check(ctx.lib.pb_adjoint(ctx.h, Cc.byref(args), seed_p, 1, P(gG), P(gc), P(gs)), "pb_adjoint")
     return gG, gc, gs
 
 
@@ -208,45 +227,38 @@ class SourceBatch:
 def group_flux(run, X, egrid=None):
     """All-particle flux of the nuclei on the common total-energy grid (torch, differentiable).
 
-    Per species: total energy A E_i, spectrum state / A, log-log interpolated to
-    the common grid ``EnergyGrid(lo, hi + log10 A_max, 4 bins/decade-multiple)``
-    and summed (``propagation.py:103-167``).  States below 1e-30 of the
-    species' maximum (including non-positive ones) are floored at that level
-    before the logarithm.
+    The reference's ``get_solution_group("CR", epow=3)`` (``propagation.py:103-167``)
+    for every column of ``X`` (n x K) at once, through the batched projector of
+    ``prince_b200.results``: positive bins interpolated in log-log, zero outside
+    each species' positive span.  Returns ``(common grid, flux (G x K))``.
     """
+    from .results import GroupProjector, common_energy_grid, select_species
+
     sm = run.spec_man
-    cr = run.cr_grid
-    nuclei = [s for s in sm.species_refs if s.is_nucleus]
+    species = select_species(sm, "CR")
     if egrid is None:
-        step = np.log10(cr.grid[1] / cr.grid[0])
-        lo = np.log10(cr.bins[0])
-        hi = np.log10(cr.bins[-1]) + np.log10(max(s.A for s in nuclei))
-        egrid = EnergyGrid(lo, hi, 4.0 / step).grid
-    lge = np.log(egrid)
-    total = torch.zeros((egrid.size, X.shape[1]), dtype=X.dtype, device=X.device)
-    for s in nuclei:
-        le = np.log(s.A * cr.grid)
-        j = np.clip(np.searchsorted(le, lge) - 1, 0, le.size - 2)
-        w = (lge - le[j]) / (le[j + 1] - le[j])
-        inside = (lge >= le[0]) & (lge <= le[-1])
-        y = X[s.lidx():s.uidx()] / s.A
-        # floor at 1e-30 of the species' maximum (per column): values below it are
-        # treated as the floor, so the logarithm and its derivative stay bounded
-        floor = (1e-30 * y.abs().amax(dim=0)).clamp(min=1e-300)
-        ly = torch.log(torch.maximum(y, floor[None, :]))
-        jt = torch.tensor(j, device=X.device)
-        wt = torch.tensor(w, dtype=X.dtype, device=X.device)[:, None]
-        val = torch.exp((1 - wt) * ly[jt] + wt * ly[jt + 1])
-        total = total + val * torch.tensor(inside.astype(np.float64), dtype=X.dtype, device=X.device)[:, None]
-    return torch.tensor(egrid, dtype=X.dtype, device=X.device), total
+        egrid = common_energy_grid(run.cr_grid, max(s.A for s in sm.species_refs))
+    key = ("_b200_group_projector", tuple(species), len(egrid), float(egrid[0]), float(egrid[-1]))
+    cache = run.__dict__.setdefault("_b200_projectors", {})
+    if key not in cache:
+        cache[key] = GroupProjector(sm, run.cr_grid.grid, species, egrid)
+    pr = cache[key]
+    F = pr(X, 3).sum(dim=0)
+    return torch.as_tensor(pr.com, dtype=X.dtype, device=X.device), F
 
 
-def log_ratio_loss(run, X, target, e_min=10 ** 9.5, dynamic_range=1e-30):
+def log_ratio_loss(run, X, target, e_min=10 ** 9.5, dynamic_range=0.0):
     """sum over bins with E > e_min of ln(F_k(E) / T(E))^2, per column (K).
 
-    Bins where the target is below ``dynamic_range`` of its maximum (beyond the
-    end of the spectra) are left out, so the loss stays finite.
+    ``F_k`` is the all-particle flux of column k (``group_flux``).  Bins where
+    the target is zero or below ``dynamic_range`` of its maximum, and bins where
+    the column's flux is zero (beyond the span of the spectra), are left out,
+    so the loss stays finite.
     """
     egrid, F = group_flux(run, X)
-    sel = (egrid > e_min) & (target > dynamic_range * target.max())
-    return ((torch.log(F[sel]) - torch.log(target[sel, None])) ** 2).sum(dim=0)
+    T = torch.as_tensor(target, dtype=F.dtype, device=F.device)
+    sel = (egrid > e_min) & (T > 0) & (T > dynamic_range * T.max())
+    Fs, Ts = F[sel], T[sel][:, None]
+    ok = Fs > 0
+    r = torch.log(torch.where(ok, Fs, torch.ones_like(Fs))) - torch.log(Ts)
+    return torch.where(ok, r * r, torch.zeros_like(r)).sum(dim=0)

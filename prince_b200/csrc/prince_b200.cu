@@ -76,6 +76,7 @@ struct DBuf {
 
 }  // namespace
 
+constexpr long long kWaitTries = 1ll << 24;  // polls of a bounded wait (well above any staging time)
 struct pb_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -161,6 +162,7 @@ struct pb_context {
   size_t slabT_smem = 0, bandT_smem = 0;
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
   int32_t tma_mode = 1;             // 1: k_slab stages by TMA when tensor maps can be encoded; 0: cp.async
+  long long staging_wait_tries = kWaitTries;  // k_slab's first staging wait (PB_OPT_STAGING_WAIT_TRIES)
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -543,6 +545,7 @@ struct StepParams {
   int64_t step;
   int step_w;        // rate window of this step (k_slab's entry values), set with step
   const CUtensorMap* tmap_src;  // k_slab: tensor map of src for the TMA staging, or null (cp.async staging)
+  long long wait_tries;         // k_slab: polls of the staging wait before it gives up (the drain keeps kWaitTries)
   int* err;          // set to a nonzero code when a bounded wait gives up
   int64_t n_steps;
   uint32_t flags;
@@ -760,15 +763,32 @@ __global__ void k_prep(StepParams p) {
 // GPU that loads the library holds it until exit).  Layout, in bytes from the
 // start: a and F(x) (n doubles each), the row factors (8 n doubles), the
 // per-step h and dl/dz (s doubles each), the window index (s ints), the row
-// list (n ints) and an all-zero row pointer (n + 1 int64), for n = the
-// state limit and s = the step limit.
+// list (n ints), an all-zero row pointer (n + 1 int64) and a 256-byte status
+// block (the CSR check's flag), for n = the state limit and s = the step limit.
 // ---------------------------------------------------------------------------
 constexpr int64_t kNaMaxStates = PB_NOALLOC_MAX_STATES;
 constexpr int64_t kNaMaxSteps = PB_NOALLOC_MAX_STEPS;
 constexpr size_t kNaBytes = (size_t)kNaMaxStates * 10 * sizeof(double) + (size_t)kNaMaxSteps * 2 * sizeof(double) +
                             (size_t)kNaMaxSteps * sizeof(int) + (size_t)kNaMaxStates * sizeof(int) +
-                            (size_t)(kNaMaxStates + 1) * sizeof(int64_t);
+                            (size_t)(kNaMaxStates + 1) * sizeof(int64_t) + 256;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+// Validates a caller's CSR before any step kernel reads through it: indptr
+// starts at 0, never decreases and ends at nnz, and every column index lies in
+// [0, n).  Reads stay inside the sizes the caller declared (n + 1 row
+// pointers, nnz indices); a violation sets bit 0 (row pointers) or bit 1
+// (indices) of *flag.
+__global__ void k_noalloc_check_csr(int64_t n, int64_t nnz, const int64_t* __restrict__ indptr,
+                                    const int32_t* __restrict__ indices, unsigned int* __restrict__ flag) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && indptr[i] > indptr[i + 1]) atomicOr(flag, 1u);
+  if (i == 0 && indptr[0] != 0) atomicOr(flag, 1u);
+  if (i == n && indptr[n] != nnz) atomicOr(flag, 1u);
+  if (i < nnz) {
+    const int32_t c = indices[i];
+    if (c < 0 || (int64_t)c >= n) atomicOr(flag, 2u);
+  }
+}
 
 __global__ void k_noalloc_fill(int64_t n, int64_t n_steps, const double* __restrict__ z, double* __restrict__ h,
                                double* __restrict__ ones, int* __restrict__ win, int* __restrict__ rows,
@@ -1074,7 +1094,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-constexpr long long kWaitTries = 1ll << 24;  // polls of a bounded wait (well above any staging time)
 constexpr int kErrStagingWait = 1;           // err code: a k_slab CTA's staging wait gave up
 
 // fdbuf = D_off (kappa v) for every row.  CTA = (species block, 32-column
@@ -1374,7 +1393,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
     src1 = p.src_ptr[col + 1];
   }
   if (p.tmap_src) {
-    if (!mbar_wait_bounded(stage_bar, 0, kWaitTries)) {  // the copies did not land: report and leave
+    if (!mbar_wait_bounded(stage_bar, 0, p.wait_tries)) {  // the copies did not land: report and leave
       if (threadIdx.x == 0) atomicExch(p.err, kErrStagingWait);
       mbar_wait_bounded(stage_bar, 0, kWaitTries);
       return;
@@ -2394,6 +2413,7 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.n = n;
   p.ld = ld;
   p.flags = flags;
+  p.wait_tries = c->staging_wait_tries;
   if (!pair) p.flags &= ~PB_PAIRPROD;
   if (!inj) p.flags &= ~PB_INJECTION;
   p.h = c->s_h.as<double>();
@@ -3480,6 +3500,11 @@ int pb_set_option(pb_context* c, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(c, PB_ERR_ARG, "pb_set_option: TMA staging must be 0 or 1");
       c->tma_mode = (int32_t)value;
       return PB_OK;
+    case PB_OPT_STAGING_WAIT_TRIES:
+      if (value < 0) c->staging_wait_tries = kWaitTries;
+      else if (value > kWaitTries) return fail(c, PB_ERR_ARG, "pb_set_option: staging wait above %lld polls", kWaitTries);
+      else c->staging_wait_tries = (long long)value;
+      return PB_OK;
   }
   return fail(c, PB_ERR_ARG, "pb_set_option: unknown key %d", key);
 }
@@ -3490,6 +3515,7 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
   switch (key) {
     case PB_OPT_BATCHED_KERNELS: *value = c->batched_mode; return PB_OK;
     case PB_OPT_TMA_STAGING: *value = c->tma_mode; return PB_OK;
+    case PB_OPT_STAGING_WAIT_TRIES: *value = c->staging_wait_tries; return PB_OK;
     case PB_INFO_LAST_TMA: *value = c->last_tma ? 1 : 0; return PB_OK;
     case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
@@ -3732,6 +3758,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)a->ckpt_every);
     put((uint64_t)blocked);
     put((uint64_t)(blocked && c->tma_ok));
+    put((uint64_t)c->staging_wait_tries);
     put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
     put((uint64_t)c->slab_nent);
     put((uint64_t)c->em_W);
@@ -4139,6 +4166,8 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
     indptr = zp.data();
   } else {
     if (indptr[0] != 0 || indptr[n] != nnz) return fail(c, PB_ERR_ARG, "pb_integrate_const: indptr must run from 0 to nnz");
+    for (int64_t r = 0; r < n; ++r)
+      if (indptr[r] > indptr[r + 1]) return fail(c, PB_ERR_ARG, "pb_integrate_const: indptr must not decrease");
     for (int64_t j = 0; j < nnz; ++j)
       if (indices[j] < 0 || indices[j] >= n) return fail(c, PB_ERR_ARG, "pb_integrate_const: column out of range");
   }
@@ -4216,7 +4245,9 @@ int pb_integrate_const(pb_context* c, int64_t n, const double* d, int64_t nnz, c
 // No-allocation variant of pb_integrate_const.  The scratch is the static
 // device array g_noalloc_scratch; its device address is looked up with
 // cudaGetSymbolAddress once per device (on that device's first call) and
-// cached.  Nothing here allocates or frees device memory.
+// cached, which assumes the device's primary context lives as long as the
+// process (a cudaDeviceReset by any component of the process invalidates the
+// cached address).  Nothing here allocates or frees device memory.
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[64] = {nullptr};
 
@@ -4256,7 +4287,26 @@ int pb_integrate_const_noalloc(pb_context* c, int64_t n, const double* d, int64_
   int* win = reinterpret_cast<int*>(ones + kNaMaxSteps);
   int* rows = win + kNaMaxSteps;
   int64_t* zero_indptr = reinterpret_cast<int64_t*>(rows + kNaMaxStates);
+  unsigned int* csr_flag = reinterpret_cast<unsigned int*>(zero_indptr + kNaMaxStates + 1);
   cudaStream_t st = c->stream;
+  if (nnz > 0) {
+    // The step kernels index state[indices[j]] for j in [indptr[r], indptr[r+1]):
+    // check the caller's CSR first, and run nothing on a malformed one.
+    unsigned int bad = 0;
+    cudaError_t e = cudaMemsetAsync(csr_flag, 0, sizeof(unsigned int), st);
+    if (e == cudaSuccess) {
+      k_noalloc_check_csr<<<blocks_for(std::max<int64_t>(n + 1, nnz), 256), 256, 0, st>>>(n, nnz, indptr, indices,
+                                                                                         csr_flag);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, csr_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_integrate_const_noalloc: %s", cudaGetErrorString(e));
+    if (bad & 1u)
+      return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: malformed CSR row pointers (need indptr[0] = 0, "
+                                 "non-decreasing, indptr[n] = nnz)");
+    if (bad & 2u) return fail(c, PB_ERR_ARG, "pb_integrate_const_noalloc: CSR column index outside [0, n)");
+  }
   const int64_t fill = std::max<int64_t>(n + 1, n_steps);
   k_noalloc_fill<<<blocks_for(fill, 256), 256, 0, st>>>(n, n_steps, z_grid, h, ones, win, rows, zero_indptr);
   StepParams p;

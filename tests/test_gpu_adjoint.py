@@ -169,15 +169,19 @@ def test_adjoint_against_oracle_differences(light):
             run.set_photon_field(pf.CMBPhotonSpectrum())
         return float(AD.log_ratio_loss(run, torch.tensor(Xo), target, dynamic_range=1e-12).sum())
 
-    for key in ("gamma", "m"):
+    for key in ("gamma", "lg_rmax", "m", "frac"):
         for k in range(K):
-            def f(step):
-                pp = {kk: np.array(v, dtype=np.float64) for kk, v in p.items()}
-                pp[key][k] += step
-                return oracle_loss(pp, 1.0)
-            fd = _central(f, 1e-5)
-            g = float(t[key].grad[k])
-            assert abs(g - fd) / abs(fd) < TOL, (key, k, g, fd)
+            for i in (range(len(species)) if key == "frac" else [None]):
+                def f(step):
+                    pp = {kk: np.array(v, dtype=np.float64) for kk, v in p.items()}
+                    if i is None:
+                        pp[key][k] += step
+                    else:
+                        pp[key][k, i] += step
+                    return oracle_loss(pp, 1.0)
+                fd = _central(f, 1e-5)
+                g = float(t[key].grad[k] if i is None else t[key].grad[k, i])
+                assert abs(g - fd) / abs(fd) < TOL, (key, k, i, g, fd)
     fd = _central(lambda st: oracle_loss(p, 1.0 + st), 1e-5)
     assert abs(float(scale.grad) - fd) / abs(fd) < TOL, (float(scale.grad), fd)
 
@@ -196,7 +200,7 @@ def test_blocked_and_row_kernel_adjoints_agree():
     plan = sb.plan(0.2, ckpt_every=16)
     ctx = plan.dev.ctx
     assert ctx.info(_lib.PB_INFO_BLOCKED_LAYOUT) == 1
-    seed = torch.tensor(rng.uniform(0.5, 1.5, (run.dim_states, K)))
+    seed = torch.tensor(rng.uniform(0.5, 1.5, (run.dim_states, K)), device="cuda:0")
     grads = []
     for mode in (0, 1):
         ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, mode)

@@ -299,3 +299,35 @@ def test_full_network_batched_short_range_vs_oracle():
     worst, above, total = local_scale_check(m.state, ref, _blocks(run), tol=TOL)
     assert worst <= TOL, (worst, above, total)
     assert above <= 1e-4 * total, (above, total)
+
+
+def test_staging_wait_gives_up_cleanly_and_the_next_solve_is_correct(medium_run):
+    """k_slab's bounded staging wait: with a zero poll limit every CTA gives up at
+    once, records the error, drains its own copies (normal limit) and returns;
+    the solve raises RuntimeError (PB_ERR_DEVICE).  With the limit restored the
+    same context solves again and matches the oracle."""
+    from prince_b200 import _lib
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, point_source
+    run = medium_run
+    K = 19
+    pts = draw_points(run, K, seed=31, z_range=(0.02, 0.04))
+    srcs = [point_source(run, p) for p in pts]
+    zi = max(p["zmax"] for p in pts)
+    m = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=K)
+    for k, s in enumerate(srcs):
+        m[k].add_source_class(s)
+    ctx = m._dev.ctx
+    ctx.set_option(_lib.PB_OPT_TMA_STAGING, 1)
+    ctx.set_option(_lib.PB_OPT_STAGING_WAIT_TRIES, 0)
+    try:
+        with pytest.raises(RuntimeError, match="gave up waiting"):
+            m.solve(dz=1e-3)
+        assert ctx.info(_lib.PB_INFO_LAST_TMA) == 1
+    finally:
+        ctx.set_option(_lib.PB_OPT_STAGING_WAIT_TRIES, -1)
+    assert ctx.info(_lib.PB_OPT_STAGING_WAIT_TRIES) == 1 << 24
+    m.solve(dz=1e-3)
+    assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == 1 and ctx.info(_lib.PB_INFO_LAST_TMA) == 1
+    ref = O.OracleSolver(run, zi, 0.0, K=K, exp="cr").solve([[s] for s in srcs], dz=1e-3)
+    assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
