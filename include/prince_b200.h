@@ -90,12 +90,25 @@ int pb_set_fold_kernel(pb_context* ctx, int64_t n_entries, int32_t n_photon,
  * Replaces: the ph_grid.grid argument of photon_vector (interaction_rates.py:105-116). */
 int pb_set_photon_grid(pb_context* ctx, int32_t n_photon, const double* energies);
 
-/* Analytic photon field: n_comp components, kinds[i] in {0: CMB black body,
- * 1: flat, 2: grey body}, params[3*i .. 3*i+2] = (p0, p1, p2) as documented in
- * prince_b200/photonfields.py.  Replaces: PhotonField.get_photon_density for
- * the analytic fields (src/prince_cr/photonfields.py:27-127). */
+/* Photon field: the sum of n_comp components, kinds[i] in {0: CMB black body,
+ * 1: flat, 2: grey body, 3: the tabulated field of pb_set_photon_table},
+ * params[3*i .. 3*i+2] = (p0, p1, p2) as documented in
+ * prince_b200/photonfields.py (ignored for kind 3).  Replaces:
+ * PhotonField.get_photon_density for the analytic fields and their sums
+ * (src/prince_cr/photonfields.py:27-127). */
 int pb_set_photon_field(pb_context* ctx, int32_t n_comp, const int32_t* kinds,
                         const double* params);
+
+/* Tabulated photon field for kind 3: log10 dn/de [GeV^-1 cm^-3] on a regular
+ * grid of nz increasing redshifts and ne increasing log10 energies [GeV]
+ * (log10_density is nz x ne, row-major), interpolated bilinearly in
+ * (z, log10 E) and zero outside the table.  Replaces: the corrected
+ * tabulated EBL models CIBGilmore2012 / CIBFranceschini2008 and their
+ * RegularGridInterpolator (src/prince_cr/photonfields.py:227-345), used by the
+ * rate fold's photon vector and by the Bethe-Heitler loss
+ * (interaction_rates.py:1296-1312). */
+int pb_set_photon_table(pb_context* ctx, int32_t nz, int32_t ne, const double* z, const double* log10_e,
+                        const double* log10_density);
 
 /* Finite-difference loss operator split into its off-diagonal CSR part
  * (D_off, nnz entries) and its diagonal (n_states).

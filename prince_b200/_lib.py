@@ -66,6 +66,7 @@ _PROTOS = {
     "pb_set_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
     "pb_set_photon_grid": (C.c_int, [_vp, C.c_int32, _d]),
     "pb_set_photon_field": (C.c_int, [_vp, C.c_int32, _i32, _d]),
+    "pb_set_photon_table": (C.c_int, [_vp, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
@@ -179,7 +180,13 @@ class Context:
         e = _f64(energies)
         self._check(self.lib.pb_set_photon_grid(self.h, int(e.size), _ptr(e, C.c_double)), "pb_set_photon_grid")
 
-    def set_photon_field(self, components):
+    def set_photon_field(self, components, table=None):
+        """Field components ``(kind, p0, p1, p2)``; ``table = (z, log10 E, log10 dn/de)`` for kind 3."""
+        if table is not None:
+            tz, tle, tv = _f64(table[0]), _f64(table[1]), _f64(table[2])
+            self._check(self.lib.pb_set_photon_table(self.h, int(tz.size), int(tle.size), _ptr(tz, C.c_double),
+                                                     _ptr(tle, C.c_double), _ptr(tv, C.c_double)),
+                        "pb_set_photon_table")
         kinds = _i32a([c[0] for c in components])
         pars = _f64([list(c[1:4]) for c in components]).reshape(-1)
         self._check(self.lib.pb_set_photon_field(self.h, int(kinds.size), _ptr(kinds, C.c_int32),

@@ -29,7 +29,7 @@ import torch
 
 from . import _lib
 from . import constants as C
-from .photonfields import device_components
+from .photonfields import device_components, device_table
 from .schedule import make_schedule, z_grid
 from .solvers import DeviceRun
 
@@ -80,7 +80,8 @@ class PropagateFunction(torch.autograd.Function):
         Gd = G.detach().cpu().numpy()[:, plan.src_order]
         cd = coeff.detach().cpu().numpy()[:, plan.src_order]
         ctx_dev.set_injection(plan.rows, np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
-        ctx_dev.set_photon_field(device_components(plan.run.photon_field))
+        ctx_dev.set_photon_field(device_components(plan.run.photon_field),
+                                 table=device_table(plan.run.photon_field))
         dev = torch.device("cuda", plan.device)
         X = torch.empty((plan.run.dim_states, plan.K), dtype=torch.float64, device=dev)  # caller's column order
         s = float(scale.detach().cpu().item())

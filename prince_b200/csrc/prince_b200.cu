@@ -103,6 +103,8 @@ struct pb_context {
   int32_t n_comp = 0;
   int32_t comp_kind[8];
   double comp_par[8][3];
+  DBuf tab_z, tab_le, tab_v;        // tabulated photon field (kind 3)
+  int32_t tab_nz = 0, tab_ne = 0;
   // FD operator
   int64_t nnzD = 0;
   DBuf d_indptr, d_indices, d_vals, d_diag;
@@ -229,7 +231,41 @@ struct FieldDesc {
   int kind[8];
   double p[8][3];
   double scale;
+  // kind 3: a tabulated field, log10 dn/de on a regular (z, log10 E) grid
+  const double* tz;    // tnz redshifts, increasing
+  const double* tle;   // tne log10 energies [GeV], increasing
+  const double* tv;    // tnz x tne log10 densities [GeV^-1 cm^-3]
+  int tnz, tne;
 };
+
+// Interval of x on an increasing grid g[0..m-1] for linear interpolation:
+// i with g[i] < x <= g[i+1], clamped to [0, m-2] (x = g[0] falls in the first).
+__device__ __forceinline__ int grid_interval(const double* __restrict__ g, int m, double x) {
+  int lo = 0, hi = m;  // first index with g[idx] >= x
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (g[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return min(max(lo - 1, 0), m - 2);
+}
+
+// Tabulated field (photonfields.py:227-345, the corrected EBL classes):
+// log10 dn/de interpolated bilinearly in (z, log10 E), zero outside the table.
+__device__ double table_density(const FieldDesc& f, double E, double z) {
+  const double x = log10(E);
+  if (!(z >= f.tz[0] && z <= f.tz[f.tnz - 1] && x >= f.tle[0] && x <= f.tle[f.tne - 1])) return 0.0;
+  const int i = grid_interval(f.tz, f.tnz, z), j = grid_interval(f.tle, f.tne, x);
+  const double u = __ddiv_rn(__dadd_rn(z, -f.tz[i]), __dadd_rn(f.tz[i + 1], -f.tz[i]));
+  const double w = __ddiv_rn(__dadd_rn(x, -f.tle[j]), __dadd_rn(f.tle[j + 1], -f.tle[j]));
+  const double* v0 = f.tv + (size_t)i * f.tne + j;
+  const double* v1 = v0 + f.tne;
+  const double cu = __dadd_rn(1.0, -u), cw = __dadd_rn(1.0, -w);
+  double y = __dmul_rn(__dmul_rn(v0[0], cu), cw);
+  y = __dadd_rn(y, __dmul_rn(__dmul_rn(v0[1], cu), w));
+  y = __dadd_rn(y, __dmul_rn(__dmul_rn(v1[0], u), cw));
+  y = __dadd_rn(y, __dmul_rn(__dmul_rn(v1[1], u), w));
+  return exp10(y);
+}
 
 __device__ __forceinline__ double field_density(const FieldDesc& f, double E, double z) {
   double total = 0.0;
@@ -238,6 +274,8 @@ __device__ __forceinline__ double field_density(const FieldDesc& f, double E, do
     double v;
     if (f.kind[c] == 1) {  // flat: (1+z)^2 * n0
       v = __dmul_rn(__dmul_rn(opz, opz), f.p[c][0]);
+    } else if (f.kind[c] == 3) {  // tabulated
+      v = table_density(f, E, z);
     } else {  // black / grey body: ((p0 (1+z)^2) Ered^p2) / (exp(Ered/p1) - 1)
       const double ered = __ddiv_rn(E, opz);
       const double eratio = __ddiv_rn(ered, f.p[c][1]);
@@ -2352,6 +2390,13 @@ FieldDesc field_desc(const pb_context* c, double scale) {
     for (int q = 0; q < 3; ++q) f.p[i][q] = i < c->n_comp ? c->comp_par[i][q] : 0.0;
   }
   f.scale = scale;
+  if (c->tab_nz > 0) {
+    f.tz = c->tab_z.as<double>();
+    f.tle = c->tab_le.as<double>();
+    f.tv = c->tab_v.as<double>();
+    f.tnz = c->tab_nz;
+    f.tne = c->tab_ne;
+  }
   return f;
 }
 
@@ -2369,7 +2414,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
-          &c->slabT_pairs, &c->slabT_wrp, &c->tmaps, &c->d_err};
+          &c->slabT_pairs, &c->slabT_wrp, &c->tmaps, &c->d_err, &c->tab_z, &c->tab_le, &c->tab_v};
 }
 
 // Every device buffer: the solve's and the adjoint's scratch.
@@ -2877,13 +2922,38 @@ int pb_set_photon_field(pb_context* c, int32_t n_comp, const int32_t* kinds, con
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
   if (n_comp < 1 || n_comp > 8 || !kinds || !params) return fail(c, PB_ERR_ARG, "pb_set_photon_field: 1..8 components required");
   for (int i = 0; i < n_comp; ++i) {
-    if (kinds[i] < 0 || kinds[i] > 2) return fail(c, PB_ERR_ARG, "pb_set_photon_field: unknown kind %d", kinds[i]);
-    if (kinds[i] != 1 && !(params[3 * i + 1] > 0.0)) return fail(c, PB_ERR_ARG, "pb_set_photon_field: temperature must be positive");
+    if (kinds[i] < 0 || kinds[i] > 3) return fail(c, PB_ERR_ARG, "pb_set_photon_field: unknown kind %d", kinds[i]);
+    if (kinds[i] == 3 && c->tab_nz == 0)
+      return fail(c, PB_ERR_STATE, "pb_set_photon_field: a tabulated component needs pb_set_photon_table first");
+    if ((kinds[i] == 0 || kinds[i] == 2) && !(params[3 * i + 1] > 0.0))
+      return fail(c, PB_ERR_ARG, "pb_set_photon_field: temperature must be positive");
     c->comp_kind[i] = kinds[i];
     for (int q = 0; q < 3; ++q) c->comp_par[i][q] = params[3 * i + q];
   }
   c->n_comp = n_comp;
   c->have_field = true;
+  return PB_OK;
+}
+
+int pb_set_photon_table(pb_context* c, int32_t nz, int32_t ne, const double* z, const double* log10_e,
+                        const double* log10_density) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (nz < 2 || ne < 2 || !z || !log10_e || !log10_density)
+    return fail(c, PB_ERR_ARG, "pb_set_photon_table: need at least 2 x 2 points and all three arrays");
+  for (int i = 1; i < nz; ++i)
+    if (!(z[i] > z[i - 1])) return fail(c, PB_ERR_ARG, "pb_set_photon_table: redshifts must increase");
+  for (int j = 1; j < ne; ++j)
+    if (!(log10_e[j] > log10_e[j - 1])) return fail(c, PB_ERR_ARG, "pb_set_photon_table: energies must increase");
+  for (int64_t k = 0; k < (int64_t)nz * ne; ++k)
+    if (!std::isfinite(log10_density[k])) return fail(c, PB_ERR_ARG, "pb_set_photon_table: non-finite density entry %lld", (long long)k);
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->tab_z, z, (size_t)nz)) || (rc = upload(c, c->tab_le, log10_e, (size_t)ne)) ||
+      (rc = upload(c, c->tab_v, log10_density, (size_t)nz * ne)))
+    return rc;
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->tab_nz = nz;
+  c->tab_ne = ne;
   return PB_OK;
 }
 

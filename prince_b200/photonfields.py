@@ -8,9 +8,10 @@ evaluator sums.  The device evaluates the same expression in the same
 order, so the per-window photon vectors and the Bethe-Heitler loss
 integrand agree with the host formula to the last bits of ``exp``.
 
-Tabulated EBL models are not describable on the device yet; passing one to
-the GPU solver raises ``NotImplementedError`` rather than evaluating the
-field on the host.
+Tabulated fields (``TabulatedPhotonField``: the corrected EBL tables of
+Gilmore 2012 and Franceschini 2008) are evaluated on the device from their
+table; a field the device cannot describe (the legacy spline EBLs) raises
+``NotImplementedError`` rather than evaluating it on the host.
 
 Kinds (mirrored in ``prince_b200/csrc/prince_b200.cu``):
 
@@ -19,6 +20,10 @@ Kinds (mirrored in ``prince_b200/csrc/prince_b200.cu``):
 * ``PF_FLAT`` (1): ``(1+z)^2 * p0``.
 * ``PF_MBB`` (2): ``((p0 (1+z)^2) Ered^p2) / (exp(Ered/p1) - 1)``, zero
   where ``Ered/p1 >= 709`` -- a modified black body (grey body).
+* ``PF_TABLE`` (3): a tabulated field, ``10^v`` with ``v`` the bilinear
+  interpolation in ``(z, log10 E)`` of a table of ``log10 dn/de``, zero
+  outside the table (the corrected tabulated EBL models of the reference,
+  ``photonfields.py:227-345``).  At most one table per field.
 """
 
 from __future__ import annotations
@@ -32,6 +37,7 @@ from . import constants as C
 PF_CMB = 0
 PF_FLAT = 1
 PF_MBB = 2
+PF_TABLE = 3
 
 
 class PhotonField:
@@ -152,6 +158,116 @@ class ScaledPhotonField(PhotonField):
         return self.field.device_components()
 
 
+class TabulatedPhotonField(PhotonField):
+    """``n(E, z) = 10^v`` with ``v`` linear in ``(z, log10 E)`` between the
+    table's nodes and the field zero outside the table: the log-log
+    interpolation of the reference's corrected EBL classes
+    (``photonfields.py:227-345``, a ``RegularGridInterpolator`` with
+    ``method="linear"`` and ``fill_value=-inf``).
+
+    ``z`` (nz, increasing), ``log10_e`` (ne, log10 E/GeV, increasing) and
+    ``log10_dnde`` (nz x ne, log10 of dn/de in GeV^-1 cm^-3).
+    """
+
+    def __init__(self, z, log10_e, log10_dnde):
+        from scipy.interpolate import RegularGridInterpolator
+
+        self.table_z = np.ascontiguousarray(z, dtype=np.float64)
+        self.table_log10_e = np.ascontiguousarray(log10_e, dtype=np.float64)
+        self.table_log10_dnde = np.ascontiguousarray(log10_dnde, dtype=np.float64)
+        if self.table_log10_dnde.shape != (self.table_z.size, self.table_log10_e.size):
+            raise ValueError("log10_dnde must be (len(z), len(log10_e))")
+        self._rgi = RegularGridInterpolator((self.table_z, self.table_log10_e), self.table_log10_dnde,
+                                            method="linear", bounds_error=False, fill_value=-np.inf)
+
+    def get_photon_density(self, E, z):
+        E = np.atleast_1d(np.asarray(E, dtype=np.float64))
+        pts = np.column_stack([np.full(E.size, float(z)), np.log10(E.reshape(-1))])
+        return (10.0 ** self._rgi(pts)).reshape(E.shape)
+
+    def device_components(self):
+        return [(PF_TABLE, 0.0, 0.0, 0.0)]
+
+    def device_table(self):
+        return self.table_z, self.table_log10_e, self.table_log10_dnde
+
+
+def _ebl_table_file(table_file, name):
+    import os
+
+    if table_file is None:
+        base = os.environ.get("PRINCE_DATA_DIR")
+        if base is None:
+            raise FileNotFoundError(
+                f"{name}: pass table_file=<path to {name}> (the reference ships it in its data "
+                "directory) or set PRINCE_DATA_DIR")
+        table_file = os.path.join(base, name)
+    return table_file
+
+
+class CIBGilmore2012(TabulatedPhotonField):
+    """Gilmore et al. (2012) EBL from the published flux tables, log-log
+    interpolated (the reference's ``CIBGilmore2012``, ``photonfields.py:227-298``).
+
+    ``table_file`` is the reference's ``gilmore2012_ebl_tables.npz`` (keys
+    ``z``, ``log10_eps_eV``, ``log10_eps_dndeps_cm3_<model>``); ``model`` is
+    ``"fiducial"`` or ``"fixed"``.
+    """
+
+    def __init__(self, model="fiducial", simple_scaling=False, table_file=None):
+        if model not in ("fixed", "fiducial"):
+            raise ValueError(f"model must be 'fiducial' or 'fixed', got {model!r}")
+        f = np.load(_ebl_table_file(table_file, "gilmore2012_ebl_tables.npz"))
+        le = f["log10_eps_eV"] - 9.0
+        super().__init__(f["z"], le, f["log10_eps_dndeps_cm3_" + model] - le[None, :])
+
+
+class CIBFranceschini2008(TabulatedPhotonField):
+    """Franceschini et al. (2008) EBL from the paper's tables, log-log
+    interpolated (the reference's ``CIBFranceschini2008``, ``photonfields.py:301-345``).
+
+    ``table_file`` is the reference's ``franceschini2008_ebl_tables.npz``.
+    """
+
+    def __init__(self, simple_scaling=False, table_file=None):
+        f = np.load(_ebl_table_file(table_file, "franceschini2008_ebl_tables.npz"))
+        le = f["log10_eps_eV"] - 9.0
+        super().__init__(f["z"], le, f["log10_eps_dndeps_cm3"] - le[None, :])
+
+
+def _reference_table(field):
+    """The table of the reference's own corrected EBL objects (same attributes as
+    ``photonfields.py:273-283`` / ``324-334``), or ``None``."""
+    if type(field).__name__ in ("CIBGilmore2012", "CIBFranceschini2008") and not hasattr(field, "device_table") \
+            and getattr(field, "_fallback", None) is None and hasattr(field, "_log_dnde"):
+        return (np.asarray(field._z, dtype=np.float64), np.asarray(field._leps_GeV, dtype=np.float64),
+                np.asarray(field._log_dnde, dtype=np.float64))
+    return None
+
+
+def device_table(field):
+    """The one tabulated component of ``field`` as ``(z, log10 E, log10 dn/de)``, or ``None``."""
+    tables = []
+
+    def walk(f):
+        if hasattr(f, "device_table"):
+            tables.append(f.device_table())
+        for sub in getattr(f, "model_list", []):
+            walk(sub)
+        if hasattr(f, "field"):
+            walk(f.field)
+
+    walk(field)
+    if _reference_table(field) is not None:
+        tables.append(_reference_table(field))
+    for sub in getattr(field, "model_list", []):
+        if _reference_table(sub) is not None:
+            tables.append(_reference_table(sub))
+    if len(tables) > 1:
+        raise NotImplementedError("the device evaluates at most one tabulated photon field")
+    return tables[0] if tables else None
+
+
 def device_components(field):
     """Device description of ``field`` (this package's classes, or the reference's
     analytic ``CMBPhotonSpectrum`` / ``FlatPhotonSpectrum`` / ``CombinedPhotonField``
@@ -160,6 +276,8 @@ def device_components(field):
     if hasattr(field, "device_components"):
         return field.device_components()
     name = type(field).__name__
+    if _reference_table(field) is not None:
+        return [(PF_TABLE, 0.0, 0.0, 0.0)]
     if name == "CMBPhotonSpectrum":
         return [(PF_CMB, CMBPhotonSpectrum.pref, C.E_CMB, 2.0)]
     if name == "FlatPhotonSpectrum":

@@ -31,12 +31,13 @@ _NEUTRINOS = (12, -12, 14, -14, 16, -16)
 def grid_triple(grid):
     """``(log10 lower edge, log10 upper edge, bins per decade)`` of a cosmic-ray grid.
 
-    ``grid`` is an :class:`EnergyGrid` (its own triple) or an array of bin
-    centres, from which the triple of the log-spaced grid is recovered.
+    ``grid`` is an :class:`EnergyGrid` (its own triple), another grid object
+    with bin centres in ``grid.grid`` (the reference's), or an array of bin
+    centres; the triple of a log-spaced grid is recovered from its centres.
     """
     if isinstance(grid, EnergyGrid):
         return grid.lower, grid.upper, grid.bins_dec
-    c = np.asarray(grid, dtype=np.float64)
+    c = np.asarray(getattr(grid, "grid", grid), dtype=np.float64)
     r = c[1] / c[0]
     lo = 2.0 * c[0] / (1.0 + r)
     hi = lo * r ** c.size

@@ -24,7 +24,7 @@ from . import constants as C
 from .cosmology import H as _H
 from .cosmology import dldz as _dldz
 from .operators import fd_loss_operator, split_diagonal
-from .photonfields import device_components
+from .photonfields import device_components, device_table
 from .results import UHECRPropagationResult  # noqa: F401  (reference API location)
 from .schedule import make_schedule, z_grid
 
@@ -302,7 +302,8 @@ class UHECRPropagationSolverETD2:
             ctx.set_injection(rows, G, src_col, K)
         else:
             flags &= ~_lib.PB_INJECTION
-        ctx.set_photon_field(device_components(self.prince_run.photon_field))
+        ctx.set_photon_field(device_components(self.prince_run.photon_field),
+                             table=device_table(self.prince_run.photon_field))
         if flags & _lib.PB_EM_CASCADE:
             ctx.set_em_windows(*self._em_windows(sched, dz))
         state = np.empty((self.dim_states, K))

@@ -7,6 +7,7 @@ source tree (the directory that holds ``src/prince_cr``)::
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py        # light network
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --em   # light network + EM cascade
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --groups  # result post-processing
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --ebl     # tabulated EBL (Gilmore 2012)
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -80,8 +81,8 @@ def _lorentz(eg, e0, w, peak, thr):
     return peak * (eg * w) ** 2 / ((eg ** 2 - e0 ** 2) ** 2 + (eg * w) ** 2) * (eg > thr)
 
 
-def build(config, base):
-    """Return (run, make_sources) for the light-nuclei workload."""
+def build(config, base, photon_field=None):
+    """Return the reference's light-nuclei run (CMB unless ``photon_field`` is given)."""
     from prince_cr import core, photonfields
 
     class SynthXS(base):
@@ -127,7 +128,7 @@ def build(config, base):
             self.set_range()
             self._optimize_and_generate_index()
 
-    run = core.PriNCeRun(max_mass=4, photon_field=photonfields.CMBPhotonSpectrum(),
+    run = core.PriNCeRun(max_mass=4, photon_field=photon_field or photonfields.CMBPhotonSpectrum(),
                          cross_sections=SynthXS())
     return run
 
@@ -432,10 +433,73 @@ def main_groups():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_ebl():
+    """The light network in CMB + the tabulated Gilmore (2012) EBL.
+
+    Records the two tabulated EBL models' tables (the inputs), the reference's
+    densities at sample points, its photon vector and Bethe-Heitler loss vector
+    at three redshifts, and a plain z = 1 -> 0 solve.
+    """
+    _prepare_reference()
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (6, 14, 8)
+    config.photon_grid = (-15, -6, 8)
+    config.tau_dec_threshold = 0.0
+    config.max_mass = 4
+    config.batch_matrix_format = "dense"
+    config.xs_dtype = "float64"
+    config.linear_algebra_backend = "scipy"
+    from prince_cr import cr_sources, photonfields
+    from prince_cr.cross_sections.base import CrossSectionBase
+    from prince_cr.solvers import UHECRPropagationSolverETD2
+
+    out = {}
+    gil = photonfields.CIBGilmore2012()
+    fra = photonfields.CIBFranceschini2008()
+    for key, f in (("gilmore", gil), ("franceschini", fra)):
+        out[f"{key}_z"] = np.asarray(f._z)
+        out[f"{key}_log10_e"] = np.asarray(f._leps_GeV)
+        out[f"{key}_log10_dnde"] = np.asarray(f._log_dnde)
+        rng = np.random.default_rng(5)
+        E = 10 ** rng.uniform(f._leps_GeV[0] - 0.3, f._leps_GeV[-1] + 0.3, 400)
+        E[:3] = 10 ** np.asarray(f._leps_GeV[[0, 7, -1]])   # table nodes and the ends
+        zs = np.concatenate([rng.uniform(0.0, f._z[-1] + 0.5, 8), [0.0, f._z[3], f._z[-1]]])
+        out[f"{key}_E"] = E
+        out[f"{key}_zs"] = zs
+        out[f"{key}_density"] = np.stack([f.get_photon_density(E, zz) for zz in zs])
+    field = photonfields.CombinedPhotonField([photonfields.CMBPhotonSpectrum, photonfields.CIBGilmore2012])
+    run = build(config, CrossSectionBase, photon_field=field)
+    run.backend.xs_dtype = "float64"
+    ir = run.int_rates
+    out["species"] = np.array(run.spec_man.known_species, dtype=np.int64)
+    out["cr_grid"] = np.array(config.cosmic_ray_grid, dtype=np.float64)
+    out["ph_grid"] = np.array(config.photon_grid, dtype=np.float64)
+    out["batch_matrix"] = np.asarray(ir._batch_matrix, dtype=np.float64)
+    out["batch_rows"] = np.asarray(ir._batch_rows, dtype=np.int64)
+    out["batch_cols"] = np.asarray(ir._batch_cols, dtype=np.int64)
+    for zz in (0.0, 0.5, 1.0):
+        tag = str(zz).replace(".", "p")
+        out[f"photon_vector_z{tag}"] = ir.photon_vector(zz)
+        out[f"kappa_pair_z{tag}"] = run.pair_loss_rates_grid.loss_vector(zz)
+    eq = {int(p): (2.0, 1e10, 1.0) for p in run.spec_man.known_species}
+    ir._sf_off_kernel = None
+    s = UHECRPropagationSolverETD2(initial_z=1.0, final_z=0.0, prince_run=run)
+    s.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=eq))
+    s.solve(dz=1e-3)
+    out["state_ebl"] = np.asarray(s.state)
+    path = os.path.join(HERE, "light_network_ebl.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     if "--em" in sys.argv:
         main_em()
     elif "--groups" in sys.argv:
         main_groups()
+    elif "--ebl" in sys.argv:
+        main_ebl()
     else:
         main()

@@ -115,3 +115,16 @@ def light_network_em():
         return cr_sources.RigdityCutoffSource(run, norm=1.0, params=params)
 
     return z, run, em, source
+
+
+def light_network_ebl():
+    """The light network in CMB + the tabulated Gilmore (2012) EBL: fixture arrays,
+    the run (this package's classes on the fixture's kernel and EBL table) and
+    the EBL field alone."""
+    z = dict(np.load(os.path.join(GOLDEN, "light_network_ebl.npz")))
+    model = FixedKernelModel(z["species"], z["batch_matrix"], z["batch_rows"], z["batch_cols"])
+    ebl = photonfields.TabulatedPhotonField(z["gilmore_z"], z["gilmore_log10_e"], z["gilmore_log10_dnde"])
+    field = photonfields.CombinedPhotonField([photonfields.CMBPhotonSpectrum(), ebl])
+    run = PriNCeRun(model, field, cosmic_ray_grid=tuple(z["cr_grid"]), photon_grid=tuple(z["ph_grid"]),
+                    max_mass=4)
+    return z, run, ebl
