@@ -86,6 +86,44 @@ int pb_set_coupling(pb_context* ctx, int64_t n_states, int64_t n_entries,
 int pb_set_fold_kernel(pb_context* ctx, int64_t n_entries, int32_t n_photon,
                        const double* kernel);
 
+/* The fold kernel built on the device from per-channel response samples,
+ * replacing pb_set_fold_kernel (no host kernel, no kernel upload).  With d
+ * cosmic-ray bins per species block, dph photon bins, na = d + dph - 1 and
+ * nb = 2 d - 1, entry e of the coupling pattern (daughter state r, mother
+ * state c, mother bin i = c mod d, daughter bin k = r mod d) gets, for each
+ * photon bin j and its channel q = entry_channel[e] = (kind, p1, p2, -):
+ *   kind 0 (boost-conserving / non-elastic): 0 + f_i resp[p1][i+j] - f_i resp[p2][i+j]
+ *          (a term is absent when its index is -1);
+ *   kind 1 (redistributed, full table):      max(g_ik ddr[p1][i+j][k-i+d-1], 0)
+ *   kind 2 (redistributed, outer product):   max(g_ik sep_a[p1][i+j] sep_b[p1][k-i+d-1], 0)
+ *          minus f_i resp[p2][i+j] on the diagonal i = k when p2 >= 0;
+ * f_i = f_mo[i] (m_p / E_i), g_ik = f_i (dE[i] / dE[k]).  Arrays are row-major
+ * FP64 on the host; entry_channel has one value per coupling entry in CSR
+ * order.  Needs pb_set_coupling.  Replaces: the Toeplitz assembly of
+ * PhotoNuclearInteractionRate._init_matrices (src/prince_cr/interaction_rates.py:251-646),
+ * given its sampled response increments (nonel_dR, incl_dR, diff_ddR). */
+typedef struct pb_kernel_spec {
+  int32_t d, dph;
+  const double* f_mo;            /* d */
+  const double* dE;              /* d */
+  int32_t n_resp;
+  const double* resp;            /* n_resp x na */
+  int32_t n_ddr;
+  const double* ddr;             /* n_ddr x na x nb */
+  int32_t n_sep;
+  const double* sep_a;           /* n_sep x na */
+  const double* sep_b;           /* n_sep x nb */
+  int32_t n_channels;
+  const int32_t* channels;       /* n_channels x 4: kind, p1, p2, unused */
+  const int32_t* entry_channel;  /* one per coupling entry, CSR order */
+} pb_kernel_spec;
+int pb_build_fold_kernel(pb_context* ctx, const pb_kernel_spec* spec);
+
+/* Copies the device fold kernel (R x dph, coupling-CSR order) to the host.
+ * No counterpart in the reference (its kernel lives on the host); exposed so
+ * a device-built kernel can be checked or saved. */
+int pb_get_fold_kernel(pb_context* ctx, int64_t n_entries, int32_t n_photon, double* kernel);
+
 /* Photon-grid bin centres (n_photon) at which the fold samples n(E, z).
  * Replaces: the ph_grid.grid argument of photon_vector (interaction_rates.py:105-116). */
 int pb_set_photon_grid(pb_context* ctx, int32_t n_photon, const double* energies);

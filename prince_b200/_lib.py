@@ -55,6 +55,27 @@ class SolveArgs(C.Structure):
     ]
 
 
+class KernelSpecArgs(C.Structure):
+    """``pb_kernel_spec``: the fold kernel as per-channel response samples."""
+
+    _fields_ = [
+        ("d", C.c_int32),
+        ("dph", C.c_int32),
+        ("f_mo", _d),
+        ("dE", _d),
+        ("n_resp", C.c_int32),
+        ("resp", _d),
+        ("n_ddr", C.c_int32),
+        ("ddr", _d),
+        ("n_sep", C.c_int32),
+        ("sep_a", _d),
+        ("sep_b", _d),
+        ("n_channels", C.c_int32),
+        ("channels", _i32),
+        ("entry_channel", _i32),
+    ]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "pb_abi_version": (C.c_int, []),
@@ -67,6 +88,8 @@ _PROTOS = {
     "pb_set_photon_grid": (C.c_int, [_vp, C.c_int32, _d]),
     "pb_set_photon_field": (C.c_int, [_vp, C.c_int32, _i32, _d]),
     "pb_set_photon_table": (C.c_int, [_vp, C.c_int32, C.c_int32, _d, _d, _d]),
+    "pb_build_fold_kernel": (C.c_int, [_vp, C.POINTER(KernelSpecArgs)]),
+    "pb_get_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
     "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
@@ -175,6 +198,40 @@ class Context:
         kernel = _f64(kernel)
         self._check(self.lib.pb_set_fold_kernel(self.h, int(kernel.shape[0]), int(kernel.shape[1]),
                                                 _ptr(kernel, C.c_double)), "pb_set_fold_kernel")
+
+    def build_fold_kernel(self, spec, entry_channel):
+        """Build the fold kernel on the device from a ``KernelSpec``; ``entry_channel``
+        is the channel of each coupling entry in CSR order."""
+        keep = []
+
+        def f(a):
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return _ptr(a, C.c_double)
+
+        def i(a):
+            a = np.ascontiguousarray(a, dtype=np.int32)
+            keep.append(a)
+            return _ptr(a, C.c_int32)
+
+        k = KernelSpecArgs()
+        k.d, k.dph = int(spec.d), int(spec.dph)
+        k.f_mo, k.dE = f(spec.f_mo), f(spec.dE)
+        k.n_resp, k.resp = int(spec.resp.shape[0]), f(spec.resp if spec.resp.size else np.zeros(1))
+        k.n_ddr, k.ddr = int(spec.ddr.shape[0]), f(spec.ddr if spec.ddr.size else np.zeros(1))
+        k.n_sep = int(spec.sep_a.shape[0])
+        k.sep_a = f(spec.sep_a if spec.sep_a.size else np.zeros(1))
+        k.sep_b = f(spec.sep_b if spec.sep_b.size else np.zeros(1))
+        k.n_channels, k.channels = int(spec.channels.shape[0]), i(spec.channels)
+        k.entry_channel = i(entry_channel if np.size(entry_channel) else np.zeros(1))
+        self._check(self.lib.pb_build_fold_kernel(self.h, C.byref(k)), "pb_build_fold_kernel")
+
+    def fold_kernel(self, R, dph):
+        """The device fold kernel (R x dph, coupling-CSR order)."""
+        out = np.empty((int(R), int(dph)))
+        self._check(self.lib.pb_get_fold_kernel(self.h, int(R), int(dph), _ptr(out, C.c_double)),
+                    "pb_get_fold_kernel")
+        return out
 
     def set_photon_grid(self, energies):
         e = _f64(energies)

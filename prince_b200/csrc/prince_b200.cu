@@ -325,6 +325,45 @@ __global__ void k_pair_rate(FieldDesc f, const double* __restrict__ pg, const do
   }
 }
 
+// Fold kernel from per-channel response samples, one thread per (coupling
+// entry, photon bin), rows in coupling-CSR order (interaction_rates.py:490-611,
+// with the reference's operation order so the values are bit-identical):
+//   kind 0:  0 [+ f_i dR_incl[i + j]] [- f_i dR_nonel[i + j]]
+//   kind 1/2: max(g_ik ddR[i + j, k - i + d - 1], 0) [- f_i dR_nonel[i + j] if i = k]
+// with i / k the mother / daughter bin, f_i = m_p / E_i, g_ik = f_i (dE_i / dE_k)
+// and ddR a full table (kind 1) or sep_a[.] sep_b[.] (kind 2).
+__global__ void k_build_kernel(const int* __restrict__ row, const int* __restrict__ col,
+                               const int* __restrict__ ent_ch, const int* __restrict__ chan,
+                               const double* __restrict__ f_mo, const double* __restrict__ dE,
+                               const double* __restrict__ resp, const double* __restrict__ ddr,
+                               const double* __restrict__ sep_a, const double* __restrict__ sep_b,
+                               int d, int dph, int64_t total, double* __restrict__ out) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int64_t e = t / dph;
+  const int j = (int)(t - e * dph);
+  const int i_mo = col[e] % d, i_da = row[e] % d;
+  const int q = ent_ch[e];
+  const int kind = chan[4 * q], p1 = chan[4 * q + 1], p2 = chan[4 * q + 2];
+  const size_t na = (size_t)d + dph - 1, nb = 2 * (size_t)d - 1;
+  const int a = i_mo + j;
+  const double f = f_mo[i_mo];
+  double v;
+  if (kind == 0) {
+    v = 0.0;
+    if (p1 >= 0) v = __dadd_rn(v, __dmul_rn(f, resp[p1 * na + a]));
+    if (p2 >= 0) v = __dadd_rn(v, -__dmul_rn(f, resp[p2 * na + a]));
+  } else {
+    const int b = i_da - i_mo + d - 1;
+    const double g = __dmul_rn(f, __ddiv_rn(dE[i_mo], dE[i_da]));
+    const double dd = kind == 1 ? ddr[(p1 * na + a) * nb + b] : __dmul_rn(sep_a[p1 * na + a], sep_b[p1 * nb + b]);
+    v = __dmul_rn(g, dd);
+    if (v < 0.0) v = 0.0;
+    if (p2 >= 0 && i_mo == i_da) v = __dadd_rn(v, -__dmul_rn(f, resp[p2 * na + a]));
+  }
+  out[t] = v;
+}
+
 __global__ void k_pair_expand(const double* __restrict__ rs, const double* __restrict__ scale,
                               const int* __restrict__ bin, int ncr, int64_t n, int W,
                               double* __restrict__ kp) {
@@ -2902,6 +2941,76 @@ int pb_set_fold_kernel(pb_context* c, int64_t R, int32_t dph, const double* K) {
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->dph = dph;
   c->have_kernel = true;
+  return PB_OK;
+}
+
+int pb_build_fold_kernel(pb_context* c, const pb_kernel_spec* k) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!k) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: spec is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_build_fold_kernel: set the coupling pattern first");
+  const int d = k->d, dph = k->dph;
+  if (d < 1 || c->n % d != 0) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: d = %d does not divide %lld states", d, (long long)c->n);
+  if (dph <= 0 || dph > kMaxPhoton) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: photon bins must be in [1, %d]", kMaxPhoton);
+  if (c->have_photon_grid && dph != c->dph) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: photon axis %d != photon grid %d", dph, c->dph);
+  if (!k->f_mo || !k->dE || k->n_resp < 0 || k->n_ddr < 0 || k->n_sep < 0 || k->n_channels < 1 || !k->channels ||
+      (c->R > 0 && !k->entry_channel) || (k->n_resp > 0 && !k->resp) || (k->n_ddr > 0 && !k->ddr) ||
+      (k->n_sep > 0 && (!k->sep_a || !k->sep_b)))
+    return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: bad arguments");
+  for (int q = 0; q < k->n_channels; ++q) {
+    const int kind = k->channels[4 * q], p1 = k->channels[4 * q + 1], p2 = k->channels[4 * q + 2];
+    const int n1 = kind == 0 ? k->n_resp : kind == 1 ? k->n_ddr : kind == 2 ? k->n_sep : -1;
+    if (n1 < 0) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: channel %d has unknown kind %d", q, kind);
+    if (p1 < (kind == 0 ? -1 : 0) || p1 >= n1 || p2 < -1 || p2 >= k->n_resp)
+      return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: channel %d indexes outside its tables", q);
+  }
+  for (int64_t e = 0; e < c->R; ++e)
+    if (k->entry_channel[e] < 0 || k->entry_channel[e] >= k->n_channels)
+      return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: entry %lld has channel %d", (long long)e, k->entry_channel[e]);
+  int rc = set_device(c);
+  if (rc) return rc;
+  const size_t na = (size_t)d + dph - 1, nb = 2 * (size_t)d - 1;
+  DBuf fm, de, rs, dd, sa, sb, ch, ec;
+  auto cleanup = [&]() { for (DBuf* b : {&fm, &de, &rs, &dd, &sa, &sb, &ch, &ec}) b->release(); };
+  const double zero = 0.0;
+  const int32_t izero = 0;
+  if ((rc = upload(c, fm, k->f_mo, (size_t)d)) || (rc = upload(c, de, k->dE, (size_t)d)) ||
+      (rc = upload(c, rs, k->n_resp ? k->resp : &zero, k->n_resp ? (size_t)k->n_resp * na : 1)) ||
+      (rc = upload(c, dd, k->n_ddr ? k->ddr : &zero, k->n_ddr ? (size_t)k->n_ddr * na * nb : 1)) ||
+      (rc = upload(c, sa, k->n_sep ? k->sep_a : &zero, k->n_sep ? (size_t)k->n_sep * na : 1)) ||
+      (rc = upload(c, sb, k->n_sep ? k->sep_b : &zero, k->n_sep ? (size_t)k->n_sep * nb : 1)) ||
+      (rc = upload(c, ch, k->channels, (size_t)4 * k->n_channels)) ||
+      (rc = upload(c, ec, c->R ? k->entry_channel : &izero, c->R ? (size_t)c->R : 1))) {
+    cleanup();
+    return rc;
+  }
+  if (c->kernel.ensure((size_t)std::max<int64_t>(c->R, 1) * dph * sizeof(double)) != cudaSuccess) {
+    cleanup();
+    return fail(c, PB_ERR_CUDA, "pb_build_fold_kernel: allocation of the %lld x %d kernel failed", (long long)c->R, dph);
+  }
+  const int64_t total = c->R * (int64_t)dph;
+  if (total > 0)
+    k_build_kernel<<<blocks_for(total, 256), 256, 0, c->stream>>>(
+        c->cpl_row.as<int>(), c->cpl_indices.as<int>(), ec.as<int>(), ch.as<int>(), fm.as<double>(), de.as<double>(),
+        rs.as<double>(), dd.as<double>(), sa.as<double>(), sb.as<double>(), d, dph, total, c->kernel.as<double>());
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cleanup();
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_build_fold_kernel: %s", cudaGetErrorString(e));
+  c->dph = dph;
+  c->have_kernel = true;
+  return PB_OK;
+}
+
+int pb_get_fold_kernel(pb_context* c, int64_t R, int32_t dph, double* K) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_kernel) return fail(c, PB_ERR_STATE, "pb_get_fold_kernel: no fold kernel on the device");
+  if (R != c->R || dph != c->dph || (R > 0 && !K))
+    return fail(c, PB_ERR_ARG, "pb_get_fold_kernel: the kernel is %lld x %d", (long long)c->R, c->dph);
+  if (R == 0) return PB_OK;
+  int rc = set_device(c);
+  if (rc) return rc;
+  PB_CUDA(c, cudaMemcpyAsync(K, c->kernel.p, (size_t)R * dph * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  PB_CUDA(c, cudaStreamSynchronize(c->stream));
   return PB_OK;
 }
 

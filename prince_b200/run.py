@@ -10,12 +10,15 @@ solvers also accept a reference run object that was built with FP64 kernel
 settings.
 
 The rate kernel comes from a *cross-section model* object with
-``known_species`` and ``build_kernel(cr_grid, ph_grid, spec_man)`` returning
-``(batch_matrix, rows, cols)``: one kernel row per coupling-matrix entry
-(daughter state ``rows[i]``, mother state ``cols[i]``), ``dph`` photon-bin
-columns.  Constructing kernels from tabulated cross sections is outside the
-ETD2 path; ``prince_b200.synth`` provides seeded synthetic models and
-``FixedKernelModel`` wraps a precomputed kernel.
+``known_species`` and either ``build_kernel_spec(cr_grid, ph_grid, spec_man)``
+returning a ``prince_b200.kernel_build.KernelSpec`` (per-channel response
+samples; the GPU expands it, the host only when the oracle asks) or
+``build_kernel(...)`` returning ``(batch_matrix, rows, cols)``: one kernel row
+per coupling-matrix entry (daughter state ``rows[i]``, mother state
+``cols[i]``), ``dph`` photon-bin columns.  Sampling response functions from
+tabulated cross sections is outside the ETD2 path; ``prince_b200.synth``
+provides seeded synthetic models and ``FixedKernelModel`` wraps a precomputed
+kernel.
 """
 
 from __future__ import annotations
@@ -50,9 +53,14 @@ class PhotoNuclearInteractionRate:
     ``_batch_matrix[i]`` is the kernel row of coupling entry ``i`` in CSR
     order, so ``_batch_matrix @ photon_vector(z)`` is the coupling matrix's
     ``data`` at redshift ``z`` (``interaction_rates.py:966-1067``).
+
+    Built from a kernel (``batch_matrix``) or from a ``kernel_spec``
+    (``prince_b200.kernel_build.KernelSpec``).  With a spec the host kernel is
+    expanded only when ``_batch_matrix`` is first read (the CPU oracle); the
+    device builds its own copy from the spec.
     """
 
-    def __init__(self, prince_run, batch_matrix, rows, cols):
+    def __init__(self, prince_run, batch_matrix, rows, cols, kernel_spec=None):
         self.prince_run = prince_run
         self.spec_man = prince_run.spec_man
         self.e_photon = prince_run.ph_grid
@@ -61,11 +69,18 @@ class PhotoNuclearInteractionRate:
         indptr, indices, order = coupling_structure(rows, cols, n)
         self._batch_rows = np.asarray(rows, dtype=np.int64)[order]
         self._batch_cols = np.asarray(cols, dtype=np.int64)[order]
-        self._batch_matrix = np.ascontiguousarray(batch_matrix[order], dtype=np.float64)
+        self.kernel_spec = kernel_spec
+        self._bm = None if batch_matrix is None else np.ascontiguousarray(batch_matrix[order], dtype=np.float64)
         self.sortidx = order
         self.coupling_mat = sp.csr_matrix(
             (np.zeros(indices.size), indices, indptr), shape=(n, n)
         )
+
+    @property
+    def _batch_matrix(self):
+        if self._bm is None:
+            self._bm = np.ascontiguousarray(self.kernel_spec.materialize()[self.sortidx])
+        return self._bm
 
     @property
     def photon_field(self):
@@ -224,8 +239,12 @@ class PriNCeRun:
         self.pair_loss_rates_grid = ContinuousPairProductionLossRate(self, "grid")
         self.adia_loss_rates_bins = ContinuousAdiabaticLossRate(self, "bins")
         self.pair_loss_rates_bins = ContinuousPairProductionLossRate(self, "bins")
-        bm, rows, cols = cross_sections.build_kernel(self.cr_grid, self.ph_grid, self.spec_man)
-        self.int_rates = PhotoNuclearInteractionRate(self, bm, rows, cols)
+        if hasattr(cross_sections, "build_kernel_spec"):
+            spec = cross_sections.build_kernel_spec(self.cr_grid, self.ph_grid, self.spec_man)
+            self.int_rates = PhotoNuclearInteractionRate(self, None, spec.rows, spec.cols, kernel_spec=spec)
+        else:
+            bm, rows, cols = cross_sections.build_kernel(self.cr_grid, self.ph_grid, self.spec_man)
+            self.int_rates = PhotoNuclearInteractionRate(self, bm, rows, cols)
         self.em_int_rates = None
         self.enable_em_cascade = bool(enable_em_cascade)
         self.em_cascade_model = em_cascade_model

@@ -55,7 +55,11 @@ class DeviceRun:
         self.n = n
         self.ctx.set_coupling(n, cm.indptr, cm.indices)
         self.ctx.set_layout(run.spec_man.nspec and n // run.spec_man.nspec)
-        self.ctx.set_fold_kernel(_dense_kernel(ir._batch_matrix))
+        spec = getattr(ir, "kernel_spec", None)
+        if spec is not None:   # expanded on the device, in coupling-CSR order
+            self.ctx.build_fold_kernel(spec, np.asarray(spec.chan)[ir.sortidx])
+        else:
+            self.ctx.set_fold_kernel(_dense_kernel(ir._batch_matrix))
         self.ctx.set_photon_grid(ir.e_photon.grid)
         D = fd_loss_operator(run.cr_grid, run.spec_man.nspec)
         self.D_diag, self.D_off = split_diagonal(D)

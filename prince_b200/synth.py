@@ -168,8 +168,16 @@ class SyntheticPhotoNuclear:
                 if da in present and key in mult and (mult[key][0] > 0 or mult[key][1] > 0):
                     self.diff[(mo, da)] = (mult[key][0], mult[key][1], rng.uniform(2.0, 4.0))
 
-    def build_kernel(self, cr_grid, ph_grid, spec_man):
-        """Assemble ``(batch_matrix, rows, cols)`` for the given grids and species."""
+    def build_kernel_spec(self, cr_grid, ph_grid, spec_man):
+        """The fold kernel as per-channel response samples (``prince_b200.kernel_build``).
+
+        Per mother: the non-elastic increments ``dR_gdr + dR_pion``; per
+        boost-conserving channel ``w_gdr dR_gdr + w_pion dR_pion``; per
+        redistributed channel the outer product of ``m_gdr dR_gdr + m_pion dR_pion``
+        (photon axis) and ``dH`` (x axis), with the x-cuts of the reference.
+        """
+        from .kernel_build import SpecBuilder, cut_pairs
+
         m_p = C.PRINCE_UNITS.m_proton
         ecr, bcr, bph = cr_grid.grid, cr_grid.bins, ph_grid.bins
         dcr, dph = cr_grid.d, ph_grid.d
@@ -178,13 +186,7 @@ class SyntheticPhotoNuclear:
             raise RuntimeError("cosmic-ray and photon grids must share the log step")
         y_edges = ecr[0] * bph[0] / m_p * 10 ** (np.arange(dcr + dph) * step)
         x_edges = bcr[0] / ecr[0] * 10 ** ((np.arange(2 * dcr) - (dcr - 1)) * step)
-        f_mo = m_p / ecr
-        dE = cr_grid.widths
-        hank = np.arange(dcr)[:, None] + np.arange(dph)[None, :]      # i + j
-        bidx = (np.arange(dcr)[None, :] - np.arange(dcr)[:, None]) + (dcr - 1)
-        xl = bcr[:-1][None, :] / ecr[:, None]
-        imo, ida = np.meshgrid(np.arange(dcr), np.arange(dcr), indexing="ij")
-
+        sb = SpecBuilder(dcr, dph, m_p / ecr, cr_grid.widths)
         resp = {}
 
         def dR(mo):
@@ -194,44 +196,34 @@ class SyntheticPhotoNuclear:
                 resp[mo] = (_response_increments(gdr, y_edges), _response_increments(pion, y_edges))
             return resp[mo]
 
-        mats, rows, cols = [], [], []
         sref = spec_man.pdgid2sref
         for mo in spec_man.known_species:
             A, _, _ = get_AZN(mo)
             if A == 0:
                 continue
             rg, rp = dR(mo)
-            nonel = f_mo[:, None] * (rg + rp)[hank]
+            nonel = sb.response(rg + rp, key=("nonel", mo))
             lo_mo = sref[mo].lidx()
             if (mo, mo) not in self.diff:
-                mats.append(-nonel)
-                rows.append(lo_mo + np.arange(dcr))
-                cols.append(lo_mo + np.arange(dcr))
+                sb.bc(-1, nonel, lo_mo, lo_mo)
             for (m2, da), (wg, wp) in self.bc.items():
                 if m2 != mo or da not in sref:
                     continue
-                mats.append(f_mo[:, None] * (wg * rg + wp * rp)[hank])
-                rows.append(sref[da].lidx() + np.arange(dcr))
-                cols.append(lo_mo + np.arange(dcr))
+                sb.bc(sb.response(wg * rg + wp * rp), -1, sref[da].lidx(), lo_mo)
             for (m2, da), (mg, mp_, a) in self.diff.items():
                 if m2 != mo or da not in sref:
                     continue
-                Hx = np.minimum(x_edges, 1.0) ** a
-                dH = np.diff(Hx)
+                dH = np.diff(np.minimum(x_edges, 1.0) ** a)
                 cut = self.x_cut_proton if da == 2212 else self.x_cut
-                keep = (xl >= cut) & (xl <= 1)
-                ki, kd = imo[keep], ida[keep]
-                fac = f_mo[ki] * dE[ki] / dE[kd]
-                tile = (fac * dH[bidx[ki, kd]])[:, None] * (mg * rg + mp_ * rp)[hank[ki]]
-                np.clip(tile, 0.0, None, out=tile)
-                if da == mo:
-                    on_diag = ki == kd
-                    tile[on_diag] -= nonel[ki[on_diag]]
-                mats.append(tile)
-                rows.append(sref[da].lidx() + kd)
-                cols.append(lo_mo + ki)
-        bm = np.concatenate(mats, axis=0) if mats else np.zeros((0, dph))
-        return bm, np.concatenate(rows), np.concatenate(cols)
+                ki, kd = cut_pairs(bcr, ecr, cut)
+                sb.diff(ki, kd, sref[da].lidx(), lo_mo, nonel=nonel if da == mo else -1,
+                        sep=(mg * rg + mp_ * rp, dH))
+        return sb.spec()
+
+    def build_kernel(self, cr_grid, ph_grid, spec_man):
+        """Assemble ``(batch_matrix, rows, cols)`` on the host from ``build_kernel_spec``."""
+        spec = self.build_kernel_spec(cr_grid, ph_grid, spec_man)
+        return spec.materialize(), spec.rows, spec.cols
 
 
 def light_network_species():

@@ -8,6 +8,7 @@ source tree (the directory that holds ``src/prince_cr``)::
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --em   # light network + EM cascade
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --groups  # result post-processing
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --ebl     # tabulated EBL (Gilmore 2012)
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --kernel  # fold-kernel construction inputs
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -494,6 +495,91 @@ def main_ebl():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_kernel():
+    """The reference's fold-kernel construction inputs, as a channel spec.
+
+    Samples the light network's response increments exactly as
+    ``PhotoNuclearInteractionRate._init_matrices`` does (its fast path: the
+    response-integral operator for the 1-D increments, the stacked bilinear
+    antiderivative for the 2-D ones), walks its channel loop with the same
+    branch conditions, and records the result as a
+    ``prince_b200.kernel_build.KernelSpec``.  The spec, expanded, must equal the
+    reference's own ``_batch_matrix`` bit for bit (checked here).
+    """
+    _prepare_reference()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (6, 14, 8)
+    config.photon_grid = (-15, -6, 8)
+    config.tau_dec_threshold = 0.0
+    config.max_mass = 4
+    config.batch_matrix_format = "dense"
+    config.xs_dtype = "float64"
+    config.linear_algebra_backend = "scipy"
+    import itertools
+
+    import prince_cr.interaction_rates as IR
+    from prince_cr.cross_sections.base import CrossSectionBase
+    from prince_cr.data import PRINCE_UNITS
+    from prince_cr.util import is_nucleus
+    from prince_b200.kernel_build import SpecBuilder, cut_pairs
+
+    run = build(config, CrossSectionBase)
+    ir = run.int_rates
+    resp = ir.cross_sections.resp
+    m_pr = PRINCE_UNITS.m_proton
+    ecr, bcr, bph = ir.e_cosmicray.grid, ir.e_cosmicray.bins, ir.e_photon.bins
+    dcr, dph = ir.e_cosmicray.d, ir.e_photon.d
+    log_step = np.log10(ecr[1] / ecr[0])
+    y_grid = ecr[0] * bph[0] / m_pr * 10 ** (np.arange(dcr + dph) * log_step)
+    x_grid = bcr[0] / ecr[0] * 10 ** ((np.arange(2 * dcr) - (dcr - 1)) * log_step)
+    M = IR._response_integral_operator(resp.response_ygrid, y_grid)
+    dRn = np.diff(resp.nonel_f_stack @ M.T, axis=1)
+    nonel_dR = {mo: dRn[i] for i, mo in enumerate(resp.nonel_keys)}
+    dRi = np.diff(resp.incl_f_stack @ M.T, axis=1)
+    incl_dR = {key: dRi[i] for i, key in enumerate(resp.incl_keys)}
+    Y2d, X2d = np.meshgrid(y_grid, x_grid, indexing="ij")
+    keys = resp.incl_diff_integral_keys
+    R_stack = resp.incl_diff_integral_stack_intp.ev(X2d.ravel(), Y2d.ravel()).reshape(*Y2d.shape, len(keys))
+    ddR_stack = R_stack[1:, 1:, :] - R_stack[1:, :-1, :] - R_stack[:-1, 1:, :] + R_stack[:-1, :-1, :]
+    diff_ddR = {key: ddR_stack[..., i] for i, key in enumerate(keys)}
+    assert len(keys) == len(resp.incl_diff_intp_integral)
+
+    sm = run.spec_man
+    sref = sm.pdgid2sref
+    sb = SpecBuilder(dcr, dph, m_pr / ecr, ir.e_cosmicray.widths)
+    bc_set = ir.cross_sections.known_bc_channels_set
+    diff_set = ir.cross_sections.known_diff_channels_set
+    rev = sm.known_species[::-1]
+    for moid, daid in itertools.product(rev, rev):
+        if not is_nucleus(moid):
+            continue
+        has_nonel = (moid == daid) and (moid in nonel_dR)
+        in_bc, in_diff = (moid, daid) in bc_set, (moid, daid) in diff_set
+        nonel = sb.response(nonel_dR[moid], key=("nonel", moid)) if has_nonel else -1
+        if in_bc or (has_nonel and not in_diff):
+            incl = sb.response(incl_dR[(moid, daid)]) if (moid, daid) in incl_dR else -1
+            sb.bc(incl, nonel, sref[daid].lidx(), sref[moid].lidx())
+        elif in_diff:
+            cut = config.x_cut_proton if daid == 2212 else config.x_cut
+            ki, kd = cut_pairs(bcr, ecr, cut)
+            if ki.size:
+                sb.diff(ki, kd, sref[daid].lidx(), sref[moid].lidx(), nonel=nonel, table=diff_ddR[(moid, daid)])
+    spec = sb.spec()
+    bm = spec.materialize()
+    order = np.lexsort((spec.cols, spec.rows))
+    assert np.array_equal(spec.rows[order], ir._batch_rows) and np.array_equal(spec.cols[order], ir._batch_cols)
+    assert np.array_equal(bm[order], ir._batch_matrix), "the spec does not reproduce the reference kernel"
+    out = dict(d=spec.d, dph=spec.dph, f_mo=spec.f_mo, dE=spec.dE, resp=spec.resp, ddr=spec.ddr,
+               sep_a=spec.sep_a, sep_b=spec.sep_b, channels=spec.channels, rows=spec.rows, cols=spec.cols,
+               chan=spec.chan)
+    path = os.path.join(HERE, "kernel_spec_light.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes;", spec.channels.shape[0], "channels,", spec.n_rows, "rows")
+
+
 if __name__ == "__main__":
     if "--em" in sys.argv:
         main_em()
@@ -501,5 +587,7 @@ if __name__ == "__main__":
         main_groups()
     elif "--ebl" in sys.argv:
         main_ebl()
+    elif "--kernel" in sys.argv:
+        main_kernel()
     else:
         main()
