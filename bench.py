@@ -182,6 +182,9 @@ def run_b200(args, dist, rank, ws, local):
     solver = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=args.points, device=local)
     for k, p in enumerate(pts):
         solver[k].add_source_class(point_source(run, p))
+    if args.band_warps:
+        from prince_b200 import _lib
+        solver._dev.ctx.set_option(_lib.PB_OPT_BAND_WARPS, args.band_warps)
 
     for _ in range(args.warmup):
         solver.solve(dz=1e-3)
@@ -280,10 +283,27 @@ def run_b200(args, dist, rank, ws, local):
     return line, run, pts, zi, sched
 
 
-# DRAM bytes per launch (dram__bytes read + write) of each stage kernel in one
-# ncu capture of this workload at K = 512 (bench.py --z-range 0.05,0.05,
-# -s 4 -c 1 per kernel); the capture is repeated after kernel changes.
-NCU_TRAFFIC_K512 = {"k_slab": 525e6, "k_band": 170e6, "k_fd_dense": 228e6, "k_fd": 227e6}
+def ncu_traffic():
+    """DRAM bytes per launch of each kernel at K = 512, read from the committed ncu
+    summaries under ``profiles/`` (the tables' "DRAM traffic per launch (MB)" /
+    "DRAM bytes per launch (MB)" rows, one column per kernel)."""
+    import glob
+    import re
+
+    out = {}
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*_512pts_*.md"))):
+        header = None
+        for line in open(path):
+            cells = [c.strip() for c in line.strip().strip("|").split("|")]
+            if line.startswith("| metric"):
+                header = cells
+            elif header and re.match(r"DRAM (traffic|bytes) per launch \(MB\)", cells[0]):
+                for name, val in zip(header[1:], cells[1:]):
+                    try:
+                        out.setdefault(name.split("<")[0].strip(), float(val) * 1e6)
+                    except ValueError:
+                        pass
+    return out
 
 
 def kernel_rooflines(solver, run, sched, n_active, n_inj):
@@ -323,18 +343,19 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
         fd_name: 16.0 * n * K + 8.0 * n,
         "k_slab": 8.0 * n * K + 12.0 * nent + 24.0 * ns * K + 24.0 * ns,
     }
+    traffic = ncu_traffic() if K == 512 else {}
     kernels = []
     for name, t in ((fd_name, ms[0]), ("k_slab", ms[1])):
         if t > 0:
             a = kb[name] / (t * 1e-3) / 1e9
             kernels.append({"kernel": name, "bound": "hbm", "achieved": a, "peak": hbm, "unit": "GB/s",
-                            "frac": a / hbm, "traffic": NCU_TRAFFIC_K512.get(name) if K == 512 else None,
+                            "frac": a / hbm, "traffic": traffic.get(name),
                             "launch_us": t * 1e3,
                             "algorithmic_bytes": kb[name], "peak_source": hbm_kind})
     if ms[2] > 0:
         a = 2.0 * nnz_band * K / (ms[2] * 1e-3) / 1e12
         kernels.append({"kernel": "k_band", "bound": "tensor", "achieved": a, "peak": fp64, "unit": "TFLOP/s",
-                        "frac": a / fp64, "traffic": NCU_TRAFFIC_K512["k_band"] if K == 512 else None,
+                        "frac": a / fp64, "traffic": traffic.get("k_band"),
                         "traffic_unit": "bytes", "launch_us": ms[2] * 1e3,
                         "algorithmic_flops": 2.0 * nnz_band * K,
                         "peak_source": "measured FP64 DMMA peak (pb_fp64_peak, register-only kernel)"})
@@ -433,6 +454,8 @@ def main():
     ap.add_argument("--plain", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="also time the adjoint gradient (1/0)")
+    ap.add_argument("--band-warps", type=int, default=0, choices=[0, 4, 8],
+                    help="warps of a band-tile CTA (0: the library default)")
     ap.add_argument("--z-range", default="0.5,1.0",
                     help="z_max range of the source points (smaller cases for profiling)")
     args = ap.parse_args()

@@ -50,6 +50,9 @@ extern "C" {
 #define PB_INFO_FD_DENSE 8       /* 1 if the forward FD term runs the register-blocked dense stencil */
 #define PB_OPT_TMA_STAGING 9     /* 1 (default): bin-local kernel stages by TMA (tensor maps); 0: cp.async */
 #define PB_INFO_LAST_TMA 10      /* 1 if the last pb_solve staged the bin-local kernel by TMA */
+#define PB_OPT_BAND_WARPS 12       /* warps of a band-tile CTA: 8 (default, 64 columns, one CTA per SM) or 4
+                                     (32 columns in half the registers and shared memory, so the band
+                                     tiles run on the tensor pipe beside the bin-local gather on each SM) */
 #define PB_OPT_STAGING_WAIT_TRIES 11 /* polls of k_slab's bounded staging wait before it gives up and the solve
                                      returns PB_ERR_DEVICE (default 2^24; < 0 restores it; 0 gives up at
                                      once, which tests the error path). The CTA still drains its copies. */

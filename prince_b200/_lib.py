@@ -25,6 +25,7 @@ PB_OPT_BATCHED_KERNELS, PB_INFO_BLOCKED_LAYOUT, PB_INFO_LAST_BLOCKED, PB_INFO_BA
 PB_INFO_BAND_ENTRIES, PB_INFO_SLAB_ENTRIES, PB_INFO_SLAB_ROWS, PB_INFO_FD_DENSE = 5, 6, 7, 8
 PB_OPT_TMA_STAGING, PB_INFO_LAST_TMA = 9, 10
 PB_OPT_STAGING_WAIT_TRIES = 11
+PB_OPT_BAND_WARPS = 12
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)

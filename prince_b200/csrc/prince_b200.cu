@@ -165,6 +165,7 @@ struct pb_context {
   int32_t batched_mode = 1;         // 0: general row kernels; 1: bin-blocked kernels when the layout allows
   int32_t tma_mode = 1;             // 1: k_slab stages by TMA when tensor maps can be encoded; 0: cp.async
   long long staging_wait_tries = kWaitTries;  // k_slab's first staging wait (PB_OPT_STAGING_WAIT_TRIES)
+  int32_t band_warps = 8;           // warps of a k_band CTA (PB_OPT_BAND_WARPS: 8 or 4)
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1568,13 +1569,14 @@ __global__ void k_slab_prep(StepParams p) {
 // keeps the species' X fragments (2 RT k-tiles of 4 mother bins) in
 // registers, loaded one species ahead.  Every tile of the static band is
 // multiplied: tiles without coupling entries hold zeros and add exact zeros.
-template <int RT, int J>
-__global__ void __launch_bounds__(256, 1) k_band(StepParams p) {
+template <int RT, int J, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) k_band(StepParams p) {
   extern __shared__ double sm[];
   constexpr int KT = 2 * RT;
   constexpr int ABLK = 2 * RT * J * 32;  // doubles of one (species, band pair) block
+  constexpr int AH = RT * J * 32;        // one band species of it
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int c0 = blockIdx.x * 64 + wid * 8;
+  const int c0 = blockIdx.x * (NW * 8) + wid * 8;
   const bool wact = c0 < p.ncols;  // c0 + 7 < ld: ld is a multiple of 32
   const int pair = blockIdx.z, g = blockIdx.y;
   const int s0 = g * p.spg, s1 = min(p.nsp, s0 + p.spg);
@@ -1603,35 +1605,75 @@ __global__ void __launch_bounds__(256, 1) k_band(StepParams p) {
       x[kt] = (wact && e < d) ? xs[(size_t)e * ld] : 0.0;
     }
   };
-  if (s0 < s1) {
-    issue(s0, 0);
-    load_x(s0, xf);
-  }
-  for (int sp = s0; sp < s1; ++sp) {
-    const int stage = (sp - s0) & 1;
-    if (sp + 1 < s1) {
-      issue(sp + 1, stage ^ 1);
-      load_x(sp + 1, xn);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+  if (NW == 8) {  // whole (species, pair) blocks, double-buffered
+    if (s0 < s1) {
+      issue(s0, 0);
+      load_x(s0, xf);
     }
-    __syncthreads();
-    const double* __restrict__ as = As + stage * ABLK + lane;
-    // consecutive DMMAs go to different accumulators (k-tile outer, row tile inner)
+    for (int sp = s0; sp < s1; ++sp) {
+      const int stage = (sp - s0) & 1;
+      if (sp + 1 < s1) {
+        issue(sp + 1, stage ^ 1);
+        load_x(sp + 1, xn);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+      const double* __restrict__ as = As + stage * ABLK + lane;
+      // consecutive DMMAs go to different accumulators (k-tile outer, row tile inner)
 #pragma unroll
-    for (int jj = 0; jj < J; ++jj)
+      for (int jj = 0; jj < J; ++jj)
 #pragma unroll
-      for (int b = 0; b < 2; ++b)
+        for (int b = 0; b < 2; ++b)
 #pragma unroll
-        for (int rt = 0; rt < RT; ++rt) {
-          const int kt = 2 * rt + jj;
-          if (kt >= KT) continue;
-          dmma884(acc[b][rt][0], acc[b][rt][1], as[((b * RT + rt) * J + jj) * 32], xf[kt]);
+          for (int rt = 0; rt < RT; ++rt) {
+            const int kt = 2 * rt + jj;
+            if (kt >= KT) continue;
+            dmma884(acc[b][rt][0], acc[b][rt][1], as[((b * RT + rt) * J + jj) * 32], xf[kt]);
+          }
+      __syncthreads();  // every warp is done with this stage before it is refilled
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) xf[kt] = xn[kt];
+    }
+  } else {  // one band species at a time through a ring of two half blocks (half the shared memory)
+    auto issue_h = [&](int sp, int b, int buf) {
+      const double* src = A + ((size_t)sp * npairs + pair) * ABLK + (size_t)b * AH;
+      for (int c = threadIdx.x; c < AH / 2; c += blockDim.x) cp_async16(As + buf * AH + 2 * c, src + 2 * c);
+      cp_async_commit();
+    };
+    int buf = 0;
+    if (s0 < s1) {
+      issue_h(s0, 0, 0);
+      load_x(s0, xf);
+    }
+    for (int sp = s0; sp < s1; ++sp) {
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const bool more = b == 0 || sp + 1 < s1;
+        if (more) {
+          issue_h(b == 0 ? sp : sp + 1, b ^ 1, buf ^ 1);
+          if (b == 0 && sp + 1 < s1) load_x(sp + 1, xn);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
         }
-    __syncthreads();  // every warp is done with this stage before it is refilled
+        __syncthreads();
+        const double* __restrict__ as = As + buf * AH + lane;
 #pragma unroll
-    for (int kt = 0; kt < KT; ++kt) xf[kt] = xn[kt];
+        for (int jj = 0; jj < J; ++jj)
+#pragma unroll
+          for (int rt = 0; rt < RT; ++rt) {
+            const int kt = 2 * rt + jj;
+            if (kt >= KT) continue;
+            dmma884(acc[b][rt][0], acc[b][rt][1], as[(rt * J + jj) * 32], xf[kt]);
+          }
+        __syncthreads();  // every warp is done with this half before it is refilled
+        buf ^= 1;
+      }
+#pragma unroll
+      for (int kt = 0; kt < KT; ++kt) xf[kt] = xn[kt];
+    }
   }
   if (!wact) return;
 #pragma unroll
@@ -1650,9 +1692,9 @@ __global__ void __launch_bounds__(256, 1) k_band(StepParams p) {
   }
 }
 
-template <int RT, int J>
+template <int RT, int J, int NW>
 size_t band_smem_bytes() {
-  return (size_t)2 * (2 * RT * J * 32) * sizeof(double);
+  return (size_t)2 * ((NW == 8 ? 2 : 1) * RT * J * 32) * sizeof(double);
 }
 
 // Band rows: add the group partials in group order, then the stage update
@@ -1702,25 +1744,32 @@ constexpr int kBandJ[] = {5, 9, 13, 17};
 struct BandInstance {
   BandKernel fn;
   size_t smem;
+  int warps;
 };
-template <int RT>
+template <int RT, int NW>
 BandInstance band_kernel_j(int J) {
   switch (J) {
-    case 5: return {k_band<RT, 5>, band_smem_bytes<RT, 5>()};
-    case 9: return {k_band<RT, 9>, band_smem_bytes<RT, 9>()};
-    case 13: return {k_band<RT, 13>, band_smem_bytes<RT, 13>()};
-    case 17: return {k_band<RT, 17>, band_smem_bytes<RT, 17>()};
+    case 5: return {k_band<RT, 5, NW>, band_smem_bytes<RT, 5, NW>(), NW};
+    case 9: return {k_band<RT, 9, NW>, band_smem_bytes<RT, 9, NW>(), NW};
+    case 13: return {k_band<RT, 13, NW>, band_smem_bytes<RT, 13, NW>(), NW};
+    case 17: return {k_band<RT, 17, NW>, band_smem_bytes<RT, 17, NW>(), NW};
   }
-  return {nullptr, 0};
+  return {nullptr, 0, 0};
 }
-BandInstance band_kernel(int RT, int J) {
+template <int NW>
+BandInstance band_kernel_w(int RT, int J) {
   switch (RT) {
-    case 4: return band_kernel_j<4>(J);
-    case 8: return band_kernel_j<8>(J);
-    case 12: return band_kernel_j<12>(J);
-    case 16: return band_kernel_j<16>(J);
+    case 4: return band_kernel_j<4, NW>(J);
+    case 8: return band_kernel_j<8, NW>(J);
+    case 12: return band_kernel_j<12, NW>(J);
+    case 16: return band_kernel_j<16, NW>(J);
   }
-  return {nullptr, 0};
+  return {nullptr, 0, 0};
+}
+// nw = 8: 64-column CTAs (one per SM); nw = 4: 32-column CTAs in half the
+// registers and shared memory, so that a k_slab CTA fits beside one.
+BandInstance band_kernel(int RT, int J, int nw = 8) {
+  return nw == 4 ? band_kernel_w<4>(RT, J) : band_kernel_w<8>(RT, J);
 }
 
 // ---------------------------------------------------------------------------
@@ -2648,6 +2697,20 @@ bool use_blocked(const pb_context* c, int K) {
 // One stage of the bin-blocked path: k_band on the second stream, k_fd then
 // k_slab on the launching stream, then k_band_finish (and the next step's row
 // factors of the bin-local rows after stage 2).
+// k_band's grid for the active columns: column blocks of 8 nw columns and
+// mother-species groups (sets p.spg, p.ngroups).  With nw = 8 the groups fill
+// at least one wave of the SMs (a CTA per SM); with nw = 4 they stay within one
+// wave, so that each SM holds at most one k_band CTA beside its k_slab CTA.
+int band_grid(const pb_context* c, StepParams& p, int nw) {
+  const int cblocks = (int)blocks_for(p.ncols, 8 * nw);
+  const int per = cblocks * std::max(c->band_npairs, 1);
+  const int want = nw == 4 ? c->num_sms / per : (c->num_sms + per - 1) / per;
+  const int G = std::max(1, std::min({want, kMaxBandGroups, p.nsp}));
+  p.spg = (p.nsp + G - 1) / G;
+  p.ngroups = (p.nsp + p.spg - 1) / p.spg;
+  return cblocks;
+}
+
 template <int STAGE>
 int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   const bool photohad = (p.flags & PB_PHOTOHAD) != 0;
@@ -2656,15 +2719,11 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   p.ngroups = 0;
   p.spg = 1;
   if (photohad && p.nb > 0) {
-    const int cblocks = (int)blocks_for(p.ncols, 64);
-    const int per = cblocks * c->band_npairs;
-    const int G = std::max(1, std::min({(c->num_sms + per - 1) / per, kMaxBandGroups, p.nsp}));
-    p.spg = (p.nsp + G - 1) / G;
-    p.ngroups = (p.nsp + p.spg - 1) / p.spg;
+    const BandInstance bi = band_kernel(c->band_RT, c->band_J, c->band_warps);
+    const int cblocks = band_grid(c, p, bi.warps);
     cudaEventRecord(c->ev_fork, st);
     cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
-    const BandInstance bi = band_kernel(c->band_RT, c->band_J);
-    bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), 256, bi.smem, c->stream2>>>(p);
+    bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), bi.warps * 32, bi.smem, c->stream2>>>(p);
     cudaEventRecord(c->ev_join, c->stream2);
     ++launches;
   }
@@ -3404,7 +3463,8 @@ int pb_set_layout(pb_context* c, int32_t d) {
   }
   const size_t max_smem = 227 * 1024;
   const size_t ssm = SlabSmem::bytes(nsp, maxbin, (nss + 1) / 2);
-  const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0};
+  const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0, 0};
+  const BandInstance bi4 = (RT && J) ? band_kernel(RT, J, 4) : BandInstance{nullptr, 0, 0};
   const bool ok = quads_fit && ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
                   (size_t)d * (kColTile + 2) * sizeof(double) <= max_smem &&
                   (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && squad.size() < ((size_t)1 << 29);
@@ -3443,6 +3503,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
     PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   }
   PB_CUDA(c, cudaFuncSetAttribute(bi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi.smem));
+  PB_CUDA(c, cudaFuncSetAttribute(bi4.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi4.smem));
   c->band_nb = nb;
   c->band_npairs = npairs;
   c->band_RT = RT;
@@ -3591,12 +3652,9 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
   cudaStream_t st = c->stream;
   const bool photohad = (flags & PB_PHOTOHAD) != 0, kap = (flags & PB_PARTIAL_DIFF) != 0;
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
-  const int cblocks = (int)blocks_for(p.ncols, 64);
-  const int per = cblocks * std::max(c->band_npairs, 1);
-  const int G = std::max(1, std::min({(c->num_sms + per - 1) / per, kMaxBandGroups, p.nsp}));
-  p.spg = (p.nsp + G - 1) / G;
-  p.ngroups = (photohad && p.nb > 0) ? (p.nsp + p.spg - 1) / p.spg : 0;
-  const BandInstance bi = band_kernel(c->band_RT, c->band_J);
+  const BandInstance bi = band_kernel(c->band_RT, c->band_J, c->band_warps);
+  const int cblocks = band_grid(c, p, bi.warps);
+  if (!(photohad && p.nb > 0)) p.ngroups = 0;
   for (int kk = 0; kk < 4; ++kk) ms[kk] = 0.0;
   for (int kk = 0; kk < 4; ++kk) {
     const bool runs = kk == 0 ? kap : kk == 1 ? true : kk == 2 ? p.ngroups > 0 : p.nb > 0;
@@ -3613,7 +3671,7 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
         if (stage == 1) k_slab<1, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
         else k_slab<2, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
       }
-      if (kk == 2) bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), 256, bi.smem, st>>>(p);
+      if (kk == 2) bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), bi.warps * 32, bi.smem, st>>>(p);
       if (kk == 3) {
         const unsigned gb = (unsigned)blocks_for((int64_t)p.nb * p.d, 8);
         if (stage == 1) k_band_finish<1><<<dim3(gb, tiles), 256, 0, st>>>(p);
@@ -3679,6 +3737,10 @@ int pb_set_option(pb_context* c, int32_t key, int64_t value) {
       if (value != 0 && value != 1) return fail(c, PB_ERR_ARG, "pb_set_option: TMA staging must be 0 or 1");
       c->tma_mode = (int32_t)value;
       return PB_OK;
+    case PB_OPT_BAND_WARPS:
+      if (value != 4 && value != 8) return fail(c, PB_ERR_ARG, "pb_set_option: band warps must be 4 or 8");
+      c->band_warps = (int32_t)value;
+      return PB_OK;
     case PB_OPT_STAGING_WAIT_TRIES:
       if (value < 0) c->staging_wait_tries = kWaitTries;
       else if (value > kWaitTries) return fail(c, PB_ERR_ARG, "pb_set_option: staging wait above %lld polls", kWaitTries);
@@ -3695,6 +3757,7 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
     case PB_OPT_BATCHED_KERNELS: *value = c->batched_mode; return PB_OK;
     case PB_OPT_TMA_STAGING: *value = c->tma_mode; return PB_OK;
     case PB_OPT_STAGING_WAIT_TRIES: *value = c->staging_wait_tries; return PB_OK;
+    case PB_OPT_BAND_WARPS: *value = c->band_warps; return PB_OK;
     case PB_INFO_LAST_TMA: *value = c->last_tma ? 1 : 0; return PB_OK;
     case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
@@ -3938,6 +4001,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)blocked);
     put((uint64_t)(blocked && c->tma_ok));
     put((uint64_t)c->staging_wait_tries);
+    put((uint64_t)c->band_warps);
     put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
     put((uint64_t)c->slab_nent);
     put((uint64_t)c->em_W);

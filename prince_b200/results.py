@@ -26,6 +26,7 @@ import numpy as np
 from .data import EnergyGrid, is_nucleus
 
 _NEUTRINOS = (12, -12, 14, -14, 16, -16)
+_TINY = np.finfo(np.float64).tiny
 
 
 def grid_triple(grid):
@@ -128,7 +129,9 @@ class GroupProjector:
         # nearest positive bin at or below / at or above every bin
         below = torch.where(pos, idx, torch.full_like(idx, -1)).cummax(dim=1).values
         above = torch.where(pos, idx, torch.full_like(idx, d)).flip(1).cummin(dim=1).values.flip(1)
-        ls = torch.log(torch.where(pos, spec, torch.ones_like(spec)))
+        # log of the positive bins; subnormal values enter at the smallest normal
+        # double, so that the derivative 1/spec stays finite
+        ls = torch.log(torch.where(pos, spec.clamp(min=_TINY), torch.ones_like(spec)))
         le = torch.as_tensor(self.le, dtype=dt, device=dev)
         lx = torch.as_tensor(self.lx, dtype=dt, device=dev)
         j = torch.as_tensor(self.j, device=dev)                                  # (S, G)
@@ -149,6 +152,9 @@ class GroupProjector:
         slope = (lsR - lsL) / span
         val = slope * (lx[None, :, None] - leL) + lsL
         val = torch.where(on, lsL, val)
+        # points outside the span are zero; their log value is masked before
+        # exp so that no overflow there reaches the derivative
+        val = torch.where(inside, val, torch.zeros_like(val))
         out = torch.where(inside, torch.exp(val), torch.zeros_like(val))
         return back(out[..., 0] if flat else out)
 

@@ -331,3 +331,33 @@ def test_staging_wait_gives_up_cleanly_and_the_next_solve_is_correct(medium_run)
     assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == 1 and ctx.info(_lib.PB_INFO_LAST_TMA) == 1
     ref = O.OracleSolver(run, zi, 0.0, K=K, exp="cr").solve([[s] for s in srcs], dz=1e-3)
     assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
+
+
+def test_band_tiles_in_four_warp_ctas_agree(medium_run):
+    """The half-size band CTAs (4 warps, one band species staged at a time)
+    against the default 8-warp CTAs: the same tiles, different group sums."""
+    from prince_b200 import _lib
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, point_source
+    run = medium_run
+    K = 70
+    pts = draw_points(run, K, seed=13, z_range=(0.02, 0.06))
+    srcs = [point_source(run, p) for p in pts]
+    zi = max(p["zmax"] for p in pts)
+    m = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=K)
+    for k, s in enumerate(srcs):
+        m[k].add_source_class(s)
+    ctx = m._dev.ctx
+    out = {}
+    try:
+        for nw in (8, 4):
+            ctx.set_option(_lib.PB_OPT_BAND_WARPS, nw)
+            m.solve(dz=1e-3)
+            assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == 1
+            out[nw] = m.state.copy()
+    finally:
+        ctx.set_option(_lib.PB_OPT_BAND_WARPS, 8)
+    worst, above, total = local_scale_check(out[4], out[8], _blocks(run), tol=TOL)
+    assert worst < 1e-13, worst
+    ref = O.OracleSolver(run, zi, 0.0, K=K, exp="cr").solve([[s] for s in srcs], dz=1e-3)
+    assert rel_err_on_support(out[4], ref, _blocks(run)) < TOL

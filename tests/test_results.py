@@ -110,3 +110,20 @@ def test_torch_projection_is_differentiable(golden):
     assert np.all(np.isfinite(g))
     # a bin that is not positive never enters the interpolation
     assert np.all(g[z["mixed_state"] <= 0, 1] == 0)
+
+
+def test_projection_derivative_stays_finite_across_dynamic_range(golden):
+    """Spectra spanning ~600 decades (subnormal tails, values next to zeros):
+    the log-log projection and its derivative stay finite."""
+    import torch
+
+    z, grid, sm = golden
+    x = np.array(z["mixed_state"])
+    d = grid.d
+    for i in range(len(sm.species_refs)):
+        blk = x[i * d:(i + 1) * d]
+        blk[-6:] = np.abs(blk[-6:]) * np.array([1e-150, 1e-300, 5e-320, 1e-310, 0.0, 1e-200])
+    X = torch.tensor(np.stack([x, z["plain_state"]], axis=1), requires_grad=True)
+    _, F = UHECRPropagationResult(X, grid.grid, sm, grid).get_solution_group("CR", epow=3)
+    (torch.log(F[F > 0]) ** 2).sum().backward()
+    assert torch.isfinite(X.grad).all()
