@@ -53,6 +53,7 @@ extern "C" {
 #define PB_OPT_BAND_WARPS 12       /* warps of a band-tile CTA: 8 (default, 64 columns, one CTA per SM) or 4
                                      (32 columns in half the registers and shared memory, so the band
                                      tiles run on the tensor pipe beside the bin-local gather on each SM) */
+#define PB_OPT_SLAB_PREFETCH 13    /* row pairs whose FD term and F(x) a bin-local warp loads ahead: 2, 3 (default), 4 */
 #define PB_OPT_STAGING_WAIT_TRIES 11 /* polls of k_slab's bounded staging wait before it gives up and the solve
                                      returns PB_ERR_DEVICE (default 2^24; < 0 restores it; 0 gives up at
                                      once, which tests the error path). The CTA still drains its copies. */
@@ -261,6 +262,24 @@ typedef struct pb_solve_args {
 } pb_solve_args;
 
 int pb_solve(pb_context* ctx, const pb_solve_args* args);
+
+/* Autotuner of the batched bin-blocked stage: runs the solve described by
+ * `args` (normally a short schedule with every column active, on the live
+ * operator, injection and photon field) `reps` + 1 times for each candidate
+ * (band-tile CTA warps 8 / 4, k_slab prefetch depth 2 / 3 / 4, k_slab staging
+ * by TMA / cp.async), scores each by its fastest step loop, and leaves the
+ * fastest set on the context (the PB_OPT_BAND_WARPS, PB_OPT_SLAB_PREFETCH and
+ * PB_OPT_TMA_STAGING options).  Writes up to max_out candidates to out, the
+ * chosen one first, and their count to n_out.  `args->state` receives the
+ * short solve's states.  Replaces: the fixed K-dependent multi-RHS tile
+ * choices of the reference's batched path (src/prince_cr/solvers/propagation.py:2375-2391),
+ * which has no tuner of its own. */
+typedef struct pb_tune_choice {
+  int32_t band_warps, slab_prefetch, tma_staging;
+  double steps_ms;   /* fastest step loop of the candidate's runs; 1e300 if it could not run */
+} pb_tune_choice;
+int pb_autotune(pb_context* ctx, const pb_solve_args* args, int32_t reps, int32_t max_out,
+                pb_tune_choice* out, int32_t* n_out);
 
 /* Discrete adjoint of the last solve: gradients of L = sum(seed * x_final) with
  * respect to the injection grids (n_rows x n_src, as passed to pb_set_injection),

@@ -26,6 +26,7 @@ PB_INFO_BAND_ENTRIES, PB_INFO_SLAB_ENTRIES, PB_INFO_SLAB_ROWS, PB_INFO_FD_DENSE 
 PB_OPT_TMA_STAGING, PB_INFO_LAST_TMA = 9, 10
 PB_OPT_STAGING_WAIT_TRIES = 11
 PB_OPT_BAND_WARPS = 12
+PB_OPT_SLAB_PREFETCH = 13
 
 _d = C.POINTER(C.c_double)
 _i32 = C.POINTER(C.c_int32)
@@ -77,6 +78,11 @@ class KernelSpecArgs(C.Structure):
     ]
 
 
+class TuneChoice(C.Structure):
+    _fields_ = [("band_warps", C.c_int32), ("slab_prefetch", C.c_int32), ("tma_staging", C.c_int32),
+                ("steps_ms", C.c_double)]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "pb_abi_version": (C.c_int, []),
@@ -90,6 +96,8 @@ _PROTOS = {
     "pb_set_photon_field": (C.c_int, [_vp, C.c_int32, _i32, _d]),
     "pb_set_photon_table": (C.c_int, [_vp, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_build_fold_kernel": (C.c_int, [_vp, C.POINTER(KernelSpecArgs)]),
+    "pb_autotune": (C.c_int, [_vp, C.POINTER(SolveArgs), C.c_int32, C.c_int32, C.POINTER(TuneChoice),
+                              C.POINTER(C.c_int32)]),
     "pb_get_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
     "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
@@ -318,6 +326,22 @@ class Context:
         """Run one solve.  ``state`` is an (n, K) float64 host array (in/out)
         unless ``state_ptr`` (a device pointer) is given.  ``out_cols`` (solve
         column -> output column) orders the returned columns."""
+        args, keep = self._solve_args(sched, flags, n_cols, coeff, n_active, state, photon_scale, init_state,
+                                      state_ptr, out_cols)
+        self._check(self.lib.pb_solve(self.h, C.byref(args)), "pb_solve")
+
+    def autotune(self, sched, flags, n_cols, coeff, n_active, state, reps=3, photon_scale=1.0):
+        """Search the batched stage's tile parameters on this solve; the fastest stays set.
+        Returns the candidates as dicts, the chosen one first."""
+        args, keep = self._solve_args(sched, flags, n_cols, coeff, n_active, state, photon_scale, False, None, None)
+        out = (TuneChoice * 32)()
+        n = C.c_int32(0)
+        self._check(self.lib.pb_autotune(self.h, C.byref(args), int(reps), 32, out, C.byref(n)), "pb_autotune")
+        return [dict(band_warps=o.band_warps, slab_prefetch=o.slab_prefetch, tma_staging=o.tma_staging,
+                     steps_ms=o.steps_ms) for o in out[: n.value]]
+
+    def _solve_args(self, sched, flags, n_cols, coeff, n_active, state, photon_scale, init_state, state_ptr,
+                    out_cols):
         keep = []
 
         def f(a):
@@ -354,7 +378,7 @@ class Context:
         args.init_state = 1 if init_state else 0
         if out_cols is not None:
             args.out_cols = i(out_cols)
-        self._check(self.lib.pb_solve(self.h, C.byref(args)), "pb_solve")
+        return args, keep
 
     def operator_pattern(self, n):
         nnz = C.c_int64(0)

@@ -77,6 +77,7 @@ struct DBuf {
 }  // namespace
 
 constexpr long long kWaitTries = 1ll << 24;  // polls of a bounded wait (well above any staging time)
+constexpr int kSlabPreDefault = 3;           // k_slab's default prefetch depth (row pairs)
 struct pb_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -166,6 +167,7 @@ struct pb_context {
   int32_t tma_mode = 1;             // 1: k_slab stages by TMA when tensor maps can be encoded; 0: cp.async
   long long staging_wait_tries = kWaitTries;  // k_slab's first staging wait (PB_OPT_STAGING_WAIT_TRIES)
   int32_t band_warps = 8;           // warps of a k_band CTA (PB_OPT_BAND_WARPS: 8 or 4)
+  int32_t slab_pre = kSlabPreDefault;  // k_slab prefetch depth in row pairs (PB_OPT_SLAB_PREFETCH: 2..4)
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -1335,7 +1337,6 @@ __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalar
 // starts on a 16-byte boundary (the quad count of a bin is even).
 constexpr int kSlabCols = 16;       // state columns of a k_slab CTA (a half-warp per row)
 constexpr int kSlabWarps = 16;      // two CTAs per SM: 32 warps hide the gather's latencies (64 registers)
-constexpr int kSlabPre = 3;         // row pairs whose FD term and F(x) a warp loads ahead
 struct SlabSmem {
   double* slab;
   double* vals;
@@ -1368,12 +1369,12 @@ struct SlabSmem {
 // preparation) arrive in shared memory by asynchronous copies; a warp then walks its row pairs (balanced over the warps when the
 // layout is built), sums each row from shared memory (four accumulators, one
 // per quad position) and applies the stage update.  The row's FD term
-// (fdbuf), F(x) in stage 2 and its injection slot are loaded kSlabPre pairs
+// (fdbuf), F(x) in stage 2 and its injection slot are loaded PREF pairs
 // ahead into registers.  REC: the adjoint's record pass (P / Q sensitivities);
 // its row and (row, column) inputs are loaded with the others, a pair less ahead.
 // Offsets into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at
 // launch).
-template <int STAGE, bool REC>
+template <int STAGE, bool REC, int PREF>
 __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   extern __shared__ __align__(128) double sm[];  // TMA boxes land at 128-byte boundaries
   const int e = blockIdx.x;
@@ -1432,7 +1433,7 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   }
   const int w0 = p.slab_wrp[e * (kSlabWarps + 1) + wid], w1 = p.slab_wrp[e * (kSlabWarps + 1) + wid + 1];
   const bool need_fd = s.kap, need_f = STAGE == 2;
-  constexpr int PRE = REC ? kSlabPre - 1 : kSlabPre;  // the record inputs take registers too
+  constexpr int PRE = REC ? PREF - 1 : PREF;  // the record inputs take registers too
   double fdr[PRE], fxr[PRE];
   int slr[PRE];
   // record pass: dsigma and phi1' / phi2' of the row, D_off (kappa_pair v) and S x of (row, column)
@@ -1550,6 +1551,21 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
     }
   }
 #undef PB_SLAB_LOAD
+}
+
+// k_slab instance for (stage, record pass, prefetch depth in row pairs).
+using SlabKernel = void (*)(StepParams);
+template <int PREF>
+SlabKernel slab_kernel_p(int stage, bool rec) {
+  if (stage == 1) return rec ? k_slab<1, true, PREF> : k_slab<1, false, PREF>;
+  return rec ? k_slab<2, true, PREF> : k_slab<2, false, PREF>;
+}
+SlabKernel slab_kernel(int stage, bool rec, int pre) {
+  switch (pre) {
+    case 2: return slab_kernel_p<2>(stage, rec);
+    case 4: return slab_kernel_p<4>(stage, rec);
+    default: return slab_kernel_p<3>(stage, rec);
+  }
 }
 
 // Stage 2: the row factors of the next step for the bin-local rows (one
@@ -2736,8 +2752,7 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
     ++launches;
   }
   const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
-  if (p.rec_P) k_slab<STAGE, true><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
-  else k_slab<STAGE, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
+  slab_kernel(STAGE, p.rec_P != nullptr, c->slab_pre)<<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
   ++launches;
   if (STAGE == 2 && p.step + 1 < p.n_steps) {
     k_slab_prep<<<blocks_for((int64_t)p.n_slab_spec * p.d, 256), 256, 0, st>>>(p);
@@ -3497,8 +3512,11 @@ int pb_set_layout(pb_context* c, int32_t d) {
   PB_CUDA(c, cudaMemsetAsync(c->slab_fac.p, 0, (size_t)2 * 3 * c->slab_nslots * sizeof(double), c->stream));
   if ((rc = upload(c, c->slab_slot, sslot.data(), sslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
-  for (const void* fn : {(const void*)k_slab<1, false>, (const void*)k_slab<2, false>, (const void*)k_slab<1, true>,
-                         (const void*)k_slab<2, true>}) {
+  std::vector<const void*> slab_fns;
+  for (int pre : {2, 3, 4})
+    for (int st = 1; st <= 2; ++st)
+      for (bool rec : {false, true}) slab_fns.push_back((const void*)slab_kernel(st, rec, pre));
+  for (const void* fn : slab_fns) {
     PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
     PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   }
@@ -3668,8 +3686,7 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
       }
       if (kk == 1) {
         const dim3 sg(p.d, (unsigned)blocks_for(p.ncols, kSlabCols));
-        if (stage == 1) k_slab<1, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
-        else k_slab<2, false><<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
+        slab_kernel(stage, false, c->slab_pre)<<<sg, kSlabWarps * 32, c->slab_smem, st>>>(p);
       }
       if (kk == 2) bi.fn<<<dim3(cblocks, p.ngroups, c->band_npairs), bi.warps * 32, bi.smem, st>>>(p);
       if (kk == 3) {
@@ -3741,6 +3758,10 @@ int pb_set_option(pb_context* c, int32_t key, int64_t value) {
       if (value != 4 && value != 8) return fail(c, PB_ERR_ARG, "pb_set_option: band warps must be 4 or 8");
       c->band_warps = (int32_t)value;
       return PB_OK;
+    case PB_OPT_SLAB_PREFETCH:
+      if (value < 2 || value > 4) return fail(c, PB_ERR_ARG, "pb_set_option: slab prefetch must be 2, 3 or 4");
+      c->slab_pre = (int32_t)value;
+      return PB_OK;
     case PB_OPT_STAGING_WAIT_TRIES:
       if (value < 0) c->staging_wait_tries = kWaitTries;
       else if (value > kWaitTries) return fail(c, PB_ERR_ARG, "pb_set_option: staging wait above %lld polls", kWaitTries);
@@ -3758,6 +3779,7 @@ int pb_get_info(pb_context* c, int32_t key, int64_t* value) {
     case PB_OPT_TMA_STAGING: *value = c->tma_mode; return PB_OK;
     case PB_OPT_STAGING_WAIT_TRIES: *value = c->staging_wait_tries; return PB_OK;
     case PB_OPT_BAND_WARPS: *value = c->band_warps; return PB_OK;
+    case PB_OPT_SLAB_PREFETCH: *value = c->slab_pre; return PB_OK;
     case PB_INFO_LAST_TMA: *value = c->last_tma ? 1 : 0; return PB_OK;
     case PB_INFO_BLOCKED_LAYOUT: *value = (c->blocked_ok && c->fd_tab_ok) ? 1 : 0; return PB_OK;
     case PB_INFO_LAST_BLOCKED: *value = c->last_blocked ? 1 : 0; return PB_OK;
@@ -4002,6 +4024,7 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     put((uint64_t)(blocked && c->tma_ok));
     put((uint64_t)c->staging_wait_tries);
     put((uint64_t)c->band_warps);
+    put((uint64_t)c->slab_pre);
     put((uint64_t)c->band_RT); put((uint64_t)c->band_J); put((uint64_t)c->band_nb); put((uint64_t)c->lay_d);
     put((uint64_t)c->slab_nent);
     put((uint64_t)c->em_W);
@@ -4077,6 +4100,56 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   c->last_K = K;
   c->last_flags = flags;
   c->last_scale = a->photon_scale;
+  return PB_OK;
+}
+
+// The tile parameters of the bin-blocked stage, searched on the live operator:
+// every (band-tile CTA warps, k_slab prefetch depth, k_slab staging) candidate
+// runs the caller's (short) solve `reps` times and is scored by its fastest
+// step loop (CUDA events around the step graph); the fastest candidate stays
+// set on the context.  Only the batched bin-blocked path has choices.
+int pb_autotune(pb_context* c, const pb_solve_args* a, int32_t reps, int32_t max_out, pb_tune_choice* out,
+                int32_t* n_out) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!a || reps < 1 || max_out < 0 || (max_out > 0 && !out) || !n_out)
+    return fail(c, PB_ERR_ARG, "pb_autotune: bad arguments");
+  *n_out = 0;
+  if (!use_blocked(c, a->n_cols)) return fail(c, PB_ERR_STATE, "pb_autotune: the solve does not run the bin-blocked kernels");
+  const int32_t keep_bw = c->band_warps, keep_pre = c->slab_pre, keep_tma = c->tma_mode;
+  std::vector<pb_tune_choice> cand;
+  for (int tma : {1, 0})
+    for (int bw : {8, 4})
+      for (int pre : {3, 2, 4}) cand.push_back(pb_tune_choice{bw, pre, tma, 0.0});
+  int best = -1;
+  for (size_t i = 0; i < cand.size(); ++i) {
+    c->band_warps = cand[i].band_warps;
+    c->slab_pre = cand[i].slab_prefetch;
+    c->tma_mode = cand[i].tma_staging;
+    double t = 1e300;
+    for (int r = 0; r < reps + 1; ++r) {  // the first run captures the candidate's graph
+      const int rc = pb_solve(c, a);
+      if (rc) {
+        c->band_warps = keep_bw;
+        c->slab_pre = keep_pre;
+        c->tma_mode = keep_tma;
+        return rc;
+      }
+      if (r > 0) t = std::min(t, (double)c->last_steps_ms);
+    }
+    if (cand[i].tma_staging == 1 && !c->last_tma) t = 1e300;  // tensor maps unavailable: not a candidate
+    cand[i].steps_ms = t;
+    if (best < 0 || t < cand[best].steps_ms) best = (int)i;
+  }
+  c->band_warps = cand[best].band_warps;
+  c->slab_pre = cand[best].slab_prefetch;
+  c->tma_mode = cand[best].tma_staging;
+  // best first, then the rest in search order
+  std::vector<pb_tune_choice> ordered{cand[best]};
+  for (size_t i = 0; i < cand.size(); ++i)
+    if ((int)i != best) ordered.push_back(cand[i]);
+  const int n = std::min<int>(max_out, (int)ordered.size());
+  for (int i = 0; i < n; ++i) out[i] = ordered[i];
+  *n_out = n;
   return PB_OK;
 }
 

@@ -306,8 +306,7 @@ class UHECRPropagationSolverETD2:
             ctx.set_injection(rows, G, src_col, K)
         else:
             flags &= ~_lib.PB_INJECTION
-        ctx.set_photon_field(device_components(self.prince_run.photon_field),
-                             table=device_table(self.prince_run.photon_field))
+        self._set_field(ctx)
         if flags & _lib.PB_EM_CASCADE:
             ctx.set_em_windows(*self._em_windows(sched, dz))
         state = np.empty((self.dim_states, K))
@@ -321,6 +320,10 @@ class UHECRPropagationSolverETD2:
             print(f"  steps: {sched.n_steps}")
             print(f"  initial z: {self.initial_z} → final z: {self.final_z}")
             print(f"  wall time: {time.time() - start:.3f} s")
+
+    def _set_field(self, ctx):
+        f = self.prince_run.photon_field
+        ctx.set_photon_field(device_components(f), table=device_table(f))
 
     def _store(self, state):
         self.state = state[:, 0].copy()
