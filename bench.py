@@ -439,7 +439,7 @@ def cpu_line(pts, zi, sched, processes=None, sampler=None):
         if own:
             sampler.close()
     rate, t_full = cpu_bench.extrapolate(samples, sched.n_steps, len(sched.z_window))
-    return {"value": rate, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": "port",
+    return {"value": rate, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": sampler.kind,
             "sample": cpu_bench.describe(sampler, CPU_SAMPLE_STEPS, sched.n_steps, len(sched.z_window), t_full),
             "sample_wall_s": wall}
 
@@ -520,7 +520,7 @@ def reference_arm(args):
         "data": "synthetic (seeded synthetic photo-nuclear model and source points)",
         "config": config,
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "spectra/s", "cores": len(sampler.chunks), "kind": sampler.kind,
                          "sample": "per step: " + cpu_bench.describe(sampler, CPU_SAMPLE_STEPS, sched.n_steps,
                                                                      len(sched.z_window), t_full),
                          "spread": [min(vals), max(vals)]},

@@ -90,6 +90,41 @@ class PhotoNuclearInteractionRate:
         pf = pfield if pfield is not None else self.photon_field
         return pf.get_photon_density(self.e_photon.grid, z)
 
+    def get_hadr_jacobian(self, z, scale_fac=1.0, force_update=False, pfield=None):
+        """The coupling matrix at redshift z on the host: its values are the fold
+        ``_batch_matrix @ photon_vector(z)`` (times ``scale_fac``), the contract of
+        ``interaction_rates.py:966-1120``.  The B200 solvers never call it; it lets
+        the reference's own CPU solver run on this run object."""
+        vec = np.dot(self._batch_matrix, self.photon_vector(z, pfield=pfield))
+        if scale_fac != 1.0:
+            vec = scale_fac * vec
+        self.coupling_mat.data[:] = vec
+        return self.coupling_mat
+
+    def build_split_fold(self, off_to_M, diag_to_M):
+        """Row-subset kernels of the off-diagonal values and the diagonal
+        (the contract of ``interaction_rates.py:780-822``), rebuilt whenever the
+        maps change (the reference keeps the first solve's, which a later solve
+        from another first window would misread)."""
+        key = (np.asarray(off_to_M).tobytes(), np.asarray(diag_to_M).tobytes())
+        if getattr(self, "_sf_key", None) != key:
+            bm = self._batch_matrix
+            present = np.asarray(diag_to_M) >= 0
+            self._sf_off_kernel = bm[np.asarray(off_to_M, dtype=np.int64)]
+            self._sf_diag_present = present
+            self._sf_diag_kernel = bm[np.asarray(diag_to_M, dtype=np.int64)[present]]
+            self._sf_key = key
+        self._split_fold_ready = True
+
+    def fold_split(self, z, moff_data_out, dmg_out):
+        """Fold straight into ``M_off.data`` and the diagonal (``interaction_rates.py:824-847``)."""
+        ph = np.asarray(self.photon_vector(z), dtype=np.float64)
+        if moff_data_out.size:
+            np.copyto(moff_data_out, self._sf_off_kernel.dot(ph))
+        dmg_out.fill(0.0)
+        if self._sf_diag_kernel.shape[0]:
+            dmg_out[self._sf_diag_present] = self._sf_diag_kernel.dot(ph)
+
 
 class _ContinuousLossBase:
     def __init__(self, prince_run, energy="grid"):

@@ -1,4 +1,4 @@
-"""Import the installed PriNCe reference for the plug-in tests.
+"""Import the installed PriNCe reference (plug-in tests, the bench's reference arm).
 
 The reference is installed (``pip install --no-deps --target baseline/_ref``)
 beside the repository and travels with it; it is not part of this package.
@@ -47,14 +47,24 @@ def _stub_h5py():
     sys.modules.setdefault("h5py", h5)
 
 
+def load_package():
+    """Import the installed reference (``prince_cr``) from a scratch copy; returns its ``config``."""
+    if "prince_cr" not in sys.modules:
+        tmp = tempfile.mkdtemp(prefix="prince_ref_")
+        shutil.copytree(INSTALLED, os.path.join(tmp, "prince_cr"))
+        os.chmod(os.path.join(tmp, "prince_cr", "data"), 0o755)
+        open(os.path.join(tmp, "prince_cr", "data", "prince_db_05.h5"), "wb").close()
+        _stub_h5py()
+        sys.path.insert(0, tmp)
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    return config
+
+
 def load_light_run():
     """``(prince_cr package, reference PriNCeRun of the light network)``."""
-    tmp = tempfile.mkdtemp(prefix="prince_ref_")
-    shutil.copytree(INSTALLED, os.path.join(tmp, "prince_cr"))
-    os.chmod(os.path.join(tmp, "prince_cr", "data"), 0o755)
-    open(os.path.join(tmp, "prince_cr", "data", "prince_db_05.h5"), "wb").close()
-    _stub_h5py()
-    sys.path.insert(0, tmp)
+    load_package()
     import prince_cr
     import prince_cr.config as config
 
