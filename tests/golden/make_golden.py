@@ -9,6 +9,7 @@ source tree (the directory that holds ``src/prince_cr``)::
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --groups  # result post-processing
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --ebl     # tabulated EBL (Gilmore 2012)
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --kernel  # fold-kernel construction inputs
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --cascade # kinetic EM-cascade transfer
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -580,6 +581,37 @@ def main_kernel():
     print("wrote", path, os.path.getsize(path), "bytes;", spec.channels.shape[0], "channels,", spec.n_rows, "rows")
 
 
+def main_cascade():
+    """The reference's kinetic EM-cascade transfer on a small EM grid.
+
+    ``kinetic_cascade_transfer_batched`` (its FP64 iteration) for CMB + the
+    synthetic 40 K grey-body CIB of ``prince_b200.photonfields``, a 40-bin
+    grid from 1e-3 to 1e14 GeV and three redshifts, per-step escape for
+    dz = 1e-3.  Records the inputs and ``(T_gamma, T_electron)`` per z.
+    """
+    _prepare_reference()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.linear_algebra_backend = "scipy"
+    from prince_cr.cascade.cascade import kinetic_cascade_transfer_batched
+    from prince_b200 import photonfields as pf
+    from prince_b200.data import EnergyGrid
+
+    grid = EnergyGrid(-3, 14, 40 / 17)
+    E = grid.grid
+    zs = [0.0, 0.37, 1.0]
+    field = pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), pf.ModifiedBlackBodyCIB()])
+    out = {"E": E, "grid": np.array([-3.0, 14.0, 40 / 17]), "zs": np.array(zs), "dz": np.array(1e-3)}
+    Ts = kinetic_cascade_transfer_batched(E, zs, field, dz=1e-3, iter_dtype="float64")
+    out["T_gamma"] = np.stack([t[0] for t in Ts])
+    out["T_electron"] = np.stack([t[1] for t in Ts])
+    path = os.path.join(HERE, "em_cascade_transfer.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     if "--em" in sys.argv:
         main_em()
@@ -589,5 +621,7 @@ if __name__ == "__main__":
         main_ebl()
     elif "--kernel" in sys.argv:
         main_kernel()
+    elif "--cascade" in sys.argv:
+        main_cascade()
     else:
         main()
