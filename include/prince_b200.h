@@ -226,6 +226,46 @@ int pb_set_em(pb_context* ctx, int32_t n_em, int64_t gamma_off, int64_t em_off, 
 int pb_set_em_windows(pb_context* ctx, int32_t n_windows, const double* Tg, const double* Te,
                       const double* R, const double* dl_step);
 
+/* Kinetic EM-cascade transfer built on the device for the context's photon
+ * field (times photon_scale): per redshift z[q] the photon transfer T_gamma
+ * and the electron transfer T_electron (n x n each, row-major, written to
+ * n_z x n x n host arrays) of the EM grid E (n increasing bin centres, GeV),
+ * with per-step escape over dl_step[q] = c |dz| / ((1+z) H(z)) [cm].  eps is
+ * the target grid of the inverse-Compton and pair kernels, eps_o / mu the
+ * grids of the gamma-gamma opacity, n_E1 the points of the per-electron
+ * IC-loss grid; m_electron [GeV], r_electron [cm] and c_cm [cm/s] are the
+ * caller's unit constants.  Field-free kernels, their contractions with the
+ * photon stacks (FP64 tensor-core GEMMs), the per-redshift matrices and the
+ * scattering iteration (at most max_scatter passes, each redshift stopping
+ * when the energy left in the box falls below tol of what entered) all run on
+ * the device, in FP64.  *iterations (if given) receives the passes run.
+ * Replaces: kinetic_cascade_transfer_batched (src/prince_cr/cascade/cascade.py:444-589),
+ * with its kernels (cascade.py:78-171, 425-441; kernels.py:68-75; opacity.py:44-75)
+ * and an FP64 iteration. */
+typedef struct pb_em_transfer_args {
+  int32_t n;
+  const double* E;
+  int32_t n_z;
+  const double* z;
+  const double* dl_step;
+  int32_t n_eps;
+  const double* eps;
+  int32_t n_eps_o;
+  const double* eps_o;
+  int32_t n_mu;
+  const double* mu;
+  int32_t n_E1;
+  double photon_scale;
+  double cool_floor_frac;
+  int32_t max_scatter;
+  double tol;
+  double m_electron, r_electron, c_cm;
+  double* T_gamma;
+  double* T_electron;
+  int32_t* iterations;
+} pb_em_transfer_args;
+int pb_em_transfer(pb_context* ctx, const pb_em_transfer_args* args);
+
 /* One solve: the redshift stepping of UHECRPropagationSolverETD2.solve /
  * MultiRHSPropagationSolverETD2.solve (propagation.py:813-890; etd2.py:478-517;
  * _operator_at / apply_F propagation.py:1360-1508; multi-RHS 2495-2618).

@@ -78,6 +78,19 @@ class KernelSpecArgs(C.Structure):
     ]
 
 
+class EmTransferArgs(C.Structure):
+    """``pb_em_transfer_args``."""
+
+    _fields_ = [
+        ("n", C.c_int32), ("E", _d), ("n_z", C.c_int32), ("z", _d), ("dl_step", _d),
+        ("n_eps", C.c_int32), ("eps", _d), ("n_eps_o", C.c_int32), ("eps_o", _d),
+        ("n_mu", C.c_int32), ("mu", _d), ("n_E1", C.c_int32), ("photon_scale", C.c_double),
+        ("cool_floor_frac", C.c_double), ("max_scatter", C.c_int32), ("tol", C.c_double),
+        ("m_electron", C.c_double), ("r_electron", C.c_double), ("c_cm", C.c_double),
+        ("T_gamma", _d), ("T_electron", _d), ("iterations", C.POINTER(C.c_int32)),
+    ]
+
+
 class TuneChoice(C.Structure):
     _fields_ = [("band_warps", C.c_int32), ("slab_prefetch", C.c_int32), ("tma_staging", C.c_int32),
                 ("steps_ms", C.c_double)]
@@ -99,6 +112,7 @@ _PROTOS = {
     "pb_autotune": (C.c_int, [_vp, C.POINTER(SolveArgs), C.c_int32, C.c_int32, C.POINTER(TuneChoice),
                               C.POINTER(C.c_int32)]),
     "pb_get_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
+    "pb_em_transfer": (C.c_int, [_vp, C.POINTER(EmTransferArgs)]),
     "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
@@ -241,6 +255,32 @@ class Context:
         self._check(self.lib.pb_get_fold_kernel(self.h, int(R), int(dph), _ptr(out, C.c_double)),
                     "pb_get_fold_kernel")
         return out
+
+    def em_transfer(self, E, zs, dl_step, eps, eps_o, mu, n_E1=400, photon_scale=1.0, cool_floor_frac=0.1,
+                    max_scatter=4000, tol=1e-4):
+        """Device kinetic cascade transfer on the context's photon field:
+        ``(T_gamma, T_electron, passes)`` with the matrices ``(n_z, n, n)``."""
+        from .constants import PRINCE_UNITS as U
+
+        keep = [_f64(E), _f64(zs), _f64(dl_step), _f64(eps), _f64(eps_o), _f64(mu)]
+        E_, z_, dl_, eps_, epso_, mu_ = keep
+        n, nz = E_.size, z_.size
+        Tg = np.empty((nz, n, n))
+        Te = np.empty((nz, n, n))
+        it = C.c_int32(0)
+        a = EmTransferArgs()
+        a.n, a.E = n, _ptr(E_, C.c_double)
+        a.n_z, a.z, a.dl_step = nz, _ptr(z_, C.c_double), _ptr(dl_, C.c_double)
+        a.n_eps, a.eps = eps_.size, _ptr(eps_, C.c_double)
+        a.n_eps_o, a.eps_o = epso_.size, _ptr(epso_, C.c_double)
+        a.n_mu, a.mu = mu_.size, _ptr(mu_, C.c_double)
+        a.n_E1, a.photon_scale = int(n_E1), float(photon_scale)
+        a.cool_floor_frac, a.max_scatter, a.tol = float(cool_floor_frac), int(max_scatter), float(tol)
+        a.m_electron, a.r_electron, a.c_cm = U.m_electron, U.r_electron, U.c
+        a.T_gamma, a.T_electron = _ptr(Tg, C.c_double), _ptr(Te, C.c_double)
+        a.iterations = C.pointer(it)
+        self._check(self.lib.pb_em_transfer(self.h, C.byref(a)), "pb_em_transfer")
+        return Tg, Te, it.value
 
     def set_photon_grid(self, energies):
         e = _f64(energies)

@@ -2871,6 +2871,8 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
 // ===========================================================================
 // C ABI
 // ===========================================================================
+#include "em_transfer.cuh"
+
 extern "C" {
 
 int pb_abi_version(void) { return kAbiVersion; }
@@ -3836,6 +3838,223 @@ int pb_set_em_windows(pb_context* c, int32_t n_windows, const double* Tg, const 
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->em_dl.assign(dl_step, dl_step + n_windows);
   c->em_W = n_windows;
+  return PB_OK;
+}
+
+
+// Kinetic EM-cascade transfer (em_transfer.cuh): field-free kernels, the
+// contractions with the photon stacks, the per-redshift matrices and the
+// scattering iteration on the device; (T_gamma, T_electron) per redshift back
+// to the host.  The small per-electron loss grid, the trapezoid weights and
+// the loss-shift indices are set up here, as the reference computes them.
+int pb_em_transfer(pb_context* c, const pb_em_transfer_args* a) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!a) return fail(c, PB_ERR_ARG, "pb_em_transfer: args is NULL");
+  if (!c->have_field) return fail(c, PB_ERR_STATE, "pb_em_transfer: set the photon field first");
+  const int n = a->n, nz = a->n_z, ne = a->n_eps, no = a->n_eps_o, nmu = a->n_mu, nE1 = a->n_E1;
+  if (n < 2 || n > 1024 || nz < 1 || ne < 2 || no < 2 || nmu < 2 || nE1 < 2 || !a->E || !a->z || !a->dl_step ||
+      !a->eps || !a->eps_o || !a->mu || !a->T_gamma || !a->T_electron || a->max_scatter < 1 || !(a->tol > 0))
+    return fail(c, PB_ERR_ARG, "pb_em_transfer: bad arguments");
+  for (int i = 1; i < n; ++i)
+    if (!(a->E[i] > a->E[i - 1])) return fail(c, PB_ERR_ARG, "pb_em_transfer: E must increase");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  if (!(a->m_electron > 0) || !(a->r_electron > 0) || !(a->c_cm > 0))
+    return fail(c, PB_ERR_ARG, "pb_em_transfer: unit constants must be positive");
+  const double me = a->m_electron;
+  const double sigma_t = 8.0 / 3.0 * M_PI * (a->r_electron * a->r_electron);
+  const EmConst K{me, 0.75 * sigma_t * a->c_cm, sigma_t};
+  // host set-up (small): trapezoid weights, per-electron loss grid, dE, loss shift
+  auto tw = [](const double* x, int m, std::vector<double>& w) {
+    w.assign((size_t)m, 0.0);
+    for (int i = 1; i + 1 < m; ++i) w[i] = (x[i + 1] - x[i - 1]) / 2.0;
+    w[0] = (x[1] - x[0]) / 2.0;
+    w[m - 1] = (x[m - 1] - x[m - 2]) / 2.0;
+  };
+  std::vector<double> w_eps, w_o, dE((size_t)n), E1((size_t)n * nE1), w1((size_t)n * nE1), epsw_eps((size_t)ne);
+  tw(a->eps, ne, w_eps);
+  tw(a->eps_o, no, w_o);
+  for (int k = 0; k < ne; ++k) epsw_eps[k] = w_eps[k] * a->eps[k];
+  for (int i = 0; i < n; ++i)  // numpy.gradient: central inside, one-sided at the ends
+    dE[i] = i == 0 ? a->E[1] - a->E[0] : i == n - 1 ? a->E[n - 1] - a->E[n - 2] : (a->E[i + 1] - a->E[i - 1]) / 2.0;
+  double emin = a->eps[0];
+  for (int k = 1; k < ne; ++k) emin = std::min(emin, a->eps[k]);
+  const double lo = log10(emin);
+  for (int j = 0; j < n; ++j) {  // numpy.logspace(lo, log10(0.9999 E_j), nE1)
+    const double hi = log10(0.9999 * a->E[j]);
+    const double step = (hi - lo) / (nE1 - 1);
+    for (int m = 0; m < nE1; ++m) E1[(size_t)j * nE1 + m] = pow(10.0, m == nE1 - 1 ? hi : m * step + lo);
+    std::vector<double> w;
+    tw(&E1[(size_t)j * nE1], nE1, w);
+    std::copy(w.begin(), w.end(), w1.begin() + (size_t)j * nE1);
+  }
+  std::vector<int> bidx((size_t)n * n, -1);
+  std::vector<double> frac((size_t)n * n, 0.0);
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j) {
+      const double Eep = a->E[j] - a->E[k];
+      if (!(Eep > a->E[0])) continue;
+      int b = (int)(std::lower_bound(a->E, a->E + n, Eep) - a->E) - 1;
+      b = std::min(std::max(b, 0), n - 2);
+      const double f = (a->E[b + 1] - Eep) / (a->E[b + 1] - a->E[b]);
+      bidx[(size_t)k * n + j] = b;
+      frac[(size_t)k * n + j] = std::min(std::max(f, 0.0), 1.0);
+    }
+  const size_t nn = (size_t)n * n, zn = (size_t)nz * n, znn = (size_t)nz * nn;
+  DBuf dE_d, E_d, z_d, dl_d, eps_d, weps_d, epso_d, wo_d, mu_d, E1_d, w1_d, b_d, f_d, N, No, Ae, Ap, Bl, Kt, raw,
+      rawdN, rawt, emis, pair, P, Sg, cold, De, Mic, loss, Pe, epsm, G, e, esc, fin, T1, ec, eh, Gh, Gc, done, Te;
+  std::vector<DBuf*> all{&dE_d, &E_d, &z_d, &dl_d, &eps_d, &weps_d, &epso_d, &wo_d, &mu_d, &E1_d, &w1_d, &b_d, &f_d,
+                         &N, &No, &Ae, &Ap, &Bl, &Kt, &raw, &rawdN, &rawt, &emis, &pair, &P, &Sg, &cold, &De,
+                         &Mic, &loss, &Pe, &epsm, &G, &e, &esc, &fin, &T1, &ec, &eh, &Gh, &Gc, &done, &Te};
+  auto cleanup = [&]() { for (DBuf* b : all) b->release(); };
+  auto fail_cuda = [&](cudaError_t err, const char* what) {
+    cleanup();
+    return fail(c, PB_ERR_CUDA, "pb_em_transfer: %s: %s", what, cudaGetErrorString(err));
+  };
+  if ((rc = upload(c, dE_d, dE.data(), dE.size())) || (rc = upload(c, E_d, a->E, (size_t)n)) ||
+      (rc = upload(c, z_d, a->z, (size_t)nz)) || (rc = upload(c, dl_d, a->dl_step, (size_t)nz)) ||
+      (rc = upload(c, eps_d, a->eps, (size_t)ne)) || (rc = upload(c, weps_d, w_eps.data(), w_eps.size())) ||
+      (rc = upload(c, epso_d, a->eps_o, (size_t)no)) || (rc = upload(c, wo_d, w_o.data(), w_o.size())) ||
+      (rc = upload(c, mu_d, a->mu, (size_t)nmu)) || (rc = upload(c, E1_d, E1.data(), E1.size())) ||
+      (rc = upload(c, w1_d, w1.data(), w1.size())) || (rc = upload(c, b_d, bidx.data(), bidx.size())) ||
+      (rc = upload(c, f_d, frac.data(), frac.size()))) {
+    cleanup();
+    return rc;
+  }
+  struct Want { DBuf* b; size_t bytes; };
+  for (const Want& w : {Want{&N, (size_t)ne * nz * 8}, Want{&No, (size_t)no * nz * 8}, Want{&Ae, nn * ne * 8},
+                        Want{&Ap, nn * ne * 8}, Want{&Bl, (size_t)n * nE1 * ne * 8}, Want{&Kt, (size_t)n * no * 8},
+                        Want{&raw, nn * nz * 8}, Want{&rawdN, (size_t)n * nE1 * nz * 8}, Want{&rawt, zn * 8},
+                        Want{&emis, znn * 8}, Want{&pair, znn * 8}, Want{&P, znn * 8}, Want{&Sg, znn * 8},
+                        Want{&cold, zn}, Want{&De, znn * 8}, Want{&Mic, znn * 8}, Want{&loss, zn * 8},
+                        Want{&Pe, zn * 8}, Want{&epsm, (size_t)nz * 8}, Want{&G, znn * 8}, Want{&e, znn * 8},
+                        Want{&esc, znn * 8}, Want{&fin, znn * 8}, Want{&T1, znn * 8}, Want{&ec, znn * 8},
+                        Want{&eh, znn * 8}, Want{&Gh, znn * 8}, Want{&Gc, znn * 8}, Want{&done, (size_t)nz * 4},
+                        Want{&Te, znn * 8}}) {
+    const cudaError_t err = w.b->ensure(w.bytes);
+    if (err != cudaSuccess) return fail_cuda(err, "allocation");
+  }
+  const FieldDesc f = field_desc(c, a->photon_scale);
+  const int T = 256;
+  auto nb = [&](int64_t work) { return (unsigned)blocks_for(work, T); };
+  // 1. photon stacks; 2. field-free kernels
+  k_em_stack<<<nb((int64_t)ne * nz), T, 0, st>>>(f, eps_d.as<double>(), ne, z_d.as<double>(), nz, N.as<double>());
+  k_em_stack<<<nb((int64_t)no * nz), T, 0, st>>>(f, epso_d.as<double>(), no, z_d.as<double>(), nz, No.as<double>());
+  k_em_ic<<<nb((int64_t)nn * ne), T, 0, st>>>(K, E_d.as<double>(), n, eps_d.as<double>(), weps_d.as<double>(), ne,
+                                               Ae.as<double>());
+  k_em_pair<<<nb((int64_t)nn * ne), T, 0, st>>>(K, E_d.as<double>(), n, eps_d.as<double>(), weps_d.as<double>(), ne,
+                                                 Ap.as<double>());
+  k_em_icloss<<<nb((int64_t)n * nE1 * ne), T, 0, st>>>(K, E_d.as<double>(), E1_d.as<double>(), n, nE1,
+                                                       eps_d.as<double>(), weps_d.as<double>(), ne, Bl.as<double>());
+  k_em_tau<<<nb((int64_t)n * no), T, 0, st>>>(K, E_d.as<double>(), n, epso_d.as<double>(), wo_d.as<double>(), no,
+                                              mu_d.as<double>(), nmu, Kt.as<double>());
+  // 3. contractions (FP64 tensor-core GEMMs) and the per-column prefactors
+  std::vector<double> pe((size_t)n), pp((size_t)n);
+  for (int j = 0; j < n; ++j) {
+    const double g = a->E[j] / me;
+    pe[j] = g > 1.0 ? K.pref_ic / (g * g) : 0.0;
+    pp[j] = K.pref_ic / (g * g * g);
+  }
+  DBuf pe_d, pp_d;
+  all.push_back(&pe_d);
+  all.push_back(&pp_d);
+  if ((rc = upload(c, pe_d, pe.data(), pe.size())) || (rc = upload(c, pp_d, pp.data(), pp.size()))) {
+    cleanup();
+    return rc;
+  }
+  const unsigned gz = nb((int64_t)znn);
+  bgemm(st, Ae.as<double>(), N.as<double>(), raw.as<double>(), (int)nn, nz, ne, ne, nz, nz, 0, 0, 0, 1, false);
+  k_em_scatter_contraction<<<gz, T, 0, st>>>(raw.as<double>(), n, nz, pe_d.as<double>(), emis.as<double>());
+  bgemm(st, Ap.as<double>(), N.as<double>(), raw.as<double>(), (int)nn, nz, ne, ne, nz, nz, 0, 0, 0, 1, false);
+  k_em_scatter_contraction<<<gz, T, 0, st>>>(raw.as<double>(), n, nz, pp_d.as<double>(), pair.as<double>());
+  bgemm(st, Bl.as<double>(), N.as<double>(), rawdN.as<double>(), n * nE1, nz, ne, ne, nz, nz, 0, 0, 0, 1, false);
+  bgemm(st, Kt.as<double>(), No.as<double>(), rawt.as<double>(), n, nz, no, no, nz, nz, 0, 0, 0, 1, false);
+  // eps_mean[z] = (w eps) N / (w N), on the host from the stack (nz x ne values)
+  std::vector<double> Nh((size_t)ne * nz), em((size_t)nz);
+  cudaError_t err = cudaMemcpyAsync(Nh.data(), N.p, Nh.size() * 8, cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  if (err != cudaSuccess) return fail_cuda(err, "photon stack");
+  for (int z = 0; z < nz; ++z) {
+    double a1 = 0.0, b1 = 0.0;
+    for (int k = 0; k < ne; ++k) {
+      a1 += epsw_eps[k] * Nh[(size_t)k * nz + z];
+      b1 += w_eps[k] * Nh[(size_t)k * nz + z];
+    }
+    em[z] = a1 / b1;
+  }
+  if ((rc = upload(c, epsm, em.data(), em.size()))) {
+    cleanup();
+    return rc;
+  }
+  // 4. per-redshift matrices
+  std::vector<double> pl = pe;
+  DBuf pl_d;
+  all.push_back(&pl_d);
+  if ((rc = upload(c, pl_d, pl.data(), pl.size()))) {
+    cleanup();
+    return rc;
+  }
+  k_em_loss<<<nb((int64_t)zn), T, 0, st>>>(rawdN.as<double>(), n, nE1, nz, pl_d.as<double>(), E1_d.as<double>(),
+                                           w1_d.as<double>(), epsm.as<double>(), loss.as<double>());
+  k_em_columns<<<nb((int64_t)zn), T, 0, st>>>(pair.as<double>(), emis.as<double>(), E_d.as<double>(),
+                                              dE_d.as<double>(), n, nz, a->cool_floor_frac, P.as<double>(),
+                                              Sg.as<double>(), cold.as<unsigned char>());
+  k_em_shift<<<gz, T, 0, st>>>(Sg.as<double>(), E_d.as<double>(), dE_d.as<double>(), b_d.as<int>(), f_d.as<double>(),
+                               n, nz, De.as<double>());
+  k_em_cooled<<<nb((int64_t)zn), T, 0, st>>>(emis.as<double>(), loss.as<double>(), E_d.as<double>(), n, nz,
+                                             Mic.as<double>());
+  k_em_normalise<<<nb((int64_t)zn), T, 0, st>>>(Mic.as<double>(), E_d.as<double>(), n, nz);
+  k_em_escape<<<nb((int64_t)zn), T, 0, st>>>(rawt.as<double>(), dl_d.as<double>(), n, nz, Pe.as<double>());
+  // 5. the scattering iteration, checked on the host every 8 passes (a
+  // redshift that has converged keeps its frozen result)
+  std::vector<double> Ein((size_t)n);
+  for (int i = 0; i < n; ++i) Ein[i] = a->E[i] * dE[i];
+  DBuf Ein_d;
+  all.push_back(&Ein_d);
+  if ((rc = upload(c, Ein_d, Ein.data(), Ein.size()))) {
+    cleanup();
+    return rc;
+  }
+  k_em_iter_init<<<gz, T, 0, st>>>(n, nz, G.as<double>(), e.as<double>(), esc.as<double>(), fin.as<double>());
+  err = cudaMemsetAsync(done.p, 0, (size_t)nz * 4, st);
+  if (err != cudaSuccess) return fail_cuda(err, "init");
+  const long long snn = (long long)nn;
+  int passes = 0;
+  std::vector<int> hd((size_t)nz);
+  while (passes < a->max_scatter) {
+    const int batch = std::min(8, a->max_scatter - passes);
+    for (int q = 0; q < batch; ++q) {
+      k_em_iter_a<<<gz, T, 0, st>>>(Pe.as<double>(), dE_d.as<double>(), n, nz, G.as<double>(), esc.as<double>(),
+                                    T1.as<double>());
+      bgemm(st, P.as<double>(), T1.as<double>(), e.as<double>(), n, n, n, n, n, n, snn, snn, snn, nz, true);
+      k_em_iter_b<<<gz, T, 0, st>>>(e.as<double>(), cold.as<unsigned char>(), dE_d.as<double>(), n, nz,
+                                    ec.as<double>(), eh.as<double>());
+      bgemm(st, Mic.as<double>(), ec.as<double>(), Gc.as<double>(), n, n, n, n, n, n, snn, snn, snn, nz, false);
+      bgemm(st, Sg.as<double>(), eh.as<double>(), Gh.as<double>(), n, n, n, n, n, n, snn, snn, snn, nz, false);
+      bgemm(st, De.as<double>(), eh.as<double>(), e.as<double>(), n, n, n, n, n, n, snn, snn, snn, nz, false);
+      k_em_iter_c<<<gz, T, 0, st>>>(Pe.as<double>(), n, nz, Gh.as<double>(), Gc.as<double>(), G.as<double>(),
+                                    esc.as<double>());
+      k_em_iter_conv<<<nz, 256, 0, st>>>(Ein_d.as<double>(), Pe.as<double>(), n, a->tol, G.as<double>(),
+                                         e.as<double>(), esc.as<double>(), fin.as<double>(), done.as<int>());
+    }
+    passes += batch;
+    err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(hd.data(), done.p, (size_t)nz * 4, cudaMemcpyDeviceToHost, st);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+    if (err != cudaSuccess) return fail_cuda(err, "iteration");
+    if (std::all_of(hd.begin(), hd.end(), [](int v) { return v != 0; })) break;
+  }
+  k_em_finish<<<gz, T, 0, st>>>(done.as<int>(), esc.as<double>(), Mic.as<double>(), dE_d.as<double>(), n, nz,
+                                fin.as<double>(), T1.as<double>());
+  bgemm(st, fin.as<double>(), T1.as<double>(), Te.as<double>(), n, n, n, n, n, n, snn, snn, snn, nz, false);
+  err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaMemcpyAsync(a->T_gamma, fin.p, znn * 8, cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaMemcpyAsync(a->T_electron, Te.p, znn * 8, cudaMemcpyDeviceToHost, st);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(st);
+  if (err != cudaSuccess) return fail_cuda(err, "results");
+  if (a->iterations) *a->iterations = passes;
+  cleanup();
   return PB_OK;
 }
 

@@ -1,0 +1,75 @@
+"""The kinetic EM-cascade transfer, built on the device.
+
+``kinetic_transfer(ctx_or_run, E, zs, dz)`` returns the per-redshift photon
+and electron transfer ``(T_gamma, T_electron)`` of an EM grid ``E`` on a
+photon field (the one set on the device context, or a run's field), for
+per-step escape at the step ``dz``: PriNCe's
+``kinetic_cascade_transfer_batched`` (``src/prince_cr/cascade/cascade.py:444-589``)
+with an FP64 iteration, computed by ``pb_em_transfer`` -- field-free
+inverse-Compton, pair and gamma-gamma opacity kernels, their contractions with
+the photon densities as FP64 tensor-core GEMMs, the per-redshift matrices and
+the scattering iteration, all on the GPU.
+
+``KineticCascadeModel(run, dz)`` is a run's ``em_cascade_model`` built on it:
+``model(z) -> (T_gamma, T_electron, R_BH)`` with the transfer from the device
+(cached per redshift; ``prefetch(zs)`` builds all windows of a solve in one
+device call) and the Bethe-Heitler pair shape from a caller-supplied function.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import constants as C
+from .cosmology import H
+from .photonfields import device_components, device_table
+
+
+def default_grids():
+    """Target, opacity and angle grids of the reference (``cascade.py:466-468``)."""
+    return np.logspace(-15, -9, 400), np.logspace(-12, -7, 256), np.linspace(-1.0, 1.0, 128)
+
+
+def dl_step(zs, dz):
+    """c |dz| / ((1+z) H(z)) [cm] per redshift (``cascade.py:505``)."""
+    return np.array([C.PRINCE_UNITS.c * abs(dz) / ((1.0 + z) * H(z)) for z in zs])
+
+
+def kinetic_transfer(ctx, field, E, zs, dz, photon_scale=1.0, **kw):
+    """``(T_gamma, T_electron, passes)``: ``(n_z, n, n)`` arrays from the device."""
+    eps, eps_o, mu = default_grids()
+    ctx.set_photon_field(device_components(field), table=device_table(field))
+    zs = np.atleast_1d(np.asarray(zs, dtype=np.float64))
+    return ctx.em_transfer(np.asarray(E, dtype=np.float64), zs, dl_step(zs, dz), eps, eps_o, mu,
+                           photon_scale=photon_scale, **kw)
+
+
+class KineticCascadeModel:
+    """``em_cascade_model`` of a run: the device kinetic transfer plus a BH pair shape.
+
+    ``bh_shape(z) -> R_BH`` (n_em x n_cr) supplies the Bethe-Heitler e+- shape.
+    """
+
+    def __init__(self, run, dz, bh_shape, device=0):
+        self.run = run
+        self.dz = float(dz)
+        self.bh_shape = bh_shape
+        self.device = device
+        self._cache = {}
+
+    def prefetch(self, zs):
+        from .solvers import DeviceRun
+
+        todo = sorted({float(z) for z in zs} - set(self._cache))
+        if not todo:
+            return
+        ctx = DeviceRun.of(self.run, self.device).ctx
+        E = self.run.cr_grid.grid
+        Tg, Te, _ = kinetic_transfer(ctx, self.run.photon_field, E, todo, self.dz)
+        for i, z in enumerate(todo):
+            self._cache[z] = (Tg[i], Te[i])
+
+    def __call__(self, z):
+        self.prefetch([z])
+        tg, te = self._cache[float(z)]
+        return tg, te, self.bh_shape(z)

@@ -1,0 +1,60 @@
+"""The kinetic EM-cascade transfer built on the device (needs a B200).
+
+``pb_em_transfer`` against PriNCe's own ``kinetic_cascade_transfer_batched``
+(FP64 iteration; ``tests/golden/em_cascade_transfer.npz``) and against the CPU
+restatement on the 128-bin EM grid of config 5 (1e-3 to 1e14 GeV) at five
+redshifts up to z = 4, CMB + the synthetic grey-body CIB.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from golden_io import GOLDEN
+from oracle import em_cascade as EC
+
+pytestmark = pytest.mark.gpu
+
+
+def _field():
+    from prince_b200 import photonfields as pf
+    return pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), pf.ModifiedBlackBodyCIB()])
+
+
+def _close(dev, ref):
+    scale = np.abs(ref).max()
+    assert np.array_equal(np.abs(dev) > 1e-12 * scale, np.abs(ref) > 1e-12 * scale)
+    np.testing.assert_allclose(dev, ref, rtol=1e-9, atol=1e-12 * scale)
+
+
+def test_device_transfer_matches_the_reference():
+    from prince_b200 import _lib
+    from prince_b200.em_cascade import kinetic_transfer
+    z = np.load(os.path.join(GOLDEN, "em_cascade_transfer.npz"))
+    ctx = _lib.Context(0)
+    Tg, Te, passes = kinetic_transfer(ctx, _field(), z["E"], z["zs"], float(z["dz"]))
+    assert 0 < passes < 4000
+    for i in range(len(z["zs"])):
+        _close(Tg[i], z["T_gamma"][i])
+        _close(Te[i], z["T_electron"][i])
+
+
+def test_device_transfer_on_the_config5_grid_matches_the_restatement():
+    from prince_b200 import _lib
+    from prince_b200.data import EnergyGrid
+    from prince_b200.em_cascade import kinetic_transfer
+    E = EnergyGrid(-3, 14, 128 / 17).grid
+    assert E.size == 128
+    zs = [0.0, 0.5, 1.0, 2.0, 4.0]
+    ctx = _lib.Context(0)
+    Tg, Te, passes = kinetic_transfer(ctx, _field(), E, zs, 1e-3)
+    ref = EC.transfer(E, zs, _field(), 1e-3)
+    for i, (tg, te) in enumerate(ref):
+        _close(Tg[i], tg)
+        _close(Te[i], te)
+    # energy conservation of the photon transfer (to the convergence tolerance)
+    dE = np.gradient(E)
+    for i in range(len(zs)):
+        ratio = ((E * dE) @ Tg[i]) / (E * dE)
+        assert np.all(np.abs(ratio - 1.0) < 2e-3)
