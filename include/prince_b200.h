@@ -266,6 +266,34 @@ typedef struct pb_em_transfer_args {
 } pb_em_transfer_args;
 int pb_em_transfer(pb_context* ctx, const pb_em_transfer_args* args);
 
+/* Bethe-Heitler e+- pair shape built on the device for the context's photon
+ * field (times photon_scale): per redshift z[q] the matrix R (n_e x n_p,
+ * row-major, written to n_z x n_e x n_p host memory): the one-sign lepton
+ * spectrum dN/dE_e at E_e[i] (GeV) of a nucleon at E_p[j], from the
+ * differential Born cross section integrated by nested fourth-order rules
+ * into a field-free kernel on the target grid eps, contracted with the photon
+ * density over ln eps (points with positive density), restricted to
+ * 1e-6 E_p < E_e <= E_p and E_p >= e_p_min, and normalised so the pair
+ * carries E_p[j].  m_electron, m_proton [GeV] are the caller's constants.
+ * Replaces: bh_pair_shape_matrix with its kernel tensor
+ * (src/prince_cr/cascade/bethe_heitler.py:27-297), as the solver's
+ * _em_bh_at builds it (src/prince_cr/solvers/propagation.py:573-618). */
+typedef struct pb_bh_shape_args {
+  int32_t n_e;
+  const double* E_e;
+  int32_t n_p;
+  const double* E_p;
+  int32_t n_eps;
+  const double* eps;
+  int32_t n_z;
+  const double* z;
+  double photon_scale;
+  double e_p_min;
+  double m_electron, m_proton;
+  double* R;
+} pb_bh_shape_args;
+int pb_bh_shape(pb_context* ctx, const pb_bh_shape_args* args);
+
 /* One solve: the redshift stepping of UHECRPropagationSolverETD2.solve /
  * MultiRHSPropagationSolverETD2.solve (propagation.py:813-890; etd2.py:478-517;
  * _operator_at / apply_F propagation.py:1360-1508; multi-RHS 2495-2618).

@@ -239,3 +239,105 @@ def transfer(E, zs, field, dz, eps=None, eps_o=None, mu=None, cool_floor_frac=0.
     final = np.where(done[:, None, None], final, escaped)
     T_e = final @ (Mic * dE[None, None, :])
     return [(final[i], T_e[i]) for i in range(Nz)]
+
+
+# ---------------------------------------------------------------------------
+# Bethe-Heitler e+- pair shape (bethe_heitler.py:27-172 for the differential
+# Born cross section and its nested fourth-order integrations, 180-240 for the
+# field-free kernel tensor, 240-297 for the per-redshift shape).
+# ---------------------------------------------------------------------------
+M_P = U.m_proton
+
+
+def dsigma_bh(k, g, u):
+    """d^2 sigma / (d gamma_e d xi) in (3 / 16 pi) sigma_T alpha units; 0 outside 2.0001 <= k <= 600."""
+    REG = 1e-30
+    with np.errstate(all="ignore"):
+        p = np.sqrt(np.maximum(g * g - 1.0, 0.0) + REG)
+        g1 = k - g
+        p1 = np.sqrt(np.maximum(g1 * g1 - 1.0, 0.0) + REG)
+        D = g - u * p
+        T = np.sqrt(np.maximum(k * k + p * p - 2.0 * k * p * u, 0.0))
+        d1T = np.log((T + p1) / np.maximum(T - p1, REG))
+        y1 = np.log(np.maximum((g1 + p1) / np.maximum(g1 - p1, REG), REG)) / np.maximum(p1, REG)
+        Y = 2.0 * np.log(np.maximum((g * g1 + p * p1 + 1.0) / k, REG)) / np.maximum(p * p, REG)
+        A0 = p * p1 / (k * k * k)
+        A1 = -4.0 * (1.0 - u * u) * (2.0 * g * g + 1.0) / np.maximum(p * p * D ** 4, REG)
+        A2 = (5.0 * g * g - 2.0 * g * g1 + 3.0) / np.maximum(p * p * D * D, REG)
+        A3 = (p * p - k * k) / np.maximum(T * T * D * D, REG)
+        A4 = 2.0 * g1 / np.maximum(p * p * D, REG)
+        A50 = Y / np.maximum(p * p1, REG)
+        A51 = 2.0 * g * (1.0 - u * u) * (3.0 * k + p * p * g1) / np.maximum(D ** 4, REG)
+        A52 = (2.0 * g * g * (g * g + g1 * g1) - 7.0 * g * g - 3.0 * g * g1 - g1 * g1 + 1.0) / np.maximum(D * D, REG)
+        A53 = k * (g * g - g * g1 - 1.0) / np.maximum(D, REG)
+        A6 = -(d1T / np.maximum(p1 * T, REG)) * (2.0 / np.maximum(D * D, REG) - 3.0 * k / np.maximum(D, REG)
+                                                 - k * (p * p - k * k) / np.maximum(T * T * D, REG))
+        A7 = -2.0 * y1 / np.maximum(D, REG)
+        res = A0 * (A1 + A2 + A3 + A4 + A50 * (A51 + A52 + A53) + A6 + A7)
+    return np.where((k >= 2.0001) & (k <= 600.0) & (T >= 1e-30), res, 0.0)
+
+
+def rk4(fn, lo, hi, n_bins=5):
+    """Simpson-weighted fourth-order rule over [lo, hi] in n_bins steps; 0 where hi <= lo."""
+    valid = hi > lo
+    dx = np.where(valid, (hi - lo) / n_bins, 0.0)
+    y = np.zeros_like(lo)
+    x = lo.copy()
+    for _ in range(n_bins):
+        k1 = dx * fn(x)
+        k2 = dx * fn(x + 0.5 * dx)
+        k4 = dx * fn(x + dx)
+        y = y + (k1 + k4) / 6.0 + 2.0 * k2 / 3.0
+        x = x + dx
+    return np.where(valid, y, 0.0)
+
+
+def bh_kernel(E_e, E_p, eps):
+    """Field-free K[i, j, k]: lepton i from nucleon j on target photon k."""
+    ge = (E_e / M_E)[:, None, None]
+    gp = (E_p / M_P)[None, :, None]
+    ke = (eps / M_E)[None, None, :]
+    GE, GP, KE = np.broadcast_arrays(ge, gp, ke)
+
+    def inner(omega, ee):
+        REG = 1e-20
+        with np.errstate(all="ignore"):
+            p_ = np.sqrt(np.maximum(ee * ee - 1.0, 0.0) + REG)
+            xi = (GP * ee - GE) / (GP * p_)
+            val = omega * dsigma_bh(omega, ee, xi) / p_
+        ok = (p_ >= REG) & (xi >= -1.0) & (xi <= 1.0) & (ee >= 1.0) & (ee <= omega - 1.0)
+        return np.where(ok, val, 0.0)
+
+    def outer(omega):
+        REG = 1e-5
+        lo = (GP * GP + GE * GE) / (2.0 * GP * GE) + REG
+        hi = omega - 1.0 - REG
+        ok = ((hi - lo) >= -1e-4 * lo) & ((hi - lo) / lo >= 1e-4)
+        res = rk4(lambda ee: inner(omega, ee), np.where(ok, lo, 1.0), np.where(ok, hi, 0.0))
+        return np.where(ok, res, 0.0)
+
+    upper = 2.0 * GP * KE
+    lower = (GP + GE) ** 2 / (2.0 * GP * GE)
+    ok = (upper - lower) / np.maximum(lower, 1e-30) >= 1e-8
+    y = rk4(outer, np.where(ok, lower, 1.0), np.where(ok, upper, 0.0))
+    return np.where(ok, y * GE / (2.0 * GP ** 3 * KE ** 2), 0.0)
+
+
+def bh_shape(E_e, E_p, eps, n_eps, e_p_min=1e5):
+    """R[i, j]: one-sign e+- spectrum of a nucleon at E_p[j], energy-normalised so
+    the pair carries E_p[j]; the eps integral runs over the points with n > 0."""
+    from scipy.integrate import trapezoid
+
+    ln_eps = np.log(eps)
+    ok = (n_eps > 0) & (eps > 0)
+    R = np.zeros((E_e.size, E_p.size))
+    if not ok.any():
+        return R
+    K = bh_kernel(E_e, E_p, eps)
+    col = trapezoid((K * (n_eps * eps)[None, None, :])[:, :, ok], ln_eps[ok], axis=2)
+    band = (E_e[:, None] <= E_p[None, :]) & (E_e[:, None] > 1e-6 * E_p[None, :])
+    col = np.where(band & (E_p[None, :] >= e_p_min), col, 0.0)
+    carried = 2.0 * trapezoid(E_e[:, None] * col, E_e, axis=0)
+    good = carried > 0
+    R[:, good] = col[:, good] * (E_p[good] / carried[good])[None, :]
+    return R

@@ -91,6 +91,16 @@ class EmTransferArgs(C.Structure):
     ]
 
 
+class BhShapeArgs(C.Structure):
+    """``pb_bh_shape_args``."""
+
+    _fields_ = [
+        ("n_e", C.c_int32), ("E_e", _d), ("n_p", C.c_int32), ("E_p", _d), ("n_eps", C.c_int32), ("eps", _d),
+        ("n_z", C.c_int32), ("z", _d), ("photon_scale", C.c_double), ("e_p_min", C.c_double),
+        ("m_electron", C.c_double), ("m_proton", C.c_double), ("R", _d),
+    ]
+
+
 class TuneChoice(C.Structure):
     _fields_ = [("band_warps", C.c_int32), ("slab_prefetch", C.c_int32), ("tma_staging", C.c_int32),
                 ("steps_ms", C.c_double)]
@@ -113,6 +123,7 @@ _PROTOS = {
                               C.POINTER(C.c_int32)]),
     "pb_get_fold_kernel": (C.c_int, [_vp, C.c_int64, C.c_int32, _d]),
     "pb_em_transfer": (C.c_int, [_vp, C.POINTER(EmTransferArgs)]),
+    "pb_bh_shape": (C.c_int, [_vp, C.POINTER(BhShapeArgs)]),
     "pb_set_fd_operator": (C.c_int, [_vp, C.c_int64, _i64, _i32, _d, _d]),
     "pb_set_losses": (C.c_int, [_vp, _d, _d, _i32, C.c_int32, C.c_int32, _d, _d, _d]),
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
@@ -281,6 +292,21 @@ class Context:
         a.iterations = C.pointer(it)
         self._check(self.lib.pb_em_transfer(self.h, C.byref(a)), "pb_em_transfer")
         return Tg, Te, it.value
+
+    def bh_shape(self, E_e, E_p, eps, zs, e_p_min=1e5, photon_scale=1.0):
+        """Device Bethe-Heitler pair shapes on the context's photon field: ``(n_z, n_e, n_p)``."""
+        from .constants import PRINCE_UNITS as U
+
+        Ee, Ep, ep, z = _f64(E_e), _f64(E_p), _f64(eps), _f64(np.atleast_1d(zs))
+        R = np.empty((z.size, Ee.size, Ep.size))
+        a = BhShapeArgs()
+        a.n_e, a.E_e, a.n_p, a.E_p = Ee.size, _ptr(Ee, C.c_double), Ep.size, _ptr(Ep, C.c_double)
+        a.n_eps, a.eps, a.n_z, a.z = ep.size, _ptr(ep, C.c_double), z.size, _ptr(z, C.c_double)
+        a.photon_scale, a.e_p_min = float(photon_scale), float(e_p_min)
+        a.m_electron, a.m_proton = U.m_electron, U.m_proton
+        a.R = _ptr(R, C.c_double)
+        self._check(self.lib.pb_bh_shape(self.h, C.byref(a)), "pb_bh_shape")
+        return R
 
     def set_photon_grid(self, energies):
         e = _f64(energies)

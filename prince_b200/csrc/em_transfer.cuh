@@ -430,4 +430,132 @@ __global__ void k_em_finish(const int* __restrict__ done, const double* __restri
   micd[t] = Mic[t] * dE[j];
 }
 
+
+// ---------------------------------------------------------------------------
+// Bethe-Heitler e+- pair shape (bethe_heitler.py:27-297): the differential
+// Born cross section, its nested fourth-order integrations into the
+// field-free kernel K[i][j][k] (lepton i, nucleon j, target photon k), and per
+// redshift the contraction with the photon density over ln eps (on the points
+// where the density is positive), the kinematic band and the per-column
+// energy normalisation.  Energies in units of m_e (leptons, photons) and the
+// nucleon Lorentz factor.
+// ---------------------------------------------------------------------------
+__device__ double dsigma_bh(double k, double g, double u) {
+  const double REG = 1e-30;
+  const double p = sqrt(fmax(g * g - 1.0, 0.0) + REG);
+  const double g1 = k - g;
+  const double p1 = sqrt(fmax(g1 * g1 - 1.0, 0.0) + REG);
+  const double D = g - u * p;
+  const double T = sqrt(fmax(k * k + p * p - 2.0 * k * p * u, 0.0));
+  if (!(k >= 2.0001 && k <= 600.0 && T >= 1e-30)) return 0.0;
+  const double d1T = log((T + p1) / fmax(T - p1, REG));
+  const double y1 = log(fmax((g1 + p1) / fmax(g1 - p1, REG), REG)) / fmax(p1, REG);
+  const double Y = 2.0 * log(fmax((g * g1 + p * p1 + 1.0) / k, REG)) / fmax(p * p, REG);
+  const double D4 = pow(D, 4.0);
+  const double A0 = p * p1 / (k * k * k);
+  const double A1 = -4.0 * (1.0 - u * u) * (2.0 * g * g + 1.0) / fmax(p * p * D4, REG);
+  const double A2 = (5.0 * g * g - 2.0 * g * g1 + 3.0) / fmax(p * p * D * D, REG);
+  const double A3 = (p * p - k * k) / fmax(T * T * D * D, REG);
+  const double A4 = 2.0 * g1 / fmax(p * p * D, REG);
+  const double A50 = Y / fmax(p * p1, REG);
+  const double A51 = 2.0 * g * (1.0 - u * u) * (3.0 * k + p * p * g1) / fmax(D4, REG);
+  const double A52 = (2.0 * g * g * (g * g + g1 * g1) - 7.0 * g * g - 3.0 * g * g1 - g1 * g1 + 1.0) / fmax(D * D, REG);
+  const double A53 = k * (g * g - g * g1 - 1.0) / fmax(D, REG);
+  const double A6 = -(d1T / fmax(p1 * T, REG)) *
+                    (2.0 / fmax(D * D, REG) - 3.0 * k / fmax(D, REG) - k * (p * p - k * k) / fmax(T * T * D, REG));
+  const double A7 = -2.0 * y1 / fmax(D, REG);
+  return A0 * (A1 + A2 + A3 + A4 + A50 * (A51 + A52 + A53) + A6 + A7);
+}
+
+__device__ __forceinline__ double bh_inner(double ge, double gp, double omega, double ee) {
+  const double REG = 1e-20;
+  const double p_ = sqrt(fmax(ee * ee - 1.0, 0.0) + REG);
+  const double xi = (gp * ee - ge) / (gp * p_);
+  const bool ok = (p_ >= REG) && (xi >= -1.0) && (xi <= 1.0) && (ee >= 1.0) && (ee <= omega - 1.0);
+  return ok ? omega * dsigma_bh(omega, ee, xi) / p_ : 0.0;
+}
+
+// Simpson-weighted fourth-order rule in 5 steps over [lo, hi] (0 when hi <= lo).
+template <class F>
+__device__ __forceinline__ double rk4_5(F f, double lo, double hi) {
+  if (!(hi > lo)) return 0.0;
+  const double dx = (hi - lo) / 5;
+  double y = 0.0, x = lo;
+  for (int s = 0; s < 5; ++s) {
+    const double k1 = dx * f(x), k2 = dx * f(x + 0.5 * dx), k4 = dx * f(x + dx);
+    y = y + (k1 + k4) / 6.0 + 2.0 * k2 / 3.0;
+    x = x + dx;
+  }
+  return y;
+}
+
+__device__ double bh_outer(double ge, double gp, double omega) {
+  const double REG = 1e-5;
+  const double lo = (gp * gp + ge * ge) / (2.0 * gp * ge) + REG;
+  const double hi = omega - 1.0 - REG;
+  const bool ok = ((hi - lo) >= -1e-4 * lo) && ((hi - lo) / lo >= 1e-4);
+  if (!ok) return 0.0;
+  return rk4_5([&](double ee) { return bh_inner(ge, gp, omega, ee); }, lo, hi);
+}
+
+__global__ void k_bh_kernel(double me, double mp, const double* __restrict__ Ee, int ne,
+                            const double* __restrict__ Ep, int np, const double* __restrict__ eps, int nk,
+                            double* __restrict__ K) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)ne * np * nk) return;
+  const int kk = (int)(t % nk);
+  const int j = (int)((t / nk) % np), i = (int)(t / ((int64_t)nk * np));
+  const double ge = Ee[i] / me, gp = Ep[j] / mp, ke = eps[kk] / me;
+  const double upper = 2.0 * gp * ke;
+  const double lower = (gp + ge) * (gp + ge) / (2.0 * gp * ge);
+  double v = 0.0;
+  if ((upper - lower) / fmax(lower, 1e-30) >= 1e-8) {
+    const double y = rk4_5([&](double om) { return bh_outer(ge, gp, om); }, lower, upper);
+    v = y * ge / (2.0 * pow(gp, 3.0) * (ke * ke));
+  }
+  K[t] = v;
+}
+
+// col[z][i][j] = trapezoid over ln eps (points with n > 0) of K n eps, in the band
+__global__ void k_bh_col(const double* __restrict__ K, const double* __restrict__ Ee, int ne,
+                         const double* __restrict__ Ep, int np, const double* __restrict__ eps,
+                         const double* __restrict__ neps, int nk, int nz, double e_p_min,
+                         double* __restrict__ col) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nz * ne * np) return;
+  const int z = (int)(t / ((int64_t)ne * np));
+  const int i = (int)((t / np) % ne), j = (int)(t % np);
+  const bool band = Ee[i] <= Ep[j] && Ee[i] > 1e-6 * Ep[j] && Ep[j] >= e_p_min;
+  double acc = 0.0, yprev = 0.0, xprev = 0.0;
+  bool have = false;
+  if (band) {
+    const double* Kij = K + ((size_t)i * np + j) * nk;
+    for (int k = 0; k < nk; ++k) {
+      const double n = neps[(size_t)k * nz + z];
+      if (!(n > 0 && eps[k] > 0)) continue;
+      const double y = Kij[k] * (n * eps[k]);
+      const double x = log(eps[k]);
+      if (have) acc += (x - xprev) * (y + yprev) / 2.0;
+      yprev = y;
+      xprev = x;
+      have = true;
+    }
+  }
+  col[t] = band ? acc : 0.0;
+}
+
+// R[z][i][j] = col * (E_p[j] / carried) with carried = 2 trapezoid_i(E_e col)
+__global__ void k_bh_norm(const double* __restrict__ col, const double* __restrict__ Ee, int ne,
+                          const double* __restrict__ Ep, int np, int nz, double* __restrict__ R) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nz * np) return;
+  const int z = t / np, j = t % np;
+  const double* c = col + (size_t)z * ne * np;
+  double acc = 0.0;
+  for (int i = 0; i + 1 < ne; ++i)
+    acc += (Ee[i + 1] - Ee[i]) * (Ee[i + 1] * c[(size_t)(i + 1) * np + j] + Ee[i] * c[(size_t)i * np + j]) / 2.0;
+  const double carried = 2.0 * acc;
+  for (int i = 0; i < ne; ++i)
+    R[(size_t)z * ne * np + (size_t)i * np + j] = carried > 0 ? c[(size_t)i * np + j] * (Ep[j] / carried) : 0.0;
+}
 }  // namespace

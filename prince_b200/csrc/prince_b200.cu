@@ -3855,6 +3855,10 @@ int pb_em_transfer(pb_context* c, const pb_em_transfer_args* a) {
   if (n < 2 || n > 1024 || nz < 1 || ne < 2 || no < 2 || nmu < 2 || nE1 < 2 || !a->E || !a->z || !a->dl_step ||
       !a->eps || !a->eps_o || !a->mu || !a->T_gamma || !a->T_electron || a->max_scatter < 1 || !(a->tol > 0))
     return fail(c, PB_ERR_ARG, "pb_em_transfer: bad arguments");
+  // grid sizes within the launch limits of the kernels below (GEMM rows / 64 and
+  // the batch of redshifts are grid dimensions)
+  if ((int64_t)n * nE1 > 4000000 || ne > 100000 || no > 100000 || nmu > 100000 || nz > 65535)
+    return fail(c, PB_ERR_ARG, "pb_em_transfer: grid sizes beyond the supported limits");
   for (int i = 1; i < n; ++i)
     if (!(a->E[i] > a->E[i - 1])) return fail(c, PB_ERR_ARG, "pb_em_transfer: E must increase");
   int rc = set_device(c);
@@ -4055,6 +4059,54 @@ int pb_em_transfer(pb_context* c, const pb_em_transfer_args* a) {
   if (err != cudaSuccess) return fail_cuda(err, "results");
   if (a->iterations) *a->iterations = passes;
   cleanup();
+  return PB_OK;
+}
+
+
+// Bethe-Heitler e+- pair shape per redshift on the device (em_transfer.cuh).
+int pb_bh_shape(pb_context* c, const pb_bh_shape_args* a) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!a) return fail(c, PB_ERR_ARG, "pb_bh_shape: args is NULL");
+  if (!c->have_field) return fail(c, PB_ERR_STATE, "pb_bh_shape: set the photon field first");
+  const int ne = a->n_e, np = a->n_p, nk = a->n_eps, nz = a->n_z;
+  if (ne < 2 || np < 1 || nk < 2 || nz < 1 || ne > 4096 || np > 4096 || nk > 4096 || nz > 65535 || !a->E_e ||
+      !a->E_p || !a->eps || !a->z || !a->R || !(a->m_electron > 0) || !(a->m_proton > 0))
+    return fail(c, PB_ERR_ARG, "pb_bh_shape: bad arguments");
+  int rc = set_device(c);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  DBuf Ee, Ep, eps, zs, K, neps, col, R;
+  auto cleanup = [&]() { for (DBuf* b : {&Ee, &Ep, &eps, &zs, &K, &neps, &col, &R}) b->release(); };
+  if ((rc = upload(c, Ee, a->E_e, (size_t)ne)) || (rc = upload(c, Ep, a->E_p, (size_t)np)) ||
+      (rc = upload(c, eps, a->eps, (size_t)nk)) || (rc = upload(c, zs, a->z, (size_t)nz))) {
+    cleanup();
+    return rc;
+  }
+  const size_t zne = (size_t)nz * ne * np;
+  for (auto w : {std::make_pair(&K, (size_t)ne * np * nk * 8), std::make_pair(&neps, (size_t)nk * nz * 8),
+                 std::make_pair(&col, zne * 8), std::make_pair(&R, zne * 8)}) {
+    const cudaError_t e = w.first->ensure(w.second);
+    if (e != cudaSuccess) {
+      cleanup();
+      return fail(c, PB_ERR_CUDA, "pb_bh_shape: allocation: %s", cudaGetErrorString(e));
+    }
+  }
+  const FieldDesc f = field_desc(c, a->photon_scale);
+  k_em_stack<<<blocks_for((int64_t)nk * nz, 256), 256, 0, st>>>(f, eps.as<double>(), nk, zs.as<double>(), nz,
+                                                                neps.as<double>());
+  k_bh_kernel<<<blocks_for((int64_t)ne * np * nk, 128), 128, 0, st>>>(a->m_electron, a->m_proton, Ee.as<double>(), ne,
+                                                                      Ep.as<double>(), np, eps.as<double>(), nk,
+                                                                      K.as<double>());
+  k_bh_col<<<blocks_for((int64_t)zne, 256), 256, 0, st>>>(K.as<double>(), Ee.as<double>(), ne, Ep.as<double>(), np,
+                                                          eps.as<double>(), neps.as<double>(), nk, nz, a->e_p_min,
+                                                          col.as<double>());
+  k_bh_norm<<<blocks_for((int64_t)nz * np, 256), 256, 0, st>>>(col.as<double>(), Ee.as<double>(), ne,
+                                                               Ep.as<double>(), np, nz, R.as<double>());
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(a->R, R.p, zne * 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cleanup();
+  if (e != cudaSuccess) return fail(c, PB_ERR_CUDA, "pb_bh_shape: %s", cudaGetErrorString(e));
   return PB_OK;
 }
 

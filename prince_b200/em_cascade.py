@@ -13,7 +13,10 @@ the scattering iteration, all on the GPU.
 ``KineticCascadeModel(run, dz)`` is a run's ``em_cascade_model`` built on it:
 ``model(z) -> (T_gamma, T_electron, R_BH)`` with the transfer from the device
 (cached per redshift; ``prefetch(zs)`` builds all windows of a solve in one
-device call) and the Bethe-Heitler pair shape from a caller-supplied function.
+device call) and the Bethe-Heitler pair shape ``R_BH`` from ``pb_bh_shape``
+(the reference solver's ``_em_bh_at``, ``src/prince_cr/solvers/propagation.py:573-618``:
+40 target energies from 10^-12.5 to 10^-7 GeV, e+- and nucleons both on the
+run's grid), or from a caller-supplied function.
 """
 
 from __future__ import annotations
@@ -44,13 +47,24 @@ def kinetic_transfer(ctx, field, E, zs, dz, photon_scale=1.0, **kw):
                            photon_scale=photon_scale, **kw)
 
 
-class KineticCascadeModel:
-    """``em_cascade_model`` of a run: the device kinetic transfer plus a BH pair shape.
+def bh_target_grid():
+    """Target photon energies of the BH pair shape (``propagation.py:592``)."""
+    return np.logspace(-12.5, -7.0, 40)
 
-    ``bh_shape(z) -> R_BH`` (n_em x n_cr) supplies the Bethe-Heitler e+- shape.
+
+def bh_shape(ctx, field, E_e, E_p, zs, e_p_min=1e5, photon_scale=1.0):
+    """Device Bethe-Heitler pair shapes ``(n_z, n_e, n_p)`` on ``field``."""
+    ctx.set_photon_field(device_components(field), table=device_table(field))
+    return ctx.bh_shape(E_e, E_p, bh_target_grid(), zs, e_p_min=e_p_min, photon_scale=photon_scale)
+
+
+class KineticCascadeModel:
+    """``em_cascade_model`` of a run: the device kinetic transfer plus the BH pair shape.
+
+    ``bh_shape(z) -> R_BH`` (n_em x n_cr), when given, replaces the device BH shape.
     """
 
-    def __init__(self, run, dz, bh_shape, device=0):
+    def __init__(self, run, dz, bh_shape=None, device=0):
         self.run = run
         self.dz = float(dz)
         self.bh_shape = bh_shape
@@ -66,10 +80,11 @@ class KineticCascadeModel:
         ctx = DeviceRun.of(self.run, self.device).ctx
         E = self.run.cr_grid.grid
         Tg, Te, _ = kinetic_transfer(ctx, self.run.photon_field, E, todo, self.dz)
+        R = (bh_shape(ctx, self.run.photon_field, E, E, todo) if self.bh_shape is None
+             else [self.bh_shape(z) for z in todo])
         for i, z in enumerate(todo):
-            self._cache[z] = (Tg[i], Te[i])
+            self._cache[z] = (Tg[i], Te[i], R[i])
 
     def __call__(self, z):
         self.prefetch([z])
-        tg, te = self._cache[float(z)]
-        return tg, te, self.bh_shape(z)
+        return self._cache[float(z)]

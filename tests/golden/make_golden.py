@@ -607,6 +607,19 @@ def main_cascade():
     Ts = kinetic_cascade_transfer_batched(E, zs, field, dz=1e-3, iter_dtype="float64")
     out["T_gamma"] = np.stack([t[0] for t in Ts])
     out["T_electron"] = np.stack([t[1] for t in Ts])
+    # the Bethe-Heitler e+- pair shape as the solver builds it (propagation.py:573-618):
+    # e+- on this EM grid from nucleons on a 24-bin nucleon grid, 40 target energies
+    from prince_cr.cascade.bethe_heitler import bh_pair_shape_matrix
+    Ep = EnergyGrid(8, 12, 6).grid
+    eps = np.logspace(-12.5, -7.0, 40)
+    out["bh_E_p"] = Ep
+    out["bh_eps"] = eps
+    Rs = []
+    for zz in zs:
+        n_eps = np.asarray(field.get_photon_density(eps, zz), dtype="double")
+        n_eps = np.where(np.isfinite(n_eps) & (n_eps > 0), n_eps, 0.0)
+        Rs.append(bh_pair_shape_matrix(E, Ep, eps, n_eps))
+    out["R_BH"] = np.stack(Rs)
     path = os.path.join(HERE, "em_cascade_transfer.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -23,3 +23,16 @@ def test_restated_transfer_matches_the_reference():
         for mine, ref in ((tg, z["T_gamma"][i]), (te, z["T_electron"][i])):
             assert np.array_equal(mine != 0, ref != 0)
             np.testing.assert_allclose(mine, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+def test_restated_bh_shape_matches_the_reference():
+    from prince_b200 import photonfields as pf
+    z = np.load(os.path.join(GOLDEN, "em_cascade_transfer.npz"))
+    field = pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), pf.ModifiedBlackBodyCIB()])
+    for i, zz in enumerate(z["zs"]):
+        n = np.asarray(field.get_photon_density(z["bh_eps"], zz))
+        n = np.where(np.isfinite(n) & (n > 0), n, 0.0)
+        R = EC.bh_shape(z["E"], z["bh_E_p"], z["bh_eps"], n)
+        ref = z["R_BH"][i]
+        assert np.array_equal(R != 0, ref != 0)
+        np.testing.assert_allclose(R, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())

@@ -1,9 +1,10 @@
-"""The kinetic EM-cascade transfer built on the device (needs a B200).
+"""The kinetic EM-cascade transfer and the Bethe-Heitler pair shape built on the device (needs a B200).
 
 ``pb_em_transfer`` against PriNCe's own ``kinetic_cascade_transfer_batched``
 (FP64 iteration; ``tests/golden/em_cascade_transfer.npz``) and against the CPU
-restatement on the 128-bin EM grid of config 5 (1e-3 to 1e14 GeV) at five
-redshifts up to z = 4, CMB + the synthetic grey-body CIB.
+restatement on a 128-bin EM grid (1e-3 to 1e14 GeV) at five redshifts up to
+z = 4, CMB + the synthetic grey-body CIB; ``pb_bh_shape`` against PriNCe's own
+``bh_pair_shape_matrix`` (the same fixture) and the restatement.
 """
 
 import os
@@ -58,3 +59,34 @@ def test_device_transfer_on_the_config5_grid_matches_the_restatement():
     for i in range(len(zs)):
         ratio = ((E * dE) @ Tg[i]) / (E * dE)
         assert np.all(np.abs(ratio - 1.0) < 2e-3)
+
+
+def test_device_bh_shape_matches_the_reference():
+    from prince_b200 import _lib
+    from prince_b200.em_cascade import bh_shape, bh_target_grid
+    z = np.load(os.path.join(GOLDEN, "em_cascade_transfer.npz"))
+    assert np.array_equal(bh_target_grid(), z["bh_eps"])
+    ctx = _lib.Context(0)
+    R = bh_shape(ctx, _field(), z["E"], z["bh_E_p"], z["zs"])
+    assert R.shape == z["R_BH"].shape
+    for i in range(len(z["zs"])):
+        _close(R[i], z["R_BH"][i])
+        # the pair carries the nucleon energy
+        carried = 2.0 * np.trapezoid(z["E"][:, None] * R[i], z["E"], axis=0)
+        good = carried > 0
+        np.testing.assert_allclose(carried[good], z["bh_E_p"][good], rtol=1e-12)
+
+
+def test_device_bh_shape_on_a_square_grid_matches_the_restatement():
+    from prince_b200 import _lib
+    from prince_b200.data import EnergyGrid
+    from prince_b200.em_cascade import bh_shape, bh_target_grid
+    E = EnergyGrid(3, 14, 8).grid
+    zs = [0.0, 1.5, 4.0]
+    ctx = _lib.Context(0)
+    R = bh_shape(ctx, _field(), E, E, zs)
+    eps = bh_target_grid()
+    for i, zz in enumerate(zs):
+        n = np.asarray(_field().get_photon_density(eps, zz))
+        n = np.where(np.isfinite(n) & (n > 0), n, 0.0)
+        _close(R[i], EC.bh_shape(E, E, eps, n))
