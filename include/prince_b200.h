@@ -192,6 +192,23 @@ int pb_set_injection(pb_context* ctx, int32_t n_src, int32_t n_rows, const int32
  * reference counterpart (the reference multiplies the whole CSR operator). */
 int pb_set_layout(pb_context* ctx, int32_t d);
 
+/* The same with species blocks only in rows [0, n_blocks) (n_blocks a multiple
+ * of d); rows [n_blocks, n) form a tail of species on another grid (gamma and
+ * e+- on a decoupled EM grid, src/prince_cr/core.py:105-137, 206-214) that the
+ * general row kernel steps beside the bin-blocked kernels.  The fold kernel's
+ * coupling entries must lie inside the blocks; with coupling entries between
+ * blocks and tail the general row kernels step everything. */
+int pb_set_layout_rows(pb_context* ctx, int32_t d, int64_t n_blocks);
+
+/* The caller's row order of the state: device row i holds the caller's row
+ * caller_row[i] (a permutation of [0, n)).  pb_solve's state and pb_adjoint's
+ * seed are read and written in the caller's order; every other per-row input
+ * (coupling, losses, injection rows, EM offsets) is in the device order.  NULL
+ * restores the identity; pb_set_coupling resets it.  No reference counterpart
+ * (the reference keeps the species layout, where the EM species come first;
+ * the device puts the species blocks of the shared grid first). */
+int pb_set_row_map(pb_context* ctx, const int32_t* caller_row);
+
 /* Execution options (PB_OPT_*) and read-only facts (PB_INFO_*) of a context.
  * No reference counterpart. */
 int pb_set_option(pb_context* ctx, int32_t key, int64_t value);

@@ -104,6 +104,21 @@ def phi_factors(h, d, exp=np.exp):
     return eD, phi1, phi2
 
 
+def fd_operator_run(run):
+    """The run's FD loss operator, one block per species on its home grid in
+    princeidx order (partial_diff.py:28-46, heterogeneous path)."""
+    sm = run.spec_man
+    grids = getattr(run, "grids", {"default": run.cr_grid})
+    refs = sorted(sm.species_refs, key=lambda s: s.princeidx)
+    if all(s.grid_tag == "default" for s in refs):
+        return fd_operator(run.cr_grid, sm.nspec)
+    blocks = {}
+    for s in refs:
+        if s.grid_tag not in blocks:
+            blocks[s.grid_tag] = fd_operator(grids[s.grid_tag], 1)
+    return sp.block_diag([blocks[s.grid_tag] for s in refs]).tocsr()
+
+
 def fd_operator(cr_grid, nspec):
     """Block-diagonal FD loss operator (partial_diff.py:28-110)."""
     h = np.log(cr_grid.bins[1] / cr_grid.bins[0])
@@ -202,7 +217,7 @@ class OracleSolver:
         self.bm = np.ascontiguousarray(ir._batch_matrix, dtype=np.float64)
         self.cpl_indptr = np.asarray(ir.coupling_mat.indptr)
         self.cpl_indices = np.asarray(ir.coupling_mat.indices)
-        self.D = fd_operator(run.cr_grid, run.spec_man.nspec)
+        self.D = fd_operator_run(run)
         self.D_diag, self.D_off = split(self.D)
         self.E = np.asarray(run.adia_loss_rates_grid.energy_vector, dtype=np.float64)
         # Explicit decay (propagation.py:1148-1358, 1418-1422, 1479-1482):

@@ -129,6 +129,8 @@ _PROTOS = {
     "pb_set_decay": (C.c_int, [_vp, _d, C.c_int64, _i64, _i32, _d]),
     "pb_set_injection": (C.c_int, [_vp, C.c_int32, C.c_int32, _i32, _d, C.c_int32, _i32]),
     "pb_set_layout": (C.c_int, [_vp, C.c_int32]),
+    "pb_set_layout_rows": (C.c_int, [_vp, C.c_int32, C.c_int64]),
+    "pb_set_row_map": (C.c_int, [_vp, _i32]),
     "pb_set_option": (C.c_int, [_vp, C.c_int32, C.c_int64]),
     "pb_get_info": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int64)]),
     "pb_profile_stage": (C.c_int, [_vp, C.c_int64, C.c_int32, C.c_int32, _d]),
@@ -352,8 +354,19 @@ class Context:
                                               _ptr(grids, C.c_double), int(n_cols), _ptr(src_col, C.c_int32)),
                     "pb_set_injection")
 
-    def set_layout(self, d):
-        self._check(self.lib.pb_set_layout(self.h, int(d)), "pb_set_layout")
+    def set_layout(self, d, n_blocks=None):
+        if n_blocks is None:
+            self._check(self.lib.pb_set_layout(self.h, int(d)), "pb_set_layout")
+        else:
+            self._check(self.lib.pb_set_layout_rows(self.h, int(d), int(n_blocks)), "pb_set_layout_rows")
+
+    def set_row_map(self, caller_row):
+        """Device row i holds the caller's row ``caller_row[i]`` (None: identity)."""
+        if caller_row is None:
+            self._check(self.lib.pb_set_row_map(self.h, None), "pb_set_row_map")
+            return
+        m = _i32a(caller_row)
+        self._check(self.lib.pb_set_row_map(self.h, _ptr(m, C.c_int32)), "pb_set_row_map")
 
     def set_option(self, key, value):
         self._check(self.lib.pb_set_option(self.h, int(key), int(value)), "pb_set_option")

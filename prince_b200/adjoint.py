@@ -10,6 +10,13 @@ transposed operator) and returns gradients for
 * ``scale``  -- the photon-density scale shared by the rate fold and the
   Bethe-Heitler loss (a 0-d tensor).
 
+With the co-evolved EM cascade (``run.enable_em_cascade``) the backward also
+runs the transposed EM hook after every step (Bethe-Heitler pairs from the
+charged nuclei, ``T_gamma`` / ``T_electron`` on gamma and e+-), so a loss on
+the photon flux reaches the source parameters; the photon scale then gets no
+gradient (the transfer's own dependence on the photon field is not
+differentiated).
+
 ``SourceBatch`` builds ``G`` and ``coeff`` from per-point parameters with torch
 operations (spectral index, log10 rigidity cutoff, five composition fractions,
 evolution index), so ``torch.autograd`` carries the gradient back to them.
@@ -31,7 +38,7 @@ from . import _lib
 from . import constants as C
 from .photonfields import device_components, device_table
 from .schedule import make_schedule, z_grid
-from .solvers import DeviceRun
+from .solvers import DeviceRun, run_em_windows
 
 FLAGS_ALL = (_lib.PB_ADIABATIC | _lib.PB_PAIRPROD | _lib.PB_PHOTOHAD | _lib.PB_INJECTION
              | _lib.PB_PARTIAL_DIFF)
@@ -42,12 +49,14 @@ class Plan:
 
     def __init__(self, run, initial_z, n_cols, rows, src_col, first_active, dz=1e-3, device=0,
                  ckpt_every=32, flags=FLAGS_ALL):
-        if getattr(run, "enable_em_cascade", False):
-            raise NotImplementedError("the co-evolved EM cascade hook has no adjoint; differentiate a run "
-                                      "without enable_em_cascade")
         self.run = run
         self.dev = DeviceRun.of(run, device)
         self.sched = make_schedule(z_grid(initial_z, 0.0, dz), run.backend.update_rates_z_threshold)
+        self.em = bool(getattr(run, "enable_em_cascade", False))
+        if self.em:
+            self.dev.ensure_em()
+            flags |= _lib.PB_EM_CASCADE
+            self.em_windows = run_em_windows(run, self.sched, dz)
         self.K = int(n_cols)
         self.rows = np.asarray(rows, dtype=np.int32)
         self.src_col = np.asarray(src_col, dtype=np.int64)       # user column of each source
@@ -79,9 +88,11 @@ class PropagateFunction(torch.autograd.Function):
         ctx_dev = plan.dev.ctx
         Gd = G.detach().cpu().numpy()[:, plan.src_order]
         cd = coeff.detach().cpu().numpy()[:, plan.src_order]
-        ctx_dev.set_injection(plan.rows, np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
+        ctx_dev.set_injection(plan.dev.dev_rows(plan.rows), np.ascontiguousarray(Gd), plan.dev_src_col, plan.K)
         ctx_dev.set_photon_field(device_components(plan.run.photon_field),
                                  table=device_table(plan.run.photon_field))
+        if plan.em:
+            ctx_dev.set_em_windows(*plan.em_windows)
         dev = torch.device("cuda", plan.device)
         X = torch.empty((plan.run.dim_states, plan.K), dtype=torch.float64, device=dev)  # caller's column order
         s = float(scale.detach().cpu().item())
@@ -105,8 +116,8 @@ class PropagateFunction(torch.autograd.Function):
         gc_user = np.empty_like(gc)
         gc_user[:, plan.src_order] = gc
         out = ctx.in_device
-        return (torch.from_numpy(gG_user).to(out), torch.from_numpy(gc_user).to(out),
-                torch.tensor(float(gs.sum()), dtype=torch.float64, device=out), None)
+        g_scale = None if gs is None else torch.tensor(float(gs.sum()), dtype=torch.float64, device=out)
+        return torch.from_numpy(gG_user).to(out), torch.from_numpy(gc_user).to(out), g_scale, None
 
 
 def _args(plan, coeff, scale, state):
@@ -168,8 +179,8 @@ def _adjoint(ctx, plan, coeff, scale, seed):
     n_src = plan.dev_src_col.size
     gG = np.zeros((plan.rows.size, n_src))
     gc = np.zeros((plan.sched.n_steps, n_src))
-    gs = np.zeros(plan.K)
-    P = lambda a: a.ctypes.data_as(Cc.POINTER(Cc.c_double))
+    gs = None if plan.em else np.zeros(plan.K)   # no photon-scale gradient through the EM transfer
+    P = lambda a: None if a is None else a.ctypes.data_as(Cc.POINTER(Cc.c_double))
     seed_p = Cc.cast(Cc.c_void_p(seed.data_ptr()), Cc.POINTER(Cc.c_double))
     ctx._check(ctx.lib.pb_adjoint(ctx.h, Cc.byref(args), seed_p, 1, P(gG), P(gc), P(gs)), "pb_adjoint")
     return gG, gc, gs

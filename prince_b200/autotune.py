@@ -83,7 +83,7 @@ def tune(solver, steps=16, reps=3, dz=1e-3, path=None, force=False):
     rows = np.unique(np.concatenate([np.flatnonzero(g) for g in grids])).astype(np.int32)
     G = np.stack([g[rows] for g in grids], axis=1)
     order = np.argsort(owner, kind="stable")
-    ctx.set_injection(rows, G[:, order], owner[order].astype(np.int32), K)
+    ctx.set_injection(solver._dev.dev_rows(rows), G[:, order], owner[order].astype(np.int32), K)
     solver._set_field(ctx)
     coeff = np.ones((sched.n_steps, len(srcs)))
     state = np.empty((solver.dim_states, K))

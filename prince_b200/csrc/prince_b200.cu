@@ -136,6 +136,9 @@ struct pb_context {
   std::vector<int64_t> h_cpl_indptr;
   std::vector<int32_t> h_cpl_indices;
   int32_t lay_d = 0, lay_nsp = 0;
+  int64_t lay_nu = 0;               // rows of the species blocks [0, lay_nu); rows [lay_nu, n) are the tail
+  int32_t n_tail = 0;               // tail rows (species on another grid), stepped by the general row kernel
+  DBuf tail_rows;
   bool blocked_ok = false;          // the coupling pattern admits the band + slab kernels
   int32_t band_nb = 0, band_RT = 0, band_J = 0, n_slab_spec = 0;
   int64_t band_stride = 0;          // band-tile doubles per window
@@ -177,6 +180,9 @@ struct pb_context {
   bool last_tma = false;            // the last solve staged k_slab by TMA
   const void* tma_key[3] = {nullptr, nullptr, nullptr};
   DBuf d_err;                       // int: a bounded wait of a kernel gave up
+  // caller's row order: device row i holds the caller's row row_map[i] (none: identity)
+  bool have_row_map = false;
+  DBuf row_map;
 
   // EM cascade
   bool have_em = false;
@@ -1857,6 +1863,53 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
   }
 }
 
+// Transpose of k_em_hook, applied in place to the adjoint state lam = dL/dX
+// after the hook (e.X = lam), for the step's window.  With l = (e- + es) + (e+ + es),
+// es = R w and w_i = sum_s cw_si X_si, the hook maps gamma <- Tg gamma + Te l and
+// e+- <- 0, so before it: lam_gamma <- Tg^T lam_gamma, lam_e+- <- Te^T lam_gamma,
+// and lam_si += cw_si (n_lep R^T Te^T lam_gamma)_i on the charged nuclei.
+__global__ void __launch_bounds__(256) k_em_hookT(EmParams e) {
+  extern __shared__ double sm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int k = blockIdx.x * 32 + lane;
+  const bool active = k < e.ncols;
+  const int kk = active ? k : 0;
+  double* lg = sm;                          // n_em x 32: lam_gamma after the hook
+  double* ml = lg + (size_t)e.n_em * 32;    // n_em x 32: Te^T lam_gamma
+  double* lw = ml + (size_t)e.n_em * 32;    // n_cr x 32: lam of w
+  for (int j = wid; j < e.n_em; j += nw) lg[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
+  __syncthreads();
+  for (int i = wid; i < e.n_em; i += nw) {
+    double tg = 0.0, te = 0.0;
+    for (int j = 0; j < e.n_em; ++j) {
+      const double l = lg[j * 32 + lane];
+      tg += e.Tg[(size_t)j * e.n_em + i] * l;
+      te += e.Te[(size_t)j * e.n_em + i] * l;
+    }
+    ml[i * 32 + lane] = te;
+    if (active) {
+      e.X[(size_t)(e.g_off + i) * e.ld + k] = tg;
+      if (e.em_off >= 0) e.X[(size_t)(e.em_off + i) * e.ld + k] = te;
+      if (e.ep_off >= 0) e.X[(size_t)(e.ep_off + i) * e.ld + k] = te;
+    }
+  }
+  __syncthreads();
+  const double nl = (double)((e.em_off >= 0) + (e.ep_off >= 0));
+  for (int i = wid; i < e.n_cr; i += nw) {
+    double acc = 0.0;
+    for (int j = 0; j < e.n_em; ++j) acc += e.R[(size_t)j * e.n_cr + i] * ml[j * 32 + lane];
+    lw[i * 32 + lane] = nl * acc;
+  }
+  __syncthreads();
+  if (!active) return;
+  for (int i = wid; i < e.n_cr; i += nw)
+    for (int s = 0; s < e.n_bh; ++s) {
+      const int64_t row = e.bh_off[s] + i;
+      const double cw = e.bh_A[s] * e.kp[row] * e.dl_step * e.invE[i] * e.dE[i];
+      e.X[(size_t)row * e.ld + k] += cw * lw[i * 32 + lane];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Bin-blocked adjoint sweep.  One backward step applies A^T twice (stage 1 to
 // v1 = Phi2 lam', stage 2 to v2 = Phi1 mu - Phi2 lam'), with
@@ -1915,22 +1968,26 @@ struct AdjBlk {
   const double* lt_vals;
 };
 
-// Y[r][cols[j]] = X[r][j]: the final states in the caller's column order (Y is n x K)
+// Y[rows[r]][cols[j]] = X[r][j]: the state in the caller's row and column order
+// (a null map is the identity; Y is n x K)
 __global__ void k_gather_cols(const double* __restrict__ X, int ld, int64_t n, int K, const int* __restrict__ cols,
-                              double* __restrict__ Y) {
+                              const int* __restrict__ rows, double* __restrict__ Y) {
   const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int j = blockIdx.y * kColTile + (threadIdx.x & 31);
   if (r >= n || j >= K) return;
-  Y[(size_t)r * K + cols[j]] = X[(size_t)r * ld + j];
+  const int64_t ro = rows ? rows[r] : r;
+  Y[(size_t)ro * K + (cols ? cols[j] : j)] = X[(size_t)r * ld + j];
 }
 
-// lam[r][j] = S[r][cols[j]]: a seed given in the caller's column order, in solve order (S is n x K)
+// lam[r][j] = S[rows[r]][cols[j]]: a state or seed given in the caller's row and
+// column order, in solve order (S is n x K; a null map is the identity)
 __global__ void k_pick_cols(const double* __restrict__ S, int64_t n, int K, const int* __restrict__ cols,
-                            double* __restrict__ lam, int ld) {
+                            const int* __restrict__ rows, double* __restrict__ lam, int ld) {
   const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int j = blockIdx.y * kColTile + (threadIdx.x & 31);
   if (r >= n || j >= K) return;
-  lam[(size_t)r * ld + j] = S[(size_t)r * K + cols[j]];
+  const int64_t ro = rows ? rows[r] : r;
+  lam[(size_t)r * ld + j] = S[(size_t)ro * K + (cols ? cols[j] : j)];
 }
 
 // v1 = Phi2 lam' for the last step of a checkpoint segment
@@ -2308,6 +2365,7 @@ __global__ void k_transpose_blocks(const int* __restrict__ bslot, const int* __r
 // ---------------------------------------------------------------------------
 struct AdjParams {
   int64_t n;
+  int64_t row0;             // first row of the launch (the tail of the bin-blocked sweep), else 0
   int ld;
   int ncols;
   int64_t step;
@@ -2345,7 +2403,7 @@ __device__ __forceinline__ double adj_v(const AdjParams& a, int c, int k) {
 template <int STAGE>
 __global__ void __launch_bounds__(256) k_adj(AdjParams a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int64_t r = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+  const int64_t r = a.row0 + (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
   if (r >= a.n) return;
   const int k = blockIdx.y * kColTile + lane;
   const bool active = k < a.ncols;
@@ -2758,6 +2816,15 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
     k_slab_prep<<<blocks_for((int64_t)p.n_slab_spec * p.d, 256), 256, 0, st>>>(p);
     ++launches;
   }
+  if (c->n_tail > 0) {  // tail rows (another grid): the general row kernel, a warp per row
+    StepParams q = p;
+    q.rows = c->tail_rows.as<int>();
+    q.nrows = c->n_tail;
+    q.nsb = (int)blocks_for(q.nrows, 8);
+    q.nseg = 0;
+    k_step_multi<STAGE><<<dim3((unsigned)q.nsb, tiles), 256, 0, st>>>(q);
+    ++launches;
+  }
   if (p.ngroups > 0) cudaStreamWaitEvent(st, c->ev_join, 0);
   if (p.nb > 0) {
     k_band_finish<STAGE><<<dim3(blocks_for((int64_t)p.nb * p.d, 8), tiles), 256, 0, st>>>(p);
@@ -2792,6 +2859,33 @@ void launch_adj_blocked(pb_context* c, AdjBlk& q, cudaStream_t st) {
   if (forked) cudaStreamWaitEvent(st, c->ev_join, 0);
   k_slabT<STAGE><<<dim3(q.d, (unsigned)blocks_for(q.ncols, kSlabCols)), kSlabTWarps * 32, c->slabT_smem, st>>>(q);
 }
+
+// The EM hook's operands for window w on the n x ld buffer X (a state, or the adjoint's lam).
+EmParams em_params(const pb_context* c, int w, int ld, int ncols, double* X) {
+  EmParams e;
+  e.n = c->n;
+  e.ld = ld;
+  e.ncols = ncols;
+  e.n_em = c->em_n;
+  e.n_cr = c->em_ncr;
+  e.n_bh = c->em_nbh;
+  e.g_off = c->em_g;
+  e.em_off = c->em_m;
+  e.ep_off = c->em_p;
+  e.bh_off = c->em_bh_off.as<int64_t>();
+  e.bh_A = c->em_bh_A.as<double>();
+  e.invE = c->em_invE.as<double>();
+  e.dE = c->em_dE.as<double>();
+  e.kp = c->kp.as<double>() + (size_t)w * c->n;
+  e.dl_step = c->em_dl[w];
+  e.Tg = c->em_Tg.as<double>() + (size_t)w * c->em_n * c->em_n;
+  e.Te = c->em_Te.as<double>() + (size_t)w * c->em_n * c->em_n;
+  e.R = c->em_R.as<double>() + (size_t)w * c->em_n * c->em_ncr;
+  e.X = X;
+  return e;
+}
+
+size_t em_smem(const pb_context* c) { return (size_t)(c->em_ncr + 2 * c->em_n) * 32 * sizeof(double); }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
 // advanced at step k; a step without active columns is skipped (every column
@@ -2837,29 +2931,8 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       ++launches;
     }
     if (c->have_em && (p.flags & PB_EM_CASCADE)) {
-      const int w = c->h_win[k];
-      EmParams e;
-      e.n = n;
-      e.ld = p.ld;
-      e.ncols = p.ncols;
-      e.n_em = c->em_n;
-      e.n_cr = c->em_ncr;
-      e.n_bh = c->em_nbh;
-      e.g_off = c->em_g;
-      e.em_off = c->em_m;
-      e.ep_off = c->em_p;
-      e.bh_off = c->em_bh_off.as<int64_t>();
-      e.bh_A = c->em_bh_A.as<double>();
-      e.invE = c->em_invE.as<double>();
-      e.dE = c->em_dE.as<double>();
-      e.kp = c->kp.as<double>() + (size_t)w * n;
-      e.dl_step = c->em_dl[w];
-      e.Tg = c->em_Tg.as<double>() + (size_t)w * c->em_n * c->em_n;
-      e.Te = c->em_Te.as<double>() + (size_t)w * c->em_n * c->em_n;
-      e.R = c->em_R.as<double>() + (size_t)w * c->em_n * c->em_ncr;
-      e.X = X;
-      const size_t smem = (size_t)(c->em_ncr + 2 * c->em_n) * 32 * sizeof(double);
-      k_em_hook<<<blocks_for(p.ncols, 32), 256, smem, st>>>(e);
+      const EmParams e = em_params(c, c->h_win[k], p.ld, p.ncols, X);
+      k_em_hook<<<blocks_for(p.ncols, 32), 256, em_smem(c), st>>>(e);
       ++launches;
     }
   }
@@ -2915,6 +2988,9 @@ int pb_create(int device, pb_context** out) {
   }
   e = cudaFuncSetAttribute(k_em_hook, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            3 * kMaxEmBins * 32 * (int)sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_em_hookT, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             3 * kMaxEmBins * 32 * (int)sizeof(double));
   if (e != cudaSuccess) {
     pb_destroy(c);
     return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_em_hook): %s", cudaGetErrorString(e));
@@ -2962,6 +3038,9 @@ int pb_set_coupling(pb_context* c, int64_t n, int64_t R, const int64_t* indptr, 
   c->h_cpl_indices.assign(indices, indices + R);
   c->blocked_ok = false;
   c->lay_d = c->lay_nsp = 0;
+  c->lay_nu = n;
+  c->n_tail = 0;
+  c->have_row_map = false;
   if ((rc = upload(c, c->cpl_indptr, indptr, (size_t)n + 1))) return rc;
   if ((rc = upload(c, c->cpl_indices, indices, (size_t)R))) return rc;
   PB_CUDA(c, c->cpl_row.ensure((size_t)std::max<int64_t>(R, 1) * sizeof(int)));
@@ -3025,7 +3104,12 @@ int pb_build_fold_kernel(pb_context* c, const pb_kernel_spec* k) {
   if (!k) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: spec is NULL");
   if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_build_fold_kernel: set the coupling pattern first");
   const int d = k->d, dph = k->dph;
-  if (d < 1 || c->n % d != 0) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: d = %d does not divide %lld states", d, (long long)c->n);
+  if (d < 1 || c->lay_nu % d != 0)
+    return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: d = %d does not divide the %lld block states", d, (long long)c->lay_nu);
+  if (c->h_cpl_indptr[c->lay_nu] != c->R)
+    return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: coupling entries in the tail rows");
+  for (int64_t j = 0; j < c->R; ++j)
+    if (c->h_cpl_indices[j] >= c->lay_nu) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: coupling entries in the tail columns");
   if (dph <= 0 || dph > kMaxPhoton) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: photon bins must be in [1, %d]", kMaxPhoton);
   if (c->have_photon_grid && dph != c->dph) return fail(c, PB_ERR_ARG, "pb_build_fold_kernel: photon axis %d != photon grid %d", dph, c->dph);
   if (!k->f_mo || !k->dE || k->n_resp < 0 || k->n_ddr < 0 || k->n_sep < 0 || k->n_channels < 1 || !k->channels ||
@@ -3151,7 +3235,12 @@ static int build_fd_table(pb_context* c) {
   c->fdT_ok = false;
   const int d = c->lay_d;
   if (!c->have_fd || d <= 0 || c->h_d_indptr.size() != (size_t)c->n + 1) return PB_OK;
-  const int nsp = (int)(c->n / d);
+  const int nsp = (int)(c->lay_nu / d);
+  {  // the species blocks' stencils stay inside the blocks
+    const std::vector<int64_t>& ip0 = c->h_d_indptr;
+    for (int64_t j = 0; j < ip0[c->lay_nu]; ++j)
+      if (c->h_d_indices[j] >= c->lay_nu) return PB_OK;
+  }
   const std::vector<int64_t>& ip = c->h_d_indptr;
   const std::vector<int32_t>& ix = c->h_d_indices;
   const std::vector<double>& dv = c->h_d_vals;
@@ -3366,16 +3455,57 @@ int pb_set_injection(pb_context* c, int32_t n_src, int32_t n_rows, const int32_t
   return PB_OK;
 }
 
+int pb_set_row_map(pb_context* c, const int32_t* caller_row) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_row_map: set the coupling pattern first");
+  if (!caller_row) {
+    c->have_row_map = false;
+    return PB_OK;
+  }
+  std::vector<char> seen((size_t)c->n, 0);
+  for (int64_t i = 0; i < c->n; ++i) {
+    const int32_t r = caller_row[i];
+    if (r < 0 || r >= c->n || seen[r]) return fail(c, PB_ERR_ARG, "pb_set_row_map: not a permutation (row %lld)", (long long)i);
+    seen[r] = 1;
+  }
+  int rc = set_device(c);
+  if (rc) return rc;
+  if ((rc = upload(c, c->row_map, caller_row, (size_t)c->n))) return rc;
+  c->have_row_map = true;
+  return PB_OK;
+}
+
 int pb_set_layout(pb_context* c, int32_t d) {
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
+  return pb_set_layout_rows(c, d, c->n);
+}
+
+int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
+  if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
   if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_layout: set the coupling pattern first");
-  if (d <= 0 || c->n % d != 0) return fail(c, PB_ERR_ARG, "pb_set_layout: %lld states are not blocks of %d bins", (long long)c->n, d);
+  if (n_blocks <= 0 || n_blocks > c->n)
+    return fail(c, PB_ERR_ARG, "pb_set_layout_rows: %lld block rows outside [1, %lld]", (long long)n_blocks, (long long)c->n);
+  if (d <= 0 || n_blocks % d != 0)
+    return fail(c, PB_ERR_ARG, "pb_set_layout: %lld states are not blocks of %d bins", (long long)n_blocks, d);
   int rc = set_device(c);
   if (rc) return rc;
   const int64_t n = c->n, R = c->R;
-  const int nsp = (int)(n / d);
+  const int nsp = (int)(n_blocks / d);
   const std::vector<int64_t>& ip = c->h_cpl_indptr;
   const std::vector<int32_t>& ix = c->h_cpl_indices;
+  // the tail: rows past the species blocks, stepped by the general row kernel
+  c->lay_nu = n_blocks;
+  c->n_tail = (int32_t)(n - n_blocks);
+  if (c->n_tail > 0) {
+    std::vector<int32_t> tr((size_t)c->n_tail);
+    for (int32_t i = 0; i < c->n_tail; ++i) tr[i] = (int32_t)(n_blocks + i);
+    if ((rc = upload(c, c->tail_rows, tr.data(), tr.size()))) return rc;
+  }
+  // the bin-blocked kernels need the coupling block-diagonal over (blocks, tail)
+  bool split_ok = true;
+  for (int64_t r = 0; r < n && split_ok; ++r)
+    for (int64_t j = ip[r]; j < ip[r + 1]; ++j)
+      if ((r < n_blocks) != (ix[j] < n_blocks)) { split_ok = false; break; }
   // band species: rows with an off-diagonal entry that leaves the row's bin
   std::vector<int32_t> bspec, sspec;
   int lo = 1 << 30, hi = -(1 << 30);
@@ -3482,7 +3612,7 @@ int pb_set_layout(pb_context* c, int32_t d) {
   const size_t ssm = SlabSmem::bytes(nsp, maxbin, (nss + 1) / 2);
   const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0, 0};
   const BandInstance bi4 = (RT && J) ? band_kernel(RT, J, 4) : BandInstance{nullptr, 0, 0};
-  const bool ok = quads_fit && ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
+  const bool ok = split_ok && quads_fit && ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
                   (size_t)d * (kColTile + 2) * sizeof(double) <= max_smem &&
                   (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && squad.size() < ((size_t)1 << 29);
   if (!ok) return PB_OK;  // the general row kernels stay in use
@@ -4198,7 +4328,15 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->scan_tmp.ensure(scan_need));
 
   double* X = c->X.as<double>();
-  if (a->init_state) {
+  const int* rmap = c->have_row_map ? c->row_map.as<int>() : nullptr;
+  if (a->init_state && rmap) {  // the caller's rows: one copy to scratch, then a gather into solve order
+    PB_CUDA(c, cudaMemcpyAsync(c->F.p, a->state, (size_t)n * K * sizeof(double),
+                               a->state_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+    if (K > 1 && ld > K) PB_CUDA(c, cudaMemsetAsync(X, 0, sbytes, st));
+    k_pick_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(c->F.as<double>(), n, K, nullptr,
+                                                                               rmap, X, ld);
+    PB_CUDA(c, cudaGetLastError());
+  } else if (a->init_state) {
     if (a->state_on_device) {
       PB_CUDA(c, cudaMemcpy2DAsync(X, ld * sizeof(double), a->state, K * sizeof(double), K * sizeof(double), n,
                                    cudaMemcpyDeviceToDevice, st));
@@ -4347,10 +4485,12 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
     launches = c->graph_launches;
   }
   const cudaMemcpyKind out_kind = a->state_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  if (a->out_cols && K > 1) {  // columns in the caller's order, gathered on the device, then one copy
-    if ((rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
+  const bool ocols = a->out_cols && K > 1;
+  if (ocols || rmap) {  // rows and columns in the caller's order, gathered on the device, then one copy
+    if (ocols && (rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
     double* Y = c->F.as<double>();  // F(x) scratch of the steps, n x ld >= n x K
-    k_gather_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(X, ld, n, K, c->outcols.as<int>(), Y);
+    k_gather_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(
+        X, ld, n, K, ocols ? c->outcols.as<int>() : nullptr, rmap, Y);
     PB_CUDA(c, cudaGetLastError());
     PB_CUDA(c, cudaMemcpyAsync(a->state, Y, (size_t)n * K * sizeof(double), out_kind, st));
   } else {
@@ -4433,8 +4573,10 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   if (a->n_steps != c->last_S || a->n_cols != c->last_K || a->flags != c->last_flags ||
       a->ckpt_every != c->last_ckpt || a->n_windows != c->last_W || a->photon_scale != c->last_scale)
     return fail(c, PB_ERR_ARG, "pb_adjoint: arguments differ from the checkpointed solve");
-  if (a->flags & PB_EM_CASCADE)
-    return fail(c, PB_ERR_ARG, "pb_adjoint: the EM cascade hook has no adjoint (solve without PB_EM_CASCADE)");
+  const bool em = (a->flags & PB_EM_CASCADE) && c->have_em;
+  if (em && grad_scale)
+    return fail(c, PB_ERR_ARG, "pb_adjoint: no photon-scale gradient through the EM cascade transfer "
+                               "(pass grad_scale = NULL with PB_EM_CASCADE)");
   const int64_t S = a->n_steps, n = c->n, R = c->R;
   const int K = a->n_cols, CK = a->ckpt_every;
   const int ld = K == 1 ? 1 : ((K + kColTile - 1) / kColTile) * kColTile;
@@ -4499,15 +4641,19 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   if (want_inj) PB_CUDA(c, c->gb_inj.ensure((size_t)std::max<int64_t>(S, 1) * std::max(n_inj, 1) * ld * sizeof(double)));
   if ((rc = upload(c, c->nact, a->n_active, (size_t)std::max<int64_t>(S, 1)))) return rc;
   PB_CUDA(c, cudaMemsetAsync(c->lam.p, 0, sb, st));
-  if (a->out_cols && K > 1) {  // the seed in the caller's column order: one copy, then a gather on the device
-    for (int j = 0; j < K; ++j)
-      if (a->out_cols[j] < 0 || a->out_cols[j] >= K) return fail(c, PB_ERR_ARG, "pb_adjoint: out_cols[%d] out of range", j);
-    if ((rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
+  const int* rmap = c->have_row_map ? c->row_map.as<int>() : nullptr;
+  const bool ocols = a->out_cols && K > 1;
+  if (ocols || rmap) {  // the seed in the caller's row and column order: one copy, then a gather on the device
+    if (ocols) {
+      for (int j = 0; j < K; ++j)
+        if (a->out_cols[j] < 0 || a->out_cols[j] >= K) return fail(c, PB_ERR_ARG, "pb_adjoint: out_cols[%d] out of range", j);
+      if ((rc = upload(c, c->outcols, a->out_cols, (size_t)K))) return rc;
+    }
     PB_CUDA(c, c->F.ensure(sb));
     PB_CUDA(c, cudaMemcpyAsync(c->F.p, seed, (size_t)n * K * sizeof(double),
                                seed_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
-    k_pick_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(c->F.as<double>(), n, K,
-                                                                               c->outcols.as<int>(), c->lam.as<double>(), ld);
+    k_pick_cols<<<dim3(blocks_for(n, 8), blocks_for(K, kColTile)), 256, 0, st>>>(
+        c->F.as<double>(), n, K, ocols ? c->outcols.as<int>() : nullptr, rmap, c->lam.as<double>(), ld);
     PB_CUDA(c, cudaGetLastError());
   } else {
     PB_CUDA(c, cudaMemcpy2DAsync(c->lam.p, ld * sizeof(double), seed, K * sizeof(double), K * sizeof(double), n,
@@ -4616,17 +4762,51 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
           q.inj_slot = c->inj_slot.as<int>();
           q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
         }
-        if (k == k1 - 1)  // v1 of the segment's last step; later steps get it from stage 2
+        if (em) {  // the hook after step k, transposed, before the step's adjoint
+          const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
+          k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
+        }
+        if (k == k1 - 1 || em)  // v1 of the segment's last step; later steps get it from stage 2
           k_adj_v1<<<dim3(blocks_for(n, 8), blocks_for(q.ncols, kColTile)), 256, 0, st>>>(
               q.rf + 2 * n, lam, n, ld, q.ncols, c->vbuf.as<double>());
+        AdjParams t;  // tail rows (species on another grid): the general adjoint kernel
+        if (c->n_tail > 0) {
+          memset(&t, 0, sizeof(t));
+          t.n = n;
+          t.row0 = c->lay_nu;
+          t.ld = ld;
+          t.ncols = q.ncols;
+          t.step = k;
+          t.flags = p.flags;
+          t.h = q.h;
+          t.dl = q.dl;
+          t.w = q.w;
+          t.t_indptr = c->t_indptr.as<int64_t>();
+          t.t_indices = c->t_indices.as<int>();
+          t.t_perm = c->t_perm.as<int>();
+          t.m_vals = c->m_vals.as<double>() + (size_t)q.w * mstride;
+          t.dt_indptr = c->dt_indptr.as<int64_t>();
+          t.dt_indices = c->dt_indices.as<int>();
+          t.dt_vals = c->dt_vals.as<double>();
+          t.lt_indptr = q.lt_indptr;
+          t.lt_indices = q.lt_indices;
+          t.lt_vals = q.lt_vals;
+          t.rf = q.rf;
+          t.lam = lam;
+          t.mu = c->mu.as<double>();
+          t.lam_out = lam2;
+        }
+        const dim3 tgrid((unsigned)blocks_for(c->n_tail, 8), blocks_for(q.ncols, kColTile));
         q.v = c->vbuf.as<double>();
         q.lam = lam;
         q.vout = c->vbuf2.as<double>();
         launch_adj_blocked<1>(c, q, st);
+        if (c->n_tail > 0) k_adj<1><<<tgrid, 256, 0, st>>>(t);
         q.v = c->vbuf2.as<double>();
         q.vout = c->vbuf.as<double>();
         q.lam_out = lam2;
         launch_adj_blocked<2>(c, q, st);
+        if (c->n_tail > 0) k_adj<2><<<tgrid, 256, 0, st>>>(t);
         std::swap(lam, lam2);
       }
       PB_CUDA(c, cudaGetLastError());
@@ -4668,6 +4848,10 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
       if (want_inj) {
         q.inj_slot = c->inj_slot.as<int>();
         q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
+      }
+      if (em) {  // the hook after step k, transposed, before the step's adjoint
+        const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
+        k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
       }
       dim3 grid(blocks_for(n, 8), K == 1 ? 1u : blocks_for(q.ncols, kColTile));
       k_adj<1><<<grid, 256, 0, st>>>(q);

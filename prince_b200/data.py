@@ -1,10 +1,13 @@
 """Energy grids, PDG helpers and the species layout of the state vector.
 
 The state vector is species-major: species are ordered by PDG id and each
-species owns one contiguous block of ``d`` energy bins.  This is the layout
-contract of the reference (``src/prince_cr/data.py:1385-1446`` for the
-ordering, ``data.py:1256-1290`` for the per-species slices); the CSR
-structure and every per-state vector in this package index into it.
+species owns one contiguous block of energy bins on its home grid (``d`` bins
+of the cosmic-ray grid, or of a separate EM grid for gamma and e+- when the
+EM sector is decoupled).  This is the layout contract of the reference
+(``src/prince_cr/data.py:1385-1446`` for the ordering, ``data.py:1256-1310``
+for the per-species slices, ``data.py:1664-1711`` for the home grids and the
+transport offsets); the CSR structure and every per-state vector in this
+package index into it.
 """
 
 from __future__ import annotations
@@ -91,6 +94,10 @@ class PrinceSpecies:
         self.princeidx = int(princeidx)
         self.grid_tag = "default"
         self._d = int(d)
+        # transport block: offset and size in the state vector, offset in the bin-edge vector
+        self._tr_lidx = self.princeidx * self._d
+        self._tr_dim = self._d
+        self._tr_lbin = self.princeidx * (self._d + 1)
         self.is_nucleus = is_nucleus(self.pdgid)
         if self.is_nucleus:
             self.A, self.Z, self.N = get_AZN(self.pdgid)
@@ -108,16 +115,16 @@ class PrinceSpecies:
         return slice(self.lidx(), self.uidx())
 
     def lidx(self):
-        return self.princeidx * self._d
+        return self._tr_lidx
 
     def uidx(self):
-        return (self.princeidx + 1) * self._d
+        return self._tr_lidx + self._tr_dim
 
     def lbin(self):
-        return self.princeidx * (self._d + 1)
+        return self._tr_lbin
 
     def ubin(self):
-        return (self.princeidx + 1) * (self._d + 1)
+        return self._tr_lbin + self._tr_dim + 1
 
     def __repr__(self):
         return f"PrinceSpecies({self.pdgid}, idx={self.princeidx})"
@@ -147,4 +154,29 @@ class SpeciesManager:
         self.dim_bins = self.nspec * (int(ed) + 1)
 
     def add_grid(self, tag, d):
+        """Register a home grid of ``d`` bins (moves no species onto it)."""
         self.grid_dims[tag] = int(d)
+
+    def set_grid_tag(self, pdgid, tag):
+        """Home species ``pdgid`` on the registered grid ``tag`` and recompute the offsets."""
+        if tag not in self.grid_dims:
+            raise KeyError(f"grid {tag!r} is not registered; call add_grid first")
+        self.pdgid2sref[int(pdgid)].grid_tag = tag
+        self.compute_transport_offsets()
+
+    def compute_transport_offsets(self):
+        """Blocks of ``grid_dims[s.grid_tag]`` states in ``princeidx`` order
+        (``data.py:1677-1700``); sets ``dim_states`` and ``dim_bins``."""
+        off = offb = 0
+        for s in sorted(self.species_refs, key=lambda x: x.princeidx):
+            d = self.grid_dims[s.grid_tag]
+            s._tr_lidx, s._tr_dim, s._tr_lbin = off, d, offb
+            off += d
+            offb += d + 1
+        self.dim_states = off
+        self.dim_bins = offb
+
+    @property
+    def decoupled(self):
+        """True when some species live on a grid other than the default one."""
+        return any(s.grid_tag != "default" for s in self.species_refs)

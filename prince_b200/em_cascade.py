@@ -15,8 +15,9 @@ the scattering iteration, all on the GPU.
 (cached per redshift; ``prefetch(zs)`` builds all windows of a solve in one
 device call) and the Bethe-Heitler pair shape ``R_BH`` from ``pb_bh_shape``
 (the reference solver's ``_em_bh_at``, ``src/prince_cr/solvers/propagation.py:573-618``:
-40 target energies from 10^-12.5 to 10^-7 GeV, e+- and nucleons both on the
-run's grid), or from a caller-supplied function.
+40 target energies from 10^-12.5 to 10^-7 GeV, e+- on the EM species' grid --
+the run's decoupled EM grid or the shared one -- and nucleons on the
+cosmic-ray grid), or from a caller-supplied function.
 """
 
 from __future__ import annotations
@@ -78,9 +79,10 @@ class KineticCascadeModel:
         if not todo:
             return
         ctx = DeviceRun.of(self.run, self.device).ctx
-        E = self.run.cr_grid.grid
+        em_grid = getattr(self.run, "em_grid", None)
+        E = (em_grid if em_grid is not None else self.run.cr_grid).grid
         Tg, Te, _ = kinetic_transfer(ctx, self.run.photon_field, E, todo, self.dz)
-        R = (bh_shape(ctx, self.run.photon_field, E, E, todo) if self.bh_shape is None
+        R = (bh_shape(ctx, self.run.photon_field, E, self.run.cr_grid.grid, todo) if self.bh_shape is None
              else [self.bh_shape(z) for z in todo])
         for i, z in enumerate(todo):
             self._cache[z] = (Tg[i], Te[i], R[i])

@@ -59,6 +59,21 @@ def fd_loss_operator(grid, nspec):
     return sp.block_diag(nspec * [blk]).tocsr()
 
 
+def run_fd_loss_operator(run):
+    """The run's FD loss operator: one block per species on its home grid, in
+    ``princeidx`` order (``partial_diff.py:28-46``, heterogeneous path)."""
+    sm = run.spec_man
+    if not sm.decoupled:
+        return fd_loss_operator(run.cr_grid, sm.nspec)
+    cache = {}
+    blocks = []
+    for s in sorted(sm.species_refs, key=lambda x: x.princeidx):
+        if s.grid_tag not in cache:
+            cache[s.grid_tag] = sp.coo_matrix(fd_block(run.grids[s.grid_tag]))
+        blocks.append(cache[s.grid_tag])
+    return sp.block_diag(blocks).tocsr()
+
+
 def split_diagonal(L):
     """``(d, L_off)``: float64 diagonal and the CSR off-diagonal part.
 

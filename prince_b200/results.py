@@ -172,13 +172,21 @@ def _as_torch(X):
 class UHECRPropagationResult:
     """Final state of a propagation (``(n,)`` or ``(n, K)``) with its grid and species."""
 
-    def __init__(self, state, egrid, spec_man, grid=None):
+    def __init__(self, state, egrid, spec_man, grid=None, grids=None):
         self.spec_man = spec_man
         self.egrid = egrid
         self.state = state
         # the grid's (lower, upper, bins/decade); recovered from the centres when not given
         self._grid = grid if grid is not None else egrid
+        # energies of the other home grids by tag (gamma and e+- on a decoupled EM grid)
+        self._grids = dict(grids or {})
         self._projectors = {}
+
+    def _energies(self, s):
+        """Energies of species ``s``: its home grid's (the shared grid's by default)."""
+        if s.grid_tag == "default":
+            return self.egrid
+        return self._grids[s.grid_tag]
 
     # -- container protocol ------------------------------------------------
     def to_dict(self):
@@ -203,23 +211,23 @@ class UHECRPropagationResult:
 
     def __add__(self, other):
         self._compatible(other)
-        return UHECRPropagationResult(self.state + other.state, self.egrid, self.spec_man, self._grid)
+        return UHECRPropagationResult(self.state + other.state, self.egrid, self.spec_man, self._grid, self._grids)
 
     def __mul__(self, number):
         if not np.isscalar(number):
             raise TypeError(f"a result scales by a scalar only, not by {type(number).__name__}")
-        return UHECRPropagationResult(self.state * number, self.egrid, self.spec_man, self._grid)
+        return UHECRPropagationResult(self.state * number, self.egrid, self.spec_man, self._grid, self._grids)
 
     # -- single species ------------------------------------------------------
     def get_solution(self, pdg_id):
         """``(egrid, n)``: the species' spectrum per energy per nucleon."""
         s = self.spec_man.pdgid2sref[pdg_id]
-        return self.egrid, self.state[s.sl]
+        return self._energies(s), self.state[s.sl]
 
     def get_solution_scale(self, pdg_id, epow=0):
         """``(A E, (A E)^epow n / A)``: the spectrum in total energy."""
         s = self.spec_man.pdgid2sref[pdg_id]
-        etot = s.A * np.asarray(self.egrid)
+        etot = s.A * np.asarray(self._energies(s))
         y = self.state[s.sl]
         scale = etot ** epow
         return etot, (scale[:, None] if np.ndim(y) == 2 else scale) * y / s.A
@@ -227,6 +235,9 @@ class UHECRPropagationResult:
     # -- groups ----------------------------------------------------------------
     def _projector(self, pdg_ids, egrid):
         species = select_species(self.spec_man, pdg_ids)
+        off = [p for p in species if self.spec_man.pdgid2sref[p].grid_tag != "default"]
+        if off:
+            raise ValueError(f"species {off} live on another grid; group projections take the shared grid's species")
         if egrid is None:
             amax = max(s.A for s in self.spec_man.species_refs)
             com = common_energy_grid(self._grid, amax)

@@ -135,6 +135,7 @@ class _ContinuousLossBase:
         self.spec_man = prince_run.spec_man
         self.e_cosmicray = prince_run.cr_grid
         self.energy = energy
+        self._grids = getattr(prince_run, "grids", {"default": prince_run.cr_grid})
         if energy == "grid":
             self._dim = prince_run.dim_states
             self._earr = prince_run.cr_grid.grid
@@ -145,6 +146,11 @@ class _ContinuousLossBase:
             self._earr = prince_run.cr_grid.bins
             self._lo = lambda s: s.lbin()
             self._hi = lambda s: s.ubin()
+
+    def _species_earr(self, s):
+        """Energies of species ``s`` on its home grid (``interaction_rates.py:1159-1165``)."""
+        g = self._grids.get(s.grid_tag, self.e_cosmicray)
+        return g.grid if self.energy == "grid" else g.bins
 
 
 class ContinuousAdiabaticLossRate(_ContinuousLossBase):
@@ -157,7 +163,7 @@ class ContinuousAdiabaticLossRate(_ContinuousLossBase):
         super().__init__(prince_run, energy)
         self.energy_vector = np.zeros(self._dim)
         for s in self.spec_man.species_refs:
-            self.energy_vector[self._lo(s):self._hi(s)] = self._earr
+            self.energy_vector[self._lo(s):self._hi(s)] = self._species_earr(s)
 
     def loss_vector(self, z, energy=None):
         from .cosmology import H
@@ -234,6 +240,17 @@ class ContinuousPairProductionLossRate(_ContinuousLossBase):
         return self.scale_vec * rate_full
 
 
+def default_em_grid(cosmic_ray_grid, bins_dec=16):
+    """The reference's decoupled EM grid (``core.py:105-129``): log10 m_e snapped
+    up to the step 1/bins_dec below the cosmic-ray grid's top."""
+    import math
+
+    top = float(cosmic_ray_grid[1])
+    m_e_log10 = float(np.log10(C.PRINCE_UNITS.m_electron))
+    steps = math.floor((top - m_e_log10) * bins_dec)
+    return (top - steps / bins_dec, top, bins_dec)
+
+
 class PriNCeRun:
     """Grids, species, photon field, loss rates and the fold kernel of one run.
 
@@ -245,16 +262,26 @@ class PriNCeRun:
         max_mass: keep species with ``A <= max_mass``.
         backend: a ``constants.BackendConfig`` (default backend ``"b200"``).
         enable_em_cascade: co-evolve gamma and e+- with the nuclei (the
-            reference run's flag of the same name); the EM species share the
-            cosmic-ray grid.
+            reference run's flag of the same name; gamma, e- and e+ join the
+            species).  The EM species share the cosmic-ray grid unless
+            ``enable_em_decoupled_grid``.
+        enable_em_decoupled_grid: home gamma and e+- on their own EM grid
+            (``core.py:44-56, 105-137, 206-214``): blocks of ``em_grid.d``
+            states while the nuclei keep the cosmic-ray grid.
+        em_grid: ``(log10 lo, log10 hi, bins per decade)`` of that grid; by
+            default the reference's: from the electron mass (snapped to the
+            step, rounded up) to the top of the cosmic-ray grid at 16 bins per
+            decade.
         em_cascade_model: ``callable(z) -> (T_gamma, T_electron, R_BH)``, the
-            per-redshift cascade transfer and Bethe-Heitler pair shape on that
-            grid, read by the solvers' ``_em_transfer_at`` / ``_em_bh_at``.
+            per-redshift cascade transfer (on the EM species' grid) and the
+            Bethe-Heitler pair shape (EM grid x cosmic-ray grid), read by the
+            solvers' ``_em_transfer_at`` / ``_em_bh_at``.
     """
 
     def __init__(self, cross_sections, photon_field, cosmic_ray_grid=(3, 14, 8),
                  photon_grid=(-15, -6, 8), max_mass=np.inf, backend=None, species_list=None,
-                 enable_em_cascade=False, em_cascade_model=None):
+                 enable_em_cascade=False, em_cascade_model=None, enable_em_decoupled_grid=False,
+                 em_grid=None):
         self.backend = backend if backend is not None else C.BackendConfig()
         self.cross_sections = cross_sections
         self.photon_field = photon_field
@@ -266,8 +293,19 @@ class PriNCeRun:
         else:
             species = [s for s in cross_sections.known_species
                        if not is_nucleus(s) or get_AZN(s)[0] <= max_mass]
+        self.enable_em_cascade = bool(enable_em_cascade)
+        self.enable_em_decoupled_grid = bool(enable_em_decoupled_grid) and self.enable_em_cascade
+        self.em_grid = None
+        if self.enable_em_cascade:
+            species = list(species) + [p for p in (22, 11, -11) if p not in species]
         lifetimes = getattr(cross_sections, "lifetimes", None)
         self.spec_man = SpeciesManager(species, self.cr_grid.d, lifetimes=lifetimes)
+        if self.enable_em_decoupled_grid:
+            self.em_grid = EnergyGrid(*(em_grid if em_grid is not None else default_em_grid(cosmic_ray_grid)))
+            self.grids["em"] = self.em_grid
+            self.spec_man.add_grid("em", self.em_grid.d)
+            for p in (22, 11, -11):
+                self.spec_man.set_grid_tag(p, "em")
         self.dim_states = self.spec_man.dim_states
         self.dim_bins = self.spec_man.dim_bins
         self.adia_loss_rates_grid = ContinuousAdiabaticLossRate(self, "grid")
@@ -281,9 +319,7 @@ class PriNCeRun:
             bm, rows, cols = cross_sections.build_kernel(self.cr_grid, self.ph_grid, self.spec_man)
             self.int_rates = PhotoNuclearInteractionRate(self, bm, rows, cols)
         self.em_int_rates = None
-        self.enable_em_cascade = bool(enable_em_cascade)
         self.em_cascade_model = em_cascade_model
-        self.em_grid = None
         self.spec_man.add_grid("ph", self.ph_grid.d)
 
     def set_photon_field(self, pfield):

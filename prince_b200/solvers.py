@@ -23,7 +23,7 @@ from . import _lib
 from . import constants as C
 from .cosmology import H as _H
 from .cosmology import dldz as _dldz
-from .operators import fd_loss_operator, split_diagonal
+from .operators import run_fd_loss_operator, split_diagonal
 from .photonfields import device_components, device_table
 from .results import UHECRPropagationResult  # noqa: F401  (reference API location)
 from .schedule import make_schedule, z_grid
@@ -38,12 +38,54 @@ def _dense_kernel(bm):
     return np.ascontiguousarray(bm, dtype=np.float64)
 
 
+def device_order(run):
+    """``(dev2run, n_blocks)``: the device's row order of the run's state.
+
+    On a shared grid the device keeps the run's layout (``dev2run`` None).
+    With species on other grids (gamma and e+- on a decoupled EM grid) the
+    device puts the species blocks of the cosmic-ray grid first, in
+    ``princeidx`` order, then the other species: device row i holds run row
+    ``dev2run[i]`` and rows ``[0, n_blocks)`` are blocks of ``cr_grid.d``
+    bins, the layout of the bin-blocked kernels.
+    """
+    sm = run.spec_man
+    if not sm.decoupled:
+        return None, run.dim_states
+    refs = sorted(sm.species_refs, key=lambda x: x.princeidx)
+    blocks = [s for s in refs if s.grid_tag == "default"]
+    tail = [s for s in refs if s.grid_tag != "default"]
+    dev2run = np.concatenate([np.arange(s.lidx(), s.uidx()) for s in blocks + tail]).astype(np.int64)
+    return dev2run, sum(s.uidx() - s.lidx() for s in blocks)
+
+
+def permute_csr(M, dev2run):
+    """``(M_dev, order)``: ``M`` with rows and columns in device order (sorted
+    CSR) and, for every entry of ``M_dev``, the index of that entry in ``M``'s
+    CSR order."""
+    M = sp.csr_matrix(M)
+    if dev2run is None:
+        return M, np.arange(M.nnz)
+    n = M.shape[0]
+    run2dev = np.empty(n, dtype=np.int64)
+    run2dev[dev2run] = np.arange(n)
+    rows = np.repeat(np.arange(n), np.diff(M.indptr))
+    r, c = run2dev[rows], run2dev[M.indices]
+    order = np.lexsort((c, r))
+    indptr = np.zeros(n + 1, dtype=np.int64)
+    np.add.at(indptr, r + 1, 1)
+    indptr = np.cumsum(indptr)
+    M_dev = sp.csr_matrix((np.asarray(M.data)[order], c[order], indptr), shape=M.shape)
+    return M_dev, order
+
+
 class DeviceRun:
     """The run's constant operators resident on one GPU (one C context).
 
     Uploaded once per (run, device): the coupling pattern, the FP64 fold
     kernel, the photon grid, the FD loss operator, the loss inputs and (if the
-    run carries one) the explicit-decay operator.
+    run carries one) the explicit-decay operator, all in the device's row
+    order (``device_order``); the solves read and write states in the run's
+    order through the context's row map.
     """
 
     def __init__(self, run, device=0):
@@ -51,17 +93,28 @@ class DeviceRun:
         self.ctx = _lib.Context(device)
         n = run.dim_states
         ir = run.int_rates
-        cm = ir.coupling_mat
         self.n = n
+        self.dev2run, n_blocks = device_order(run)
+        p = self.dev2run
+        self.run2dev = None
+        if p is not None:
+            self.run2dev = np.empty(n, dtype=np.int64)
+            self.run2dev[p] = np.arange(n)
+        cm, order = permute_csr(ir.coupling_mat, p)
         self.ctx.set_coupling(n, cm.indptr, cm.indices)
-        self.ctx.set_layout(run.spec_man.nspec and n // run.spec_man.nspec)
+        if p is None:
+            self.ctx.set_layout(run.spec_man.nspec and n // run.spec_man.nspec)
+        else:
+            self.ctx.set_layout(run.cr_grid.d, n_blocks)
+            self.ctx.set_row_map(p)
         spec = getattr(ir, "kernel_spec", None)
         if spec is not None:   # expanded on the device, in coupling-CSR order
-            self.ctx.build_fold_kernel(spec, np.asarray(spec.chan)[ir.sortidx])
+            self.ctx.build_fold_kernel(spec, np.asarray(spec.chan)[ir.sortidx][order])
         else:
-            self.ctx.set_fold_kernel(_dense_kernel(ir._batch_matrix))
+            bm = _dense_kernel(ir._batch_matrix)
+            self.ctx.set_fold_kernel(bm if p is None else np.ascontiguousarray(bm[order]))
         self.ctx.set_photon_grid(ir.e_photon.grid)
-        D = fd_loss_operator(run.cr_grid, run.spec_man.nspec)
+        D, _ = permute_csr(run_fd_loss_operator(run), p)
         self.D_diag, self.D_off = split_diagonal(D)
         self.ctx.set_fd_operator(self.D_off, self.D_diag)
         pl = run.pair_loss_rates_grid
@@ -69,14 +122,24 @@ class DeviceRun:
         for s in run.spec_man.species_refs:
             if s.is_nucleus:
                 pair_bin[s.lidx():s.uidx()] = np.arange(s.uidx() - s.lidx())
-        self.ctx.set_losses(run.adia_loss_rates_grid.energy_vector, pl.scale_vec, pair_bin, pl.xi, pl.phi_xi2,
-                            pl.photon_grid)
+        self.ctx.set_losses(self.dev_vec(run.adia_loss_rates_grid.energy_vector), self.dev_vec(pl.scale_vec),
+                            self.dev_vec(pair_bin), pl.xi, pl.phi_xi2, pl.photon_grid)
         self.has_decay = False
         dec = getattr(run, "decay_operator", None)
         if dec is not None:
             diag, off = dec
-            self.ctx.set_decay(diag, None if off is None else sp.csr_matrix(off))
+            self.ctx.set_decay(self.dev_vec(diag), None if off is None else permute_csr(off, p)[0])
             self.has_decay = True
+
+    def dev_vec(self, v):
+        """A per-state vector of the run in device order."""
+        v = np.asarray(v)
+        return v if self.dev2run is None else np.ascontiguousarray(v[self.dev2run])
+
+    def dev_rows(self, rows):
+        """Run state rows as device rows."""
+        rows = np.asarray(rows)
+        return rows if self.run2dev is None else self.run2dev[rows].astype(rows.dtype)
 
     def ensure_em(self):
         """Upload the EM-cascade layout once: gamma / e+- blocks and the charged
@@ -84,19 +147,23 @@ class DeviceRun:
         if getattr(self, "_em_ready", False):
             return
         run = self.run
-        if getattr(run, "em_grid", None) is not None:
-            raise NotImplementedError("EM cascade on a separate (decoupled) EM grid is not supported; "
-                                      "put gamma and e+- on the cosmic-ray grid")
         sm = run.spec_man
         if 22 not in sm.pdgid2sref:
             raise ValueError("enable_em_cascade needs the photon (22) among the run's species")
         g = sm.pdgid2sref[22]
-        lep = [sm.pdgid2sref[p].lidx() if p in sm.pdgid2sref else -1 for p in (11, -11)]
-        bh = [(s.lidx(), float(s.A)) for s in sm.species_refs if s.is_nucleus and abs(s.charge) >= 1]
+
+        def off(s):  # device row of the species block's first bin
+            return int(self.dev_rows(np.array([s.lidx()]))[0])
+
+        for p in (11, -11):
+            if p in sm.pdgid2sref and sm.pdgid2sref[p].grid_tag != g.grid_tag:
+                raise ValueError("gamma and e+- must share one grid")
+        lep = [off(sm.pdgid2sref[p]) if p in sm.pdgid2sref else -1 for p in (11, -11)]
+        bh = [(off(s), float(s.A)) for s in sm.species_refs if s.is_nucleus and abs(s.charge) >= 1]
         E = run.cr_grid.grid
         with np.errstate(divide="ignore"):
             inv_E = np.where(E > 0, 1.0 / E, 0.0)
-        self.ctx.set_em(g.uidx() - g.lidx(), g.lidx(), lep[0], lep[1], E.size,
+        self.ctx.set_em(g.uidx() - g.lidx(), off(g), lep[0], lep[1], E.size,
                         np.array([b[0] for b in bh], dtype=np.int64), np.array([b[1] for b in bh]),
                         inv_E, np.gradient(E))
         self._em_ready = True
@@ -118,6 +185,27 @@ class DeviceRun:
 # ---------------------------------------------------------------------------
 # solvers
 # ---------------------------------------------------------------------------
+def run_em_windows(run, sched, dz):
+    """Per-window ``(T_gamma, T_electron, R_BH, dl_step)`` of a run's
+    ``em_cascade_model`` at the windows' redshifts (the solvers' ``_em_windows``
+    without their override points)."""
+    model = getattr(run, "em_cascade_model", None)
+    if model is None:
+        raise NotImplementedError("enable_em_cascade needs the run's em_cascade_model(z) -> (T_gamma, T_electron, R_BH)")
+    if hasattr(model, "prefetch"):
+        model.prefetch([float(zw) for zw in sched.z_window])
+    out = [model(float(zw)) for zw in sched.z_window]
+    dl = [C.PRINCE_UNITS.c * abs(dz) / ((1.0 + float(zw)) * _H(float(zw))) for zw in sched.z_window]
+    return (np.stack([np.asarray(o[0], dtype=np.float64) for o in out]),
+            np.stack([np.asarray(o[1], dtype=np.float64) for o in out]),
+            np.stack([np.asarray(o[2], dtype=np.float64) for o in out]), np.array(dl))
+
+
+def _other_grids(run):
+    """Energies of the run's home grids other than the shared one, by tag."""
+    return {t: g.grid for t, g in getattr(run, "grids", {}).items() if t != "default"}
+
+
 def _coefficients(sources, zs):
     """(n_steps, n_src) table of norm * evolution(z_k) per source."""
     if not sources:
@@ -185,7 +273,8 @@ class UHECRPropagationSolverETD2:
     @property
     def res(self):
         if self.result is None:
-            self.result = UHECRPropagationResult(self.state, self.egrid, self.spec_man, self.prince_run.cr_grid)
+            self.result = UHECRPropagationResult(self.state, self.egrid, self.spec_man, self.prince_run.cr_grid,
+                                                 _other_grids(self.prince_run))
         return self.result
 
     def add_source_class(self, source_instance):
@@ -227,6 +316,9 @@ class UHECRPropagationSolverETD2:
         all at the window's redshift (``_refresh_z_caches`` and
         ``_inject_bh_pairs``, ``propagation.py:620-665``)."""
         Tg, Te, R, dl = [], [], [], []
+        model = getattr(self.prince_run, "em_cascade_model", None)
+        if hasattr(model, "prefetch"):   # build every window's matrices in one device call
+            model.prefetch([float(zw) for zw in sched.z_window])
         for zw in sched.z_window:
             zw = float(zw)
             tg, te = self._em_transfer_at(zw)
@@ -303,7 +395,7 @@ class UHECRPropagationSolverETD2:
         ctx = self._dev.ctx
         flags = self._flags()
         if use_inj:
-            ctx.set_injection(rows, G, src_col, K)
+            ctx.set_injection(self._dev.dev_rows(rows), G, src_col, K)
         else:
             flags &= ~_lib.PB_INJECTION
         self._set_field(ctx)
@@ -356,7 +448,7 @@ class _MultiRHSView:
     @property
     def res(self):
         return UHECRPropagationResult(self.state, self.parent.egrid, self.parent.spec_man,
-                                      self.parent.prince_run.cr_grid)
+                                      self.parent.prince_run.cr_grid, _other_grids(self.parent.prince_run))
 
 
 class MultiRHSPropagationSolverETD2(UHECRPropagationSolverETD2):

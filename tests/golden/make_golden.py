@@ -6,6 +6,7 @@ source tree (the directory that holds ``src/prince_cr``)::
 
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py        # light network
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --em   # light network + EM cascade
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --em-decoupled  # ... on a decoupled EM grid
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --groups  # result post-processing
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --ebl     # tabulated EBL (Gilmore 2012)
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --kernel  # fold-kernel construction inputs
@@ -386,6 +387,96 @@ def main_em():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_em_decoupled():
+    """Light network with the co-evolved EM cascade on a decoupled EM grid.
+
+    gamma and e+- live on the reference's own EM grid (from the electron mass
+    to the top of the nuclear grid, 8 bins per decade) while the nuclei keep
+    the 8-12 nuclear grid; the per-window transfer (EM grid) and the
+    Bethe-Heitler pair shape (EM grid x nuclear grid) are the synthetic
+    stand-ins of ``prince_b200.synth.em_cascade_matrices``, patched into the
+    reference solver as in ``main_em``.
+    """
+    _prepare_reference()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from prince_b200 import synth
+    from prince_b200.data import EnergyGrid
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.cosmic_ray_grid = (8, 12, 8)
+    config.em_grid_bins_dec = 8
+    config.photon_grid = (-15, -6, 8)
+    config.tau_dec_threshold = 0.0
+    config.max_mass = 4
+    config.batch_matrix_format = "dense"
+    config.xs_dtype = "float64"
+    config.linear_algebra_backend = "scipy"
+
+    from prince_cr import core, cr_sources
+    from prince_cr.cross_sections.base import CrossSectionBase
+    from prince_cr.solvers import MultiRHSPropagationSolverETD2, UHECRPropagationSolverETD2
+
+    orig = core.PriNCeRun
+
+    def em_run(*a, **k):
+        k.update(enable_em_cascade=True, enable_em_decoupled_grid=True)
+        return orig(*a, **k)
+
+    core.PriNCeRun = em_run
+    run = build(config, CrossSectionBase)
+    core.PriNCeRun = orig
+    assert run.em_grid is not None
+    ir = run.int_rates
+    grid, egrid = run.cr_grid, run.em_grid
+    lo, hi = np.log10(grid.bins[0]), np.log10(grid.bins[-1])
+    elo, ehi = np.log10(egrid.bins[0]), np.log10(egrid.bins[-1])
+    mine = EnergyGrid(lo, hi, 8)
+    mine_em = EnergyGrid(elo, ehi, 8)
+    assert np.allclose(mine.grid, grid.grid, rtol=1e-14)
+    assert np.allclose(mine_em.grid, egrid.grid, rtol=1e-14)
+
+    def patch(s):
+        s._em_transfer_at = lambda z: synth.em_cascade_matrices(mine_em, mine, float(z))[:2]
+        s._em_bh_at = lambda z: synth.em_cascade_matrices(mine_em, mine, float(z))[2]
+        return s
+
+    eq = {2212: (2.0, 1e10, 1.0), 1000020040: (2.0, 1e10, 1.0)}
+    soft = {2212: (2.5, 3e10, 1.0)}
+    out = {}
+    out["species"] = np.array(run.spec_man.known_species, dtype=np.int64)
+    out["cr_grid"] = np.array([lo, hi, 8.0])
+    out["em_grid"] = np.array([elo, ehi, 8.0])
+    out["ph_grid"] = np.array(config.photon_grid, dtype=np.float64)
+    out["dim_states"] = np.array(run.dim_states)
+    out["lidx"] = np.array([s.lidx() for s in sorted(run.spec_man.species_refs, key=lambda s: s.princeidx)])
+    out["adia_energy"] = np.asarray(run.adia_loss_rates_grid.energy_vector)
+    out["batch_matrix"] = np.asarray(ir._batch_matrix, dtype=np.float64)
+    out["batch_rows"] = np.asarray(ir._batch_rows, dtype=np.int64)
+    out["batch_cols"] = np.asarray(ir._batch_cols, dtype=np.int64)
+    out["cpl_indptr"] = np.asarray(ir.coupling_mat.indptr, dtype=np.int64)
+    out["cpl_indices"] = np.asarray(ir.coupling_mat.indices, dtype=np.int64)
+    s = patch(UHECRPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run))
+    s._ensure_D_split()
+    out["D_diag"] = np.asarray(s._etd2_D_diag)
+    out["D_off_indptr"] = np.asarray(s._etd2_D_off.indptr, dtype=np.int64)
+    out["D_off_indices"] = np.asarray(s._etd2_D_off.indices, dtype=np.int64)
+    out["D_off_data"] = np.asarray(s._etd2_D_off.data)
+    s.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=eq))
+    s.solve(dz=1e-3)
+    out["state_em"] = np.asarray(s.state)
+    m = patch(MultiRHSPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run, K=2))
+    m[0].add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=eq))
+    m[1].add_source_class(cr_sources.SimpleSource(run, norm=1.0, params=soft, m=("simple", 2.0)))
+    m.solve(dz=1e-3)
+    out["state_em_multi"] = np.asarray(m.state)
+    out["src_eq"] = np.array(repr(eq))
+    out["src_soft"] = np.array(repr(soft))
+    path = os.path.join(HERE, "light_network_em_decoupled.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 def main_groups():
     """The reference's result post-processing on recorded states."""
     _prepare_reference()
@@ -626,7 +717,9 @@ def main_cascade():
 
 
 if __name__ == "__main__":
-    if "--em" in sys.argv:
+    if "--em-decoupled" in sys.argv:
+        main_em_decoupled()
+    elif "--em" in sys.argv:
         main_em()
     elif "--groups" in sys.argv:
         main_groups()

@@ -117,6 +117,33 @@ def light_network_em():
     return z, run, em, source
 
 
+def light_network_em_decoupled():
+    """The decoupled-grid EM fixture: gamma and e+- on the reference's EM grid,
+    the nuclei on the nuclear grid, and the synthetic per-window transfer."""
+    from prince_b200 import synth
+    from prince_b200.data import EnergyGrid
+
+    z = dict(np.load(os.path.join(GOLDEN, "light_network_em_decoupled.npz")))
+    model = FixedKernelModel(z["species"], z["batch_matrix"], z["batch_rows"], z["batch_cols"])
+    grid = EnergyGrid(*tuple(z["cr_grid"]))
+    egrid = EnergyGrid(*tuple(z["em_grid"]))
+
+    def em(zz):
+        return synth.em_cascade_matrices(egrid, grid, float(zz))
+
+    run = PriNCeRun(model, photonfields.CMBPhotonSpectrum(), cosmic_ray_grid=tuple(z["cr_grid"]),
+                    photon_grid=tuple(z["ph_grid"]), enable_em_cascade=True, em_cascade_model=em,
+                    enable_em_decoupled_grid=True, em_grid=tuple(z["em_grid"]))
+
+    def source(key):
+        params = ast.literal_eval(str(z[f"src_{key}"]))
+        if key == "soft":
+            return cr_sources.SimpleSource(run, norm=1.0, params=params, m=("simple", 2.0))
+        return cr_sources.RigdityCutoffSource(run, norm=1.0, params=params)
+
+    return z, run, em, source
+
+
 def light_network_ebl():
     """The light network in CMB + the tabulated Gilmore (2012) EBL: fixture arrays,
     the run (this package's classes on the fixture's kernel and EBL table) and

@@ -216,3 +216,50 @@ def test_blocked_and_row_kernel_adjoints_agree():
     for g0, g1 in zip(grads[0], grads[1]):
         g0, g1 = np.asarray(g0), np.asarray(g1)
         np.testing.assert_allclose(g1, g0, rtol=1e-9, atol=1e-12 * np.abs(g0).max())
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_adjoint_through_the_em_cascade(mode):
+    """Decoupled EM grid: a loss on the photons reaches the source parameters only
+    through the Bethe-Heitler pairs and the cascade transfer (the transposed hook)."""
+    from golden_io import light_network_em_decoupled
+    from prince_b200 import _lib
+    z, run, em, source = light_network_em_decoupled()
+    species = [2212, 1000020040]
+    K = 3
+    sb = AD.SourceBatch(run, species, z_max=[0.2, 0.16, 0.12], initial_z=0.2)
+    plan = sb.plan(0.2, ckpt_every=8)
+    plan.dev.ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, mode)
+    t = _tensors(_params(K, 3, len(species)))
+    scale = torch.tensor(1.0, dtype=torch.float64)
+    with torch.no_grad():
+        X0 = _forward(sb, plan, {k: v.detach() for k, v in t.items()}, scale)
+    g = run.spec_man.pdgid2sref[22].sl
+    w = torch.zeros_like(X0)
+    blk = X0[g]
+    good = blk.abs() > 1e-12 * blk.abs().max(dim=0).values
+    assert good.any()
+    w[g] = torch.where(good, 1.0 / torch.where(good, blk, torch.ones_like(blk)), torch.zeros_like(blk))
+    p = run.spec_man.pdgid2sref[2212].sl
+    w[p] = 1e-3 / X0[p].abs().max()
+
+    def fun(tt, sc):
+        return (w * _forward(sb, plan, tt, sc)).sum()
+
+    L = fun(t, scale)
+    L.backward()
+    worst, where = 0.0, None
+    for key in ["gamma", "lg_rmax", "frac", "m"]:
+        gr = t[key].grad.detach().numpy()
+        for idx in np.ndindex(t[key].shape):
+            def f(step):
+                tt = {k: v.detach().clone() for k, v in t.items()}
+                tt[key][idx] += step
+                with torch.no_grad():
+                    return float(fun(tt, scale))
+            fd = _central(f, 1e-5)
+            err = abs(gr[idx] - fd) / max(abs(fd), 1e-300)
+            if not err <= worst:
+                worst, where = err, (key, idx, float(gr[idx]), fd)
+    plan.dev.ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, 1)
+    assert worst < TOL, where

@@ -70,8 +70,17 @@ def test_em_cascade_ragged_batch_vs_oracle(em_golden):
     assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
 
 
-def test_em_cascade_has_no_adjoint(em_golden):
-    from prince_b200 import adjoint
+def test_em_cascade_adjoint_refuses_the_photon_scale_gradient(em_golden):
+    """The transfer's dependence on the photon field is not differentiated."""
+    import torch
+    from prince_b200 import adjoint as AD
     z, run, em, source = em_golden
-    with pytest.raises(NotImplementedError):
-        adjoint.Plan(run, 0.2, 1, np.arange(4, dtype=np.int32), [0], [0], dz=1e-3)
+    sb = AD.SourceBatch(run, [2212], z_max=[0.1], initial_z=0.1)
+    plan = sb.plan(0.1, ckpt_every=8)
+    assert plan.em
+    G = sb.grids(torch.tensor([2.0]), torch.tensor([10.0]), torch.tensor([[1.0]]))
+    coeff = sb.coefficients(torch.tensor([0.0]))
+    scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    X = AD.PropagateFunction.apply(G, coeff, scale, plan)
+    X.sum().backward()
+    assert scale.grad is None

@@ -145,3 +145,32 @@ def test_host_correctly_rounded_exp():
                          np.exp(rng.uniform(np.log(1e-9), np.log(709), 1000)), [0.0, 1e-6, -1e-6]])
     exact = np.array([float(Decimal(float(x)).exp()) for x in xs])
     assert np.array_equal(crexp.exp(xs), exact)
+
+
+def test_device_order_puts_the_shared_grid_blocks_first():
+    """Decoupled EM grid: nuclei first on the device, the EM blocks as the tail; the
+    permuted CSR keeps every entry and maps back to the run's entry order."""
+    import scipy.sparse as sp
+    from golden_io import light_network_em_decoupled
+    from prince_b200.solvers import device_order, permute_csr
+
+    z, run, em, source = light_network_em_decoupled()
+    dev2run, nb = device_order(run)
+    sm = run.spec_man
+    assert nb == sum(s.uidx() - s.lidx() for s in sm.species_refs if s.grid_tag == "default")
+    assert nb % run.cr_grid.d == 0
+    assert sorted(dev2run.tolist()) == list(range(run.dim_states))
+    g = sm.pdgid2sref[22]
+    assert set(dev2run[nb:].tolist()) >= set(range(g.lidx(), g.uidx()))
+    cm = run.int_rates.coupling_mat
+    M = sp.csr_matrix((np.arange(1, cm.nnz + 1, dtype=float), cm.indices, cm.indptr), shape=cm.shape)
+    Md, order = permute_csr(M, dev2run)
+    assert Md.has_sorted_indices
+    np.testing.assert_array_equal(Md.data, M.data[order])
+    np.testing.assert_array_equal(Md.toarray(), M.toarray()[np.ix_(dev2run, dev2run)])
+    assert device_order(light_run_shared())[0] is None
+
+
+def light_run_shared():
+    from golden_io import light_network_em
+    return light_network_em()[1]

@@ -168,3 +168,31 @@ def test_oracle_em_cascade_single_and_multi():
     assert rel_err_on_support(x, z["state_em"], blocks) < TOL
     X = O.OracleSolver(run, 0.2, 0.0, K=2, em=em).solve([[source("eq")], [source("soft")]], dz=1e-3)
     assert rel_err_on_support(X, z["state_em_multi"], blocks) < TOL
+
+
+def test_decoupled_em_grid_layout_matches_the_reference():
+    """gamma and e+- on their own EM grid: offsets, sizes and the per-grid loss energies."""
+    from golden_io import light_network_em_decoupled
+
+    z, run, em, source = light_network_em_decoupled()
+    refs = sorted(run.spec_man.species_refs, key=lambda s: s.princeidx)
+    assert run.dim_states == int(z["dim_states"])
+    assert [s.lidx() for s in refs] == list(z["lidx"])
+    assert np.array_equal(run.adia_loss_rates_grid.energy_vector, z["adia_energy"])
+    D = operators.run_fd_loss_operator(run)
+    d, off = operators.split_diagonal(D)
+    assert np.array_equal(d, z["D_diag"])
+    assert np.array_equal(off.indptr, z["D_off_indptr"]) and np.array_equal(off.indices, z["D_off_indices"])
+    assert np.array_equal(off.data, z["D_off_data"])
+
+
+def test_oracle_em_cascade_on_a_decoupled_grid():
+    """The EM hooks with gamma/e+- on the EM grid and R_BH (EM x nuclear) against the reference."""
+    from golden_io import light_network_em_decoupled
+
+    z, run, em, source = light_network_em_decoupled()
+    blocks = [s.sl for s in run.spec_man.species_refs]
+    x = O.OracleSolver(run, 0.2, 0.0, em=em).solve([source("eq")], dz=1e-3)
+    assert rel_err_on_support(x, z["state_em"], blocks) < TOL
+    X = O.OracleSolver(run, 0.2, 0.0, K=2, em=em).solve([[source("eq")], [source("soft")]], dz=1e-3)
+    assert rel_err_on_support(X, z["state_em_multi"], blocks) < TOL

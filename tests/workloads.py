@@ -23,6 +23,23 @@ def network_run(max_mass=56, n_species=350, seed=2):
     return PriNCeRun(model, cib_field(), cosmic_ray_grid=CFG2_GRID, photon_grid=CFG2_PHOTON)
 
 
+EM_GRID = (-3, 14, 128 / 17)    # 128 bins, 1e-3 to 1e14 GeV
+
+
+def em_network_run(max_mass=56, n_species=350, seed=2, dz=1e-3):
+    """The A <= max_mass network with the co-evolved EM cascade: gamma and e+- on
+    the 128-bin EM grid, the cascade transfer and the Bethe-Heitler pair shape
+    built on the device from the CMB + synthetic CIB."""
+    from prince_b200.em_cascade import KineticCascadeModel
+
+    species = synth.full_network_species(max_mass, n_species=n_species)
+    model = synth.SyntheticPhotoNuclear(species, seed=seed, x_cut_proton=1e-4)
+    run = PriNCeRun(model, cib_field(), cosmic_ray_grid=CFG2_GRID, photon_grid=CFG2_PHOTON,
+                    enable_em_cascade=True, enable_em_decoupled_grid=True, em_grid=EM_GRID)
+    run.em_cascade_model = KineticCascadeModel(run, dz)
+    return run
+
+
 def light_run(seed=1):
     """p, n, 2H, 3H, 3He, 4He on 1e6-1e14 GeV at 8 bins/decade, CMB only."""
     model = synth.SyntheticPhotoNuclear(synth.light_network_species(), seed=seed)
