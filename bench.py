@@ -241,6 +241,10 @@ def run_b200(args, dist, rank, ws, local):
         plain = len(pm) / (sum(pm) / 1e3)
 
     adj = adjoint_timing(run, pts, zi, local) if args.adjoint else None
+    cfg5 = None
+    if args.config5 and rank == 0:
+        del solver
+        cfg5 = config5_timing(local, adjoint=bool(args.adjoint))
 
     pk, pk_kind = _peaks()
     avg_steps_ms = statistics.mean(steps_ms)
@@ -278,6 +282,8 @@ def run_b200(args, dist, rank, ws, local):
         adj["adjoint_over_forward"] = adj["adjoint_s"] / fwd_wall
         adj["gradient_over_forward"] = adj["gradient_s"] / fwd_wall
         line["adjoint"] = adj
+    if cfg5:
+        line["config5"] = cfg5
     if clk:
         line["clocks"] = clk
     return line, run, pts, zi, sched
@@ -422,6 +428,92 @@ def adjoint_timing(run, pts, zi, device):
             "params_per_point": 8, "with_photon_scale": True, "grads_finite": grads_finite}
 
 
+def config5_timing(device, points=2048, adjoint=True):
+    """Config 5: the A <= 56 network with the co-evolved EM cascade -- gamma and
+    e+- on the decoupled 128-bin EM grid (1e-3 to 1e14 GeV), pair production and
+    inverse Compton on CMB + the synthetic CIB (transfer and Bethe-Heitler
+    shape built on the device for every rate window) -- over 2048 seeded
+    points with z_max ~ U[0.5, 4].  Timed: the EM build of all windows, one
+    forward solve (device events and wall clock), and the gradient of a loss
+    on the z = 0 all-particle flux and photon spectrum with respect to the
+    8 source parameters of every point (the adjoint through the EM hook)."""
+    import torch
+    from prince_b200 import adjoint as AD
+    from prince_b200.schedule import make_schedule, z_grid
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, em_network_run, point_source
+
+    t0 = time.perf_counter()
+    run = em_network_run()
+    pts = draw_points(run, points, seed=5000, z_range=(0.5, 4.0))
+    zi = max(p["zmax"] for p in pts)
+    sched = make_schedule(z_grid(zi, 0.0, 1e-3), run.backend.update_rates_z_threshold)
+    solver = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=points, device=device)
+    for k, p in enumerate(pts):
+        solver[k].add_source_class(point_source(run, p))
+    setup_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run.em_cascade_model.prefetch([float(z) for z in sched.z_window])
+    torch.cuda.synchronize()
+    em_build_s = time.perf_counter() - t0
+    solver.solve(dz=1e-3)   # warm-up: operator set-up and graph capture
+    t0 = time.perf_counter()
+    solver.solve(dz=1e-3)
+    wall = time.perf_counter() - t0
+    solve_ms, device_ms, steps_ms, launches = solver.last_timing
+    sched_, K, coeff, rows, G, src_col, n_active, perm, use_inj = solver._prepare(1e-3)
+    col_steps = int(np.sum(n_active))
+    out = {"workload": "A<=56 network + gamma/e+- on a 128-bin EM grid (1e-3-1e14 GeV), CMB + synthetic CIB, "
+                       "2048 points, z_max ~ U[0.5,4], dz = 1e-3",
+           "n_states": run.dim_states, "em_bins": run.em_grid.d, "points": points, "steps": int(sched.n_steps),
+           "windows": len(sched.z_window), "column_steps": col_steps,
+           "setup_s": setup_s, "em_build_s": em_build_s, "em_build_windows": len(sched.z_window),
+           "forward_device_s": device_ms / 1e3, "forward_steps_s": steps_ms / 1e3, "forward_wall_s": wall,
+           "spectra_per_s": points / (device_ms / 1e3), "spectra_per_s_e2e": points / wall,
+           "gpu_launches": int(launches)}
+    if adjoint:
+        species = list(pts[0]["species"])
+        hidden = draw_points(run, 1, seed=4243, z_range=(2.0, 2.0))
+
+        def tensors(ps, grad=True):
+            return {"gamma": torch.tensor([p["gamma"] for p in ps], requires_grad=grad),
+                    "lg_rmax": torch.tensor([np.log10(p["rmax"]) for p in ps], requires_grad=grad),
+                    "frac": torch.tensor(np.array([p["frac"] for p in ps]), requires_grad=grad),
+                    "m": torch.tensor([p["m"] for p in ps], requires_grad=grad)}
+
+        one = torch.tensor(1.0, dtype=torch.float64)
+        sbh = AD.SourceBatch(run, species, z_max=[hidden[0]["zmax"]], initial_z=hidden[0]["zmax"])
+        th = tensors(hidden, grad=False)
+        with torch.no_grad():
+            Xh = AD.PropagateFunction.apply(sbh.grids(th["gamma"], th["lg_rmax"], th["frac"]),
+                                            sbh.coefficients(th["m"]), one,
+                                            sbh.plan(hidden[0]["zmax"], device=device))
+            tgt_cr = AD.group_flux(run, Xh)[1][:, 0]
+            g = run.spec_man.pdgid2sref[22]
+            tgt_g = Xh[g.lidx():g.uidx(), 0]
+        sb = AD.SourceBatch(run, species, z_max=[p["zmax"] for p in pts], initial_z=zi)
+        ck = 128
+        plan = sb.plan(zi, device=device, ckpt_every=ck)
+        t = tensors(pts)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        X = AD.PropagateFunction.apply(sb.grids(t["gamma"], t["lg_rmax"], t["frac"]), sb.coefficients(t["m"]),
+                                       one, plan)
+        loss = (AD.log_ratio_loss(run, X, tgt_cr) + AD.photon_log_ratio_loss(run, X, tgt_g)).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out["adjoint"] = {"loss": "sum_k [sum_{E>10^9.5} ln(F_k/T)^2 + sum_{0.1<=E<=1e3 GeV} ln(n_gamma,k/T_gamma)^2]",
+                          "ckpt_every": ck, "params_per_point": 8, "with_photon_scale": False,
+                          "forward_ckpt_s": t1 - t0, "adjoint_s": t2 - t1, "gradient_s": t2 - t0,
+                          "gradient_over_forward": (t2 - t0) / wall,
+                          "grads_finite": all(bool(torch.isfinite(v.grad).all()) for v in t.values())}
+    return out
+
+
 CPU_SAMPLE_STEPS = 20   # two rate windows at dz = 1e-3 and the 0.01 refresh threshold
 
 
@@ -454,6 +546,8 @@ def main():
     ap.add_argument("--plain", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="also time the adjoint gradient (1/0)")
+    ap.add_argument("--config5", type=int, default=1,
+                    help="also time the coupled EM cascade workload, forward and gradient (1/0)")
     ap.add_argument("--band-warps", type=int, default=0, choices=[0, 4, 8],
                     help="warps of a band-tile CTA (0: the library default)")
     ap.add_argument("--z-range", default="0.5,1.0",

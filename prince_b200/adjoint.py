@@ -274,3 +274,23 @@ def log_ratio_loss(run, X, target, e_min=10 ** 9.5, dynamic_range=0.0):
     ok = Fs > 0
     r = torch.log(torch.where(ok, Fs, torch.ones_like(Fs))) - torch.log(Ts)
     return torch.where(ok, r * r, torch.zeros_like(r)).sum(dim=0)
+
+
+def photon_log_ratio_loss(run, X, target, e_min=1e-1, e_max=1e3, dynamic_range=1e-30):
+    """sum over photon bins with e_min <= E <= e_max of ln(n_k(E) / T(E))^2, per column.
+
+    ``n_k`` is column k's z = 0 photon spectrum on the photon's home grid (the
+    decoupled EM grid when the run has one) and ``T`` a target spectrum on the
+    same grid.  Bins where the target is zero or below ``dynamic_range`` of its
+    maximum, and bins where the column's spectrum is not positive, are left out.
+    """
+    s = run.spec_man.pdgid2sref[22]
+    grid = (run.em_grid if s.grid_tag != "default" else run.cr_grid).grid
+    E = torch.as_tensor(grid, dtype=X.dtype, device=X.device)
+    n = X[s.lidx():s.uidx()]
+    T = torch.as_tensor(target, dtype=X.dtype, device=X.device)
+    sel = (E >= e_min) & (E <= e_max) & (T > 0) & (T > dynamic_range * T.max())
+    ns, Ts = n[sel], T[sel][:, None]
+    ok = ns > 0
+    r = torch.log(torch.where(ok, ns, torch.ones_like(ns))) - torch.log(Ts)
+    return torch.where(ok, r * r, torch.zeros_like(r)).sum(dim=0)
