@@ -101,6 +101,9 @@ class PropagateFunction(torch.autograd.Function):
         _solve(ctx_dev, plan, cd, X, s)   # returns after the library stream completed
         ctx.plan = plan
         ctx.in_device = G.device
+        # the photon-scale gradient needs the recorded state sensitivities; without
+        # it the adjoint records only the operator factors (no state recompute)
+        ctx.want_scale = bool(ctx.needs_input_grad[2]) and not plan.em
         return X
 
     @staticmethod
@@ -110,7 +113,7 @@ class PropagateFunction(torch.autograd.Function):
         seed = grad_X.detach().to(device=dev, dtype=torch.float64).contiguous()  # caller's column order
         torch.cuda.current_stream(dev).synchronize()
         cd, s = plan.last_args
-        gG, gc, gs = _adjoint(plan.dev.ctx, plan, cd, s, seed)
+        gG, gc, gs = _adjoint(plan.dev.ctx, plan, cd, s, seed, ctx.want_scale)
         gG_user = np.empty_like(gG)
         gG_user[:, plan.src_order] = gG
         gc_user = np.empty_like(gc)
@@ -170,8 +173,9 @@ def _solve(ctx, plan, coeff, out, scale):
     ctx._check(ctx.lib.pb_solve(ctx.h, Cc.byref(args)), "pb_solve")
 
 
-def _adjoint(ctx, plan, coeff, scale, seed):
-    """Device adjoint; ``seed`` is a contiguous CUDA tensor (n x K, caller's column order)."""
+def _adjoint(ctx, plan, coeff, scale, seed, want_scale=True):
+    """Device adjoint; ``seed`` is a contiguous CUDA tensor (n x K, caller's column order).
+    The photon-scale gradient (``want_scale``) is None for EM runs or when not wanted."""
     import ctypes as Cc
 
     dummy = np.zeros(1)  # the adjoint reads no state through args
@@ -179,7 +183,7 @@ def _adjoint(ctx, plan, coeff, scale, seed):
     n_src = plan.dev_src_col.size
     gG = np.zeros((plan.rows.size, n_src))
     gc = np.zeros((plan.sched.n_steps, n_src))
-    gs = None if plan.em else np.zeros(plan.K)   # no photon-scale gradient through the EM transfer
+    gs = np.zeros(plan.K) if (want_scale and not plan.em) else None
     P = lambda a: None if a is None else a.ctypes.data_as(Cc.POINTER(Cc.c_double))
     seed_p = Cc.cast(Cc.c_void_p(seed.data_ptr()), Cc.POINTER(Cc.c_double))
     ctx._check(ctx.lib.pb_adjoint(ctx.h, Cc.byref(args), seed_p, 1, P(gG), P(gc), P(gs)), "pb_adjoint")

@@ -4707,11 +4707,20 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
     int64_t kf = k0;
     while (kf < k1 && a->n_active[kf] == 0) ++kf;
     if (kf == k1) continue;  // no active column in this segment
-    PB_CUDA(c, cudaMemcpyAsync(c->X.p, c->ckpt.as<double>() + (size_t)sg * n * ld, sb, cudaMemcpyDeviceToDevice, st));
     p.rec_k0 = k0;
     p.rec_len = (int)(k1 - k0);
-    PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max<size_t>(c->h_long_rows.size(), 1) * ctiles * sizeof(int), st));
-    launch_steps(c, p, K, a->n_active, k0, k1, st, nullptr, 0);
+    if (want_scale) {  // the sensitivities P, Q need the states: recompute the segment from its checkpoint
+      PB_CUDA(c, cudaMemcpyAsync(c->X.p, c->ckpt.as<double>() + (size_t)sg * n * ld, sb, cudaMemcpyDeviceToDevice, st));
+      PB_CUDA(c, cudaMemsetAsync(c->counter.p, 0, (size_t)std::max<size_t>(c->h_long_rows.size(), 1) * ctiles * sizeof(int), st));
+      launch_steps(c, p, K, a->n_active, k0, k1, st, nullptr, 0);
+    } else {  // the operator factors depend on z alone: record them without recomputing the states
+      for (int64_t k = kf; k < k1; ++k) {
+        if (a->n_active[k] == 0) continue;
+        p.step = k;
+        p.step_w = c->h_win[k];
+        k_prep<<<blocks_for(n, 256), 256, 0, st>>>(p);
+      }
+    }
     if (blockedT) {
       for (int64_t k = k1 - 1; k >= kf; --k) {
         const size_t j = (size_t)(k - k0);

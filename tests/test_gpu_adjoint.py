@@ -263,3 +263,23 @@ def test_adjoint_through_the_em_cascade(mode):
                 worst, where = err, (key, idx, float(gr[idx]), fd)
     plan.dev.ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, 1)
     assert worst < TOL, where
+
+
+def test_adjoint_without_the_photon_scale_records_factors_only(light):
+    """A scale that needs no gradient skips the state recompute of the sweep: the
+    operator factors alone are recorded, and the source gradients are unchanged."""
+    run = light
+    species = [2212, 1000020040]
+    K = 3
+    sb = AD.SourceBatch(run, species, z_max=[0.3, 0.24, 0.17], initial_z=0.3)
+    plan = sb.plan(0.3, ckpt_every=8)
+    grads = []
+    for want in (True, False):
+        t = _tensors(_params(K, 7, len(species)))
+        scale = torch.tensor(1.0, dtype=torch.float64, requires_grad=want)
+        X = _forward(sb, plan, t, scale)
+        (X.sum() / X.detach().abs().max()).backward()
+        assert (scale.grad is not None) == want
+        grads.append({k: v.grad.detach().numpy().copy() for k, v in t.items()})
+    for k in grads[0]:
+        np.testing.assert_allclose(grads[1][k], grads[0][k], rtol=1e-13, atol=0)

@@ -11,8 +11,8 @@ the one nearest 2.5 -- are solved by the oracle on the same redshift grid with
 the same per-window EM matrices, and
 held to the headline criterion: relative 1e-10 per bin wherever the oracle's
 flux exceeds 1e-20 of the species maximum, except on bins whose value the
-oracle's own 1e-15 operator perturbations move by more than that, where the
-GPU must stay within the oracle's spread.
+oracle's own 1e-15 operator perturbations (four draws) move by more than that,
+where the GPU must stay within the oracle's spread.
 """
 
 import multiprocessing as mp
@@ -48,8 +48,8 @@ def test_config5_batch_vs_oracle():
     sched = make_schedule(z_grid(zi, 0.0, 1e-3), run.backend.update_rates_z_threshold)
     model = run.em_cascade_model
     table = {float(z): tuple(np.asarray(a) for a in model(float(z))) for z in sched.z_window}
-    with mp.get_context("spawn").Pool(3) as pool:
-        ref, *pert = pool.map(config5_oracle, [(cols, zi, s, table) for s in (None, 0, 1)])
+    with mp.get_context("spawn").Pool(5) as pool:
+        ref, *pert = pool.map(config5_oracle, [(cols, zi, s, table) for s in (None, 0, 1, 2, 3)])
     blocks = [s.sl for s in run.spec_man.species_refs]
     rep = _check(X[:, cols], ref, pert, blocks)
     assert rep["worst_on_stable_bins"] <= TOL, rep

@@ -56,7 +56,7 @@ def _per_bin(x, ref, blocks):
 
 def _check(gpu, ref, perturbed, blocks):
     err, sup = _per_bin(gpu, ref, blocks)
-    spread = np.maximum(*[_per_bin(p, ref, blocks)[0] for p in perturbed])
+    spread = np.max([_per_bin(p, ref, blocks)[0] for p in perturbed], axis=0)
     stable = sup & (spread <= TOL)
     shaky = sup & ~stable
     worst_stable = float(err[stable].max()) if stable.any() else 0.0
