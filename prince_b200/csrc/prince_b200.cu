@@ -188,7 +188,7 @@ struct pb_context {
   bool have_em = false;
   int32_t em_n = 0, em_ncr = 0, em_nbh = 0, em_W = 0;
   int64_t em_g = -1, em_m = -1, em_p = -1;
-  DBuf em_bh_off, em_bh_A, em_invE, em_dE, em_Tg, em_Te, em_R;
+  DBuf em_bh_off, em_bh_A, em_invE, em_dE, em_Tg, em_Te, em_R, em_wbuf;
   std::vector<double> em_dl;
 
   // transposed constant operators (adjoint)
@@ -1817,7 +1817,46 @@ struct EmParams {
   const double* Te;               // n_em x n_em
   const double* R;                // n_em x n_cr
   double* X;
+  double* w;                      // n_cr x ld: Bethe-Heitler pair weights (forward) or their adjoint
 };
+
+// w[i][k] = sum_s cw_si X[s, i][k] over the charged nuclei in species order, with
+// cw_si = A_s kappa_pair dl_step / E_i dE_i: the Bethe-Heitler pair weights of the
+// hook (propagation.py:640-661).  A warp per (bin, 32-column tile), so the
+// nuclear state is read by many warps at once.
+__global__ void __launch_bounds__(256) k_em_w(EmParams e) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int i = blockIdx.x * 8 + wid;
+  if (i >= e.n_cr) return;
+  const int k = blockIdx.y * 32 + lane;
+  const bool active = k < e.ncols;
+  const int kk = active ? k : 0;
+  double acc = 0.0;
+#pragma unroll 8
+  for (int s = 0; s < e.n_bh; ++s) {
+    const int64_t row = e.bh_off[s] + i;
+    const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(e.bh_A[s], e.kp[row]), e.dl_step), e.invE[i]), e.dE[i]);
+    const double term = __dmul_rn(cw, e.X[(size_t)row * e.ld + kk]);
+    acc = (s == 0) ? term : __dadd_rn(acc, term);
+  }
+  if (active) e.w[(size_t)i * e.ld + k] = acc;
+}
+
+// Adjoint of the pair weights: X[s, i][k] += cw_si lw[i][k] (e.X = lam, e.w = lw).
+__global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int i = blockIdx.x * 8 + wid;
+  if (i >= e.n_cr) return;
+  const int k = blockIdx.y * 32 + lane;
+  if (k >= e.ncols) return;
+  const double l = e.w[(size_t)i * e.ld + k];
+#pragma unroll 8
+  for (int s = 0; s < e.n_bh; ++s) {
+    const int64_t row = e.bh_off[s] + i;
+    const double cw = e.bh_A[s] * e.kp[row] * e.dl_step * e.invE[i] * e.dE[i];
+    e.X[(size_t)row * e.ld + k] += cw * l;
+  }
+}
 
 __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
   extern __shared__ double sm[];
@@ -1825,19 +1864,10 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
   const int k = blockIdx.x * 32 + lane;
   const bool active = k < e.ncols;
   const int kk = active ? k : 0;
-  double* wv = sm;                       // n_cr x 32
+  double* wv = sm;                       // n_cr x 32: the pair weights from k_em_w
   double* gam = wv + (size_t)e.n_cr * 32;  // n_em x 32
   double* lep = gam + (size_t)e.n_em * 32; // n_em x 32
-  for (int i = wid; i < e.n_cr; i += nw) {
-    double acc = 0.0;
-    for (int s = 0; s < e.n_bh; ++s) {
-      const int64_t row = e.bh_off[s] + i;
-      const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(e.bh_A[s], e.kp[row]), e.dl_step), e.invE[i]), e.dE[i]);
-      const double term = __dmul_rn(cw, e.X[(size_t)row * e.ld + kk]);
-      acc = (s == 0) ? term : __dadd_rn(acc, term);
-    }
-    wv[i * 32 + lane] = acc;
-  }
+  for (int i = wid; i < e.n_cr; i += nw) wv[i * 32 + lane] = e.w[(size_t)i * e.ld + kk];
   for (int j = wid; j < e.n_em; j += nw) gam[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
   __syncthreads();
   for (int j = wid; j < e.n_em; j += nw) {
@@ -1867,7 +1897,8 @@ __global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
 // after the hook (e.X = lam), for the step's window.  With l = (e- + es) + (e+ + es),
 // es = R w and w_i = sum_s cw_si X_si, the hook maps gamma <- Tg gamma + Te l and
 // e+- <- 0, so before it: lam_gamma <- Tg^T lam_gamma, lam_e+- <- Te^T lam_gamma,
-// and lam_si += cw_si (n_lep R^T Te^T lam_gamma)_i on the charged nuclei.
+// and lam_si += cw_si lw_i on the charged nuclei (k_em_wT) with
+// lw = n_lep R^T Te^T lam_gamma written to e.w here.
 __global__ void __launch_bounds__(256) k_em_hookT(EmParams e) {
   extern __shared__ double sm[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -1876,7 +1907,6 @@ __global__ void __launch_bounds__(256) k_em_hookT(EmParams e) {
   const int kk = active ? k : 0;
   double* lg = sm;                          // n_em x 32: lam_gamma after the hook
   double* ml = lg + (size_t)e.n_em * 32;    // n_em x 32: Te^T lam_gamma
-  double* lw = ml + (size_t)e.n_em * 32;    // n_cr x 32: lam of w
   for (int j = wid; j < e.n_em; j += nw) lg[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
   __syncthreads();
   for (int i = wid; i < e.n_em; i += nw) {
@@ -1898,16 +1928,8 @@ __global__ void __launch_bounds__(256) k_em_hookT(EmParams e) {
   for (int i = wid; i < e.n_cr; i += nw) {
     double acc = 0.0;
     for (int j = 0; j < e.n_em; ++j) acc += e.R[(size_t)j * e.n_cr + i] * ml[j * 32 + lane];
-    lw[i * 32 + lane] = nl * acc;
+    if (active) e.w[(size_t)i * e.ld + k] = nl * acc;  // k_em_wT adds cw lw to the nuclei
   }
-  __syncthreads();
-  if (!active) return;
-  for (int i = wid; i < e.n_cr; i += nw)
-    for (int s = 0; s < e.n_bh; ++s) {
-      const int64_t row = e.bh_off[s] + i;
-      const double cw = e.bh_A[s] * e.kp[row] * e.dl_step * e.invE[i] * e.dE[i];
-      e.X[(size_t)row * e.ld + k] += cw * lw[i * 32 + lane];
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2572,7 +2594,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->X, &c->A, &c->F, &c->rowf, &c->scan_tmp, &c->seg_cb, &c->seg_ce, &c->seg_lr, &c->lr_seg0, &c->lr_nseg,
           &c->seg_mb, &c->seg_me, &c->partial, &c->counter, &c->dt_indptr, &c->dt_indices, &c->dt_vals,
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
-          &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R,
+          &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R, &c->em_wbuf,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
@@ -2778,8 +2800,26 @@ bool use_blocked(const pb_context* c, int K) {
 int band_grid(const pb_context* c, StepParams& p, int nw) {
   const int cblocks = (int)blocks_for(p.ncols, 8 * nw);
   const int per = cblocks * std::max(c->band_npairs, 1);
-  const int want = nw == 4 ? c->num_sms / per : (c->num_sms + per - 1) / per;
-  const int G = std::max(1, std::min({want, kMaxBandGroups, p.nsp}));
+  int G;
+  if (nw == 4) {
+    G = std::max(1, std::min({c->num_sms / per, kMaxBandGroups, p.nsp}));
+  } else {
+    // One CTA per SM: the launch takes ceil(CTAs / SMs) waves of CTAs that each
+    // walk ceil(nsp / G) mother species, so pick the G with the fewest
+    // waves x species, the smaller on ties; beyond one wave's worth of groups
+    // at most 16 (the partial sums grow with G x columns).
+    const int gmax = std::min({kMaxBandGroups, p.nsp, std::max(16, c->num_sms / per)});
+    G = 1;
+    int64_t best = -1;
+    for (int g = 1; g <= gmax; ++g) {
+      const int64_t waves = ((int64_t)per * g + c->num_sms - 1) / c->num_sms;
+      const int64_t cost = waves * ((p.nsp + g - 1) / g);
+      if (best < 0 || cost < best) {
+        best = cost;
+        G = g;
+      }
+    }
+  }
   p.spg = (p.nsp + G - 1) / G;
   p.ngroups = (p.nsp + p.spg - 1) / p.spg;
   return cblocks;
@@ -2882,6 +2922,7 @@ EmParams em_params(const pb_context* c, int w, int ld, int ncols, double* X) {
   e.Te = c->em_Te.as<double>() + (size_t)w * c->em_n * c->em_n;
   e.R = c->em_R.as<double>() + (size_t)w * c->em_n * c->em_ncr;
   e.X = X;
+  e.w = c->em_wbuf.as<double>();
   return e;
 }
 
@@ -2932,8 +2973,9 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
     }
     if (c->have_em && (p.flags & PB_EM_CASCADE)) {
       const EmParams e = em_params(c, c->h_win[k], p.ld, p.ncols, X);
+      k_em_w<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(p.ncols, 32)), 256, 0, st>>>(e);
       k_em_hook<<<blocks_for(p.ncols, 32), 256, em_smem(c), st>>>(e);
-      ++launches;
+      launches += 2;
     }
   }
   return launches;
@@ -4298,6 +4340,8 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->X.ensure(sbytes));
   PB_CUDA(c, c->A.ensure(sbytes));
   PB_CUDA(c, c->F.ensure(sbytes));
+  if ((flags & PB_EM_CASCADE) && c->have_em)
+    PB_CUDA(c, c->em_wbuf.ensure((size_t)c->em_ncr * ld * sizeof(double)));
   PB_CUDA(c, c->rowf.ensure((size_t)8 * n * sizeof(double)));
   const int ctiles = ld / (K == 1 ? 1 : kColTile);
   const int nlong_rows = (int)c->h_long_rows.size();
@@ -4774,6 +4818,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
         if (em) {  // the hook after step k, transposed, before the step's adjoint
           const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
           k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
+          k_em_wT<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(q.ncols, 32)), 256, 0, st>>>(e);
         }
         if (k == k1 - 1 || em)  // v1 of the segment's last step; later steps get it from stage 2
           k_adj_v1<<<dim3(blocks_for(n, 8), blocks_for(q.ncols, kColTile)), 256, 0, st>>>(
@@ -4861,6 +4906,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
       if (em) {  // the hook after step k, transposed, before the step's adjoint
         const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
         k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
+        k_em_wT<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(q.ncols, 32)), 256, 0, st>>>(e);
       }
       dim3 grid(blocks_for(n, 8), K == 1 ? 1u : blocks_for(q.ncols, kColTile));
       k_adj<1><<<grid, 256, 0, st>>>(q);

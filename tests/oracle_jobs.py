@@ -42,7 +42,7 @@ def config5_oracle(args):
     """One oracle solve of the coupled-EM network (decoupled 128-bin EM grid) in a
     spawned process; ``em_table`` maps each window's redshift to the device-built
     (T_gamma, T_electron, R_BH) the GPU solve used."""
-    cols, zi, seed, em_table = args
+    cols, zi, seed, em_table, size = args
     import os
     import sys
 
@@ -61,7 +61,7 @@ def config5_oracle(args):
                     enable_em_cascade=True, enable_em_decoupled_grid=True, em_grid=EM_GRID)
     pts = draw_points(run, 2048, seed=5000, z_range=(0.5, 4.0))
     srcs = [[point_source(run, pts[k])] for k in cols]
-    perturb = None if seed is None else (PERTURB, seed)
+    perturb = None if seed is None else (size, seed)
 
     def em(z):
         return em_table[float(z)]
