@@ -182,9 +182,22 @@ def run_b200(args, dist, rank, ws, local):
     solver = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=args.points, device=local)
     for k, p in enumerate(pts):
         solver[k].add_source_class(point_source(run, p))
+    tuned = None
     if args.band_warps:
         from prince_b200 import _lib
         solver._dev.ctx.set_option(_lib.PB_OPT_BAND_WARPS, args.band_warps)
+    elif args.autotune:
+        import tempfile
+        from prince_b200 import autotune
+        # a fresh search on this box (a scratch cache), reported beside the line
+        with tempfile.TemporaryDirectory() as tdir:
+            choice, cands = autotune.tune(solver, path=os.path.join(tdir, "autotune.json"), force=True)
+        default = next((c for c in cands if c["band_warps"] == 8 and c["slab_prefetch"] == 3
+                        and c["tma_staging"] == 1), None)
+        tuned = {"choice": {k: choice[k] for k in ("band_warps", "slab_prefetch", "tma_staging")},
+                 "tuned_steps_ms": choice["steps_ms"],
+                 "default_steps_ms": default["steps_ms"] if default else None,
+                 "candidates": len(cands), "search": "16 fully active steps per candidate, fastest of 3"}
 
     for _ in range(args.warmup):
         solver.solve(dz=1e-3)
@@ -282,6 +295,8 @@ def run_b200(args, dist, rank, ws, local):
         adj["adjoint_over_forward"] = adj["adjoint_s"] / fwd_wall
         adj["gradient_over_forward"] = adj["gradient_s"] / fwd_wall
         line["adjoint"] = adj
+    if tuned:
+        line["autotune"] = tuned
     if cfg5:
         line["config5"] = cfg5
     if clk:
@@ -548,6 +563,7 @@ def main():
     ap.add_argument("--adjoint", type=int, default=1, help="also time the adjoint gradient (1/0)")
     ap.add_argument("--config5", type=int, default=1,
                     help="also time the coupled EM cascade workload, forward and gradient (1/0)")
+    ap.add_argument("--autotune", type=int, default=1, help="search the stage's tile choices before timing (1/0)")
     ap.add_argument("--band-warps", type=int, default=0, choices=[0, 4, 8],
                     help="warps of a band-tile CTA (0: the library default)")
     ap.add_argument("--z-range", default="0.5,1.0",

@@ -63,6 +63,12 @@ def get_AZN(pdg_id: int):
     return A, Z, A - Z
 
 
+def is_decoupled(spec_man):
+    """True when some species of a species manager (this package's or the
+    reference's) live on a home grid other than the default one."""
+    return any(getattr(s, "grid_tag", "default") != "default" for s in spec_man.species_refs)
+
+
 class EnergyGrid:
     """Log-spaced bins: ``bins`` (edges), ``grid`` (centres), ``widths``, ``d``.
 
@@ -179,4 +185,4 @@ class SpeciesManager:
     @property
     def decoupled(self):
         """True when some species live on a grid other than the default one."""
-        return any(s.grid_tag != "default" for s in self.species_refs)
+        return is_decoupled(self)

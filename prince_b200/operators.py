@@ -20,6 +20,8 @@ from __future__ import annotations
 import numpy as np
 import scipy.sparse as sp
 
+from .data import is_decoupled
+
 # (first row, column offsets, integer weights, denominator) per stencil class.
 _EDGE0 = ((1, 2, 3), (-3, 4, -1), 2.0)
 _EDGE12 = ((-1, 0, 1, 2), (-2, -3, 6, -1), 6.0)
@@ -63,7 +65,7 @@ def run_fd_loss_operator(run):
     """The run's FD loss operator: one block per species on its home grid, in
     ``princeidx`` order (``partial_diff.py:28-46``, heterogeneous path)."""
     sm = run.spec_man
-    if not sm.decoupled:
+    if not is_decoupled(sm):
         return fd_loss_operator(run.cr_grid, sm.nspec)
     cache = {}
     blocks = []

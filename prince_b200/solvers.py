@@ -19,6 +19,8 @@ import time
 import numpy as np
 import scipy.sparse as sp
 
+from .data import is_decoupled
+
 from . import _lib
 from . import constants as C
 from .cosmology import H as _H
@@ -49,7 +51,7 @@ def device_order(run):
     bins, the layout of the bin-blocked kernels.
     """
     sm = run.spec_man
-    if not sm.decoupled:
+    if not is_decoupled(sm):
         return None, run.dim_states
     refs = sorted(sm.species_refs, key=lambda x: x.princeidx)
     blocks = [s for s in refs if s.grid_tag == "default"]
