@@ -188,7 +188,8 @@ struct pb_context {
   bool have_em = false;
   int32_t em_n = 0, em_ncr = 0, em_nbh = 0, em_W = 0;
   int64_t em_g = -1, em_m = -1, em_p = -1;
-  DBuf em_bh_off, em_bh_A, em_invE, em_dE, em_Tg, em_Te, em_R, em_wbuf;
+  DBuf em_bh_off, em_bh_A, em_invE, em_dE, em_Tg, em_Te, em_R, em_wbuf, em_es, em_lep, em_y;
+  DBuf em_TgT, em_TeT, em_RT;       // per-window transposes (adjoint)
   std::vector<double> em_dl;
 
   // transposed constant operators (adjoint)
@@ -222,6 +223,10 @@ int fail(pb_context* c, int code, const char* fmt, ...) {
   va_end(ap);
   if (c) c->err = buf; else g_error = buf;
   return code;
+}
+
+unsigned blocks_for(int64_t work, int per_block) {
+  return (unsigned)((work + per_block - 1) / per_block);
 }
 
 #define PB_CUDA(ctx, call)                                                              \
@@ -1801,6 +1806,13 @@ BandInstance band_kernel(int RT, int J, int nw = 8) {
 //   gamma <- T_gamma gamma + T_electron (e- + e+),   e+- <- 0
 // One CTA per 32-column tile (lane = column), the per-column vectors in shared memory.
 // ---------------------------------------------------------------------------
+}  // namespace
+
+// batched FP64 GEMM on the tensor pipe and the cascade-transfer kernels
+#include "em_transfer.cuh"
+
+namespace {
+
 struct EmParams {
   int64_t n;
   int ld;
@@ -1818,7 +1830,52 @@ struct EmParams {
   const double* R;                // n_em x n_cr
   double* X;
   double* w;                      // n_cr x ld: Bethe-Heitler pair weights (forward) or their adjoint
+  double* es;                     // n_em x ld: R w (forward) or Te^T lam_gamma (adjoint)
+  double* lep;                    // n_em x ld: e- + e+ with the pairs (forward)
+  double* y;                      // n_em x ld: the new gamma rows (forward) or Tg^T lam_gamma (adjoint)
+  const double* TgT;              // transposes of the window's matrices (adjoint)
+  const double* TeT;
+  const double* RT;               // n_cr x n_em
 };
+
+// l = (e- + es) + (e+ + es) with es = R w, then e+- <- 0 (the lepton half of the hook).
+__global__ void k_em_lep(EmParams e) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)e.n_em * e.ncols) return;
+  const int j = (int)(t / e.ncols), k = (int)(t % e.ncols);
+  const double es = e.es[(size_t)j * e.ld + k];
+  double l = 0.0;
+  if (e.em_off >= 0) {
+    double* x = e.X + (size_t)(e.em_off + j) * e.ld + k;
+    l = __dadd_rn(l, __dadd_rn(*x, es));
+    *x = 0.0;
+  }
+  if (e.ep_off >= 0) {
+    double* x = e.X + (size_t)(e.ep_off + j) * e.ld + k;
+    l = __dadd_rn(l, __dadd_rn(*x, es));
+    *x = 0.0;
+  }
+  e.lep[(size_t)j * e.ld + k] = l;
+}
+
+// Adjoint lepton rows: lam_e+- <- Te^T lam_gamma (e.es), and lw = n_lep R^T (that) is a GEMM after.
+__global__ void k_em_lepT(EmParams e) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)e.n_em * e.ncols) return;
+  const int j = (int)(t / e.ncols), k = (int)(t % e.ncols);
+  const double m = e.es[(size_t)j * e.ld + k];
+  if (e.em_off >= 0) e.X[(size_t)(e.em_off + j) * e.ld + k] = m;
+  if (e.ep_off >= 0) e.X[(size_t)(e.ep_off + j) * e.ld + k] = m;
+}
+
+// Scales the first n_cr x ncols block of e.w by s (the lepton count of the adjoint pair weights).
+__global__ void k_em_scale_w(EmParams e, double s) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)e.n_cr * e.ncols) return;
+  const int i = (int)(t / e.ncols), k = (int)(t % e.ncols);
+  e.w[(size_t)i * e.ld + k] *= s;
+}
+
 
 // w[i][k] = sum_s cw_si X[s, i][k] over the charged nuclei in species order, with
 // cw_si = A_s kappa_pair dl_step / E_i dE_i: the Bethe-Heitler pair weights of the
@@ -1858,79 +1915,37 @@ __global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_em_hook(EmParams e) {
-  extern __shared__ double sm[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int k = blockIdx.x * 32 + lane;
-  const bool active = k < e.ncols;
-  const int kk = active ? k : 0;
-  double* wv = sm;                       // n_cr x 32: the pair weights from k_em_w
-  double* gam = wv + (size_t)e.n_cr * 32;  // n_em x 32
-  double* lep = gam + (size_t)e.n_em * 32; // n_em x 32
-  for (int i = wid; i < e.n_cr; i += nw) wv[i * 32 + lane] = e.w[(size_t)i * e.ld + kk];
-  for (int j = wid; j < e.n_em; j += nw) gam[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
-  __syncthreads();
-  for (int j = wid; j < e.n_em; j += nw) {
-    double es = 0.0;
-    for (int i = 0; i < e.n_cr; ++i) es += e.R[(size_t)j * e.n_cr + i] * wv[i * 32 + lane];
-    double l = 0.0;
-    if (e.em_off >= 0) l = __dadd_rn(l, __dadd_rn(e.X[(size_t)(e.em_off + j) * e.ld + kk], es));
-    if (e.ep_off >= 0) l = __dadd_rn(l, __dadd_rn(e.X[(size_t)(e.ep_off + j) * e.ld + kk], es));
-    lep[j * 32 + lane] = l;
-  }
-  __syncthreads();
-  for (int j = wid; j < e.n_em; j += nw) {
-    double tg = 0.0, te = 0.0;
-    for (int i = 0; i < e.n_em; ++i) {
-      tg += e.Tg[(size_t)j * e.n_em + i] * gam[i * 32 + lane];
-      te += e.Te[(size_t)j * e.n_em + i] * lep[i * 32 + lane];
-    }
-    if (active) {
-      e.X[(size_t)(e.g_off + j) * e.ld + k] = __dadd_rn(tg, te);
-      if (e.em_off >= 0) e.X[(size_t)(e.em_off + j) * e.ld + k] = 0.0;
-      if (e.ep_off >= 0) e.X[(size_t)(e.ep_off + j) * e.ld + k] = 0.0;
-    }
-  }
+// The hook after a step, on the tensor pipe where it is dense (propagation.py:555-571, 620-665):
+//   w = pair weights (k_em_w), es = R w, l = e- + e+ + 2 es (k_em_lep, e+- <- 0),
+//   y = Tg gamma + Te l, gamma <- y.
+void em_hook_forward(const EmParams& e, cudaStream_t st) {
+  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, 0, st>>>(e);
+  bgemm(st, e.R, e.w, e.es, e.n_em, e.ncols, e.n_cr, e.n_cr, e.ld, e.ld, 0, 0, 0, 1, false);
+  k_em_lep<<<(unsigned)blocks_for((int64_t)e.n_em * e.ncols, 256), 256, 0, st>>>(e);
+  double* gam = e.X + (size_t)e.g_off * e.ld;
+  bgemm(st, e.Tg, gam, e.y, e.n_em, e.ncols, e.n_em, e.n_em, e.ld, e.ld, 0, 0, 0, 1, false);
+  bgemm(st, e.Te, e.lep, e.y, e.n_em, e.ncols, e.n_em, e.n_em, e.ld, e.ld, 0, 0, 0, 1, true);
+  cudaMemcpy2DAsync(gam, (size_t)e.ld * sizeof(double), e.y, (size_t)e.ld * sizeof(double),
+                    (size_t)e.ncols * sizeof(double), (size_t)e.n_em, cudaMemcpyDeviceToDevice, st);
 }
 
-// Transpose of k_em_hook, applied in place to the adjoint state lam = dL/dX
-// after the hook (e.X = lam), for the step's window.  With l = (e- + es) + (e+ + es),
-// es = R w and w_i = sum_s cw_si X_si, the hook maps gamma <- Tg gamma + Te l and
-// e+- <- 0, so before it: lam_gamma <- Tg^T lam_gamma, lam_e+- <- Te^T lam_gamma,
-// and lam_si += cw_si lw_i on the charged nuclei (k_em_wT) with
-// lw = n_lep R^T Te^T lam_gamma written to e.w here.
-__global__ void __launch_bounds__(256) k_em_hookT(EmParams e) {
-  extern __shared__ double sm[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int k = blockIdx.x * 32 + lane;
-  const bool active = k < e.ncols;
-  const int kk = active ? k : 0;
-  double* lg = sm;                          // n_em x 32: lam_gamma after the hook
-  double* ml = lg + (size_t)e.n_em * 32;    // n_em x 32: Te^T lam_gamma
-  for (int j = wid; j < e.n_em; j += nw) lg[j * 32 + lane] = e.X[(size_t)(e.g_off + j) * e.ld + kk];
-  __syncthreads();
-  for (int i = wid; i < e.n_em; i += nw) {
-    double tg = 0.0, te = 0.0;
-    for (int j = 0; j < e.n_em; ++j) {
-      const double l = lg[j * 32 + lane];
-      tg += e.Tg[(size_t)j * e.n_em + i] * l;
-      te += e.Te[(size_t)j * e.n_em + i] * l;
-    }
-    ml[i * 32 + lane] = te;
-    if (active) {
-      e.X[(size_t)(e.g_off + i) * e.ld + k] = tg;
-      if (e.em_off >= 0) e.X[(size_t)(e.em_off + i) * e.ld + k] = te;
-      if (e.ep_off >= 0) e.X[(size_t)(e.ep_off + i) * e.ld + k] = te;
-    }
-  }
-  __syncthreads();
+// Its transpose on lam (e.X): mu = Te^T lam_gamma, lam_gamma <- Tg^T lam_gamma,
+// lam_e+- <- mu, lam_nuclei += cw (n_lep R^T mu) (k_em_wT).
+void em_hook_adjoint(const EmParams& e, cudaStream_t st) {
+  double* gam = e.X + (size_t)e.g_off * e.ld;
+  bgemm(st, e.TeT, gam, e.es, e.n_em, e.ncols, e.n_em, e.n_em, e.ld, e.ld, 0, 0, 0, 1, false);
+  bgemm(st, e.TgT, gam, e.y, e.n_em, e.ncols, e.n_em, e.n_em, e.ld, e.ld, 0, 0, 0, 1, false);
+  cudaMemcpy2DAsync(gam, (size_t)e.ld * sizeof(double), e.y, (size_t)e.ld * sizeof(double),
+                    (size_t)e.ncols * sizeof(double), (size_t)e.n_em, cudaMemcpyDeviceToDevice, st);
+  k_em_lepT<<<(unsigned)blocks_for((int64_t)e.n_em * e.ncols, 256), 256, 0, st>>>(e);
+  bgemm(st, e.RT, e.es, e.w, e.n_cr, e.ncols, e.n_em, e.n_em, e.ld, e.ld, 0, 0, 0, 1, false);
   const double nl = (double)((e.em_off >= 0) + (e.ep_off >= 0));
-  for (int i = wid; i < e.n_cr; i += nw) {
-    double acc = 0.0;
-    for (int j = 0; j < e.n_em; ++j) acc += e.R[(size_t)j * e.n_cr + i] * ml[j * 32 + lane];
-    if (active) e.w[(size_t)i * e.ld + k] = nl * acc;  // k_em_wT adds cw lw to the nuclei
-  }
+  if (nl != 1.0)
+    k_em_scale_w<<<(unsigned)blocks_for((int64_t)e.n_cr * e.ncols, 256), 256, 0, st>>>(e, nl);
+  k_em_wT<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, 0, st>>>(e);
 }
+
+
 
 // ---------------------------------------------------------------------------
 // Bin-blocked adjoint sweep.  One backward step applies A^T twice (stage 1 to
@@ -2595,6 +2610,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->seg_mb, &c->seg_me, &c->partial, &c->counter, &c->dt_indptr, &c->dt_indices, &c->dt_vals,
           &c->lt_indptr, &c->lt_indices, &c->lt_vals, &c->inj_rows, &c->src_col_d, &c->ckpt,
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R, &c->em_wbuf,
+          &c->em_es, &c->em_lep, &c->em_y, &c->em_TgT, &c->em_TeT, &c->em_RT,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
           &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
@@ -2627,10 +2643,6 @@ void csr_transpose(int64_t n, int64_t nnz, const int64_t* ip, const int32_t* ix,
       tix[t] = (int32_t)r;
       tv[t] = v[j];
     }
-}
-
-unsigned blocks_for(int64_t work, int per_block) {
-  return (unsigned)((work + per_block - 1) / per_block);
 }
 
 
@@ -2923,10 +2935,15 @@ EmParams em_params(const pb_context* c, int w, int ld, int ncols, double* X) {
   e.R = c->em_R.as<double>() + (size_t)w * c->em_n * c->em_ncr;
   e.X = X;
   e.w = c->em_wbuf.as<double>();
+  e.es = c->em_es.as<double>();
+  e.lep = c->em_lep.as<double>();
+  e.y = c->em_y.as<double>();
+  e.TgT = c->em_TgT.as<double>() + (size_t)w * c->em_n * c->em_n;
+  e.TeT = c->em_TeT.as<double>() + (size_t)w * c->em_n * c->em_n;
+  e.RT = c->em_RT.as<double>() + (size_t)w * c->em_n * c->em_ncr;
   return e;
 }
 
-size_t em_smem(const pb_context* c) { return (size_t)(c->em_ncr + 2 * c->em_n) * 32 * sizeof(double); }
 
 // Enqueue the ETD2 steps [k0, k1) on `st`.  Columns [0, n_active[k]) are
 // advanced at step k; a step without active columns is skipped (every column
@@ -2972,10 +2989,8 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       ++launches;
     }
     if (c->have_em && (p.flags & PB_EM_CASCADE)) {
-      const EmParams e = em_params(c, c->h_win[k], p.ld, p.ncols, X);
-      k_em_w<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(p.ncols, 32)), 256, 0, st>>>(e);
-      k_em_hook<<<blocks_for(p.ncols, 32), 256, em_smem(c), st>>>(e);
-      launches += 2;
+      em_hook_forward(em_params(c, c->h_win[k], p.ld, p.ncols, X), st);
+      launches += 5;
     }
   }
   return launches;
@@ -2986,7 +3001,6 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
 // ===========================================================================
 // C ABI
 // ===========================================================================
-#include "em_transfer.cuh"
 
 extern "C" {
 
@@ -3027,15 +3041,6 @@ int pb_create(int device, pb_context** out) {
   if (e != cudaSuccess) {
     pb_destroy(c);
     return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_fold_gemm): %s", cudaGetErrorString(e));
-  }
-  e = cudaFuncSetAttribute(k_em_hook, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           3 * kMaxEmBins * 32 * (int)sizeof(double));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_em_hookT, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             3 * kMaxEmBins * 32 * (int)sizeof(double));
-  if (e != cudaSuccess) {
-    pb_destroy(c);
-    return fail(nullptr, PB_ERR_CUDA, "cudaFuncSetAttribute(k_em_hook): %s", cudaGetErrorString(e));
   }
   *out = c;
   return PB_OK;
@@ -4003,10 +4008,25 @@ int pb_set_em_windows(pb_context* c, int32_t n_windows, const double* Tg, const 
   if (n_windows < 1 || !Tg || !Te || !R || !dl_step) return fail(c, PB_ERR_ARG, "pb_set_em_windows: bad arguments");
   int rc = set_device(c);
   if (rc) return rc;
-  const size_t nn = (size_t)c->em_n * c->em_n;
+  const size_t nn = (size_t)c->em_n * c->em_n, nr = (size_t)c->em_n * c->em_ncr;
   if ((rc = upload(c, c->em_Tg, Tg, nn * n_windows))) return rc;
   if ((rc = upload(c, c->em_Te, Te, nn * n_windows))) return rc;
-  if ((rc = upload(c, c->em_R, R, (size_t)c->em_n * c->em_ncr * n_windows))) return rc;
+  if ((rc = upload(c, c->em_R, R, nr * n_windows))) return rc;
+  {  // transposes for the adjoint's GEMMs
+    std::vector<double> tg(nn * n_windows), te(nn * n_windows), rt(nr * n_windows);
+    const int m = c->em_n, q = c->em_ncr;
+    for (int32_t w = 0; w < n_windows; ++w)
+      for (int i = 0; i < m; ++i) {
+        for (int j = 0; j < m; ++j) {
+          tg[w * nn + (size_t)j * m + i] = Tg[w * nn + (size_t)i * m + j];
+          te[w * nn + (size_t)j * m + i] = Te[w * nn + (size_t)i * m + j];
+        }
+        for (int j = 0; j < q; ++j) rt[w * nr + (size_t)j * m + i] = R[w * nr + (size_t)i * q + j];
+      }
+    if ((rc = upload(c, c->em_TgT, tg.data(), tg.size()))) return rc;
+    if ((rc = upload(c, c->em_TeT, te.data(), te.size()))) return rc;
+    if ((rc = upload(c, c->em_RT, rt.data(), rt.size()))) return rc;
+  }
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   c->em_dl.assign(dl_step, dl_step + n_windows);
   c->em_W = n_windows;
@@ -4340,8 +4360,10 @@ int pb_solve(pb_context* c, const pb_solve_args* a) {
   PB_CUDA(c, c->X.ensure(sbytes));
   PB_CUDA(c, c->A.ensure(sbytes));
   PB_CUDA(c, c->F.ensure(sbytes));
-  if ((flags & PB_EM_CASCADE) && c->have_em)
+  if ((flags & PB_EM_CASCADE) && c->have_em) {
     PB_CUDA(c, c->em_wbuf.ensure((size_t)c->em_ncr * ld * sizeof(double)));
+    for (DBuf* b : {&c->em_es, &c->em_lep, &c->em_y}) PB_CUDA(c, b->ensure((size_t)c->em_n * ld * sizeof(double)));
+  }
   PB_CUDA(c, c->rowf.ensure((size_t)8 * n * sizeof(double)));
   const int ctiles = ld / (K == 1 ? 1 : kColTile);
   const int nlong_rows = (int)c->h_long_rows.size();
@@ -4815,11 +4837,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
           q.inj_slot = c->inj_slot.as<int>();
           q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
         }
-        if (em) {  // the hook after step k, transposed, before the step's adjoint
-          const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
-          k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
-          k_em_wT<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(q.ncols, 32)), 256, 0, st>>>(e);
-        }
+        if (em) em_hook_adjoint(em_params(c, a->window[k], ld, q.ncols, lam), st);  // the hook after step k
         if (k == k1 - 1 || em)  // v1 of the segment's last step; later steps get it from stage 2
           k_adj_v1<<<dim3(blocks_for(n, 8), blocks_for(q.ncols, kColTile)), 256, 0, st>>>(
               q.rf + 2 * n, lam, n, ld, q.ncols, c->vbuf.as<double>());
@@ -4903,11 +4921,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
         q.inj_slot = c->inj_slot.as<int>();
         q.gb_inj = c->gb_inj.as<double>() + (size_t)k * n_inj * ld;
       }
-      if (em) {  // the hook after step k, transposed, before the step's adjoint
-        const EmParams e = em_params(c, a->window[k], ld, q.ncols, lam);
-        k_em_hookT<<<blocks_for(q.ncols, 32), 256, em_smem(c), st>>>(e);
-        k_em_wT<<<dim3(blocks_for(c->em_ncr, 8), blocks_for(q.ncols, 32)), 256, 0, st>>>(e);
-      }
+      if (em) em_hook_adjoint(em_params(c, a->window[k], ld, q.ncols, lam), st);  // the hook after step k
       dim3 grid(blocks_for(n, 8), K == 1 ? 1u : blocks_for(q.ncols, kColTile));
       k_adj<1><<<grid, 256, 0, st>>>(q);
       k_adj<2><<<grid, 256, 0, st>>>(q);
