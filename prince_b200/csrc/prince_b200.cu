@@ -46,7 +46,8 @@ constexpr int kLongRow = 256;      // rows with more coupling entries are cut in
 constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
 constexpr int kColTile = 32;       // state columns per warp in the batched step
 constexpr int kSegLen = 256;       // coupling entries per long-row segment
-constexpr int kMaxEmBins = 160;    // EM / nucleon bins of the cascade hook (shared-memory tiles)
+constexpr int kMaxEmBins = 160;    // EM / nucleon bins of the cascade hook
+constexpr int kMaxBhSpecies = 3072;  // charged nuclei of the hook's pair weights (their table in shared memory)
 
 thread_local std::string g_error;
 
@@ -1880,38 +1881,84 @@ __global__ void k_em_scale_w(EmParams e, double s) {
 // w[i][k] = sum_s cw_si X[s, i][k] over the charged nuclei in species order, with
 // cw_si = A_s kappa_pair dl_step / E_i dE_i: the Bethe-Heitler pair weights of the
 // hook (propagation.py:640-661).  A warp per (bin, 32-column tile), so the
-// nuclear state is read by many warps at once.
+// nuclear state is read by many warps at once; the species table sits in
+// shared memory and each warp loads kEmWBatch species' states ahead of the
+// (ordered) sum.
+constexpr int kEmWBatch = 16;
+
 __global__ void __launch_bounds__(256) k_em_w(EmParams e) {
+  extern __shared__ unsigned char em_w_smem[];
+  int64_t* soff = reinterpret_cast<int64_t*>(em_w_smem);
+  double* sA = reinterpret_cast<double*>(soff + e.n_bh);
+  for (int t = threadIdx.x; t < e.n_bh; t += blockDim.x) {
+    soff[t] = e.bh_off[t];
+    sA[t] = e.bh_A[t];
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int i = blockIdx.x * 8 + wid;
   if (i >= e.n_cr) return;
   const int k = blockIdx.y * 32 + lane;
   const bool active = k < e.ncols;
   const int kk = active ? k : 0;
+  const double ie = e.invE[i], de = e.dE[i];
   double acc = 0.0;
-#pragma unroll 8
-  for (int s = 0; s < e.n_bh; ++s) {
-    const int64_t row = e.bh_off[s] + i;
-    const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(e.bh_A[s], e.kp[row]), e.dl_step), e.invE[i]), e.dE[i]);
-    const double term = __dmul_rn(cw, e.X[(size_t)row * e.ld + kk]);
-    acc = (s == 0) ? term : __dadd_rn(acc, term);
+  for (int s0 = 0; s0 < e.n_bh; s0 += kEmWBatch) {
+    double xv[kEmWBatch], kv[kEmWBatch];
+#pragma unroll
+    for (int u = 0; u < kEmWBatch; ++u) {
+      xv[u] = 0.0;
+      kv[u] = 0.0;
+      if (s0 + u < e.n_bh) {
+        const int64_t row = soff[s0 + u] + i;
+        xv[u] = __ldg(e.X + (size_t)row * e.ld + kk);
+        kv[u] = __ldg(e.kp + row);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kEmWBatch; ++u) {
+      const int s = s0 + u;
+      if (s < e.n_bh) {
+        const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(sA[s], kv[u]), e.dl_step), ie), de);
+        const double term = __dmul_rn(cw, xv[u]);
+        acc = (s == 0) ? term : __dadd_rn(acc, term);
+      }
+    }
   }
   if (active) e.w[(size_t)i * e.ld + k] = acc;
 }
 
 // Adjoint of the pair weights: X[s, i][k] += cw_si lw[i][k] (e.X = lam, e.w = lw).
 __global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
+  extern __shared__ unsigned char em_w_smem[];
+  int64_t* soff = reinterpret_cast<int64_t*>(em_w_smem);
+  double* sA = reinterpret_cast<double*>(soff + e.n_bh);
+  for (int t = threadIdx.x; t < e.n_bh; t += blockDim.x) {
+    soff[t] = e.bh_off[t];
+    sA[t] = e.bh_A[t];
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int i = blockIdx.x * 8 + wid;
   if (i >= e.n_cr) return;
   const int k = blockIdx.y * 32 + lane;
   if (k >= e.ncols) return;
-  const double l = e.w[(size_t)i * e.ld + k];
-#pragma unroll 8
-  for (int s = 0; s < e.n_bh; ++s) {
-    const int64_t row = e.bh_off[s] + i;
-    const double cw = e.bh_A[s] * e.kp[row] * e.dl_step * e.invE[i] * e.dE[i];
-    e.X[(size_t)row * e.ld + k] += cw * l;
+  const double l = e.w[(size_t)i * e.ld + k] * e.dl_step * e.invE[i] * e.dE[i];
+  for (int s0 = 0; s0 < e.n_bh; s0 += kEmWBatch) {
+    double xv[kEmWBatch], kv[kEmWBatch];
+#pragma unroll
+    for (int u = 0; u < kEmWBatch; ++u)
+      if (s0 + u < e.n_bh) {
+        const int64_t row = soff[s0 + u] + i;
+        xv[u] = e.X[(size_t)row * e.ld + k];
+        kv[u] = __ldg(e.kp + row);
+      }
+#pragma unroll
+    for (int u = 0; u < kEmWBatch; ++u)
+      if (s0 + u < e.n_bh) {
+        const int64_t row = soff[s0 + u] + i;
+        e.X[(size_t)row * e.ld + k] = xv[u] + sA[s0 + u] * kv[u] * l;
+      }
   }
 }
 
@@ -1919,7 +1966,8 @@ __global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
 //   w = pair weights (k_em_w), es = R w, l = e- + e+ + 2 es (k_em_lep, e+- <- 0),
 //   y = Tg gamma + Te l, gamma <- y.
 void em_hook_forward(const EmParams& e, cudaStream_t st) {
-  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, 0, st>>>(e);
+  const size_t wsm = (size_t)e.n_bh * (sizeof(int64_t) + sizeof(double));
+  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, wsm, st>>>(e);
   bgemm(st, e.R, e.w, e.es, e.n_em, e.ncols, e.n_cr, e.n_cr, e.ld, e.ld, 0, 0, 0, 1, false);
   k_em_lep<<<(unsigned)blocks_for((int64_t)e.n_em * e.ncols, 256), 256, 0, st>>>(e);
   double* gam = e.X + (size_t)e.g_off * e.ld;
@@ -1942,7 +1990,8 @@ void em_hook_adjoint(const EmParams& e, cudaStream_t st) {
   const double nl = (double)((e.em_off >= 0) + (e.ep_off >= 0));
   if (nl != 1.0)
     k_em_scale_w<<<(unsigned)blocks_for((int64_t)e.n_cr * e.ncols, 256), 256, 0, st>>>(e, nl);
-  k_em_wT<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, 0, st>>>(e);
+  const size_t wsm = (size_t)e.n_bh * (sizeof(int64_t) + sizeof(double));
+  k_em_wT<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, wsm, st>>>(e);
 }
 
 
@@ -3975,9 +4024,10 @@ int pb_set_em(pb_context* c, int32_t n_em, int64_t gamma_off, int64_t em_off, in
               int32_t n_bh, const int64_t* bh_off, const double* bh_A, const double* inv_E, const double* dE) {
   if (!c) return fail(nullptr, PB_ERR_ARG, "context is NULL");
   if (!c->have_coupling) return fail(c, PB_ERR_STATE, "pb_set_em: set the coupling pattern first");
-  if (n_em < 1 || n_em > kMaxEmBins || n_cr < 1 || n_cr > kMaxEmBins || n_bh < 0 || (n_bh > 0 && (!bh_off || !bh_A)) ||
-      !inv_E || !dE)
-    return fail(c, PB_ERR_ARG, "pb_set_em: bad arguments (bins must be in [1, %d])", kMaxEmBins);
+  if (n_em < 1 || n_em > kMaxEmBins || n_cr < 1 || n_cr > kMaxEmBins || n_bh < 0 || n_bh > kMaxBhSpecies ||
+      (n_bh > 0 && (!bh_off || !bh_A)) || !inv_E || !dE)
+    return fail(c, PB_ERR_ARG, "pb_set_em: bad arguments (bins must be in [1, %d], at most %d nuclei)", kMaxEmBins,
+                kMaxBhSpecies);
   if (gamma_off < 0 || gamma_off + n_em > c->n) return fail(c, PB_ERR_ARG, "pb_set_em: gamma block out of range");
   for (int64_t off : {em_off, ep_off})
     if (off >= 0 && off + n_em > c->n) return fail(c, PB_ERR_ARG, "pb_set_em: lepton block out of range");
