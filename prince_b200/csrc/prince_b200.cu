@@ -1880,13 +1880,13 @@ __global__ void k_em_scale_w(EmParams e, double s) {
 
 // w[i][k] = sum_s cw_si X[s, i][k] over the charged nuclei in species order, with
 // cw_si = A_s kappa_pair dl_step / E_i dE_i: the Bethe-Heitler pair weights of the
-// hook (propagation.py:640-661).  A warp per (bin, 32-column tile), so the
-// nuclear state is read by many warps at once; the species table sits in
-// shared memory and each warp loads kEmWBatch species' states ahead of the
-// (ordered) sum.
-constexpr int kEmWBatch = 16;
+// hook (propagation.py:640-661).  A warp per (bin, 64-column tile), each lane
+// two adjacent columns (16-byte loads), so the nuclear state is read by many
+// warps at once; the species table sits in shared memory and each warp loads
+// kEmWBatch species' states ahead of the (ordered) sum.
+constexpr int kEmWBatch = 8;
 
-__global__ void __launch_bounds__(256) k_em_w(EmParams e) {
+__global__ void __launch_bounds__(256, 3) k_em_w(EmParams e) {
   extern __shared__ unsigned char em_w_smem[];
   int64_t* soff = reinterpret_cast<int64_t*>(em_w_smem);
   double* sA = reinterpret_cast<double*>(soff + e.n_bh);
@@ -1898,20 +1898,21 @@ __global__ void __launch_bounds__(256) k_em_w(EmParams e) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int i = blockIdx.x * 8 + wid;
   if (i >= e.n_cr) return;
-  const int k = blockIdx.y * 32 + lane;
+  const int k = blockIdx.y * 64 + 2 * lane;  // columns k, k + 1 (ld is a multiple of 32)
   const bool active = k < e.ncols;
   const int kk = active ? k : 0;
   const double ie = e.invE[i], de = e.dE[i];
-  double acc = 0.0;
+  double acc0 = 0.0, acc1 = 0.0;
   for (int s0 = 0; s0 < e.n_bh; s0 += kEmWBatch) {
-    double xv[kEmWBatch], kv[kEmWBatch];
+    double2 xv[kEmWBatch];
+    double kv[kEmWBatch];
 #pragma unroll
     for (int u = 0; u < kEmWBatch; ++u) {
-      xv[u] = 0.0;
+      xv[u] = make_double2(0.0, 0.0);
       kv[u] = 0.0;
       if (s0 + u < e.n_bh) {
         const int64_t row = soff[s0 + u] + i;
-        xv[u] = __ldg(e.X + (size_t)row * e.ld + kk);
+        xv[u] = __ldg(reinterpret_cast<const double2*>(e.X + (size_t)row * e.ld + kk));
         kv[u] = __ldg(e.kp + row);
       }
     }
@@ -1920,12 +1921,17 @@ __global__ void __launch_bounds__(256) k_em_w(EmParams e) {
       const int s = s0 + u;
       if (s < e.n_bh) {
         const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(sA[s], kv[u]), e.dl_step), ie), de);
-        const double term = __dmul_rn(cw, xv[u]);
-        acc = (s == 0) ? term : __dadd_rn(acc, term);
+        const double t0 = __dmul_rn(cw, xv[u].x), t1 = __dmul_rn(cw, xv[u].y);
+        acc0 = (s == 0) ? t0 : __dadd_rn(acc0, t0);
+        acc1 = (s == 0) ? t1 : __dadd_rn(acc1, t1);
       }
     }
   }
-  if (active) e.w[(size_t)i * e.ld + k] = acc;
+  if (active) {
+    double* o = e.w + (size_t)i * e.ld + k;
+    o[0] = acc0;
+    if (k + 1 < e.ncols) o[1] = acc1;
+  }
 }
 
 // Adjoint of the pair weights: X[s, i][k] += cw_si lw[i][k] (e.X = lam, e.w = lw).
@@ -1967,7 +1973,7 @@ __global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
 //   y = Tg gamma + Te l, gamma <- y.
 void em_hook_forward(const EmParams& e, cudaStream_t st) {
   const size_t wsm = (size_t)e.n_bh * (sizeof(int64_t) + sizeof(double));
-  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, wsm, st>>>(e);
+  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 64)), 256, wsm, st>>>(e);
   bgemm(st, e.R, e.w, e.es, e.n_em, e.ncols, e.n_cr, e.n_cr, e.ld, e.ld, 0, 0, 0, 1, false);
   k_em_lep<<<(unsigned)blocks_for((int64_t)e.n_em * e.ncols, 256), 256, 0, st>>>(e);
   double* gam = e.X + (size_t)e.g_off * e.ld;
