@@ -1880,12 +1880,15 @@ __global__ void k_em_scale_w(EmParams e, double s) {
 
 // w[i][k] = sum_s cw_si X[s, i][k] over the charged nuclei in species order, with
 // cw_si = A_s kappa_pair dl_step / E_i dE_i: the Bethe-Heitler pair weights of the
-// hook (propagation.py:640-661).  A warp per (bin, 64-column tile), each lane
-// two adjacent columns (16-byte loads), so the nuclear state is read by many
-// warps at once; the species table sits in shared memory and each warp loads
-// kEmWBatch species' states ahead of the (ordered) sum.
+// hook (propagation.py:640-661).  A warp per (bin, 32 V-column tile), each lane
+// V adjacent columns (V = 2: 16-byte loads, used when the leading dimension is
+// even; V = 1 for one-column solves, whose leading dimension is 1), so the
+// nuclear state is read by many warps at once; the species table sits in
+// shared memory and each warp loads kEmWBatch species' states ahead of the
+// (ordered) sum.
 constexpr int kEmWBatch = 8;
 
+template <int V>
 __global__ void __launch_bounds__(256, 3) k_em_w(EmParams e) {
   extern __shared__ unsigned char em_w_smem[];
   int64_t* soff = reinterpret_cast<int64_t*>(em_w_smem);
@@ -1898,21 +1901,31 @@ __global__ void __launch_bounds__(256, 3) k_em_w(EmParams e) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int i = blockIdx.x * 8 + wid;
   if (i >= e.n_cr) return;
-  const int k = blockIdx.y * 64 + 2 * lane;  // columns k, k + 1 (ld is a multiple of 32)
+  const int k = blockIdx.y * (32 * V) + V * lane;  // columns k .. k + V - 1
   const bool active = k < e.ncols;
   const int kk = active ? k : 0;
   const double ie = e.invE[i], de = e.dE[i];
-  double acc0 = 0.0, acc1 = 0.0;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
   for (int s0 = 0; s0 < e.n_bh; s0 += kEmWBatch) {
-    double2 xv[kEmWBatch];
+    double xv[kEmWBatch][V];
     double kv[kEmWBatch];
 #pragma unroll
     for (int u = 0; u < kEmWBatch; ++u) {
-      xv[u] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int v = 0; v < V; ++v) xv[u][v] = 0.0;
       kv[u] = 0.0;
       if (s0 + u < e.n_bh) {
         const int64_t row = soff[s0 + u] + i;
-        xv[u] = __ldg(reinterpret_cast<const double2*>(e.X + (size_t)row * e.ld + kk));
+        const double* src = e.X + (size_t)row * e.ld + kk;
+        if (V == 2) {
+          const double2 x2 = __ldg(reinterpret_cast<const double2*>(src));
+          xv[u][0] = x2.x;
+          xv[u][V - 1] = x2.y;
+        } else {
+          xv[u][0] = __ldg(src);
+        }
         kv[u] = __ldg(e.kp + row);
       }
     }
@@ -1921,17 +1934,17 @@ __global__ void __launch_bounds__(256, 3) k_em_w(EmParams e) {
       const int s = s0 + u;
       if (s < e.n_bh) {
         const double cw = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(sA[s], kv[u]), e.dl_step), ie), de);
-        const double t0 = __dmul_rn(cw, xv[u].x), t1 = __dmul_rn(cw, xv[u].y);
-        acc0 = (s == 0) ? t0 : __dadd_rn(acc0, t0);
-        acc1 = (s == 0) ? t1 : __dadd_rn(acc1, t1);
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+          const double t = __dmul_rn(cw, xv[u][v]);
+          acc[v] = (s == 0) ? t : __dadd_rn(acc[v], t);
+        }
       }
     }
   }
-  if (active) {
-    double* o = e.w + (size_t)i * e.ld + k;
-    o[0] = acc0;
-    if (k + 1 < e.ncols) o[1] = acc1;
-  }
+#pragma unroll
+  for (int v = 0; v < V; ++v)
+    if (k + v < e.ncols) e.w[(size_t)i * e.ld + k + v] = acc[v];
 }
 
 // Adjoint of the pair weights: X[s, i][k] += cw_si lw[i][k] (e.X = lam, e.w = lw).
@@ -1973,7 +1986,10 @@ __global__ void __launch_bounds__(256) k_em_wT(EmParams e) {
 //   y = Tg gamma + Te l, gamma <- y.
 void em_hook_forward(const EmParams& e, cudaStream_t st) {
   const size_t wsm = (size_t)e.n_bh * (sizeof(int64_t) + sizeof(double));
-  k_em_w<<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 64)), 256, wsm, st>>>(e);
+  if (e.ld % 2 == 0)
+    k_em_w<2><<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 64)), 256, wsm, st>>>(e);
+  else
+    k_em_w<1><<<dim3((unsigned)blocks_for(e.n_cr, 8), (unsigned)blocks_for(e.ncols, 32)), 256, wsm, st>>>(e);
   bgemm(st, e.R, e.w, e.es, e.n_em, e.ncols, e.n_cr, e.n_cr, e.ld, e.ld, 0, 0, 0, 1, false);
   k_em_lep<<<(unsigned)blocks_for((int64_t)e.n_em * e.ncols, 256), 256, 0, st>>>(e);
   double* gam = e.X + (size_t)e.g_off * e.ld;
