@@ -203,6 +203,19 @@ def run_em_windows(run, sched, dz):
             np.stack([np.asarray(o[2], dtype=np.float64) for o in out]), np.array(dl))
 
 
+def _host_buffer(shape):
+    """A page-locked float64 host array for a solve's states (the device-to-host
+    copy runs at the link's rate instead of through a staging buffer); a plain
+    array when pinned memory is not available.  torch's caching host allocator
+    reuses the blocks of released results."""
+    try:
+        import torch
+
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    except Exception:
+        return np.empty(shape)
+
+
 def _other_grids(run):
     """Energies of the run's home grids other than the shared one, by tag."""
     return {t: g.grid for t, g in getattr(run, "grids", {}).items() if t != "default"}
@@ -403,7 +416,7 @@ class UHECRPropagationSolverETD2:
         self._set_field(ctx)
         if flags & _lib.PB_EM_CASCADE:
             ctx.set_em_windows(*self._em_windows(sched, dz))
-        state = np.empty((self.dim_states, K))
+        state = _host_buffer((self.dim_states, K)) if K > 1 else np.empty((self.dim_states, K))
         ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, state, photon_scale=self._photon_scale(),
                   out_cols=perm)
         self.last_timing = ctx.last_timing()
