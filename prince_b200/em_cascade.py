@@ -85,6 +85,12 @@ class KineticCascadeModel:
         R = (bh_shape(ctx, self.run.photon_field, E, self.run.cr_grid.grid, todo) if self.bh_shape is None
              else [self.bh_shape(z) for z in todo])
         for i, z in enumerate(todo):
+            if not (np.isfinite(Tg[i]).all() and np.isfinite(Te[i]).all() and np.isfinite(R[i]).all()):
+                raise FloatingPointError(
+                    f"the cascade transfer at z = {z} is not finite on this EM grid (the pair-production "
+                    "normalisation divides by the energy a near-threshold column carries, as the reference's "
+                    "cascade.py:513-515 does, and overflows); choose a grid whose top bins lie above the pair "
+                    "threshold, e.g. up to 1e14 GeV")
             self._cache[z] = (Tg[i], Te[i], R[i])
 
     def __call__(self, z):

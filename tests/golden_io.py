@@ -38,7 +38,10 @@ def light_network():
 
 
 def rel_err_on_support(x, ref, species_blocks, floor=1e-20):
-    """Max relative error over bins whose |ref| exceeds ``floor`` x the species max."""
+    """Max relative error over bins whose |ref| exceeds ``floor`` x the species max
+    (infinite when either side holds a non-finite value)."""
+    if not (np.isfinite(np.asarray(x)).all() and np.isfinite(np.asarray(ref)).all()):
+        return np.inf
     worst = 0.0
     for sl in species_blocks:
         r = ref[sl]
@@ -70,6 +73,8 @@ def local_scale_check(x, ref, species_blocks, tol=1e-10, floor=1e-20):
     Returns ``(worst local error, bins whose strict error exceeds tol, bins on
     the support)``.
     """
+    if not (np.isfinite(np.asarray(x)).all() and np.isfinite(np.asarray(ref)).all()):
+        return np.inf, -1, 0
     worst, above, total = 0.0, 0, 0
     for sl in species_blocks:
         r, v = ref[sl], x[sl]
