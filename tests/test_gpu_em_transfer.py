@@ -24,6 +24,7 @@ def _field():
 
 
 def _close(dev, ref):
+    assert np.isfinite(dev).all() and np.isfinite(ref).all()
     scale = np.abs(ref).max()
     assert np.array_equal(np.abs(dev) > 1e-12 * scale, np.abs(ref) > 1e-12 * scale)
     np.testing.assert_allclose(dev, ref, rtol=1e-9, atol=1e-12 * scale)

@@ -174,3 +174,23 @@ def test_device_order_puts_the_shared_grid_blocks_first():
 def light_run_shared():
     from golden_io import light_network_em
     return light_network_em()[1]
+
+
+def test_config5_run_layout():
+    """The coupled-EM workload: nuclei in 350 blocks of 96 bins, gamma / e+- on the
+    128-bin EM grid ahead of them in the run's order and as the device's tail."""
+    from prince_b200.solvers import device_order
+    from workloads import em_network_run
+
+    run = em_network_run()
+    sm = run.spec_man
+    assert run.em_grid.d == 128 and np.isclose(run.em_grid.bins[0], 1e-3) and np.isclose(run.em_grid.bins[-1], 1e14)
+    assert run.dim_states == 350 * 96 + 3 * 128
+    assert [sm.pdgid2sref[p].lidx() for p in (-11, 11, 22)] == [0, 128, 256]
+    dev2run, nb = device_order(run)
+    assert nb == 350 * 96
+    assert np.array_equal(np.sort(dev2run[nb:]), np.arange(384))
+    assert np.array_equal(dev2run[:nb], np.arange(384, run.dim_states))
+    E = run.adia_loss_rates_grid.energy_vector
+    assert np.array_equal(E[256:384], run.em_grid.grid)
+    assert np.array_equal(E[384:480], run.cr_grid.grid)
