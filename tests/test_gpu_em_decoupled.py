@@ -76,3 +76,35 @@ def test_decoupled_ragged_batch_vs_oracle(em_golden):
         m.solve(dz=1e-3)
         m._dev.ctx.set_option(_lib.PB_OPT_BATCHED_KERNELS, 1)
         assert rel_err_on_support(m.state, ref, _blocks(run)) < TOL
+
+
+def test_layout_rows_and_row_map_arguments():
+    """The species-block / tail split and the caller row map, at the C ABI."""
+    import scipy.sparse as sp
+    from prince_b200 import _lib
+    ctx = _lib.Context(0)
+    n, d = 10, 4                      # two species blocks of 4 bins, two tail rows
+    M = sp.lil_matrix((n, n))
+    M[1, 5] = 1.0                     # block to block (bin-local)
+    M[5, 1] = 1.0
+    M = M.tocsr()
+    ctx.set_coupling(n, M.indptr, M.indices)
+    with pytest.raises(ValueError):
+        ctx.set_layout(d, 9)          # not whole blocks
+    with pytest.raises(ValueError):
+        ctx.set_layout(d, 12)         # more block rows than states
+    ctx.set_layout(d, 8)
+    assert ctx.info(_lib.PB_INFO_BLOCKED_LAYOUT) in (0, 1)
+    with pytest.raises(ValueError):
+        ctx.set_row_map(np.array([0, 1, 2, 3, 4, 5, 6, 7, 8, 8]))   # not a permutation
+    with pytest.raises(ValueError):
+        ctx.set_row_map(np.array([0, 1, 2, 3, 4, 5, 6, 7, 8, 10]))  # out of range
+    ctx.set_row_map(np.arange(n)[::-1].copy())
+    ctx.set_row_map(None)
+    # a coupling entry between the blocks and the tail keeps the general row kernels
+    M2 = sp.lil_matrix((n, n))
+    M2[9, 1] = 1.0
+    M2 = M2.tocsr()
+    ctx.set_coupling(n, M2.indptr, M2.indices)
+    ctx.set_layout(d, 8)
+    assert ctx.info(_lib.PB_INFO_BLOCKED_LAYOUT) == 0
