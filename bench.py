@@ -255,7 +255,7 @@ def run_b200(args, dist, rank, ws, local):
 
     adj = adjoint_timing(run, pts, zi, local) if args.adjoint else None
     cfg5 = None
-    if args.config5 and rank == 0:
+    if args.config5 and ws == 1:   # one GPU only: the other ranks would wait for it at the final barrier
         del solver
         cfg5 = config5_timing(local, adjoint=bool(args.adjoint))
 
