@@ -254,10 +254,10 @@ def run_b200(args, dist, rank, ws, local):
         plain = len(pm) / (sum(pm) / 1e3)
 
     adj = adjoint_timing(run, pts, zi, local) if args.adjoint else None
-    cfg5 = None
-    if args.config5 and ws == 1:   # one GPU only: the other ranks would wait for it at the final barrier
+    cem = None
+    if args.coupled_em and ws == 1:   # one GPU only: the other ranks would wait for it at the final barrier
         del solver
-        cfg5 = config5_timing(local, adjoint=bool(args.adjoint))
+        cem = coupled_em_timing(local, adjoint=bool(args.adjoint))
 
     pk, pk_kind = _peaks()
     avg_steps_ms = statistics.mean(steps_ms)
@@ -297,8 +297,8 @@ def run_b200(args, dist, rank, ws, local):
         line["adjoint"] = adj
     if tuned:
         line["autotune"] = tuned
-    if cfg5:
-        line["config5"] = cfg5
+    if cem:
+        line["coupled_em"] = cem
     if clk:
         line["clocks"] = clk
     return line, run, pts, zi, sched
@@ -389,7 +389,7 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
 
 
 def adjoint_timing(run, pts, zi, device):
-    """Gradient of the flux loss of all points (config 4): the squared log-ratio of
+    """Gradient of the flux loss of all points: the squared log-ratio of
     each point's z = 0 all-particle flux to a target flux from one hidden
     parameter point, summed over bins above 10^9.5 GeV.  Timed: the
     forward with checkpoints every 32 steps (parameters -> grids on the host,
@@ -443,8 +443,8 @@ def adjoint_timing(run, pts, zi, device):
             "params_per_point": 8, "with_photon_scale": True, "grads_finite": grads_finite}
 
 
-def config5_timing(device, points=2048, adjoint=True):
-    """Config 5: the A <= 56 network with the co-evolved EM cascade -- gamma and
+def coupled_em_timing(device, points=2048, adjoint=True):
+    """The coupled EM cascade at scale: the A <= 56 network with the co-evolved EM cascade -- gamma and
     e+- on the decoupled 128-bin EM grid (1e-3 to 1e14 GeV), pair production and
     inverse Compton on CMB + the synthetic CIB (transfer and Bethe-Heitler
     shape built on the device for every rate window) -- over 2048 seeded
@@ -561,7 +561,7 @@ def main():
     ap.add_argument("--plain", type=int, default=5)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--adjoint", type=int, default=1, help="also time the adjoint gradient (1/0)")
-    ap.add_argument("--config5", type=int, default=1,
+    ap.add_argument("--coupled-em", type=int, default=1,
                     help="also time the coupled EM cascade workload, forward and gradient (1/0)")
     ap.add_argument("--autotune", type=int, default=1, help="search the stage's tile choices before timing (1/0)")
     ap.add_argument("--band-warps", type=int, default=0, choices=[0, 4, 8],

@@ -24,7 +24,7 @@ def headline_oracle(args):
     run = network_run()
     from prince_b200 import cr_sources
 
-    if kind == "cfg2":
+    if kind == "single":
         params = {p: (2.0, 1e10, 0.2) for p in INJECTED}
         srcs = [cr_sources.RigdityCutoffSource(run, norm=1.0, params=params)]
         K = None
@@ -38,7 +38,7 @@ def headline_oracle(args):
     return O.OracleSolver(run, zi, 0.0, K=K, exp="cr", perturb=perturb).solve(srcs, dz=1e-3)
 
 
-def config5_oracle(args):
+def coupled_em_oracle(args):
     """One oracle solve of the coupled-EM network (decoupled 128-bin EM grid) in a
     spawned process; ``em_table`` maps each window's redshift to the device-built
     (T_gamma, T_electron, R_BH) the GPU solve used."""
@@ -53,11 +53,11 @@ def config5_oracle(args):
     from oracle import etd2_oracle as O
     from prince_b200 import synth
     from prince_b200.run import PriNCeRun
-    from workloads import CFG2_GRID, CFG2_PHOTON, EM_GRID, cib_field, draw_points, point_source
+    from workloads import A56_GRID, A56_PHOTON, EM_GRID, cib_field, draw_points, point_source
 
     species = synth.full_network_species(56, n_species=350)
     model = synth.SyntheticPhotoNuclear(species, seed=2, x_cut_proton=1e-4)
-    run = PriNCeRun(model, cib_field(), cosmic_ray_grid=CFG2_GRID, photon_grid=CFG2_PHOTON,
+    run = PriNCeRun(model, cib_field(), cosmic_ray_grid=A56_GRID, photon_grid=A56_PHOTON,
                     enable_em_cascade=True, enable_em_decoupled_grid=True, em_grid=EM_GRID)
     pts = draw_points(run, 2048, seed=5000, z_range=(0.5, 4.0))
     srcs = [[point_source(run, pts[k])] for k in cols]

@@ -28,13 +28,13 @@ import multiprocessing as mp
 import numpy as np
 import pytest
 
-from oracle_jobs import config5_oracle
+from oracle_jobs import coupled_em_oracle
 from test_gpu_headline_parity import TOL, _check
 
 pytestmark = pytest.mark.gpu
 
 
-def test_config5_batch_vs_oracle():
+def test_coupled_em_batch_vs_oracle():
     from prince_b200.schedule import make_schedule, z_grid
     from prince_b200.solvers import MultiRHSPropagationSolverETD2
     from workloads import draw_points, em_network_run, point_source
@@ -57,7 +57,7 @@ def test_config5_batch_vs_oracle():
     model = run.em_cascade_model
     table = {float(z): tuple(np.asarray(a) for a in model(float(z))) for z in sched.z_window}
     with mp.get_context("spawn").Pool(5) as pool:
-        ref, *pert = pool.map(config5_oracle, [(cols, zi, s, table, PERTURB) for s in (None, 0, 1, 2, 3)])
+        ref, *pert = pool.map(coupled_em_oracle, [(cols, zi, s, table, PERTURB) for s in (None, 0, 1, 2, 3)])
     blocks = [s.sl for s in run.spec_man.species_refs]
     rep = _check(X[:, cols], ref, pert, blocks)
     assert rep["worst_on_stable_bins"] <= TOL, rep

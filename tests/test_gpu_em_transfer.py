@@ -42,7 +42,7 @@ def test_device_transfer_matches_the_reference():
         _close(Te[i], z["T_electron"][i])
 
 
-def test_device_transfer_on_the_config5_grid_matches_the_restatement():
+def test_device_transfer_on_the_128_bin_grid_matches_the_restatement():
     from prince_b200 import _lib
     from prince_b200.data import EnergyGrid
     from prince_b200.em_cascade import kinetic_transfer

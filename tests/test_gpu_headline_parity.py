@@ -1,10 +1,10 @@
 """Parity at the configurations the bench times, over their full redshift range (needs a B200).
 
-* Config 2: the A <= 56 network (350 species x 96 bins), one column, H/He/N/Si/Fe
+* One column: the A <= 56 network (350 species x 96 bins), one column, H/He/N/Si/Fe
   injection, z = 1 -> 0 (1000 steps, 100 rate windows), against the oracle:
   relative 1e-10 per bin wherever the oracle's flux exceeds 1e-20 of that
   species' maximum.
-* Config 3: the first 16 of the bench's 512 seeded points (seed 1000,
+* The batch: the first 16 of the bench's 512 seeded points (seed 1000,
   z_max ~ U[0.5, 1]), propagated inside the full 512-column batch exactly as
   the bench runs it, against the oracle over the full range.
 
@@ -75,7 +75,7 @@ def a56():
     return network_run()
 
 
-def test_config2_plain_full_range_vs_oracle(a56):
+def test_one_column_full_range_vs_oracle(a56):
     from prince_b200 import cr_sources
     from prince_b200.solvers import UHECRPropagationSolverETD2
     from workloads import INJECTED
@@ -85,7 +85,7 @@ def test_config2_plain_full_range_vs_oracle(a56):
     s = UHECRPropagationSolverETD2(initial_z=1.0, final_z=0.0, prince_run=run)
     s.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=params))
     s.solve(dz=1e-3)
-    ref, p0, p1 = _oracles("cfg2", None, 1.0)
+    ref, p0, p1 = _oracles("single", None, 1.0)
     blocks = [sp.sl for sp in run.spec_man.species_refs]
     rep = _check(s.state, ref, (p0, p1), blocks)
     assert rep["worst_on_stable_bins"] < TOL, rep
@@ -93,7 +93,7 @@ def test_config2_plain_full_range_vs_oracle(a56):
     assert rep["strict_misses"] == 0, rep    # one column: every support bin meets the strict bar
 
 
-def test_config3_bench_columns_full_range_vs_oracle(a56):
+def test_bench_columns_full_range_vs_oracle(a56):
     from prince_b200.solvers import MultiRHSPropagationSolverETD2
     from workloads import draw_points, point_source
 
@@ -106,7 +106,7 @@ def test_config3_bench_columns_full_range_vs_oracle(a56):
     m.solve(dz=1e-3)
     cols = list(range(16))
     gpu = m.state[:, cols].copy()
-    ref, p0, p1 = _oracles("cfg3", cols, zi)
+    ref, p0, p1 = _oracles("batch", cols, zi)
     blocks = [sp.sl for sp in run.spec_man.species_refs]
     rep = _check(gpu, ref, (p0, p1), blocks)
     assert rep["worst_on_stable_bins"] < TOL, rep

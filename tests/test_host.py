@@ -176,7 +176,7 @@ def light_run_shared():
     return light_network_em()[1]
 
 
-def test_config5_run_layout():
+def test_coupled_em_run_layout():
     """The coupled-EM workload: nuclei in 350 blocks of 96 bins, gamma / e+- on the
     128-bin EM grid ahead of them in the run's order and as the device's tail."""
     from prince_b200.solvers import device_order

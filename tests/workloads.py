@@ -7,8 +7,8 @@ import numpy as np
 from prince_b200 import cr_sources, photonfields as pf, synth
 from prince_b200.run import PriNCeRun
 
-CFG2_GRID = (5, 14, 96 / 9)      # 96 bins, log step 0.09375
-CFG2_PHOTON = (-15, -6, 96 / 9)  # 96 photon bins, same step
+A56_GRID = (5, 14, 96 / 9)      # 96 bins, log step 0.09375
+A56_PHOTON = (-15, -6, 96 / 9)  # 96 photon bins, same step
 INJECTED = (2212, 1000020040, 1000070140, 1000140280, 1000260560)  # H, He, N, Si, Fe
 
 
@@ -20,7 +20,7 @@ def network_run(max_mass=56, n_species=350, seed=2):
     """The A <= max_mass network on the 96-bin grid, CMB + synthetic CIB."""
     species = synth.full_network_species(max_mass, n_species=n_species)
     model = synth.SyntheticPhotoNuclear(species, seed=seed, x_cut_proton=1e-4)
-    return PriNCeRun(model, cib_field(), cosmic_ray_grid=CFG2_GRID, photon_grid=CFG2_PHOTON)
+    return PriNCeRun(model, cib_field(), cosmic_ray_grid=A56_GRID, photon_grid=A56_PHOTON)
 
 
 EM_GRID = (-3, 14, 128 / 17)    # 128 bins, 1e-3 to 1e14 GeV
@@ -34,7 +34,7 @@ def em_network_run(max_mass=56, n_species=350, seed=2, dz=1e-3):
 
     species = synth.full_network_species(max_mass, n_species=n_species)
     model = synth.SyntheticPhotoNuclear(species, seed=seed, x_cut_proton=1e-4)
-    run = PriNCeRun(model, cib_field(), cosmic_ray_grid=CFG2_GRID, photon_grid=CFG2_PHOTON,
+    run = PriNCeRun(model, cib_field(), cosmic_ray_grid=A56_GRID, photon_grid=A56_PHOTON,
                     enable_em_cascade=True, enable_em_decoupled_grid=True, em_grid=EM_GRID)
     run.em_cascade_model = KineticCascadeModel(run, dz)
     return run
