@@ -93,6 +93,7 @@ class PropagateFunction(torch.autograd.Function):
                                  table=device_table(plan.run.photon_field))
         if plan.em:
             ctx_dev.set_em_windows(*plan.em_windows)
+            plan.dev.em_key = None   # the solvers' resident windows are replaced
         dev = torch.device("cuda", plan.device)
         X = torch.empty((plan.run.dim_states, plan.K), dtype=torch.float64, device=dev)  # caller's column order
         s = float(scale.detach().cpu().item())
