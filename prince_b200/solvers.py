@@ -418,11 +418,13 @@ class UHECRPropagationSolverETD2:
             # the window matrices stay on the device while the windows, the
             # model, its photon field and the solver's hooks are the same
             model = getattr(self.prince_run, "em_cascade_model", None)
+            cacheable = (hasattr(model, "prefetch") and "_em_transfer_at" not in self.__dict__
+                         and "_em_bh_at" not in self.__dict__)
             key = (tuple(float(z) for z in sched.z_window), float(dz), id(model),
                    id(self.prince_run.photon_field), type(self)._em_transfer_at, type(self)._em_bh_at)
-            if model is None or not hasattr(model, "prefetch") or getattr(self._dev, "em_key", None) != key:
+            if not cacheable or getattr(self._dev, "em_key", None) != key:
                 ctx.set_em_windows(*self._em_windows(sched, dz))
-                self._dev.em_key = key if hasattr(model, "prefetch") else None
+                self._dev.em_key = key if cacheable else None
         state = _host_buffer((self.dim_states, K)) if K > 1 else np.empty((self.dim_states, K))
         ctx.solve(sched, flags, K, coeff if use_inj else None, n_active, state, photon_scale=self._photon_scale(),
                   out_cols=perm)
