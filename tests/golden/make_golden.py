@@ -11,6 +11,7 @@ source tree (the directory that holds ``src/prince_cr``)::
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --ebl     # tabulated EBL (Gilmore 2012)
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --kernel  # fold-kernel construction inputs
     PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --cascade # kinetic EM-cascade transfer
+    PRINCE_REFERENCE=<path> python tests/golden/make_golden.py --cascade-128  # ... on the 128-bin EM grid
 
 The reference package is copied to a scratch directory (it tries to
 download its HDF5 database at import unless a file is present, and it
@@ -716,6 +717,41 @@ def main_cascade():
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def main_cascade_128():
+    """The reference's kinetic transfer on the 128-bin EM grid of the coupled-EM
+    workload (1e-3 to 1e14 GeV), CMB + the synthetic grey-body CIB, five
+    redshifts up to z = 4, per-step escape at dz = 1e-3, FP64 iteration; and its
+    Bethe-Heitler shape on that grid against the 96-bin nuclear grid."""
+    _prepare_reference()
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    import prince_cr.config as config
+
+    config.debug_level = 0
+    config.linear_algebra_backend = "scipy"
+    from prince_cr.cascade.cascade import kinetic_cascade_transfer_batched
+    from prince_cr.cascade.bethe_heitler import bh_pair_shape_matrix
+    from prince_b200 import photonfields as pf
+    from prince_b200.data import EnergyGrid
+
+    E = EnergyGrid(-3, 14, 128 / 17).grid
+    Ep = EnergyGrid(5, 14, 96 / 9).grid
+    zs = [0.0, 0.5, 1.0, 2.0, 4.0]
+    field = pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), pf.ModifiedBlackBodyCIB()])
+    Ts = kinetic_cascade_transfer_batched(E, zs, field, dz=1e-3, iter_dtype="float64")
+    eps = np.logspace(-12.5, -7.0, 40)
+    Rs = []
+    for zz in zs:
+        n_eps = np.asarray(field.get_photon_density(eps, zz), dtype="double")
+        n_eps = np.where(np.isfinite(n_eps) & (n_eps > 0), n_eps, 0.0)
+        Rs.append(bh_pair_shape_matrix(E, Ep, eps, n_eps))
+    out = {"E": E, "E_p": Ep, "zs": np.array(zs), "dz": np.array(1e-3), "bh_eps": eps,
+           "T_gamma": np.stack([t[0] for t in Ts]), "T_electron": np.stack([t[1] for t in Ts]),
+           "R_BH": np.stack(Rs)}
+    path = os.path.join(HERE, "em_cascade_transfer_128.npz")
+    np.savez_compressed(path, **out)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
 if __name__ == "__main__":
     if "--em-decoupled" in sys.argv:
         main_em_decoupled()
@@ -727,6 +763,8 @@ if __name__ == "__main__":
         main_ebl()
     elif "--kernel" in sys.argv:
         main_kernel()
+    elif "--cascade-128" in sys.argv:
+        main_cascade_128()
     elif "--cascade" in sys.argv:
         main_cascade()
     else:

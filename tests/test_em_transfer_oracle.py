@@ -36,3 +36,18 @@ def test_restated_bh_shape_matches_the_reference():
         ref = z["R_BH"][i]
         assert np.array_equal(R != 0, ref != 0)
         np.testing.assert_allclose(R, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())
+
+
+def test_restated_transfer_on_the_128_bin_grid():
+    """The transfer on the coupled-EM workload's 128-bin EM grid (1e-3 to 1e14
+    GeV), five redshifts up to z = 4, against ``em_cascade_transfer_128.npz``
+    (its Bethe-Heitler shapes are checked against the device)."""
+    from prince_b200 import photonfields as pf
+    z = np.load(os.path.join(GOLDEN, "em_cascade_transfer_128.npz"))
+    field = pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), pf.ModifiedBlackBodyCIB()])
+    Ts = EC.transfer(z["E"], list(z["zs"]), field, float(z["dz"]))
+    for i, (tg, te) in enumerate(Ts):
+        for mine, ref in ((tg, z["T_gamma"][i]), (te, z["T_electron"][i])):
+            assert np.isfinite(mine).all()
+            assert np.array_equal(mine != 0, ref != 0)
+            np.testing.assert_allclose(mine, ref, rtol=1e-12, atol=1e-14 * np.abs(ref).max())

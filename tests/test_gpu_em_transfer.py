@@ -91,3 +91,21 @@ def test_device_bh_shape_on_a_square_grid_matches_the_restatement():
         n = np.asarray(_field().get_photon_density(eps, zz))
         n = np.where(np.isfinite(n) & (n > 0), n, 0.0)
         _close(R[i], EC.bh_shape(E, E, eps, n))
+
+
+def test_device_transfer_and_bh_shape_match_the_reference_on_the_128_bin_grid():
+    """The coupled-EM workload's 128-bin EM grid, five redshifts up to z = 4,
+    against the reference's own transfer and Bethe-Heitler shape
+    (``em_cascade_transfer_128.npz``; e+- on the EM grid, nucleons on the
+    96-bin nuclear grid)."""
+    from prince_b200 import _lib
+    from prince_b200.em_cascade import bh_shape, kinetic_transfer
+    z = np.load(os.path.join(GOLDEN, "em_cascade_transfer_128.npz"))
+    ctx = _lib.Context(0)
+    Tg, Te, passes = kinetic_transfer(ctx, _field(), z["E"], z["zs"], float(z["dz"]))
+    for i in range(len(z["zs"])):
+        _close(Tg[i], z["T_gamma"][i])
+        _close(Te[i], z["T_electron"][i])
+    R = bh_shape(ctx, _field(), z["E"], z["E_p"], z["zs"])
+    for i in range(len(z["zs"])):
+        _close(R[i], z["R_BH"][i])
