@@ -46,7 +46,7 @@ constexpr int kLongRow = 256;      // rows with more coupling entries are cut in
 constexpr int kMaxPhoton = 200;    // photon bins held in shared memory by the fold (208 KB tile)
 constexpr int kColTile = 32;       // state columns per warp in the batched step
 constexpr int kSegLen = 256;       // coupling entries per long-row segment
-constexpr int kMaxEmBins = 160;    // EM / nucleon bins of the cascade hook
+constexpr int kMaxEmBins = 1024;   // EM / nucleon bins of the cascade hook (as the transfer build)
 constexpr int kMaxBhSpecies = 3072;  // charged nuclei of the hook's pair weights (their table in shared memory)
 
 thread_local std::string g_error;

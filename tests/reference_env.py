@@ -85,3 +85,24 @@ def load_light_run():
     run = mg.build(config, CrossSectionBase)
     run.backend.xs_dtype = "float64"
     return prince_cr, run
+
+
+def load_light_em_run(bins_dec=16):
+    """``(prince_cr, reference PriNCeRun)`` of the light network with the
+    co-evolved EM cascade on the reference's decoupled EM grid (from the
+    electron mass to 1e14 GeV at ``bins_dec`` bins per decade) and the FP64
+    cascade iteration; the EM switches are restored on the config afterwards."""
+    load_package()
+    import prince_cr.config as config
+
+    keys = ("enable_em_cascade", "enable_em_decoupled_grid", "em_grid_bins_dec", "em_cascade_iter_dtype")
+    saved = {k: getattr(config, k, None) for k in keys}
+    config.enable_em_cascade = True
+    config.enable_em_decoupled_grid = True
+    config.em_grid_bins_dec = bins_dec
+    config.em_cascade_iter_dtype = "float64"
+    try:
+        return load_light_run()
+    finally:
+        for k, v in saved.items():
+            setattr(config, k, v)

@@ -99,3 +99,38 @@ def test_reference_multi_rhs_factory_with_reference_sources(ref):
     finally:
         run.backend.linear_algebra_backend = "scipy"
     assert rel_err_on_support(m.state, z["state_multi"], _blocks(run)) < TOL
+
+
+def test_reference_em_run_through_the_b200_backend():
+    """PriNCe's own run with the co-evolved EM cascade on its decoupled EM grid
+    (276 bins, 16 per decade, native coupling) and its own CPU solver (per-window
+    kinetic transfer and Bethe-Heitler shape, FP64) against the b200 backend on
+    the same run object, with the transfer and shape built on the device."""
+    import prince_cr.solvers.propagation as P
+    from prince_cr import cr_sources
+    from prince_b200 import plugin, solvers as B
+    from prince_b200.em_cascade import KineticCascadeModel
+
+    prince_cr, run = reference_env.load_light_em_run()
+    plugin.register(P)
+    assert run.em_grid is not None and run.em_grid.d == 276
+    params = {2212: (2.0, 1e10, 1.0), 1000020040: (2.0, 1e10, 1.0)}
+    run.backend.linear_algebra_backend = "scipy"
+    cpu = P.UHECRPropagationSolverETD2(initial_z=0.02, final_z=0.0, prince_run=run)
+    assert type(cpu).__name__ == "ETD2SolverCPU" and cpu.enable_em_cascade
+    cpu.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=params))
+    cpu.solve(dz=1e-3)
+    ref = np.asarray(cpu.state)
+    assert np.isfinite(ref).all()
+    run.em_cascade_model = KineticCascadeModel(run, 1e-3)
+    run.backend.linear_algebra_backend = "b200"
+    try:
+        s = P.UHECRPropagationSolverETD2(initial_z=0.02, final_z=0.0, prince_run=run)
+        assert isinstance(s, B.UHECRPropagationSolverETD2)
+        s.add_source_class(cr_sources.RigdityCutoffSource(run, norm=1.0, params=params))
+        s.solve(dz=1e-3)
+    finally:
+        run.backend.linear_algebra_backend = "scipy"
+    g = run.spec_man.pdgid2sref[22].sl
+    assert np.abs(ref[g]).max() > 0
+    assert rel_err_on_support(s.state, ref, _blocks(run)) < TOL
