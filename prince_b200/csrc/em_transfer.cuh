@@ -23,8 +23,9 @@ namespace {
 
 // ---------------------------------------------------------------------------
 // Batched FP64 GEMM on the tensor pipe: C[b] (=|+=) A[b] B[b], row-major,
-// DMMA m8n8k4.  CTA tile 64 x 32 (8 warps, 16 x 16 each), k in chunks of 16
-// through shared memory (zero-padded at the edges).
+// DMMA m8n8k4.  CTA tile (16 WM) x 32 (2 WM warps of 16 x 16 each; WM = 4 for
+// large grids, 2 when 64-row tiles would leave most SMs idle), k in chunks of
+// 16 through shared memory (zero-padded at the edges).
 // ---------------------------------------------------------------------------
 struct BGemm {
   const double* A;
@@ -35,13 +36,15 @@ struct BGemm {
   int accumulate;
 };
 
-constexpr int kGm = 64, kGn = 32, kGk = 16;
+constexpr int kGn = 32, kGk = 16;
 
-__global__ void __launch_bounds__(256) k_bgemm(BGemm g) {
+template <int WM>
+__global__ void __launch_bounds__(WM * 64) k_bgemm(BGemm g) {
+  constexpr int kGm = 16 * WM;
   __shared__ double As[kGm][kGk + 1];
   __shared__ double Bs[kGk][kGn + 1];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wm = wid & 3, wn = wid >> 2;
+  const int wm = wid % WM, wn = wid / WM;
   const int m0 = blockIdx.y * kGm, n0 = blockIdx.x * kGn;
   const double* __restrict__ A = g.A + (size_t)blockIdx.z * g.sA;
   const double* __restrict__ B = g.B + (size_t)blockIdx.z * g.sB;
@@ -94,7 +97,11 @@ __global__ void __launch_bounds__(256) k_bgemm(BGemm g) {
 void bgemm(cudaStream_t st, const double* A, const double* B, double* C, int M, int N, int K, int lda, int ldb,
            int ldc, long long sA, long long sB, long long sC, int batch, bool accumulate) {
   BGemm g{A, B, C, M, N, K, lda, ldb, ldc, sA, sB, sC, accumulate ? 1 : 0};
-  k_bgemm<<<dim3((N + kGn - 1) / kGn, (M + kGm - 1) / kGm, batch), 256, 0, st>>>(g);
+  const long long ctas64 = (long long)((N + kGn - 1) / kGn) * ((M + 63) / 64) * batch;
+  if (ctas64 < 256)
+    k_bgemm<2><<<dim3((N + kGn - 1) / kGn, (M + 31) / 32, batch), 128, 0, st>>>(g);
+  else
+    k_bgemm<4><<<dim3((N + kGn - 1) / kGn, (M + 63) / 64, batch), 256, 0, st>>>(g);
 }
 
 // ---------------------------------------------------------------------------
