@@ -1648,17 +1648,20 @@ __global__ void __launch_bounds__(NW * 32, 1) k_band(StepParams p) {
         cp_async_wait<0>();
       }
       __syncthreads();
-      const double* __restrict__ as = As + stage * ABLK + lane;
+      // a lane's fragments of row tiles 2p and 2p + 1 are one 16-byte word
+      const double2* __restrict__ as = reinterpret_cast<const double2*>(As + stage * ABLK) + lane;
       // consecutive DMMAs go to different accumulators (k-tile outer, row tile inner)
 #pragma unroll
       for (int jj = 0; jj < J; ++jj)
 #pragma unroll
         for (int b = 0; b < 2; ++b)
 #pragma unroll
-          for (int rt = 0; rt < RT; ++rt) {
-            const int kt = 2 * rt + jj;
+          for (int rp = 0; rp < RT / 2; ++rp) {
+            const int kt = 4 * rp + jj;
             if (kt >= KT) continue;
-            dmma884(acc[b][rt][0], acc[b][rt][1], as[((b * RT + rt) * J + jj) * 32], xf[kt]);
+            const double2 a2 = as[((b * (RT / 2) + rp) * J + jj) * 32];
+            dmma884(acc[b][2 * rp][0], acc[b][2 * rp][1], a2.x, xf[kt]);
+            if (kt + 2 < KT) dmma884(acc[b][2 * rp + 1][0], acc[b][2 * rp + 1][1], a2.y, xf[kt + 2]);
           }
       __syncthreads();  // every warp is done with this stage before it is refilled
 #pragma unroll
@@ -1687,14 +1690,16 @@ __global__ void __launch_bounds__(NW * 32, 1) k_band(StepParams p) {
           cp_async_wait<0>();
         }
         __syncthreads();
-        const double* __restrict__ as = As + buf * AH + lane;
+        const double2* __restrict__ as = reinterpret_cast<const double2*>(As + buf * AH) + lane;
 #pragma unroll
         for (int jj = 0; jj < J; ++jj)
 #pragma unroll
-          for (int rt = 0; rt < RT; ++rt) {
-            const int kt = 2 * rt + jj;
+          for (int rp = 0; rp < RT / 2; ++rp) {
+            const int kt = 4 * rp + jj;
             if (kt >= KT) continue;
-            dmma884(acc[b][rt][0], acc[b][rt][1], as[(rt * J + jj) * 32], xf[kt]);
+            const double2 a2 = as[(rp * J + jj) * 32];
+            dmma884(acc[b][2 * rp][0], acc[b][2 * rp][1], a2.x, xf[kt]);
+            if (kt + 2 < KT) dmma884(acc[b][2 * rp + 1][0], acc[b][2 * rp + 1][1], a2.y, xf[kt + 2]);
           }
         __syncthreads();  // every warp is done with this half before it is refilled
         buf ^= 1;
@@ -1805,7 +1810,7 @@ BandInstance band_kernel(int RT, int J, int nw = 8) {
 //   w      = sum over charged nuclei s of (A_s kappa_pair_s dl_step / E dE) n_s   (per nucleon bin)
 //   e_src  = R_BH(z_w) w                     added to e- and e+
 //   gamma <- T_gamma gamma + T_electron (e- + e+),   e+- <- 0
-// One CTA per 32-column tile (lane = column), the per-column vectors in shared memory.
+// The pair weights by k_em_w, the products as batched DMMA GEMMs (em_hook_forward).
 // ---------------------------------------------------------------------------
 }  // namespace
 
@@ -3739,7 +3744,7 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
                   (size_t)d * (kColTile + 2) * sizeof(double) <= max_smem &&
                   (int64_t)nsp * 2 * npairs * RT * J * 32 < ((int64_t)1 << 31) && squad.size() < ((size_t)1 << 29);
   if (!ok) return PB_OK;  // the general row kernels stay in use
-  // band tiles: [species][band pair][2][RT][J][32] DMMA A fragments per window
+  // band tiles: [species][band pair][2][RT / 2][J][32][2] DMMA A fragments per window
   std::vector<int32_t> bslot((size_t)std::max<int64_t>(R, 1), -1);
   for (int b = 0; b < nb; ++b)
     for (int e = 0; e < d; ++e) {
@@ -3749,8 +3754,9 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
         if (ix[j] == r) continue;
         const int sp = ix[j] / d, e2 = ix[j] % d;
         const int jj = e2 / 4 - 2 * rt;
-        const size_t tile = ((size_t)sp * 2 * npairs + b) * RT + rt;
-        bslot[j] = (int32_t)((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4));
+        // row tiles in pairs: lane l holds the fragments of tiles 2p and 2p + 1 side by side
+        const size_t tile = ((size_t)sp * 2 * npairs + b) * (RT / 2) + rt / 2;
+        bslot[j] = (int32_t)(((tile * J + jj) * 32 + (e % 8) * 4 + (e2 % 4)) * 2 + (rt & 1));
         ++band_nnz;
       }
     }
