@@ -175,6 +175,10 @@ struct pb_context {
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // the EM hook of a step beside the next step's nuclear stage (decoupled EM grid)
+  cudaStream_t stream3 = nullptr;
+  cudaEvent_t ev_hook_fork = nullptr, ev_hook_done = nullptr;
+  bool tail_wait = false;           // the next tail launch waits for ev_hook_done
   int num_sms = 148;
   DBuf tmaps;                       // [2] CUtensorMap of X and A for k_slab's TMA staging (64-byte aligned)
   bool tma_ok = false;              // tmaps hold maps of the current X / A / ld
@@ -2950,6 +2954,10 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
     ++launches;
   }
   if (c->n_tail > 0) {  // tail rows (another grid): the general row kernel, a warp per row
+    if (c->tail_wait) {  // the previous step's EM hook (on its own stream) writes the tail rows
+      cudaStreamWaitEvent(st, c->ev_hook_done, 0);
+      c->tail_wait = false;
+    }
     StepParams q = p;
     q.rows = c->tail_rows.as<int>();
     q.nrows = c->n_tail;
@@ -3037,9 +3045,22 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
   const size_t sbytes = (size_t)n * p.ld * sizeof(double);
   int64_t launches = 0;
   bool prepared = false;
+  const bool em = c->have_em && (p.flags & PB_EM_CASCADE);
+  // With the EM rows as the tail of the bin-blocked layout, a step's EM hook
+  // (it reads the nuclei and writes only the EM rows) runs on stream3 beside
+  // the next step's first stage; that stage's tail kernel, and everything
+  // after it on the launching stream, waits for it.
+  bool hook_pending = false;
+  auto join_hook = [&]() {
+    if (hook_pending) cudaStreamWaitEvent(st, c->ev_hook_done, 0);
+    hook_pending = false;
+    c->tail_wait = false;
+  };
   for (int64_t k = k0; k < k1; ++k) {
-    if (ckpt && every > 0 && k % every == 0)
+    if (ckpt && every > 0 && k % every == 0) {
+      join_hook();
       cudaMemcpyAsync(ckpt + (size_t)(k / every) * n * p.ld, X, sbytes, cudaMemcpyDeviceToDevice, st);
+    }
     p.step = k;
     p.step_w = c->h_win[k];
     p.ncols = n_active[k];
@@ -3050,6 +3071,9 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       prepared = true;
     }
     const bool blocked = use_blocked(c, K) && (!p.rec_P || p.fdkp || !(p.flags & PB_PAIRPROD));
+    const bool overlap = em && blocked && c->n_tail > 0;
+    if (!overlap) join_hook();
+    c->tail_wait = hook_pending;
     for (int stage = 1; stage <= 2; ++stage) {
       p.src = stage == 1 ? X : c->A.as<double>();
       p.x = X;
@@ -3069,11 +3093,23 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       }
       ++launches;
     }
-    if (c->have_em && (p.flags & PB_EM_CASCADE)) {
-      em_hook_forward(em_params(c, c->h_win[k], p.ld, p.ncols, X), st);
+    if (c->tail_wait) join_hook();  // no tail launch consumed the wait
+    hook_pending = false;
+    if (em) {
+      const EmParams e = em_params(c, c->h_win[k], p.ld, p.ncols, X);
+      if (overlap) {
+        cudaEventRecord(c->ev_hook_fork, st);
+        cudaStreamWaitEvent(c->stream3, c->ev_hook_fork, 0);
+        em_hook_forward(e, c->stream3);
+        cudaEventRecord(c->ev_hook_done, c->stream3);
+        hook_pending = true;
+      } else {
+        em_hook_forward(e, st);
+      }
       launches += 5;
     }
   }
+  join_hook();
   return launches;
 }
 
@@ -3113,7 +3149,10 @@ int pb_create(int device, pb_context** out) {
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
       cudaEventCreate(&c->ev2) != cudaSuccess || cudaEventCreate(&c->ev3) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->stream3, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_hook_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_hook_done, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
     return fail(nullptr, PB_ERR_CUDA, "stream/event creation failed");
   }
@@ -3132,6 +3171,7 @@ void pb_destroy(pb_context* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   if (c->stream2) cudaStreamSynchronize(c->stream2);
+  if (c->stream3) cudaStreamSynchronize(c->stream3);
   for (DBuf* b : all_buffers(c)) b->release();
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph_exec2) cudaGraphExecDestroy(c->graph_exec2);
@@ -3142,6 +3182,9 @@ void pb_destroy(pb_context* c) {
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->stream2) cudaStreamDestroy(c->stream2);
+  if (c->ev_hook_fork) cudaEventDestroy(c->ev_hook_fork);
+  if (c->ev_hook_done) cudaEventDestroy(c->ev_hook_done);
+  if (c->stream3) cudaStreamDestroy(c->stream3);
   cudaStreamDestroy(c->stream);
   delete c;
 }
