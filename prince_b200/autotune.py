@@ -85,6 +85,9 @@ def tune(solver, steps=16, reps=3, dz=1e-3, path=None, force=False):
     order = np.argsort(owner, kind="stable")
     ctx.set_injection(solver._dev.dev_rows(rows), G[:, order], owner[order].astype(np.int32), K)
     solver._set_field(ctx)
+    if solver._flags() & _lib.PB_EM_CASCADE:   # the short schedule's own EM windows
+        ctx.set_em_windows(*solver._em_windows(sched, dz))
+        solver._dev.em_key = None
     coeff = np.ones((sched.n_steps, len(srcs)))
     state = np.empty((solver.dim_states, K))
     cands = ctx.autotune(sched, solver._flags(), K, coeff, np.full(sched.n_steps, K, dtype=np.int32), state,
