@@ -108,3 +108,20 @@ def test_layout_rows_and_row_map_arguments():
     ctx.set_coupling(n, M2.indptr, M2.indices)
     ctx.set_layout(d, 8)
     assert ctx.info(_lib.PB_INFO_BLOCKED_LAYOUT) == 0
+
+
+def test_autotune_on_a_decoupled_em_solver(em_golden):
+    """The stage autotuner runs on an EM solver (its short schedule carries its
+    own EM windows) and the tuned solve still matches the reference."""
+    import tempfile
+    from prince_b200 import autotune
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    z, run, em, source = em_golden
+    m = MultiRHSPropagationSolverETD2(initial_z=0.2, final_z=0.0, prince_run=run, K=2)
+    m[0].add_source_class(source("eq"))
+    m[1].add_source_class(source("soft"))
+    with tempfile.TemporaryDirectory() as tdir:
+        choice, cands = autotune.tune(m, path=tdir + "/autotune.json", force=True, steps=8, reps=1)
+    assert cands and choice["steps_ms"] > 0
+    m.solve(dz=1e-3)
+    assert rel_err_on_support(m.state, z["state_em_multi"], _blocks(run)) < TOL
