@@ -3821,7 +3821,9 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
     for (int st = 1; st <= 2; ++st)
       for (bool rec : {false, true}) slab_fns.push_back((const void*)slab_kernel(st, rec, pre));
   for (const void* fn : slab_fns) {
-    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    // the attribute belongs to the kernel, not the context: the largest limit,
+    // so that a smaller layout on another context never lowers it under ours
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem));
     PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   }
   PB_CUDA(c, cudaFuncSetAttribute(bi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi.smem));
@@ -3934,7 +3936,7 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
   if ((rc = upload(c, c->slabT_slot, tslot.data(), tslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   for (const void* fn : {(const void*)k_slabT<1>, (const void*)k_slabT<2>}) {
-    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+    PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));  // per kernel
     PB_CUDA(c, cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
   }
   PB_CUDA(c, cudaFuncSetAttribute(bti.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bti.smem));
