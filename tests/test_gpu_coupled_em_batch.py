@@ -62,3 +62,34 @@ def test_coupled_em_batch_vs_oracle():
     rep = _check(X[:, cols], ref, pert, blocks)
     assert rep["worst_on_stable_bins"] <= TOL, rep
     assert rep["gpu_beyond_oracle_spread"] == 0, rep
+
+
+@pytest.mark.skipif(not __import__("os").environ.get("PRINCE_B200_LONG"),
+                    reason="about 6 minutes of oracle time; set PRINCE_B200_LONG=1")
+def test_coupled_em_batch_full_range_vs_oracle():
+    """The bench's own solve (all 2048 points from the largest z_max, 3,998 steps)
+    against the oracle on its two deepest columns, over the whole range."""
+    from prince_b200.schedule import make_schedule, z_grid
+    from prince_b200.solvers import MultiRHSPropagationSolverETD2
+    from workloads import draw_points, em_network_run, point_source
+
+    run = em_network_run()
+    pts = draw_points(run, 2048, seed=5000, z_range=(0.5, 4.0))
+    zmax = np.array([p["zmax"] for p in pts])
+    order = np.argsort(zmax)
+    cols = [int(order[-1]), int(order[-2])]
+    zi = float(zmax.max())
+    m = MultiRHSPropagationSolverETD2(initial_z=zi, final_z=0.0, prince_run=run, K=len(pts))
+    for k, p in enumerate(pts):
+        m[k].add_source_class(point_source(run, p))
+    m.solve(dz=1e-3)
+    X = np.asarray(m.state)
+    sched = make_schedule(z_grid(zi, 0.0, 1e-3), run.backend.update_rates_z_threshold)
+    model = run.em_cascade_model
+    table = {float(z): tuple(np.asarray(a) for a in model(float(z))) for z in sched.z_window}
+    with mp.get_context("spawn").Pool(5) as pool:
+        ref, *pert = pool.map(coupled_em_oracle, [(cols, zi, s, table, PERTURB) for s in (None, 0, 1, 2, 3)])
+    blocks = [s.sl for s in run.spec_man.species_refs]
+    rep = _check(X[:, cols], ref, pert, blocks)
+    assert rep["worst_on_stable_bins"] <= TOL, rep
+    assert rep["gpu_beyond_oracle_spread"] == 0, rep
