@@ -109,3 +109,31 @@ def test_device_transfer_and_bh_shape_match_the_reference_on_the_128_bin_grid():
     R = bh_shape(ctx, _field(), z["E"], z["E_p"], z["zs"])
     for i in range(len(z["zs"])):
         _close(R[i], z["R_BH"][i])
+
+
+def test_device_transfer_on_a_tabulated_ebl_matches_the_restatement():
+    """The cascade transfer and the Bethe-Heitler shape on CMB + the Gilmore (2012)
+    EBL table (the device's log-log table evaluation) against the restatement,
+    which evaluates the same table on the host."""
+    from golden_io import light_network_ebl
+    from prince_b200 import _lib
+    from prince_b200 import photonfields as pf
+    from prince_b200.data import EnergyGrid
+    from prince_b200.em_cascade import bh_shape, bh_target_grid, kinetic_transfer
+    _, _, ebl = light_network_ebl()
+    field = pf.CombinedPhotonField([pf.CMBPhotonSpectrum(), ebl])
+    E = EnergyGrid(-3, 14, 40 / 17).grid
+    zs = [0.1, 1.5]
+    ctx = _lib.Context(0)
+    Tg, Te, _ = kinetic_transfer(ctx, field, E, zs, 1e-3)
+    ref = EC.transfer(E, zs, field, 1e-3)
+    for i, (tg, te) in enumerate(ref):
+        _close(Tg[i], tg)
+        _close(Te[i], te)
+    Ep = EnergyGrid(8, 12, 6).grid
+    R = bh_shape(ctx, field, E, Ep, zs)
+    eps = bh_target_grid()
+    for i, zz in enumerate(zs):
+        n = np.asarray(field.get_photon_density(eps, zz))
+        n = np.where(np.isfinite(n) & (n > 0), n, 0.0)
+        _close(R[i], EC.bh_shape(E, Ep, eps, n))
