@@ -1,9 +1,9 @@
 """The kinetic EM-cascade transfer, built on the device.
 
-``kinetic_transfer(ctx_or_run, E, zs, dz)`` returns the per-redshift photon
+``kinetic_transfer(ctx, field, E, zs, dz)`` returns the per-redshift photon
 and electron transfer ``(T_gamma, T_electron)`` of an EM grid ``E`` on a
-photon field (the one set on the device context, or a run's field), for
-per-step escape at the step ``dz``: PriNCe's
+photon field (set on the device context ``ctx``), for per-step escape at the
+step ``dz``: PriNCe's
 ``kinetic_cascade_transfer_batched`` (``src/prince_cr/cascade/cascade.py:444-589``)
 with an FP64 iteration, computed by ``pb_em_transfer`` -- field-free
 inverse-Compton, pair and gamma-gamma opacity kernels, their contractions with
@@ -17,7 +17,9 @@ device call) and the Bethe-Heitler pair shape ``R_BH`` from ``pb_bh_shape``
 (the reference solver's ``_em_bh_at``, ``src/prince_cr/solvers/propagation.py:573-618``:
 40 target energies from 10^-12.5 to 10^-7 GeV, e+- on the EM species' grid --
 the run's decoupled EM grid or the shared one -- and nucleons on the
-cosmic-ray grid), or from a caller-supplied function.
+cosmic-ray grid), or from a caller-supplied function.  It refuses a
+transfer that is not finite (the reference's pair normalisation overflows on
+EM grids whose top stops near the pair threshold).
 """
 
 from __future__ import annotations
