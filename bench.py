@@ -192,7 +192,7 @@ def run_b200(args, dist, rank, ws, local):
         # a fresh search on this box (a scratch cache), reported beside the line
         with tempfile.TemporaryDirectory() as tdir:
             choice, cands = autotune.tune(solver, path=os.path.join(tdir, "autotune.json"), force=True)
-        default = next((c for c in cands if c["band_warps"] == 8 and c["slab_prefetch"] == 3
+        default = next((c for c in cands if c["band_warps"] == 8 and c["slab_prefetch"] == 2
                         and c["tma_staging"] == 1), None)
         tuned = {"choice": {k: choice[k] for k in ("band_warps", "slab_prefetch", "tma_staging")},
                  "tuned_steps_ms": choice["steps_ms"],

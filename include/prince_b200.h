@@ -53,7 +53,7 @@ extern "C" {
 #define PB_OPT_BAND_WARPS 12       /* warps of a band-tile CTA: 8 (default, 64 columns, one CTA per SM) or 4
                                      (32 columns in half the registers and shared memory, so the band
                                      tiles run on the tensor pipe beside the bin-local gather on each SM) */
-#define PB_OPT_SLAB_PREFETCH 13    /* row pairs whose FD term and F(x) a bin-local warp loads ahead: 2, 3 (default), 4 */
+#define PB_OPT_SLAB_PREFETCH 13    /* row quartets whose FD term and F(x) a bin-local warp loads ahead: 1, 2 (default), 3 */
 #define PB_OPT_STAGING_WAIT_TRIES 11 /* polls of k_slab's bounded staging wait before it gives up and the solve
                                      returns PB_ERR_DEVICE (default 2^24; < 0 restores it; 0 gives up at
                                      once, which tests the error path). The CTA still drains its copies. */

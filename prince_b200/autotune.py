@@ -3,7 +3,7 @@
 The bin-blocked batched stage has three tunable choices (``pb_autotune``):
 the warps of a band-tile CTA (8: a CTA per SM; 4: half the registers and
 shared memory, so it runs beside the bin-local gather), the bin-local
-kernel's prefetch depth (2, 3 or 4 row pairs) and its staging (TMA tensor
+kernel's prefetch depth (1, 2 or 3 row quartets) and its staging (TMA tensor
 maps or ``cp.async``).  ``tune(solver)`` times every candidate on the
 solver's live operator with a short solve that has all K columns active
 (the states are discarded), keeps the fastest on the device context and

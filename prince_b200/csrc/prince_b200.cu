@@ -78,7 +78,7 @@ struct DBuf {
 }  // namespace
 
 constexpr long long kWaitTries = 1ll << 24;  // polls of a bounded wait (well above any staging time)
-constexpr int kSlabPreDefault = 3;           // k_slab's default prefetch depth (row pairs)
+constexpr int kSlabPreDefault = 2;           // k_slab's default prefetch depth (row quartets)
 struct pb_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -146,8 +146,8 @@ struct pb_context {
   int32_t band_npairs = 0;
   DBuf band_slot, band_spec, slab_spec, band_vals, band_part;
   // bin-local rows: coupling entries in bin-major order
-  DBuf slab_rp, slab_sidx, slab_slot, slab_vals, slab_pairs, slab_wrp, slab_rowslot, slab_fac;
-  int64_t slab_nslots = 0;          // pair slots over all bins (two per pair)  // slab_rp: quad base per bin; slab_sidx: quads
+  DBuf slab_rp, slab_sidx, slab_slot, slab_vals, slab_quart, slab_wrp, slab_rowslot, slab_fac;
+  int64_t slab_nslots = 0;          // quartet slots over all bins (four per quartet)  // slab_rp: quad base per bin; slab_sidx: quads
   int64_t slab_nent = 0;            // value slots per window (4 per quad)
   int32_t slab_maxbin = 0;          // quads of the largest bin
   size_t slab_smem = 0, band_smem = 0;
@@ -171,7 +171,7 @@ struct pb_context {
   int32_t tma_mode = 1;             // 1: k_slab stages by TMA when tensor maps can be encoded; 0: cp.async
   long long staging_wait_tries = kWaitTries;  // k_slab's first staging wait (PB_OPT_STAGING_WAIT_TRIES)
   int32_t band_warps = 8;           // warps of a k_band CTA (PB_OPT_BAND_WARPS: 8 or 4)
-  int32_t slab_pre = kSlabPreDefault;  // k_slab prefetch depth in row pairs (PB_OPT_SLAB_PREFETCH: 2..4)
+  int32_t slab_pre = kSlabPreDefault;  // k_slab prefetch depth in row quartets (PB_OPT_SLAB_PREFETCH: 1..3)
   bool last_blocked = false;
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -715,14 +715,14 @@ struct StepParams {
   int n_slab_spec;
   const int* slab_qbase;    // [d + 1] first entry quad of each bin (even)
   const unsigned long long* slab_q;  // per quad: byte offsets of the 4 entries' mother rows in k_slab's slab, 16 bits each
-  const int4* slab_pairs;   // row pairs of k_slab's warps: species A, B (-1: none), q0 << 16 | quads of A, of B
-  const int* slab_wrp;      // [d][kSlabWarps + 1] first pair of each warp of a bin's CTA
+  const int4* slab_quart;   // row quartets of k_slab's warps: species 0 | 1 << 16, 2 | 3 << 16 (0xffff: none), first quad, quads per row
+  const int* slab_wrp;      // [d][kSlabWarps + 1] first quartet of each warp of a bin's CTA
   const double* slab_vals;  // [W][slab_stride] M_off values of the quads (4 per quad, zero padding)
   int64_t slab_stride;
   int slab_maxq;            // quads of the largest bin (shared-memory sizing)
-  int slab_maxp;            // row pairs of the largest bin
-  const int* slab_rowslot;  // [n] pair slot of each bin-local row (-1: other rows)
-  double* slab_fac;         // [2][3][slab_nslots] eD, phi1, phi2 of the bin-local rows in pair-slot order
+  int slab_maxp;            // row quartets of a bin
+  const int* slab_rowslot;  // [n] quartet slot of each bin-local row (-1: other rows)
+  double* slab_fac;         // [2][3][slab_nslots] eD, phi1, phi2 of the bin-local rows in quartet-slot order
   int64_t slab_nslots;
   const int* fd_cnt;        // per bin: FD stencil entries, row offsets and values
   const int* fd_off;
@@ -1348,74 +1348,97 @@ __device__ __forceinline__ void record_pre(const StepParams& p, const StepScalar
 }
 
 // k_slab's shared memory: the state slab of one bin (nsp x 16 columns), the
-// bin's entry values (4 per quad), mother-row byte offsets (4 x 16 bits per quad), row
-// pairs and the row factors (eD, phi1, phi2) of each pair slot.  Every block
-// starts on a 16-byte boundary (the quad count of a bin is even).
-constexpr int kSlabCols = 16;       // state columns of a k_slab CTA (a half-warp per row)
-constexpr int kSlabWarps = 16;      // two CTAs per SM: 32 warps hide the gather's latencies (64 registers)
+// bin's entry values (4 per quad), mother-row byte offsets (4 x 16 bits per
+// quad), the row quartets of the bin and the row factors (eD, phi1, phi2) of
+// each quartet slot.  Every block starts on a 16-byte boundary (the quad count
+// of a bin is a multiple of 4).
+constexpr int kSlabCols = 16;       // state columns of a k_slab CTA
+constexpr int kSlabRows = 4;        // rows per warp: a quarter-warp per row, two columns per lane
+constexpr int kSlabWarps = 12;      // two CTAs per SM: 24 warps of 80 registers (loads in flight per warp)
 struct SlabSmem {
   double* slab;
   double* vals;
   unsigned long long* sidx;
-  int4* pairs;
-  double* fac;  // [3][2 maxp]
+  int4* quart;
+  double* fac;  // [3][kSlabRows maxg]
   unsigned long long* bar;  // the TMA staging barrier
   // species rows of the slab, padded to whole TMA boxes of at most 256 species
   __host__ __device__ static int nbox(int nsp) { return (nsp + 255) / 256; }
   __host__ __device__ static int box_rows(int nsp) { return (nsp + nbox(nsp) - 1) / nbox(nsp); }
   __host__ __device__ static int rows(int nsp) { return nbox(nsp) * box_rows(nsp); }
-  __host__ __device__ static size_t bytes(int nsp, int maxq, int maxp) {
+  __host__ __device__ static size_t bytes(int nsp, int maxq, int maxg) {
     return (size_t)rows(nsp) * kSlabCols * sizeof(double) +
-           (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) + (size_t)maxp * (sizeof(int4) + 6 * sizeof(double)) +
-           sizeof(unsigned long long);
+           (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) +
+           (size_t)maxg * (sizeof(int4) + 3 * kSlabRows * sizeof(double)) + sizeof(unsigned long long);
   }
-  __device__ SlabSmem(double* base, int nsp, int maxq, int maxp) {
+  __device__ SlabSmem(double* base, int nsp, int maxq, int maxg) {
     slab = base;
     vals = slab + (size_t)rows(nsp) * kSlabCols;
     sidx = reinterpret_cast<unsigned long long*>(vals + (size_t)maxq * 4);
-    pairs = reinterpret_cast<int4*>(sidx + maxq);
-    fac = reinterpret_cast<double*>(pairs + maxp);
-    bar = reinterpret_cast<unsigned long long*>(fac + 6 * (size_t)maxp);
+    quart = reinterpret_cast<int4*>(sidx + maxq);
+    fac = reinterpret_cast<double*>(quart + maxg);
+    bar = reinterpret_cast<unsigned long long*>(fac + 3 * kSlabRows * (size_t)maxg);
   }
 };
 
-// Bin-local rows.  CTA = (bin e, 16-column tile); a half-warp owns a row, its
-// lane c owns column col0 + c.  The state slab of bin e, the bin's entry quads,
-// its row pairs and their row factors (written in pair-slot order by the row
-// preparation) arrive in shared memory by asynchronous copies; a warp then walks its row pairs (balanced over the warps when the
-// layout is built), sums each row from shared memory (four accumulators, one
-// per quad position) and applies the stage update.  The row's FD term
-// (fdbuf), F(x) in stage 2 and its injection slot are loaded PREF pairs
-// ahead into registers.  REC: the adjoint's record pass (P / Q sensitivities);
-// its row and (row, column) inputs are loaded with the others, a pair less ahead.
-// Offsets into the (n x ld) state buffers are 32-bit (n ld < 2^31, checked at
-// launch).
+// Species of row g of a quartet descriptor (0xffff: no row).
+__device__ __forceinline__ unsigned quart_species(const int4& qd, int g) {
+  return ((unsigned)(g < 2 ? qd.x : qd.y) >> (16 * (g & 1))) & 0xffffu;
+}
+__device__ __forceinline__ double2 dadd2(double2 a, double2 b) {
+  return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+// The injection of one column (rows of injected species only).
+__device__ __forceinline__ double slab_inj(const StepParams& p, int slot, int src0, int src1) {
+  const double* cf = p.coeff + (size_t)p.step * p.n_src;
+  const double* g = p.G + (size_t)slot * p.n_src;
+  double a = __dmul_rn(cf[src0], g[src0]);
+  for (int q = src0 + 1; q < src1; ++q) a = __dadd_rn(a, __dmul_rn(cf[q], g[q]));
+  return a;
+}
+
+// Bin-local rows.  CTA = (bin e, 16-column tile); a warp takes four rows at
+// a time (a quartet), a quarter-warp per row, and lane j of the quarter owns
+// columns col0 + 2j and col0 + 2j + 1.  The state slab of bin e, the bin's
+// entry quads, its quartets and their row factors (written in slot order by
+// the row preparation) arrive in shared memory by asynchronous copies; a
+// warp then walks its quartets (balanced over the warps when the layout is
+// built), sums each row from shared memory (four accumulators per column, one
+// per quad position, in the row's CSR order) and applies the stage update.
+// The four rows' quads interleave, so that one 16-byte value load and one
+// offset load serve four rows without bank conflicts, and a slab load of
+// 16 bytes per lane serves two columns; a quad's offsets are loaded one quad
+// ahead.  The row's FD term (fdbuf), F(x) in stage 2 and its injection slot
+// are loaded PREF quartets ahead into registers.  REC: the adjoint's record
+// pass (P / Q sensitivities); its row and (row, column) inputs are loaded with
+// the others, a quartet less ahead.  Offsets into the (n x ld) state buffers
+// are 32-bit (n ld < 2^31, checked at launch).
 template <int STAGE, bool REC, int PREF>
 __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   extern __shared__ __align__(128) double sm[];  // TMA boxes land at 128-byte boundaries
   const int e = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int half = lane >> 4, c = lane & 15;
+  const int g = lane >> 3, j = lane & 7;
   const int col0 = blockIdx.y * kSlabCols;
-  const int col = col0 + c;  // < ld
-  const bool active = col < p.ncols;
+  const int colA = col0 + 2 * j;  // this lane's columns colA, colA + 1 (< ld)
+  const bool actA = colA < p.ncols, actB = colA + 1 < p.ncols;
   const StepScalars s = load_scalars(p, p.step);
   const size_t o0 = (size_t)(p.step & 1) * p.n;
   const int ld = p.ld, d = p.d;
   SlabSmem L(sm, p.nsp, p.slab_maxq, p.slab_maxp);
   const int qb = p.slab_qbase[e], nqb = p.slab_qbase[e + 1] - qb;
-  const int pb0 = p.slab_wrp[e * (kSlabWarps + 1)], npb = p.slab_wrp[e * (kSlabWarps + 1) + kSlabWarps] - pb0;
-  const int fs = 2 * p.slab_maxp;  // stride of the three row-factor arrays
+  const int gb0 = p.slab_wrp[e * (kSlabWarps + 1)], ngb = p.slab_wrp[e * (kSlabWarps + 1) + kSlabWarps] - gb0;
+  const int fs = kSlabRows * p.slab_maxp;  // stride of the three row-factor arrays
   unsigned long long* stage_bar = L.bar;
   const double* mv = p.slab_vals + (size_t)p.step_w * p.slab_stride + (size_t)qb * 4;
-  const double* fc = p.slab_fac + (size_t)(p.step & 1) * 3 * p.slab_nslots + 2 * (size_t)pb0;
+  const double* fc = p.slab_fac + (size_t)(p.step & 1) * 3 * p.slab_nslots + (size_t)kSlabRows * gb0;
   if (p.tmap_src) {  // TMA: the slab as tensor boxes, the rest as bulk copies, one barrier
     if (threadIdx.x == 0) mbar_init(stage_bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
       const int nb = SlabSmem::nbox(p.nsp), br = SlabSmem::box_rows(p.nsp);
-      unsigned bytes = (unsigned)(nb * br * kSlabCols * sizeof(double)) + (unsigned)(npb * sizeof(int4)) +
-                       (unsigned)(6 * npb * sizeof(double));
+      unsigned bytes = (unsigned)(nb * br * kSlabCols * sizeof(double)) + (unsigned)(ngb * sizeof(int4)) +
+                       (unsigned)(3 * kSlabRows * ngb * sizeof(double));
       if (s.photohad) bytes += (unsigned)(nqb * (4 * sizeof(double) + sizeof(unsigned long long)));
       mbar_expect_tx(stage_bar, bytes);
       for (int b = 0; b < nb; ++b) tma_load_3d(L.slab + (size_t)b * br * kSlabCols, p.tmap_src, col0, e, b * br, stage_bar);
@@ -1423,10 +1446,10 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
         bulk_load(L.vals, mv, (unsigned)(nqb * 4 * sizeof(double)), stage_bar);
         bulk_load(L.sidx, p.slab_q + qb, (unsigned)(nqb * sizeof(unsigned long long)), stage_bar);
       }
-      if (npb > 0) {
-        bulk_load(L.pairs, p.slab_pairs + pb0, (unsigned)(npb * sizeof(int4)), stage_bar);
+      if (ngb > 0) {
+        bulk_load(L.quart, p.slab_quart + gb0, (unsigned)(ngb * sizeof(int4)), stage_bar);
         for (int k = 0; k < 3; ++k)
-          bulk_load(L.fac + k * fs, fc + (size_t)k * p.slab_nslots, (unsigned)(2 * npb * sizeof(double)), stage_bar);
+          bulk_load(L.fac + k * fs, fc + (size_t)k * p.slab_nslots, (unsigned)(kSlabRows * ngb * sizeof(double)), stage_bar);
       }
     }
   } else {
@@ -1440,52 +1463,57 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
       const unsigned long long* mq = p.slab_q + qb;
       for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
     }
-    for (int t = threadIdx.x; t < npb; t += blockDim.x) cp_async16(L.pairs + t, p.slab_pairs + pb0 + t);
-    for (int t = threadIdx.x; t < 3 * npb; t += blockDim.x) {  // 2 npb slots per factor, 16 bytes a copy
-      const int k = t / npb, u = t - k * npb;
+    for (int t = threadIdx.x; t < ngb; t += blockDim.x) cp_async16(L.quart + t, p.slab_quart + gb0 + t);
+    for (int t = threadIdx.x; t < 3 * 2 * ngb; t += blockDim.x) {  // kSlabRows ngb slots per factor, 16 bytes a copy
+      const int k = t / (2 * ngb), u = t - k * 2 * ngb;
       cp_async16(L.fac + k * fs + 2 * u, fc + (size_t)k * p.slab_nslots + 2 * u);
     }
     cp_async_commit();
   }
   const int w0 = p.slab_wrp[e * (kSlabWarps + 1) + wid], w1 = p.slab_wrp[e * (kSlabWarps + 1) + wid + 1];
   const bool need_fd = s.kap, need_f = STAGE == 2;
-  constexpr int PRE = REC ? PREF - 1 : PREF;  // the record inputs take registers too
-  double fdr[PRE], fxr[PRE];
+  constexpr int PRE = (REC && PREF > 1) ? PREF - 1 : PREF;  // the record inputs take registers too
+  const double2 z2 = make_double2(0.0, 0.0);
+  double2 fdr[PRE], fxr[PRE];
   int slr[PRE];
   // record pass: dsigma and phi1' / phi2' of the row, D_off (kappa_pair v) and S x of (row, column)
   const int64_t rj = p.step - p.rec_k0;
   const bool rec_on = REC && rj >= 0 && rj < p.rec_len;
-  double rds[PRE], rd12[PRE], rkp[PRE], rsx[PRE];
-  // the FD term, F(x) and injection slot of pair pi's row (staged: the pair
-  // comes from shared memory; the first pairs are read from global memory)
-#define PB_SLAB_LOAD(U, PI, PR)                                              \
-  do {                                                                       \
-    fdr[U] = 0.0;                                                            \
-    fxr[U] = 0.0;                                                            \
-    slr[U] = -1;                                                             \
-    if ((PI) < w1) {                                                         \
-      const int4 pr_ = (PR);                                                 \
-      const int sp_ = half ? pr_.y : pr_.x;                                  \
-      if (sp_ >= 0) {                                                        \
-        const int r_ = sp_ * d + e;                                          \
-        if (need_fd) fdr[U] = p.fdbuf[r_ * ld + col];                        \
-        if (need_f) fxr[U] = p.f[r_ * ld + col];                             \
-        if (s.inj) slr[U] = p.inj_slot[r_];                                  \
-        if (rec_on) {                                                        \
-          rds[U] = p.dsig[o0 + r_];                                          \
-          rd12[U] = STAGE == 1 ? p.dphi1[o0 + r_] : p.dphi2[o0 + r_];        \
-          rkp[U] = (s.kap && s.pair) ? p.fdkp[r_ * ld + col] : 0.0;          \
-          rsx[U] = STAGE == 2 ? p.rec_sx[r_ * ld + col] : 0.0;               \
-        }                                                                    \
-      }                                                                      \
-    }                                                                        \
+  double rds[PRE], rd12[PRE];
+  double2 rkp[PRE], rsx[PRE];
+  // the FD term, F(x) and injection slot of quartet pi's row g (staged: the
+  // quartet comes from shared memory; the first ones are read from global memory)
+#define PB_SLAB_LOAD(U, PI, QD)                                                                          \
+  do {                                                                                                   \
+    fdr[U] = z2;                                                                                         \
+    fxr[U] = z2;                                                                                         \
+    slr[U] = -1;                                                                                         \
+    if ((PI) < w1) {                                                                                     \
+      const unsigned sp_ = quart_species((QD), g);                                                       \
+      if (sp_ != 0xffffu) {                                                                              \
+        const int r_ = (int)sp_ * d + e;                                                                 \
+        if (need_fd) fdr[U] = *reinterpret_cast<const double2*>(p.fdbuf + r_ * ld + colA);               \
+        if (need_f) fxr[U] = *reinterpret_cast<const double2*>(p.f + r_ * ld + colA);                    \
+        if (s.inj) slr[U] = p.inj_slot[r_];                                                              \
+        if (rec_on) {                                                                                    \
+          rds[U] = p.dsig[o0 + r_];                                                                      \
+          rd12[U] = STAGE == 1 ? p.dphi1[o0 + r_] : p.dphi2[o0 + r_];                                    \
+          rkp[U] = (s.kap && s.pair) ? *reinterpret_cast<const double2*>(p.fdkp + r_ * ld + colA) : z2;  \
+          rsx[U] = STAGE == 2 ? *reinterpret_cast<const double2*>(p.rec_sx + r_ * ld + colA) : z2;       \
+        }                                                                                                \
+      }                                                                                                  \
+    }                                                                                                    \
   } while (0)
 #pragma unroll
-  for (int u = 0; u < PRE; ++u) PB_SLAB_LOAD(u, w0 + u, __ldg(p.slab_pairs + w0 + u));
-  int src0 = 0, src1 = 0;
-  if (s.inj && active) {
-    src0 = p.src_ptr[col];
-    src1 = p.src_ptr[col + 1];
+  for (int u = 0; u < PRE; ++u) {
+    const int pi = w0 + u;
+    PB_SLAB_LOAD(u, pi, pi < w1 ? __ldg(p.slab_quart + pi) : make_int4(-1, -1, 0, 0));
+  }
+  int srcA0 = 0, srcA1 = 0, srcB1 = 0;
+  if (s.inj && actA) {
+    srcA0 = p.src_ptr[colA];
+    srcA1 = p.src_ptr[colA + 1];
+    if (actB) srcB1 = p.src_ptr[colA + 2];
   }
   if (p.tmap_src) {
     if (!mbar_wait_bounded(stage_bar, 0, p.wait_tries)) {  // the copies did not land: report and leave
@@ -1498,78 +1526,99 @@ __global__ void __launch_bounds__(kSlabWarps * 32, 2) k_slab(StepParams p) {
   }
   __syncthreads();
 
-  const char* slb = reinterpret_cast<const char*>(L.slab + c);
+  const char* slb = reinterpret_cast<const char*>(L.slab + 2 * j);
   const double2* vq = reinterpret_cast<const double2*>(L.vals);
   for (int pb = w0; pb < w1; pb += PRE) {
 #pragma unroll
     for (int u = 0; u < PRE; ++u) {
       const int pi = pb + u;
       if (pi >= w1) break;
-      const int4 pr = L.pairs[pi - pb0];
-      const int sp = half ? pr.y : pr.x;
-      const int qq = half ? pr.w : pr.z;
-      const int r = sp * d + e;
-      double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-      if (sp >= 0 && s.photohad) {
-        const int q0 = qq >> 16, q1 = q0 + (qq & 0xffff);
-#pragma unroll 2
-        for (int q = q0; q < q1; ++q) {
+      const int4 qd = L.quart[pi - gb0];
+      const unsigned spw = quart_species(qd, g);
+      double2 acc0 = z2, acc1 = z2, acc2 = z2, acc3 = z2;
+      if (s.photohad) {  // uniform over the warp: rows without entries walk zero quads
+        const int q1 = qd.z + kSlabRows * qd.w;
+        unsigned long long mn = qd.w > 0 ? L.sidx[qd.z + g] : 0ull;  // the offsets one quad ahead
+#pragma unroll 1
+        for (int q = qd.z + g; q < q1; q += kSlabRows) {
+          const unsigned long long m = mn;
+          if (q + kSlabRows < q1) mn = L.sidx[q + kSlabRows];
           const double2 va = vq[2 * q], vb = vq[2 * q + 1];
-          const unsigned long long m = L.sidx[q];
-          const double x0 = *reinterpret_cast<const double*>(slb + ((unsigned)m & 0xffffu));
-          const double x1 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 16) & 0xffffu));
-          const double x2 = *reinterpret_cast<const double*>(slb + ((unsigned)(m >> 32) & 0xffffu));
-          const double x3 = *reinterpret_cast<const double*>(slb + (unsigned)(m >> 48));
-          acc0 = __fma_rn(va.x, x0, acc0);
-          acc1 = __fma_rn(va.y, x1, acc1);
-          acc2 = __fma_rn(vb.x, x2, acc2);
-          acc3 = __fma_rn(vb.y, x3, acc3);
+          const double2 x0 = *reinterpret_cast<const double2*>(slb + ((unsigned)m & 0xffffu));
+          const double2 x1 = *reinterpret_cast<const double2*>(slb + ((unsigned)(m >> 16) & 0xffffu));
+          const double2 x2 = *reinterpret_cast<const double2*>(slb + ((unsigned)(m >> 32) & 0xffffu));
+          const double2 x3 = *reinterpret_cast<const double2*>(slb + (unsigned)(m >> 48));
+          acc0.x = __fma_rn(va.x, x0.x, acc0.x);
+          acc0.y = __fma_rn(va.x, x0.y, acc0.y);
+          acc1.x = __fma_rn(va.y, x1.x, acc1.x);
+          acc1.y = __fma_rn(va.y, x1.y, acc1.y);
+          acc2.x = __fma_rn(vb.x, x2.x, acc2.x);
+          acc2.y = __fma_rn(vb.x, x2.y, acc2.y);
+          acc3.x = __fma_rn(vb.y, x3.x, acc3.x);
+          acc3.y = __fma_rn(vb.y, x3.y, acc3.y);
         }
       }
-      if (sp >= 0 && active) {
-        const double sM = __dadd_rn(__dadd_rn(acc0, acc1), __dadd_rn(acc2, acc3));
-        double out = sM;
-        if (s.kap) out = __dadd_rn(out, fdr[u]);
+      if (spw != 0xffffu && actA) {
+        const int sp = (int)spw;
+        const int r = sp * d + e;
+        const double2 sM = dadd2(dadd2(acc0, acc1), dadd2(acc2, acc3));
+        double2 out = sM;
+        if (s.kap) out = dadd2(out, fdr[u]);
         if (s.decay) {
-          double sL = 0.0;
-          for (int64_t j = p.l_indptr[r]; j < p.l_indptr[r + 1]; ++j)
-            sL = __dadd_rn(sL, __dmul_rn(p.l_vals[j], p.src[(size_t)p.l_indices[j] * ld + col]));
-          out = __dadd_rn(out, sL);
+          double2 sL = z2;
+          for (int64_t jj = p.l_indptr[r]; jj < p.l_indptr[r + 1]; ++jj) {
+            const double lv = p.l_vals[jj];
+            const double2 xv = *reinterpret_cast<const double2*>(p.src + (size_t)p.l_indices[jj] * ld + colA);
+            sL.x = __dadd_rn(sL.x, __dmul_rn(lv, xv.x));
+            sL.y = __dadd_rn(sL.y, __dmul_rn(lv, xv.y));
+          }
+          out = dadd2(out, sL);
         }
-        out = __dmul_rn(out, s.dl);
-        if (slr[u] >= 0 && src1 > src0) {  // injection (rows of injected species only)
-          const double* cf = p.coeff + (size_t)p.step * p.n_src;
-          const double* g = p.G + (size_t)slr[u] * p.n_src;
-          double a = __dmul_rn(cf[src0], g[src0]);
-          for (int q = src0 + 1; q < src1; ++q) a = __dadd_rn(a, __dmul_rn(cf[q], g[q]));
-          out = __dadd_rn(out, __dmul_rn(s.finj, a));
+        out.x = __dmul_rn(out.x, s.dl);
+        out.y = __dmul_rn(out.y, s.dl);
+        if (slr[u] >= 0) {  // injection (rows of injected species only)
+          if (srcA1 > srcA0) out.x = __dadd_rn(out.x, __dmul_rn(s.finj, slab_inj(p, slr[u], srcA0, srcA1)));
+          if (actB && srcB1 > srcA1) out.y = __dadd_rn(out.y, __dmul_rn(s.finj, slab_inj(p, slr[u], srcA1, srcB1)));
         }
-        const double own = L.slab[sp * kSlabCols + c];
-        const int slot = 2 * (pi - pb0) + half;
-        const int ro = r * ld + col;
+        const double2 own = *reinterpret_cast<const double2*>(L.slab + sp * kSlabCols + 2 * j);
+        const int slot = kSlabRows * (pi - gb0) + g;
+        const int ro = r * ld + colA;
         if (rec_on) {
-          const RecIn rin{rds[u], rd12[u], STAGE == 1 ? L.fac[slot] : L.fac[2 * fs + slot], L.fac[fs + slot], rkp[u],
-                          rsx[u], true};
-          record_pre<STAGE>(p, s, r, col, sM, out, own, fxr[u], rin);
+          const double f0 = STAGE == 1 ? L.fac[slot] : L.fac[2 * fs + slot], f1 = L.fac[fs + slot];
+          record_pre<STAGE>(p, s, r, colA, sM.x, out.x, own.x, fxr[u].x, RecIn{rds[u], rd12[u], f0, f1, rkp[u].x, rsx[u].x, true});
+          if (actB)
+            record_pre<STAGE>(p, s, r, colA + 1, sM.y, out.y, own.y, fxr[u].y,
+                              RecIn{rds[u], rd12[u], f0, f1, rkp[u].y, rsx[u].y, true});
         }
         if (STAGE == 1) {
           // a = eD x + (phi1 F(x)) h
-          p.a[ro] = __dadd_rn(__dmul_rn(L.fac[slot], own), __dmul_rn(__dmul_rn(L.fac[fs + slot], out), s.h));
-          p.f[ro] = out;
+          const double eD = L.fac[slot], p1 = L.fac[fs + slot];
+          const double2 av = make_double2(__dadd_rn(__dmul_rn(eD, own.x), __dmul_rn(__dmul_rn(p1, out.x), s.h)),
+                                          __dadd_rn(__dmul_rn(eD, own.y), __dmul_rn(__dmul_rn(p1, out.y), s.h)));
+          if (actB) {
+            *reinterpret_cast<double2*>(p.a + ro) = av;
+            *reinterpret_cast<double2*>(p.f + ro) = out;
+          } else {
+            p.a[ro] = av.x;
+            p.f[ro] = out.x;
+          }
         } else {
           // x = a + ((F(a) - F(x)) h) phi2
-          const double dF = __dmul_rn(__dadd_rn(out, -fxr[u]), s.h);
-          p.xout[ro] = __dadd_rn(own, __dmul_rn(dF, L.fac[2 * fs + slot]));
+          const double p2 = L.fac[2 * fs + slot];
+          const double2 xv = make_double2(__dadd_rn(own.x, __dmul_rn(__dmul_rn(__dadd_rn(out.x, -fxr[u].x), s.h), p2)),
+                                          __dadd_rn(own.y, __dmul_rn(__dmul_rn(__dadd_rn(out.y, -fxr[u].y), s.h), p2)));
+          if (actB) *reinterpret_cast<double2*>(p.xout + ro) = xv;
+          else p.xout[ro] = xv.x;
         }
       }
       const int pn = pi + PRE;
-      PB_SLAB_LOAD(u, pn, L.pairs[pn - pb0]);
+      PB_SLAB_LOAD(u, pn, pn < w1 ? L.quart[pn - gb0] : make_int4(-1, -1, 0, 0));
     }
   }
 #undef PB_SLAB_LOAD
 }
 
-// k_slab instance for (stage, record pass, prefetch depth in row pairs).
+// k_slab instance for (stage, record pass, prefetch depth in quartets).
 using SlabKernel = void (*)(StepParams);
 template <int PREF>
 SlabKernel slab_kernel_p(int stage, bool rec) {
@@ -1578,9 +1627,9 @@ SlabKernel slab_kernel_p(int stage, bool rec) {
 }
 SlabKernel slab_kernel(int stage, bool rec, int pre) {
   switch (pre) {
-    case 2: return slab_kernel_p<2>(stage, rec);
-    case 4: return slab_kernel_p<4>(stage, rec);
-    default: return slab_kernel_p<3>(stage, rec);
+    case 1: return slab_kernel_p<1>(stage, rec);
+    case 3: return slab_kernel_p<3>(stage, rec);
+    default: return slab_kernel_p<2>(stage, rec);
   }
 }
 
@@ -2060,7 +2109,7 @@ struct AdjBlk {
   int64_t slabT_stride;
   const int* slabT_qbase;   // [d + 1] first quad of each bin (even)
   const unsigned long long* slabT_q;  // per quad: byte offsets of the 4 daughters' rows in the v slab, 16 bits each
-  const int4* slabT_pairs;  // mother-row pairs of k_slabT's warps (as k_slab's row pairs)
+  const int4* slabT_pairs;  // mother-row pairs of k_slabT's warps: species A, B (-1: none), q0 << 16 | quads of A, of B
   const int* slabT_wrp;     // [d][kSlabTWarps + 1] first pair of each warp of a bin's CTA
   int slabT_maxq;           // quads of the largest bin
   int slabT_maxp;           // row pairs of a bin
@@ -2692,7 +2741,7 @@ std::vector<DBuf*> solve_buffers(pb_context* c) {
           &c->em_bh_off, &c->em_bh_A, &c->em_invE, &c->em_dE, &c->em_Tg, &c->em_Te, &c->em_R, &c->em_wbuf,
           &c->em_es, &c->em_lep, &c->em_y, &c->em_TgT, &c->em_TeT, &c->em_RT,
           &c->band_slot, &c->band_spec, &c->slab_spec, &c->band_vals, &c->band_part, &c->slab_rp,
-          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_pairs, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
+          &c->slab_sidx, &c->slab_slot, &c->slab_vals, &c->slab_quart, &c->slab_wrp, &c->slab_rowslot, &c->slab_fac, &c->fd_cnt, &c->fd_off, &c->fd_val, &c->fd_dense, &c->fdT_dense, &c->fdbuf,
           &c->bandT_slot, &c->slabT_rp, &c->slabT_offs, &c->slabT_slot, &c->fdT_cnt, &c->fdT_off, &c->fdT_val,
           &c->slabT_pairs, &c->slabT_wrp, &c->tmaps, &c->d_err, &c->tab_z, &c->tab_le, &c->tab_v};
 }
@@ -2792,12 +2841,12 @@ void fill_step_params(pb_context* c, StepParams& p, int K, int ld, uint32_t flag
   p.n_slab_spec = c->n_slab_spec;
   p.slab_qbase = c->slab_rp.as<int>();
   p.slab_q = c->slab_sidx.as<unsigned long long>();
-  p.slab_pairs = c->slab_pairs.as<int4>();
+  p.slab_quart = c->slab_quart.as<int4>();
   p.slab_wrp = c->slab_wrp.as<int>();
   p.slab_vals = c->slab_vals.as<double>();
   p.slab_stride = c->slab_nent;
   p.slab_maxq = c->slab_maxbin;
-  p.slab_maxp = (c->n_slab_spec + 1) / 2;
+  p.slab_maxp = (c->n_slab_spec + kSlabRows - 1) / kSlabRows;
   p.slab_rowslot = c->blocked_ok ? c->slab_rowslot.as<int>() : nullptr;
   p.slab_fac = c->slab_fac.as<double>();
   p.slab_nslots = c->slab_nslots;
@@ -3713,15 +3762,20 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
   for (int v : kBandRT) if (!RT && v >= RTr) RT = v;
   for (int v : kBandJ) if (!J && v >= Jr) J = v;
   // bin-local rows, per bin: rows ordered by entry quads (longest first) and
-  // paired for the two half-warps of a warp; pairs spread over k_slab's warps
-  // longest-processing-time first; each row's entries in CSR order in quads of
-  // 4 (zero values pad the last quad); every bin starts on an even quad.
+  // grouped in quartets, a quarter-warp of k_slab per row; quartets spread
+  // over k_slab's warps longest-processing-time first.  Each row's entries in
+  // CSR order in quads of 4; zero values pad the row's last quad and the row
+  // up to the longest row of its quartet.  The quads of a quartet's four rows
+  // interleave (row g's quad t at q0 + 4 t + g), so that the four rows' entry
+  // loads fall into distinct shared-memory banks; every bin and quartet starts
+  // on a multiple of 4 quads.
   int64_t band_nnz = 0, slab_nnz = 0;
-  std::vector<int32_t> qbase((size_t)d + 1, 0), wrp((size_t)d * (kSlabWarps + 1), 0), spairs;
+  std::vector<int32_t> qbase((size_t)d + 1, 0), wrp((size_t)d * (kSlabWarps + 1), 0), squart;
   std::vector<unsigned long long> squad;
   std::vector<int32_t> sslot((size_t)std::max<int64_t>(R, 1), -1), rowslot((size_t)n, -1);
   int32_t maxbin = 0;
-  bool quads_fit = (size_t)nsp * kSlabCols * sizeof(double) <= (1 << 16);  // 16-bit slab byte offsets
+  // 16-bit slab byte offsets and 16-bit species (0xffff marks an empty quartet row)
+  bool quads_fit = (size_t)nsp * kSlabCols * sizeof(double) <= (1 << 16) && nsp < 0xffff;
   {
     std::vector<int32_t> nq(nss), order(nss);
     std::vector<std::vector<int32_t>> wl(kSlabWarps);
@@ -3738,49 +3792,55 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
       std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return nq[a] > nq[b]; });
       for (auto& v : wl) v.clear();
       std::fill(load.begin(), load.end(), 0);
-      for (int k = 0; k < nss; k += 2) {  // pair k/2 = rows order[k], order[k + 1]
+      for (int k = 0; k < nss; k += kSlabRows) {  // quartet k / 4 = rows order[k .. k + 3], the longest first
         const int w = (int)(std::min_element(load.begin(), load.end()) - load.begin());
         wl[w].push_back(k);
         load[w] += nq[order[k]] + 1;
       }
       for (int w = 0; w < kSlabWarps; ++w) {
-        wrp[(size_t)e * (kSlabWarps + 1) + w] = (int32_t)(spairs.size() / 4);
+        wrp[(size_t)e * (kSlabWarps + 1) + w] = (int32_t)(squart.size() / 4);
         for (int k : wl[w]) {
-          int32_t pr[4] = {-1, -1, 0, 0};
-          for (int hf = 0; hf < 2; ++hf) {
-            if (k + hf >= nss) continue;
-            const int i = order[k + hf];
+          const int nqmax = nq[order[k]];
+          const int64_t q0 = (int64_t)squad.size() - qbase[e];
+          const size_t qa = squad.size();
+          squad.resize(qa + (size_t)kSlabRows * nqmax, 0);
+          int32_t sp4[kSlabRows] = {0xffff, 0xffff, 0xffff, 0xffff};
+          for (int g = 0; g < kSlabRows; ++g) {
+            if (k + g >= nss) continue;
+            const int i = order[k + g];
             const int64_t r = (int64_t)sspec[i] * d + e;
-            const int64_t q0 = (int64_t)squad.size() - qbase[e];
             int t = 0, pad_sp = sspec[i];
             for (int64_t j = ip[r]; j < ip[r + 1]; ++j) {
               if (ix[j] == r) continue;
               if (t == 0) pad_sp = ix[j] / d;
-              if (t % 4 == 0) squad.push_back(0);
-              squad.back() |= (unsigned long long)((ix[j] / d) * kSlabCols * sizeof(double)) << (16 * (t % 4));
-              sslot[j] = (int32_t)((squad.size() - 1) * 4 + t % 4);
+              const size_t q = qa + (size_t)kSlabRows * (t / 4) + g;
+              squad[q] |= (unsigned long long)((ix[j] / d) * kSlabCols * sizeof(double)) << (16 * (t % 4));
+              sslot[j] = (int32_t)(q * 4 + t % 4);
               ++slab_nnz;
               ++t;
             }
-            for (; t % 4; ++t) squad.back() |= (unsigned long long)(pad_sp * kSlabCols * sizeof(double)) << (16 * (t % 4));
-            if (q0 >= (1 << 15) || nq[i] >= (1 << 16)) quads_fit = false;
-            pr[hf] = sspec[i];
-            pr[2 + hf] = (int32_t)((q0 << 16) | nq[i]);
-            rowslot[r] = (int32_t)(spairs.size() / 2 + hf);  // pair index * 2 + half
+            for (; t < 4 * nqmax; ++t) {  // zero values on a mother row of the slab
+              const size_t q = qa + (size_t)kSlabRows * (t / 4) + g;
+              squad[q] |= (unsigned long long)(pad_sp * kSlabCols * sizeof(double)) << (16 * (t % 4));
+            }
+            sp4[g] = sspec[i];
+            rowslot[r] = (int32_t)(squart.size() + g);  // quartet index * 4 + row
           }
-          spairs.insert(spairs.end(), pr, pr + 4);
+          if (q0 >= (1 << 30)) quads_fit = false;
+          const int32_t qd[4] = {(int32_t)((uint32_t)sp4[0] | ((uint32_t)sp4[1] << 16)),
+                                 (int32_t)((uint32_t)sp4[2] | ((uint32_t)sp4[3] << 16)), (int32_t)q0, nqmax};
+          squart.insert(squart.end(), qd, qd + 4);
         }
       }
-      wrp[(size_t)e * (kSlabWarps + 1) + kSlabWarps] = (int32_t)(spairs.size() / 4);
-      if ((squad.size() - qbase[e]) % 2) squad.push_back(0);
+      wrp[(size_t)e * (kSlabWarps + 1) + kSlabWarps] = (int32_t)(squart.size() / 4);
       maxbin = std::max<int32_t>(maxbin, (int32_t)(squad.size() - qbase[e]));
     }
     qbase[d] = (int32_t)squad.size();
-    if (squad.empty()) squad.assign(2, 0);
-    if (spairs.empty()) spairs.assign(4, -1);
+    if (squad.empty()) squad.assign(4, 0);
+    if (squart.empty()) squart.assign(4, 0);
   }
   const size_t max_smem = 227 * 1024;
-  const size_t ssm = SlabSmem::bytes(nsp, maxbin, (nss + 1) / 2);
+  const size_t ssm = SlabSmem::bytes(nsp, maxbin, (nss + kSlabRows - 1) / kSlabRows);
   const BandInstance bi = (RT && J) ? band_kernel(RT, J) : BandInstance{nullptr, 0, 0};
   const BandInstance bi4 = (RT && J) ? band_kernel(RT, J, 4) : BandInstance{nullptr, 0, 0};
   const bool ok = split_ok && quads_fit && ssm <= max_smem && bi.fn && bi.smem <= max_smem && (bspec.empty() || lo >= 0) &&
@@ -3808,16 +3868,16 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
   if ((rc = upload(c, c->slab_spec, sspec.data(), sspec.size()))) return rc;
   if ((rc = upload(c, c->slab_rp, qbase.data(), qbase.size()))) return rc;
   if ((rc = upload(c, c->slab_sidx, squad.data(), squad.size()))) return rc;
-  if ((rc = upload(c, c->slab_pairs, spairs.data(), spairs.size()))) return rc;
+  if ((rc = upload(c, c->slab_quart, squart.data(), squart.size()))) return rc;
   if ((rc = upload(c, c->slab_wrp, wrp.data(), wrp.size()))) return rc;
   if ((rc = upload(c, c->slab_rowslot, rowslot.data(), rowslot.size()))) return rc;
-  c->slab_nslots = (int64_t)(spairs.size() / 2);
+  c->slab_nslots = (int64_t)squart.size();
   PB_CUDA(c, c->slab_fac.ensure((size_t)2 * 3 * c->slab_nslots * sizeof(double)));
   PB_CUDA(c, cudaMemsetAsync(c->slab_fac.p, 0, (size_t)2 * 3 * c->slab_nslots * sizeof(double), c->stream));
   if ((rc = upload(c, c->slab_slot, sslot.data(), sslot.size()))) return rc;
   PB_CUDA(c, cudaStreamSynchronize(c->stream));
   std::vector<const void*> slab_fns;
-  for (int pre : {2, 3, 4})
+  for (int pre : {1, 2, 3})
     for (int st = 1; st <= 2; ++st)
       for (bool rec : {false, true}) slab_fns.push_back((const void*)slab_kernel(st, rec, pre));
   for (const void* fn : slab_fns) {
@@ -4065,7 +4125,7 @@ int pb_set_option(pb_context* c, int32_t key, int64_t value) {
       c->band_warps = (int32_t)value;
       return PB_OK;
     case PB_OPT_SLAB_PREFETCH:
-      if (value < 2 || value > 4) return fail(c, PB_ERR_ARG, "pb_set_option: slab prefetch must be 2, 3 or 4");
+      if (value < 1 || value > 3) return fail(c, PB_ERR_ARG, "pb_set_option: slab prefetch must be 1, 2 or 3");
       c->slab_pre = (int32_t)value;
       return PB_OK;
     case PB_OPT_STAGING_WAIT_TRIES:
@@ -4724,7 +4784,7 @@ int pb_autotune(pb_context* c, const pb_solve_args* a, int32_t reps, int32_t max
   std::vector<pb_tune_choice> cand;
   for (int tma : {1, 0})
     for (int bw : {8, 4})
-      for (int pre : {3, 2, 4}) cand.push_back(pb_tune_choice{bw, pre, tma, 0.0});
+      for (int pre : {2, 1, 3}) cand.push_back(pb_tune_choice{bw, pre, tma, 0.0});
   int best = -1;
   for (size_t i = 0; i < cand.size(); ++i) {
     c->band_warps = cand[i].band_warps;

@@ -50,7 +50,7 @@ def test_tuned_choice_is_fastest_cached_and_gives_the_same_states(tmp_path):
         assert worst < 1e-13
     # every prefetch depth and staging with the default band CTAs: identical states
     try:
-        for pre in (2, 4):
+        for pre in (1, 3):
             for tma in (1, 0):
                 autotune.apply(ctx, dict(band_warps=8, slab_prefetch=pre, tma_staging=tma))
                 m.solve(dz=1e-3)
