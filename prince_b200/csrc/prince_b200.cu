@@ -184,6 +184,9 @@ struct pb_context {
   bool tma_ok = false;              // tmaps hold maps of the current X / A / ld
   bool last_tma = false;            // the last solve staged k_slab by TMA
   const void* tma_key[3] = {nullptr, nullptr, nullptr};
+  DBuf tmapsT;                      // [2] CUtensorMap of the adjoint's v buffers for k_slabT's TMA staging
+  bool tmaT_ok = false;             // tmapsT hold maps of the current vbuf / vbuf2 / ld
+  const void* tmaT_key[3] = {nullptr, nullptr, nullptr};
   DBuf d_err;                       // int: a bounded wait of a kernel gave up
   // caller's row order: device row i holds the caller's row row_map[i] (none: identity)
   bool have_row_map = false;
@@ -2127,6 +2130,9 @@ struct AdjBlk {
   const double* P;          // recorded sensitivities of this step, or null
   const double* Q;
   double* gs;               // d x ld: photon-scale gradient, summed over the rows of each bin
+  const CUtensorMap* tmap_v;  // k_slabT: tensor map of v for the TMA staging, or null (cp.async staging)
+  int* err;                 // k_slabT: set when its staging wait gives up
+  long long wait_tries;     // k_slabT: polls of the staging wait
   const int* inj_slot;
   double* gb_inj;
   const int64_t* lt_indptr; // Lambda_off^T, or null
@@ -2322,17 +2328,19 @@ size_t bandT_smem_bytes() {
 constexpr int kSlabTPre = 2;        // row pairs whose inputs a warp loads ahead
 constexpr int kSlabTWarps = 12;     // two CTAs per SM (80 registers)
 struct SlabTSmem {
-  double* slab;
+  double* slab;  // rows padded to whole TMA boxes (as k_slab's)
+  unsigned long long* bar;  // the TMA staging barrier (a 16-byte slot)
   double* vals;
   unsigned long long* sidx;
   int4* pairs;
   __host__ __device__ static size_t bytes(int nsp, int maxq, int maxp) {
-    return (size_t)nsp * kSlabCols * sizeof(double) + (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) +
-           (size_t)maxp * sizeof(int4);
+    return (size_t)SlabSmem::rows(nsp) * kSlabCols * sizeof(double) + 16 +
+           (size_t)maxq * (4 * sizeof(double) + sizeof(unsigned long long)) + (size_t)maxp * sizeof(int4);
   }
   __device__ SlabTSmem(double* base, int nsp, int maxq) {
     slab = base;
-    vals = slab + (size_t)nsp * kSlabCols;
+    bar = reinterpret_cast<unsigned long long*>(slab + (size_t)SlabSmem::rows(nsp) * kSlabCols);
+    vals = slab + (size_t)SlabSmem::rows(nsp) * kSlabCols + 2;
     sidx = reinterpret_cast<unsigned long long*>(vals + (size_t)maxq * 4);
     pairs = reinterpret_cast<int4*>(sidx + maxq);
   }
@@ -2340,15 +2348,17 @@ struct SlabTSmem {
 
 // Bin-local part of M_off^T v and the adjoint stage update for every row of
 // bin e.  CTA = (bin e, 16-column tile); a half-warp owns a mother row, its
-// lane c owns column col0 + c.  The v slab of bin e, the bin's entry quads and
-// row pairs arrive by asynchronous copies; each row is summed from shared
+// lane c owns column col0 + c.  The v slab of bin e arrives by TMA (boxes of a
+// tensor map over v, as in k_slab), the bin's entry quads and row pairs by
+// bulk copies, all on one bounded mbarrier wait (cp.async when TMA is off);
+// each row is summed from shared
 // memory (four accumulators, one per quad position).  The row's band term, FD
 // term, lam' (stage 1) or mu (stage 2), P and Q, and its recorded factors are
 // loaded kSlabTPre pairs ahead into registers.  Stage 1 reduces the
 // photon-scale gradient of the bin's rows inside the CTA.
 template <int STAGE>
 __global__ void __launch_bounds__(kSlabTWarps * 32, 2) k_slabT(AdjBlk q) {
-  extern __shared__ double sm[];
+  extern __shared__ __align__(128) double sm[];  // TMA boxes land at 128-byte boundaries
   const int nsp = q.nsp, e = blockIdx.x, d = q.d, ld = q.ld;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int half = lane >> 4, c = lane & 15;
@@ -2358,14 +2368,29 @@ __global__ void __launch_bounds__(kSlabTWarps * 32, 2) k_slabT(AdjBlk q) {
   const int qb = q.slabT_qbase[e], nqb = q.slabT_qbase[e + 1] - qb;
   const int pb0 = q.slabT_wrp[e * (kSlabTWarps + 1)], npb = q.slabT_wrp[e * (kSlabTWarps + 1) + kSlabTWarps] - pb0;
   const bool photohad = (q.flags & PB_PHOTOHAD) != 0, kap = (q.flags & PB_PARTIAL_DIFF) != 0;
-  {
+  const double* mv = q.slabT + (size_t)q.w * q.slabT_stride + (size_t)qb * 4;
+  if (q.tmap_v) {  // TMA: the v slab as tensor boxes, the entries and pairs as bulk copies, one barrier
+    if (threadIdx.x == 0) mbar_init(L.bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int nb = SlabSmem::nbox(nsp), br = SlabSmem::box_rows(nsp);
+      unsigned bytes = (unsigned)(nb * br * kSlabCols * sizeof(double)) + (unsigned)(npb * sizeof(int4));
+      if (photohad) bytes += (unsigned)(nqb * (4 * sizeof(double) + sizeof(unsigned long long)));
+      mbar_expect_tx(L.bar, bytes);
+      for (int b = 0; b < nb; ++b) tma_load_3d(L.slab + (size_t)b * br * kSlabCols, q.tmap_v, col0, e, b * br, L.bar);
+      if (photohad && nqb > 0) {
+        bulk_load(L.vals, mv, (unsigned)(nqb * 4 * sizeof(double)), L.bar);
+        bulk_load(L.sidx, q.slabT_q + qb, (unsigned)(nqb * sizeof(unsigned long long)), L.bar);
+      }
+      if (npb > 0) bulk_load(L.pairs, q.slabT_pairs + pb0, (unsigned)(npb * sizeof(int4)), L.bar);
+    }
+  } else {
     const double* vs = q.v + (size_t)e * ld + col0;
     for (int t = threadIdx.x; t < nsp * (kSlabCols / 2); t += blockDim.x) {
       const int sp = t / (kSlabCols / 2), cc = 2 * (t - sp * (kSlabCols / 2));
       cp_async16(L.slab + sp * kSlabCols + cc, vs + (size_t)sp * d * ld + cc);
     }
     if (photohad) {
-      const double* mv = q.slabT + (size_t)q.w * q.slabT_stride + (size_t)qb * 4;
       for (int t = threadIdx.x; t < 2 * nqb; t += blockDim.x) cp_async16(L.vals + 2 * t, mv + 2 * t);
       const unsigned long long* mq = q.slabT_q + qb;
       for (int t = threadIdx.x; t < nqb / 2; t += blockDim.x) cp_async16(L.sidx + 2 * t, mq + 2 * t);
@@ -2403,7 +2428,15 @@ __global__ void __launch_bounds__(kSlabTWarps * 32, 2) k_slabT(AdjBlk q) {
   } while (0)
 #pragma unroll
   for (int u = 0; u < PRE; ++u) PB_SLABT_LOAD(u, w0 + u, __ldg(q.slabT_pairs + w0 + u));
-  cp_async_wait<0>();
+  if (q.tmap_v) {
+    if (!mbar_wait_bounded(L.bar, 0, q.wait_tries)) {  // the copies did not land: report and leave
+      if (threadIdx.x == 0) atomicExch(q.err, kErrStagingWait);
+      mbar_wait_bounded(L.bar, 0, kWaitTries);
+      return;
+    }
+  } else {
+    cp_async_wait<0>();
+  }
   __syncthreads();
 
   double gsa = 0.0;  // this lane's column of the photon-scale gradient over its rows
@@ -2752,7 +2785,7 @@ std::vector<DBuf*> all_buffers(pb_context* c) {
   for (DBuf* x : {&c->nact, &c->lam, &c->lam2, &c->mu, &c->rec_rf, &c->rec_P, &c->rec_Q, &c->rec_sx, &c->dsig, &c->gb_inj,
                   &c->gs, &c->g_out, &c->erow, &c->tkeys, &c->tvals, &c->skeys, &c->svals, &c->t_indptr,
                   &c->t_indices, &c->t_perm, &c->sort_tmp, &c->fdkp, &c->bandT_vals, &c->slabT_vals, &c->vbuf,
-                  &c->vbuf2, &c->bTbuf, &c->fdTbuf, &c->outcols})
+                  &c->vbuf2, &c->bTbuf, &c->fdTbuf, &c->outcols, &c->tmapsT})
     b.push_back(x);
   return b;
 }
@@ -2912,11 +2945,44 @@ int ensure_tmaps(pb_context* c, bool blocked, int ld) {
   return PB_OK;
 }
 
+// Tensor maps of the adjoint sweep's v buffers (vbuf: stage 1, vbuf2: stage 2)
+// for k_slabT's TMA staging, shaped as k_slab's.  Leaves tmaT_ok false
+// (cp.async staging) when TMA is switched off or a map is refused.
+int ensure_tmapsT(pb_context* c, int ld) {
+  const bool want = c->tma_mode == 1 && ld % kSlabCols == 0;
+  if (want && c->tmaT_ok && c->tmaT_key[0] == c->vbuf.p && c->tmaT_key[1] == c->vbuf2.p &&
+      c->tmaT_key[2] == reinterpret_cast<const void*>((intptr_t)ld))
+    return PB_OK;
+  c->tmaT_ok = false;
+  if (!want) return PB_OK;
+  const EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) return PB_OK;
+  const int d = c->lay_d, nsp = c->lay_nsp;
+  CUtensorMap maps[2];
+  for (int k = 0; k < 2; ++k) {
+    const cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)d, (cuuint64_t)nsp};
+    const cuuint64_t strides[2] = {(cuuint64_t)ld * sizeof(double), (cuuint64_t)d * ld * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)kSlabCols, 1u, (cuuint32_t)SlabSmem::box_rows(nsp)};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    if (enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, k == 0 ? c->vbuf.p : c->vbuf2.p, dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return PB_OK;
+  }
+  PB_CUDA(c, c->tmapsT.ensure(sizeof(maps)));
+  PB_CUDA(c, cudaMemcpy(c->tmapsT.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
+  c->tmaT_key[0] = c->vbuf.p;
+  c->tmaT_key[1] = c->vbuf2.p;
+  c->tmaT_key[2] = reinterpret_cast<const void*>((intptr_t)ld);
+  c->tmaT_ok = true;
+  return PB_OK;
+}
+
 // Reports a bounded wait that gave up inside a kernel of the last enqueued work.
 int check_wait_flag(pb_context* c, const char* who) {
   int herr = 0;
   PB_CUDA(c, cudaMemcpy(&herr, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (herr) return fail(c, PB_ERR_DEVICE, "%s: a k_slab CTA gave up waiting for its staging copies (code %d)", who, herr);
+  if (herr) return fail(c, PB_ERR_DEVICE, "%s: a bin-local CTA gave up waiting for its staging copies (code %d)", who, herr);
   return PB_OK;
 }
 
@@ -4942,6 +5008,7 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
   if (blockedT) {
     PB_CUDA(c, c->vbuf.ensure(sb));
     PB_CUDA(c, c->vbuf2.ensure(sb));
+    if ((rc = ensure_tmapsT(c, ld))) return rc;
     PB_CUDA(c, c->bTbuf.ensure(sb));
     PB_CUDA(c, c->fdTbuf.ensure(sb));
     PB_CUDA(c, c->bandT_vals.ensure((size_t)W * std::max<int64_t>(c->band_stride, 1) * sizeof(double)));
@@ -5057,12 +5124,17 @@ int pb_adjoint(pb_context* c, const pb_solve_args* a, const double* seed, int32_
           t.lam_out = lam2;
         }
         const dim3 tgrid((unsigned)blocks_for(c->n_tail, 8), blocks_for(q.ncols, kColTile));
+        q.err = c->d_err.as<int>();
+        q.wait_tries = c->staging_wait_tries;
+        const CUtensorMap* tm = c->tmaT_ok ? reinterpret_cast<const CUtensorMap*>(c->tmapsT.p) : nullptr;
         q.v = c->vbuf.as<double>();
+        q.tmap_v = tm;
         q.lam = lam;
         q.vout = c->vbuf2.as<double>();
         launch_adj_blocked<1>(c, q, st);
         if (c->n_tail > 0) k_adj<1><<<tgrid, 256, 0, st>>>(t);
         q.v = c->vbuf2.as<double>();
+        q.tmap_v = tm ? tm + 1 : nullptr;
         q.vout = c->vbuf.as<double>();
         q.lam_out = lam2;
         launch_adj_blocked<2>(c, q, st);

@@ -283,3 +283,41 @@ def test_adjoint_without_the_photon_scale_records_factors_only(light):
         grads.append({k: v.grad.detach().numpy().copy() for k, v in t.items()})
     for k in grads[0]:
         np.testing.assert_allclose(grads[1][k], grads[0][k], rtol=1e-13, atol=0)
+
+
+def test_sweep_staging_wait_gives_up_cleanly_and_the_next_gradient_is_exact():
+    """The transposed sweep's bin-local kernel stages by TMA behind a bounded
+    wait.  With its poll limit at 0 (and no photon-scale gradient, so that the
+    sweep's staging is the backward's first wait) the backward raises
+    RuntimeError (PB_ERR_DEVICE); with the limit restored the same context
+    returns the gradient of a clean run bit for bit."""
+    from prince_b200 import _lib
+    from workloads import network_run
+    run = network_run(max_mass=16, n_species=60, seed=5)
+    species = [2212, 1000020040, 1000070140]
+    K = 37
+    rng = np.random.default_rng(4)
+    sb = AD.SourceBatch(run, species, z_max=list(rng.uniform(0.05, 0.2, K)), initial_z=0.2)
+    plan = sb.plan(0.2, ckpt_every=16)
+    ctx = plan.dev.ctx
+    seed = torch.tensor(rng.uniform(0.5, 1.5, (run.dim_states, K)), device="cuda:0")
+    scale = torch.tensor(1.0, dtype=torch.float64)
+
+    def gradient():
+        t = _tensors(_params(K, 9, len(species)))
+        (seed * _forward(sb, plan, t, scale)).sum().backward()
+        return [t[k].grad.numpy().copy() for k in ("gamma", "lg_rmax", "frac", "m")]
+
+    ref = gradient()
+    assert ctx.info(_lib.PB_INFO_LAST_BLOCKED) == 1
+    t = _tensors(_params(K, 9, len(species)))
+    X = _forward(sb, plan, t, scale)
+    ctx.set_option(_lib.PB_OPT_STAGING_WAIT_TRIES, 0)
+    try:
+        with pytest.raises(RuntimeError, match="gave up waiting"):
+            (seed * X).sum().backward()
+    finally:
+        ctx.set_option(_lib.PB_OPT_STAGING_WAIT_TRIES, -1)
+    again = gradient()
+    for a, b in zip(ref, again):
+        assert np.array_equal(a, b)
