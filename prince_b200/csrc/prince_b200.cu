@@ -180,8 +180,10 @@ struct pb_context {
   cudaEvent_t ev_hook_fork = nullptr, ev_hook_done = nullptr;
   bool tail_wait = false;           // the next tail launch waits for ev_hook_done
   int num_sms = 148;
-  DBuf tmaps;                       // [2] CUtensorMap of X and A for k_slab's TMA staging (64-byte aligned)
-  bool tma_ok = false;              // tmaps hold maps of the current X / A / ld
+  DBuf tmaps;                       // [4] CUtensorMap of X and A for k_slab's and k_band_tma's TMA staging
+  bool tma_ok = false;              // tmaps hold k_slab's maps of the current X / A / ld
+  bool tma_band_ok = false;         // tmaps also hold k_band_tma's maps (entries 2, 3)
+  bool band_tma_fits = false;       // k_band_tma's shared memory fits the layout's band tiles
   bool last_tma = false;            // the last solve staged k_slab by TMA
   const void* tma_key[3] = {nullptr, nullptr, nullptr};
   DBuf tmapsT;                      // [2] CUtensorMap of the adjoint's v buffers for k_slabT's TMA staging
@@ -644,6 +646,7 @@ struct StepParams {
   int64_t step;
   int step_w;        // rate window of this step (k_slab's entry values), set with step
   const CUtensorMap* tmap_src;  // k_slab: tensor map of src for the TMA staging, or null (cp.async staging)
+  const CUtensorMap* tmap_band;  // k_band_tma: tensor map of src as (64 columns x d bins) boxes, or null
   long long wait_tries;         // k_slab: polls of the staging wait before it gives up (the drain keeps kWaitTries)
   int* err;          // set to a nonzero code when a bounded wait gives up
   int64_t n_steps;
@@ -1825,6 +1828,120 @@ __global__ void __launch_bounds__(256) k_band_finish(StepParams p) {
   if (STAGE == 2 && blockIdx.y == 0 && lane == 0) prep_next(p, r);
 }
 
+// Band partial sums with TMA staging (8 warps; the same tiles and arithmetic
+// as k_band).  Per mother species one thread issues the pair's A tiles as one
+// bulk copy (double-buffered) and the species' X block (d bins x 64 columns)
+// as one tensor-map box; each warp reads its X fragments from shared memory,
+// so no register copy of the next species is held.  One CTA barrier per
+// species; every mbarrier wait is bounded: a CTA that gives up sets p.err,
+// stops issuing, waits (bounded) for the copies it issued and leaves.
+constexpr int kErrBandWait = 2;  // err code: a k_band CTA's staging wait gave up
+template <int RT, int J>
+__global__ void __launch_bounds__(256, 1) k_band_tma(StepParams p) {
+  extern __shared__ __align__(128) double sm[];
+  constexpr int KT = 2 * RT;
+  constexpr int ABLK = 2 * RT * J * 32;  // doubles of one (species, band pair) block
+  constexpr int XS = 8 * RT * 64;        // X of one species: bins x 64 columns
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int cb = blockIdx.x * 64, c0 = cb + wid * 8;
+  const bool wact = c0 < p.ncols;  // c0 + 7 < ld: ld is a multiple of 32
+  const int pair = blockIdx.z, g = blockIdx.y;
+  const int s0 = g * p.spg, s1 = min(p.nsp, s0 + p.spg);
+  const int d = p.d, ld = p.ld;
+  const int w = p.win[p.step];
+  const double* __restrict__ A = p.band_vals + (size_t)w * p.band_stride;
+  const int npairs = gridDim.z;
+  double* As = sm;             // [2][ABLK]
+  double* Xs = As + 2 * ABLK;  // [bin][64 columns]
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(Xs + XS);  // A stage 0, A stage 1, X
+  int* abort_s = reinterpret_cast<int*>(bar + 3);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_init(bar + 2, 1);
+    *abort_s = 0;
+  }
+  __syncthreads();
+  auto issue = [&](int sp, int stage) {  // thread 0
+    mbar_expect_tx(bar + stage, (unsigned)(ABLK * sizeof(double)));
+    bulk_load(As + stage * ABLK, A + ((size_t)sp * npairs + pair) * ABLK, (unsigned)(ABLK * sizeof(double)), bar + stage);
+    mbar_expect_tx(bar + 2, (unsigned)(64 * d * sizeof(double)));
+    tma_load_3d(Xs, p.tmap_band, cb, 0, sp, bar + 2);
+  };
+  if (threadIdx.x == 0 && s0 < s1) issue(s0, 0);
+  double acc[2][RT][2];
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) acc[b][rt][0] = acc[b][rt][1] = 0.0;
+  const int kr = lane & 3;
+  int last = s0 - 1;  // the last species whose copies were issued (thread 0)
+  if (s0 < s1) last = s0;
+  for (int sp = s0; sp < s1; ++sp) {
+    const int it = sp - s0, stage = it & 1;
+    bool ok = mbar_wait_bounded(bar + 2, (unsigned)(it & 1), p.wait_tries);
+    double xf[KT];
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const int e = 4 * kt + kr;
+      xf[kt] = (wact && e < d) ? Xs[e * 64 + wid * 8 + (lane >> 2)] : 0.0;
+    }
+    ok = mbar_wait_bounded(bar + stage, (unsigned)((it >> 1) & 1), p.wait_tries) && ok;
+    if (!ok) {
+      atomicExch(p.err, kErrBandWait);
+      *abort_s = 1;
+    }
+    __syncthreads();  // every warp holds X(sp) and is done with A(sp - 1)
+    if (*abort_s) break;
+    if (threadIdx.x == 0 && sp + 1 < s1) {
+      issue(sp + 1, stage ^ 1);
+      last = sp + 1;
+    }
+    // a lane's fragments of row tiles 2p and 2p + 1 are one 16-byte word
+    const double2* __restrict__ as = reinterpret_cast<const double2*>(As + stage * ABLK) + lane;
+#pragma unroll
+    for (int jj = 0; jj < J; ++jj)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+#pragma unroll
+        for (int rp = 0; rp < RT / 2; ++rp) {
+          const int kt = 4 * rp + jj;
+          if (kt >= KT) continue;
+          const double2 a2 = as[((b * (RT / 2) + rp) * J + jj) * 32];
+          dmma884(acc[b][2 * rp][0], acc[b][2 * rp][1], a2.x, xf[kt]);
+          if (kt + 2 < KT) dmma884(acc[b][2 * rp + 1][0], acc[b][2 * rp + 1][1], a2.y, xf[kt + 2]);
+        }
+  }
+  if (*abort_s) {  // the copies this CTA issued land before it leaves
+    if (threadIdx.x == 0 && last >= s0) {
+      const int it = last - s0;
+      mbar_wait_bounded(bar + 2, (unsigned)(it & 1), kWaitTries);
+      mbar_wait_bounded(bar + (it & 1), (unsigned)((it >> 1) & 1), kWaitTries);
+    }
+    return;
+  }
+  if (!wact) return;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    if (2 * pair + b >= p.nb) continue;
+    double* __restrict__ P = p.band_part + (size_t)(g * p.nb + 2 * pair + b) * d * ld;
+#pragma unroll
+    for (int rt = 0; rt < RT; ++rt) {
+      const int row = 8 * rt + (lane >> 2);
+      if (row >= d) continue;
+      double2 o;
+      o.x = acc[b][rt][0];
+      o.y = acc[b][rt][1];
+      *reinterpret_cast<double2*>(P + (size_t)row * ld + c0 + kr * 2) = o;
+    }
+  }
+}
+
+template <int RT, int J>
+size_t band_tma_smem_bytes() {
+  return (size_t)(2 * 2 * RT * J * 32 + 8 * RT * 64) * sizeof(double) + 4 * sizeof(unsigned long long);
+}
+
 // Instances of k_band: row tiles RT (d <= 8 RT) x k-tiles per row tile J
 // (band offsets up to 4 J - 8 bins).
 using BandKernel = void (*)(StepParams);
@@ -1859,6 +1976,26 @@ BandInstance band_kernel_w(int RT, int J) {
 // registers and shared memory, so that a k_slab CTA fits beside one.
 BandInstance band_kernel(int RT, int J, int nw = 8) {
   return nw == 4 ? band_kernel_w<4>(RT, J) : band_kernel_w<8>(RT, J);
+}
+// The TMA-staged 8-warp instance.
+template <int RT>
+BandInstance band_kernel_tma_j(int J) {
+  switch (J) {
+    case 5: return {k_band_tma<RT, 5>, band_tma_smem_bytes<RT, 5>(), 8};
+    case 9: return {k_band_tma<RT, 9>, band_tma_smem_bytes<RT, 9>(), 8};
+    case 13: return {k_band_tma<RT, 13>, band_tma_smem_bytes<RT, 13>(), 8};
+    case 17: return {k_band_tma<RT, 17>, band_tma_smem_bytes<RT, 17>(), 8};
+  }
+  return {nullptr, 0, 0};
+}
+BandInstance band_kernel_tma(int RT, int J) {
+  switch (RT) {
+    case 4: return band_kernel_tma_j<4>(J);
+    case 8: return band_kernel_tma_j<8>(J);
+    case 12: return band_kernel_tma_j<12>(J);
+    case 16: return band_kernel_tma_j<16>(J);
+  }
+  return {nullptr, 0, 0};
 }
 
 // ---------------------------------------------------------------------------
@@ -2912,29 +3049,38 @@ EncodeTiledFn tensor_map_encoder() {
   return fn;
 }
 
-// Tensor maps of X and A as (column, bin, species) for k_slab's TMA staging:
-// box = 16 columns x 1 bin x box_rows species.  Leaves tma_ok false (cp.async
-// staging) when TMA is switched off, the encoder is missing or a map is refused.
+// Tensor maps of X and A as (column, bin, species) for k_slab's TMA staging
+// (box = 16 columns x 1 bin x box_rows species) and for k_band_tma's (box =
+// 64 columns x d bins x 1 species).  Leaves tma_ok false (cp.async staging)
+// when TMA is switched off, the encoder is missing or a map is refused, and
+// tma_band_ok false when only the band maps are refused.
 int ensure_tmaps(pb_context* c, bool blocked, int ld) {
   const bool want = blocked && c->tma_mode == 1 && ld % kSlabCols == 0;
   if (want && c->tma_ok && c->tma_key[0] == c->X.p && c->tma_key[1] == c->A.p &&
       c->tma_key[2] == reinterpret_cast<const void*>((intptr_t)ld))
     return PB_OK;
   c->tma_ok = false;
+  c->tma_band_ok = false;
   if (!want) return PB_OK;
   const EncodeTiledFn enc = tensor_map_encoder();
   if (!enc) return PB_OK;
   const int d = c->lay_d, nsp = c->lay_nsp;
-  CUtensorMap maps[2];
-  for (int k = 0; k < 2; ++k) {
+  CUtensorMap maps[4];
+  bool band_ok = d <= 256;
+  for (int k = 0; k < 4; ++k) {
+    const bool band = k >= 2;
+    if (band && !band_ok) break;
     const cuuint64_t dims[3] = {(cuuint64_t)ld, (cuuint64_t)d, (cuuint64_t)nsp};
     const cuuint64_t strides[2] = {(cuuint64_t)ld * sizeof(double), (cuuint64_t)d * ld * sizeof(double)};
-    const cuuint32_t box[3] = {(cuuint32_t)kSlabCols, 1u, (cuuint32_t)SlabSmem::box_rows(nsp)};
+    const cuuint32_t box[3] = {band ? 64u : (cuuint32_t)kSlabCols, band ? (cuuint32_t)d : 1u,
+                               band ? 1u : (cuuint32_t)SlabSmem::box_rows(nsp)};
     const cuuint32_t es[3] = {1u, 1u, 1u};
-    if (enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, k == 0 ? c->X.p : c->A.p, dims, strides, box, es,
+    if (enc(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, k % 2 == 0 ? c->X.p : c->A.p, dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return PB_OK;
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      if (!band) return PB_OK;
+      band_ok = false;
+    }
   }
   PB_CUDA(c, c->tmaps.ensure(sizeof(maps)));
   PB_CUDA(c, cudaMemcpy(c->tmaps.p, maps, sizeof(maps), cudaMemcpyHostToDevice));
@@ -2942,6 +3088,7 @@ int ensure_tmaps(pb_context* c, bool blocked, int ld) {
   c->tma_key[1] = c->A.p;
   c->tma_key[2] = reinterpret_cast<const void*>((intptr_t)ld);
   c->tma_ok = true;
+  c->tma_band_ok = band_ok;
   return PB_OK;
 }
 
@@ -2989,6 +3136,11 @@ int check_wait_flag(pb_context* c, const char* who) {
 // The k_slab staging of a stage: the tensor map of its source, or null.
 const CUtensorMap* stage_tmap(const pb_context* c, int stage) {
   return c->tma_ok ? reinterpret_cast<const CUtensorMap*>(c->tmaps.p) + (stage == 1 ? 0 : 1) : nullptr;
+}
+// k_band_tma's map of a stage's source, or null (the cp.async k_band runs).
+const CUtensorMap* stage_tmap_band(const pb_context* c, int stage) {
+  return (c->tma_ok && c->tma_band_ok && c->band_tma_fits) ? reinterpret_cast<const CUtensorMap*>(c->tmaps.p) + (stage == 1 ? 2 : 3)
+                                                          : nullptr;
 }
 
 // Whether a solve with K columns runs the bin-blocked kernels.
@@ -3045,7 +3197,8 @@ int64_t launch_blocked_stage(pb_context* c, StepParams& p, cudaStream_t st) {
   p.ngroups = 0;
   p.spg = 1;
   if (photohad && p.nb > 0) {
-    const BandInstance bi = band_kernel(c->band_RT, c->band_J, c->band_warps);
+    const BandInstance bi = (c->band_warps == 8 && p.tmap_band) ? band_kernel_tma(c->band_RT, c->band_J)
+                                                                : band_kernel(c->band_RT, c->band_J, c->band_warps);
     const int cblocks = band_grid(c, p, bi.warps);
     cudaEventRecord(c->ev_fork, st);
     cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
@@ -3194,6 +3347,7 @@ int64_t launch_steps(pb_context* c, StepParams& p, int K, const int32_t* n_activ
       p.x = X;
       p.xout = X;
       p.tmap_src = blocked ? stage_tmap(c, stage) : nullptr;
+      p.tmap_band = blocked ? stage_tmap_band(c, stage) : nullptr;
       p.err = c->d_err.as<int>();
       if (blocked) {
         launches += stage == 1 ? launch_blocked_stage<1>(c, p, st) : launch_blocked_stage<2>(c, p, st);
@@ -3817,6 +3971,7 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
     std::stable_sort(sspec.begin(), sspec.end(), [&](int32_t a, int32_t b) { return cnt[a] > cnt[b]; });
   }
   c->blocked_ok = false;
+  c->band_tma_fits = false;
   c->lay_d = d;
   c->lay_nsp = nsp;
   if ((rc = build_fd_table(c))) return rc;
@@ -3954,6 +4109,11 @@ int pb_set_layout_rows(pb_context* c, int32_t d, int64_t n_blocks) {
   }
   PB_CUDA(c, cudaFuncSetAttribute(bi.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi.smem));
   PB_CUDA(c, cudaFuncSetAttribute(bi4.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bi4.smem));
+  {
+    const BandInstance bt = band_kernel_tma(RT, J);
+    c->band_tma_fits = bt.fn && bt.smem <= max_smem;
+    if (c->band_tma_fits) PB_CUDA(c, cudaFuncSetAttribute(bt.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bt.smem));
+  }
   c->band_nb = nb;
   c->band_npairs = npairs;
   c->band_RT = RT;
@@ -4097,12 +4257,14 @@ int pb_profile_stage(pb_context* c, int64_t step, int32_t stage, int32_t reps, d
   p.x = c->X.as<double>();
   p.xout = c->X.as<double>();
   p.tmap_src = stage_tmap(c, stage);
+  p.tmap_band = stage_tmap_band(c, stage);
   PB_CUDA(c, c->d_err.ensure(sizeof(int)));
   p.err = c->d_err.as<int>();
   cudaStream_t st = c->stream;
   const bool photohad = (flags & PB_PHOTOHAD) != 0, kap = (flags & PB_PARTIAL_DIFF) != 0;
   const unsigned tiles = (unsigned)blocks_for(p.ncols, kColTile);
-  const BandInstance bi = band_kernel(c->band_RT, c->band_J, c->band_warps);
+  const BandInstance bi = (c->band_warps == 8 && p.tmap_band) ? band_kernel_tma(c->band_RT, c->band_J)
+                                                              : band_kernel(c->band_RT, c->band_J, c->band_warps);
   const int cblocks = band_grid(c, p, bi.warps);
   if (!(photohad && p.nb > 0)) p.ngroups = 0;
   for (int kk = 0; kk < 4; ++kk) ms[kk] = 0.0;
