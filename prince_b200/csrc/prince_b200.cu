@@ -3129,7 +3129,7 @@ int ensure_tmapsT(pb_context* c, int ld) {
 int check_wait_flag(pb_context* c, const char* who) {
   int herr = 0;
   PB_CUDA(c, cudaMemcpy(&herr, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-  if (herr) return fail(c, PB_ERR_DEVICE, "%s: a bin-local CTA gave up waiting for its staging copies (code %d)", who, herr);
+  if (herr) return fail(c, PB_ERR_DEVICE, "%s: a CTA gave up waiting for its staging copies (code %d: 1 bin-local rows, 2 band tiles)", who, herr);
   return PB_OK;
 }
 
