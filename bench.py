@@ -377,7 +377,7 @@ def kernel_rooflines(solver, run, sched, n_active, n_inj):
     if ms[2] > 0:
         a = 2.0 * nnz_band * K / (ms[2] * 1e-3) / 1e12
         kernels.append({"kernel": "k_band", "bound": "tensor", "achieved": a, "peak": fp64, "unit": "TFLOP/s",
-                        "frac": a / fp64, "traffic": traffic.get("k_band"),
+                        "frac": a / fp64, "traffic": traffic.get("k_band_tma", traffic.get("k_band")),
                         "traffic_unit": "bytes", "launch_us": ms[2] * 1e3,
                         "algorithmic_flops": 2.0 * nnz_band * K,
                         "peak_source": "measured FP64 DMMA peak (pb_fp64_peak, register-only kernel)"})
