@@ -48,7 +48,8 @@ extern "C" {
 #define PB_INFO_SLAB_ENTRIES 6   /* off-diagonal coupling entries of the bin-local rows */
 #define PB_INFO_SLAB_ROWS 7      /* bin-local rows */
 #define PB_INFO_FD_DENSE 8       /* 1 if the forward FD term runs the register-blocked dense stencil */
-#define PB_OPT_TMA_STAGING 9     /* 1 (default): bin-local kernel stages by TMA (tensor maps); 0: cp.async */
+#define PB_OPT_TMA_STAGING 9     /* 1 (default): the bin-local and band-tile kernels stage by TMA (tensor maps,
+                                    bulk copies); 0: cp.async */
 #define PB_INFO_LAST_TMA 10      /* 1 if the last pb_solve staged the bin-local kernel by TMA */
 #define PB_OPT_BAND_WARPS 12       /* warps of a band-tile CTA: 8 (default, 64 columns, one CTA per SM) or 4
                                      (32 columns in half the registers and shared memory, so the band
